@@ -1,0 +1,311 @@
+// Test-infrastructure driver that links the UNMODIFIED ml_prec sources (compiled
+// from the read-only reference tree by oracle/Makefile) and runs them on a given
+// problem, dumping everything the parity tests compare against:
+//   * the per-level hierarchy (N, nnz, M, Md, map, L, U, next-level A, dval),
+//   * the PCG iteration count, the solution x and wall-clock timings.
+// It is the checker, never the product: only tests/, the golden-fixture script
+// and bench.py's CPU-baseline leg run it.
+//
+// The reference keeps the hierarchy in private members (multi_split_prec.h:68,
+// cheb_prec.h:43), so this translation unit opens them up after the standard
+// headers have been included.
+//
+// Problem inputs (both in the reference's own formats):
+//   --perm FILE    3 x 1,122,000 doubles (kx, ky, kz blocks, raw binary); the
+//                  driver writes them as the text spe_perm.dat that SPEMesh reads
+//                  (spe.cc:11-67, "%.17g" round-trips exactly) and builds A with
+//                  SPEMesh::construct_matrix (spe.cc:69-131);
+//   --csr FILE     load A with SkylineMatrix::load(BINARY) (csrmatrix.cc:172-190).
+// On top of the reference stencil the driver adds the Dirichlet x-faces used by
+// the benchmark problems (p=1 at i=0, p=0 at i=nx-1, half-cell transmissibility
+// 2*kx/hx^2 on the diagonal, p=1 face term moved to b). That is a problem-setup
+// decision of this project, not reference behaviour.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <iterator>
+#include <map>
+#include <memory>
+#include <set>
+#include <sstream>
+#include <stack>
+#include <string>
+#include <vector>
+#include <sys/time.h>
+#include <unistd.h>
+
+#define private public
+#define protected public
+#include "modules/mesh/mesh.h"
+#include "modules/matrix/matrix.h"
+#include "modules/prec/multi_split/multi_split_prec.h"
+#include "modules/prec/cheb/cheb_prec.h"
+#include "modules/solvers/solvers.h"
+#include "project/config.h"
+#undef private
+#undef protected
+
+static double now() {
+    struct timeval tv;
+    gettimeofday(&tv, 0);
+    return tv.tv_sec + 1e-6 * tv.tv_usec;
+}
+
+static void write_raw(const std::string& fn, const void* p, size_t bytes) {
+    FILE* f = fopen(fn.c_str(), "wb");
+    if (!f) { fprintf(stderr, "cannot write %s\n", fn.c_str()); exit(2); }
+    if (bytes) fwrite(p, 1, bytes, f);
+    fclose(f);
+}
+
+static std::vector<double> read_f64(const std::string& fn) {
+    std::vector<double> v;
+    FILE* f = fopen(fn.c_str(), "rb");
+    if (!f) { fprintf(stderr, "cannot read %s\n", fn.c_str()); exit(2); }
+    fseek(f, 0, SEEK_END);
+    long n = ftell(f) / 8;
+    fseek(f, 0, SEEK_SET);
+    v.resize(n);
+    if (n && fread(&v[0], 8, n, f) != (size_t)n) { fprintf(stderr, "short read %s\n", fn.c_str()); exit(2); }
+    fclose(f);
+    return v;
+}
+
+template <class M>
+static void dump_csr(const std::string& fn, const M& A) {
+    // Written in the reference's BINARY CSR layout (csrmatrix.cc:314-320):
+    // uint nrow, uint ncol, ia[nrow+1], ja[nnz], a[nnz].
+    std::string path = fn;
+    FILE* f = fopen(path.c_str(), "wb");
+    uint nr = A.nrow, nc = A.ncol;
+    fwrite(&nr, 4, 1, f);
+    fwrite(&nc, 4, 1, f);
+    uint zero = 0;
+    if (A.ia.size()) fwrite(&A.ia[0], 4, A.ia.size(), f);
+    else fwrite(&zero, 4, 1, f);
+    if (A.ja.size()) fwrite(&A.ja[0], 4, A.ja.size(), f);
+    if (A.a.size()) fwrite(&A.a[0], 8, A.a.size(), f);
+    fclose(f);
+}
+
+struct Args {
+    std::string perm, csr, rhs, out = ".", cfgfile, prec = "msplit";
+    uint nx = 60, ny = 220, nz = 85;
+    double c = 0.1, eps = 1e-8;
+    bool dirichlet = true, dump = false, no_solve = false;
+    std::vector<double> sigmas;
+    std::vector<uint> niters;
+    std::string apply_in;  // optional: one preconditioner apply on this vector
+    int reps = 1;
+};
+
+static std::vector<double> parse_list_d(const char* s) {
+    std::vector<double> v;
+    std::istringstream is(s);
+    std::string tok;
+    while (std::getline(is, tok, ',')) v.push_back(atof(tok.c_str()));
+    return v;
+}
+
+int main(int argc, char** argv) {
+    Args a;
+    for (int i = 1; i < argc; i++) {
+        std::string k = argv[i];
+        auto val = [&]() -> const char* {
+            if (i + 1 >= argc) { fprintf(stderr, "missing value for %s\n", k.c_str()); exit(2); }
+            return argv[++i];
+        };
+        if (k == "--perm") a.perm = val();
+        else if (k == "--csr") a.csr = val();
+        else if (k == "--rhs") a.rhs = val();
+        else if (k == "--out") a.out = val();
+        else if (k == "--cfg") a.cfgfile = val();
+        else if (k == "--prec") a.prec = val();
+        else if (k == "--nx") a.nx = atoi(val());
+        else if (k == "--ny") a.ny = atoi(val());
+        else if (k == "--nz") a.nz = atoi(val());
+        else if (k == "--c") a.c = atof(val());
+        else if (k == "--eps") a.eps = atof(val());
+        else if (k == "--no-dirichlet") a.dirichlet = false;
+        else if (k == "--dump") a.dump = true;
+        else if (k == "--no-solve") a.no_solve = true;
+        else if (k == "--sigmas") a.sigmas = parse_list_d(val());
+        else if (k == "--niters") { std::vector<double> d = parse_list_d(val()); for (double x : d) a.niters.push_back((uint)x); }
+        else if (k == "--apply") a.apply_in = val();
+        else if (k == "--reps") a.reps = atoi(val());
+        else { fprintf(stderr, "unknown arg %s\n", k.c_str()); return 2; }
+    }
+
+    // Absolute paths before the chdir into the output folder.
+    auto absify = [](std::string& p) {
+        if (!p.empty() && p[0] != '/') { char buf[4096]; getcwd(buf, sizeof buf); p = std::string(buf) + "/" + p; }
+    };
+    absify(a.perm); absify(a.csr); absify(a.rhs); absify(a.out); absify(a.cfgfile); absify(a.apply_in);
+
+    SkylineMatrix A;
+    Vector b;
+    double t0 = now();
+    if (!a.perm.empty()) {
+        if (chdir(a.out.c_str()) != 0) { fprintf(stderr, "chdir %s failed\n", a.out.c_str()); return 2; }
+        {
+            std::vector<double> kv = read_f64(a.perm);
+            if (kv.size() != 3u * 1122000u) { fprintf(stderr, "perm file must hold 3*1122000 doubles\n"); return 2; }
+            FILE* f = fopen("spe_perm.dat", "w");
+            for (size_t i = 0; i < kv.size(); i++) fprintf(f, "%.17g\n", kv[i]);
+            fclose(f);
+        }
+        t0 = now();
+        SPEMesh mesh(a.nx, a.ny, a.nz);
+        unlink("spe_perm.dat");
+        mesh.construct_matrix(A, a.c);
+        b = Vector(A.size(), 0.);
+        if (a.dirichlet) {
+            for (uint k = 0; k < a.nz; k++)
+                for (uint j = 0; j < a.ny; j++) {
+                    uint faces[2] = {0, a.nx - 1};
+                    for (int f = 0; f < 2; f++) {
+                        uint i = faces[f];
+                        uint row = mesh.index(i, j, k);
+                        double tD = 2 * mesh.kx[mesh.index_k(i, j, k)] / (mesh.hx * mesh.hx);
+                        A.a[A.ia[row]] += tD;
+                        if (f == 0) b[row] += tD * 1.0;
+                    }
+                }
+        }
+    } else if (!a.csr.empty()) {
+        A.load(a.csr, BINARY, false);
+        if (!a.rhs.empty()) {
+            std::vector<double> bv = read_f64(a.rhs);
+            b = Vector(bv.size());
+            for (size_t i = 0; i < bv.size(); i++) b[i] = bv[i];
+        } else {
+            b = Vector(A.size(), 0.);
+        }
+    } else {
+        fprintf(stderr, "need --perm or --csr\n");
+        return 2;
+    }
+    double t_assemble = now() - t0;
+    if (chdir(a.out.c_str()) != 0) { fprintf(stderr, "chdir %s failed\n", a.out.c_str()); return 2; }
+
+    if (a.dump) {
+        dump_csr("A0.csr", A);
+        write_raw("b.f64", &b[0], 8 * (size_t)b.size());
+    }
+
+    Config cfg;
+    cfg.c = a.c;
+    cfg.nx = a.nx; cfg.ny = a.ny; cfg.nz = a.nz;
+    cfg.ntests = 1;
+    cfg.use_tails = true;
+    cfg.coarse_n = 0;
+    cfg.max_levels = 0;
+    cfg.optimize_storage = true;
+    cfg.nonsym_matrix = false;
+    cfg.nonsym_shift = 0.1;
+    cfg.solver = PCG_SOLVER;
+    cfg.dump_data = false;
+    cfg.analysis = ANAL_NONE;
+    cfg.transform = TRANS_NONE;
+    cfg.sigmas = a.sigmas.empty() ? std::vector<double>(1, 3.0) : a.sigmas;
+    cfg.niters = a.niters.empty() ? std::vector<uint>(1, 2) : a.niters;
+
+    std::ofstream js("result.json");
+    js << std::setprecision(17);
+    js << "{\n  \"N\": " << A.size() << ",\n  \"nnz\": " << A.nnz() << ",\n  \"t_assemble\": " << t_assemble;
+
+    PrecBase* B = 0;
+    double t_setup = 0;
+    for (int r = 0; r < a.reps; r++) {
+        delete B;
+        double ts = now();
+        if (a.prec == "msplit") {
+            cfg.prec = MULTI_SPLIT_PREC;
+            cfg.prec_conf_file = a.cfgfile;
+            B = new MultiSplitPrec(A, cfg);
+        } else if (a.prec == "cheb") {
+            cfg.prec = UH_CHEB_PREC;
+            B = new Prec(A, cfg);
+        } else {
+            fprintf(stderr, "unknown prec %s\n", a.prec.c_str());
+            return 2;
+        }
+        double te = now() - ts;
+        if (r == 0 || te < t_setup) t_setup = te;
+    }
+    js << ",\n  \"t_setup\": " << t_setup;
+
+    // Hierarchy dump.
+    std::vector<uint> lvN;
+    if (a.prec == "msplit") {
+        MultiSplitPrec* P = (MultiSplitPrec*)B;
+        js << ",\n  \"nlevels\": " << P->nlevels << ",\n  \"levels\": [";
+        for (uint l = 0; l < P->nlevels; l++) {
+            const MultiSplitPrec::Level& L = P->levels[l];
+            js << (l ? "," : "") << "\n    {\"N\": " << L.N << ", \"nnz\": " << L.nnz << ", \"M\": " << L.M
+               << ", \"Md\": " << L.Md << ", \"niter\": " << L.niter << ", \"q\": " << L.q << "}";
+            if (a.dump) {
+                char fn[256];
+                if (l) { snprintf(fn, sizeof fn, "l%u_A.csr", l); dump_csr(fn, L.A); }
+                snprintf(fn, sizeof fn, "l%u_L.csr", l); dump_csr(fn, L.L);
+                snprintf(fn, sizeof fn, "l%u_U.csr", l); dump_csr(fn, L.U);
+                snprintf(fn, sizeof fn, "l%u_map.u32", l); write_raw(fn, L.map.size() ? &L.map[0] : 0, 4 * (size_t)L.map.size());
+                snprintf(fn, sizeof fn, "l%u_dval.f64", l); write_raw(fn, L.dval.size() ? &L.dval[0] : 0, 8 * (size_t)L.dval.size());
+            }
+        }
+        js << "\n  ]";
+    } else {
+        Prec* P = (Prec*)B;
+        js << ",\n  \"nlevels\": " << P->nlevels << ",\n  \"levels\": [";
+        for (uint l = 0; l < P->nlevels; l++) {
+            const Prec::Level& L = P->levels[l];
+            js << (l ? "," : "") << "\n    {\"N\": " << L.N << ", \"nnz\": " << L.nnz << ", \"M\": " << L.M
+               << ", \"Md\": " << L.Md << ", \"ncheb\": " << L.ncheb << ", \"alpha\": " << L.alpha
+               << ", \"beta\": " << L.beta << ", \"lmin\": " << L.lmin << ", \"lmax\": " << L.lmax << "}";
+            if (a.dump) {
+                char fn[256];
+                if (l) { snprintf(fn, sizeof fn, "l%u_A.csr", l); dump_csr(fn, L.A); }
+                snprintf(fn, sizeof fn, "l%u_L.csr", l); dump_csr(fn, L.L);
+                snprintf(fn, sizeof fn, "l%u_U.csr", l); dump_csr(fn, L.U);
+                snprintf(fn, sizeof fn, "l%u_map.u32", l); write_raw(fn, L.map.size() ? &L.map[0] : 0, 4 * (size_t)L.map.size());
+                snprintf(fn, sizeof fn, "l%u_dval.f64", l); write_raw(fn, L.dval.size() ? &L.dval[0] : 0, 8 * (size_t)L.dval.size());
+            }
+        }
+        js << "\n  ]";
+    }
+
+    if (!a.apply_in.empty()) {
+        std::vector<double> fv = read_f64(a.apply_in);
+        Vector f(fv.size()), z(fv.size());
+        for (size_t i = 0; i < fv.size(); i++) f[i] = fv[i];
+        double ts = now();
+        B->solve(f, z);
+        js << ",\n  \"t_apply\": " << now() - ts;
+        write_raw("apply_out.f64", &z[0], 8 * (size_t)z.size());
+    }
+
+    if (!a.no_solve) {
+        Vector x(A.size());
+        SolverStats stats;
+        double best = 0;
+        for (int r = 0; r < a.reps; r++) {
+            double ts = now();
+            PCGSolver(A, b, *B, x, stats, a.eps, NORM_L2, true);
+            double te = now() - ts;
+            if (r == 0 || te < best) best = te;
+        }
+        js << ",\n  \"niter\": " << stats.niter << ",\n  \"t_solve\": " << best
+           << ",\n  \"t_prec_avg\": " << stats.t_prec << ",\n  \"t_resid_avg\": " << stats.t_resid;
+        write_raw("x.f64", &x[0], 8 * (size_t)x.size());
+    }
+    js << "\n}\n";
+    js.close();
+    delete B;
+    return 0;
+}
