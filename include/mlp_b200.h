@@ -1,0 +1,159 @@
+/*
+ * ml_prec_b200 — C ABI of the B200 (sm_100a) implementation of ml_prec's hot
+ * path: PCG on the 7-point reservoir-pressure matrix preconditioned by the
+ * multilevel multi-split or Chebyshev ("uh_cheb") preconditioner.
+ *
+ * Every function returns an int status (MLP_OK = 0); on failure
+ * mlp_last_error() returns a message for the calling thread. Pointers named
+ * *_host are host memory; pointers named *_dev are device memory of the
+ * current CUDA device. Handles are not thread-safe: use one per thread/stream
+ * (the reference's solve() mutates `mutable` scratch the same way,
+ * multi_split_prec.h:40-41).
+ *
+ * Each entry point names the reference interface it replaces (paths inside
+ * the ml_prec source tree).
+ */
+#ifndef MLP_B200_H
+#define MLP_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define MLP_OK 0
+#define MLP_ERR_ARG 1         /* invalid argument or size                            */
+#define MLP_ERR_CONFIG 2      /* bad preconditioner configuration (ConfigFile keys)  */
+#define MLP_ERR_LEVELS 3      /* "Too many levels" (cheb_constr.cc:282-283)          */
+#define MLP_ERR_CURVATURE 4   /* <Ap, p> <= 0 (pcg.cc:51-55)                         */
+#define MLP_ERR_NOT_FINITE 5  /* NaN / Inf in a PCG scalar                           */
+#define MLP_ERR_MAXIT 6       /* iteration cap reached                               */
+#define MLP_ERR_CUDA 7        /* CUDA runtime error                                  */
+#define MLP_ERR_NO_ITER 8     /* "No need to iterate" (pcg.cc:94-96)                 */
+#define MLP_ERR_LIMIT 9       /* a documented size limit was exceeded                */
+#define MLP_ERR_INTERNAL 10   /* device-side consistency check failed                */
+
+typedef struct mlp_matrix mlp_matrix; /* device-resident CSR, diagonal first per row */
+typedef struct mlp_prec mlp_prec;     /* device-resident preconditioner hierarchy     */
+
+/* Preconditioner kinds. */
+#define MLP_PREC_MSPLIT 0 /* MultiSplitPrec, multi_split_prec.h:15-113 */
+#define MLP_PREC_CHEB 1   /* Prec ("uh_cheb"), cheb_prec.h:13-127     */
+
+/* Node orderings (msplit.cfg key elim_order, multi_split_constr.cc:246-249). */
+#define MLP_ORDER_NONE 0
+#define MLP_ORDER_ORIGINAL 1
+#define MLP_ORDER_BLOCK 2
+#define MLP_ORDER_SIMPLE_1 3
+
+/* Plain-old-data configuration, the parsed form of msplit.cfg / Config.
+ * Replaces the ConfigFile reads of MultiSplitPrec::MultiSplitPrec
+ * (multi_split_constr.cc:179-233) and the Config fields Prec reads
+ * (cheb_constr.cc:292-365, project/config.h:54-86). */
+typedef struct {
+    int32_t kind;            /* MLP_PREC_MSPLIT or MLP_PREC_CHEB                      */
+    uint32_t nq;             /* multi-split: q per level (last value repeats)         */
+    const double* q;
+    uint32_t nniter;         /* multi-split: level_niter per level (entry 0 ignored)  */
+    const uint32_t* niter;
+    uint32_t coarse_n;       /* coarsest-level size for the direct solve (0 = none)   */
+    uint32_t max_levels;     /* multi-split max_levels                                */
+    uint32_t degree_max;     /* multi-split simple_1 elimination bound                */
+    int32_t order;           /* MLP_ORDER_*                                           */
+    int32_t use_tails;       /* uh_cheb tail elimination (Config::use_tails)          */
+    uint32_t nsigma;         /* uh_cheb sigma (= beta) per level                      */
+    const double* sigma;
+    uint32_t nncheb;         /* uh_cheb Chebyshev degree per level                    */
+    const uint32_t* ncheb;
+    int32_t fp32;            /* 1: store and apply the hierarchy in FP32              */
+} mlp_prec_cfg;
+
+/* Solver statistics, the fields of SolverStats (solvers.h:15-28) plus the
+ * quantities the GPU path reports. */
+typedef struct {
+    uint32_t niter;
+    uint32_t napply;
+    double init_norm;
+    double final_norm;
+    double final_rel;
+    double t_solve_ms;   /* device time of the whole PCG call              */
+    double t_setup_ms;   /* device time of the preconditioner construction */
+} mlp_stats;
+
+/* Per-level summary, the fields printed by operator<< for MultiSplitPrec::Level
+ * (multi_split_misc.cc:228-240) and Prec::Level (cheb_misc.cc:61-74). */
+typedef struct {
+    uint32_t N, nnz, M, Md, n;
+    uint32_t niter, ncheb;
+    int32_t direct;            /* 1 if the level is solved with the dense inverse */
+    double q, alpha, beta, lmin, lmax;
+    uint32_t L_nnz, U_nnz;
+    uint32_t nwave_l, nwave_u; /* wavefronts of the level-scheduled L / U solves  */
+} mlp_level_info;
+
+const char* mlp_last_error(void);
+int mlp_version(void);
+int mlp_device_count(int* count);
+int mlp_set_device(int device);
+
+/* ---- matrices ------------------------------------------------------------
+ * Replaces CSRMatrix / SkylineMatrix storage (matrix.h:187-291): uint32 ia
+ * (n+1), ja and FP64 a (nnz), diagonal first in every row. The library keeps a
+ * device copy; the host arrays may be released after the call. */
+int mlp_matrix_create(uint32_t n, const uint32_t* ia_host, const uint32_t* ja_host, const double* a_host,
+                      mlp_matrix** out);
+/* SPEMesh(nx,ny,nz) + construct_matrix(A, c) (spe.cc:11-131) on the device,
+ * from the SPE10-layout permeability blocks (1,122,000 values each, host).
+ * dirichlet != 0 adds the benchmark's x-face Dirichlet terms; b_host (n values,
+ * may be NULL) receives the matching right-hand side. */
+int mlp_matrix_create_spe(uint32_t nx, uint32_t ny, uint32_t nz, const double* kx_host, const double* ky_host,
+                          const double* kz_host, double c, int32_t dirichlet, mlp_matrix** out, double* b_host);
+int mlp_matrix_destroy(mlp_matrix* A);
+int mlp_matrix_size(const mlp_matrix* A, uint32_t* n, uint32_t* nnz);
+int mlp_matrix_download(const mlp_matrix* A, uint32_t* ia_host, uint32_t* ja_host, double* a_host);
+/* y = A x (multiply(A, v, res, 'o'), csrmatrix.cc:260-274), device vectors. */
+int mlp_spmv(const mlp_matrix* A, const double* x_dev, double* y_dev, void* stream);
+
+/* ---- preconditioners -------------------------------------------------------
+ * mlp_prec_create replaces MultiSplitPrec(const SkylineMatrix&, const Config&)
+ * (multi_split_prec.h:105) and Prec(const SkylineMatrix&, const Config&)
+ * (cheb_prec.h:115); the hierarchy is built on the device. */
+int mlp_prec_create(const mlp_matrix* A, const mlp_prec_cfg* cfg, mlp_prec** out);
+int mlp_prec_destroy(mlp_prec* P);
+/* x = B f (PrecBase::solve(Vector& f, Vector& x) const, prec_base.h:8-12),
+ * device vectors in the matrix's natural order. */
+int mlp_prec_apply(mlp_prec* P, const double* f_dev, double* x_dev, void* stream);
+/* Same with host vectors (copies in and out). */
+int mlp_prec_apply_host(mlp_prec* P, const double* f_host, double* x_host);
+int mlp_prec_nlevels(const mlp_prec* P, uint32_t* nlevels);
+int mlp_prec_level_info(const mlp_prec* P, uint32_t level, mlp_level_info* info);
+/* Level data in the reference's indexing, for parity checks: map (N), L
+ * (ia: N-Md+1, ja/a: L_nnz), U (ia: M+1, ja/a: U_nnz), the level matrix A
+ * (ia: N+1, ja/a: nnz; level 0 is the input) and dval (Md). Any pointer may
+ * be NULL to skip that array. */
+int mlp_prec_level_export(const mlp_prec* P, uint32_t level, uint32_t* map, uint32_t* L_ia, uint32_t* L_ja,
+                          double* L_a, uint32_t* U_ia, uint32_t* U_ja, double* U_a, uint32_t* A_ia,
+                          uint32_t* A_ja, double* A_a, double* dval);
+/* Algorithmic HBM bytes of one apply (the roofline numerator). */
+int mlp_prec_bytes_per_apply(const mlp_prec* P, uint64_t* bytes);
+
+/* ---- solver ----------------------------------------------------------------
+ * PCGSolver(A, b, B, x, stats, eps, NORM_L2) (solvers.h:31-32, pcg.cc:8-102):
+ * x0 from generate_x0 (solvers.cc:9-21), stop when ||r||/||r0|| <= eps (eps
+ * raised so that the absolute stop is >= 1e-14, solvers.cc:49-58).
+ * flexible != 0 uses the Polak-Ribiere beta (needed with an FP32 hierarchy).
+ * maxit = 0 means no cap. */
+int mlp_pcg(const mlp_matrix* A, const double* b_host, mlp_prec* P, double* x_host, double eps, uint32_t maxit,
+            int32_t flexible, mlp_stats* stats);
+int mlp_pcg_device(const mlp_matrix* A, const double* b_dev, mlp_prec* P, double* x_dev, double eps,
+                   uint32_t maxit, int32_t flexible, mlp_stats* stats, void* stream);
+
+/* generate_x0 (solvers.cc:9-21) on the host: srandom(3), glibc random(). */
+int mlp_generate_x0(double* x_host, uint32_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,359 @@
+// extern "C" entry points (include/mlp_b200.h). Each one converts exceptions
+// into a status code plus a per-thread message.
+#include <cstring>
+
+#include "../../include/mlp_b200.h"
+#include "solve.cuh"
+
+using namespace mlp;
+
+struct mlp_matrix {
+    DCSR A;
+    cudaStream_t s = nullptr;
+    ~mlp_matrix() {
+        if (s) cudaStreamDestroy(s);
+    }
+};
+
+struct mlp_prec {
+    std::unique_ptr<Prec> P;
+    cudaStream_t s = nullptr;
+    double setup_ms = 0;
+    DBuf<double> tmp_in, tmp_out;
+    ~mlp_prec() {
+        P.reset();
+        if (s) cudaStreamDestroy(s);
+    }
+};
+
+#define API_BEGIN try {
+#define API_END                                                 \
+    }                                                           \
+    catch (const mlp::Error& e) {                               \
+        set_last_error(e.what());                               \
+        return e.code;                                          \
+    }                                                           \
+    catch (const std::bad_alloc&) {                             \
+        set_last_error("host out of memory");                   \
+        return MLP_ERR_LIMIT;                                   \
+    }                                                           \
+    catch (const std::exception& e) {                           \
+        set_last_error(e.what());                               \
+        return MLP_ERR_INTERNAL;                                \
+    }                                                           \
+    return MLP_OK;
+
+static cudaStream_t new_stream() {
+    cudaStream_t s;
+    CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    return s;
+}
+
+extern "C" {
+
+const char* mlp_last_error(void) { return last_error(); }
+
+int mlp_version(void) { return 100; }
+
+int mlp_device_count(int* count) {
+    API_BEGIN
+    CK(cudaGetDeviceCount(count));
+    API_END
+}
+
+int mlp_set_device(int device) {
+    API_BEGIN
+    CK(cudaSetDevice(device));
+    API_END
+}
+
+int mlp_matrix_create(uint32_t n, const uint32_t* ia, const uint32_t* ja, const double* a, mlp_matrix** out) {
+    API_BEGIN
+    if (!out || !ia || (n && (!ja || !a))) MLP_THROW(ERR_ARG, "null pointer");
+    if (ia[0] != 0) MLP_THROW(ERR_ARG, "ia[0] must be 0");
+    uint32_t nnz = ia[n];
+    for (uint32_t i = 0; i < n; i++) {
+        if (ia[i + 1] <= ia[i]) MLP_THROW(ERR_ARG, "every row needs at least its diagonal (row " + std::to_string(i) + ")");
+        if (ja[ia[i]] != i) MLP_THROW(ERR_ARG, "diagonal must come first in row " + std::to_string(i));
+    }
+    for (uint32_t k = 0; k < nnz; k++)
+        if (ja[k] >= n) MLP_THROW(ERR_ARG, "column index out of range");
+    auto* M = new mlp_matrix();
+    try {
+        M->s = new_stream();
+        M->A.alloc(n, n, nnz);
+        M->A.ia.upload(ia, (size_t)n + 1, M->s);
+        M->A.ja.upload(ja, nnz, M->s);
+        M->A.a.upload(a, nnz, M->s);
+        CK(cudaStreamSynchronize(M->s));
+    } catch (...) {
+        delete M;
+        throw;
+    }
+    *out = M;
+    API_END
+}
+
+int mlp_matrix_create_spe(uint32_t nx, uint32_t ny, uint32_t nz, const double* kx, const double* ky,
+                          const double* kz, double c, int32_t dirichlet, mlp_matrix** out, double* b_host) {
+    API_BEGIN
+    if (!out || !kx || !ky || !kz) MLP_THROW(ERR_ARG, "null pointer");
+    if (!nx || !ny || !nz) MLP_THROW(ERR_ARG, "empty mesh");
+    if ((uint64_t)nx * ny * nz > 0xffffffffull / 8) MLP_THROW(ERR_LIMIT, "mesh too large for 32-bit indices");
+    const size_t KN = 1122000;
+    auto* M = new mlp_matrix();
+    try {
+        M->s = new_stream();
+        DBuf<double> dk(3 * KN);
+        CK(cudaMemcpyAsync(dk.p, kx, KN * 8, cudaMemcpyHostToDevice, M->s));
+        CK(cudaMemcpyAsync(dk.p + KN, ky, KN * 8, cudaMemcpyHostToDevice, M->s));
+        CK(cudaMemcpyAsync(dk.p + 2 * KN, kz, KN * 8, cudaMemcpyHostToDevice, M->s));
+        uint32_t N = nx * ny * nz;
+        DBuf<double> b(b_host ? N : 0);
+        spe_assemble(nx, ny, nz, dk.p, dk.p + KN, dk.p + 2 * KN, c, dirichlet, M->A, b_host ? b.p : nullptr, M->s);
+        if (b_host) CK(cudaMemcpyAsync(b_host, b.p, (size_t)N * 8, cudaMemcpyDeviceToHost, M->s));
+        CK(cudaStreamSynchronize(M->s));
+    } catch (...) {
+        delete M;
+        throw;
+    }
+    *out = M;
+    API_END
+}
+
+int mlp_matrix_destroy(mlp_matrix* A) {
+    API_BEGIN
+    delete A;
+    API_END
+}
+
+int mlp_matrix_size(const mlp_matrix* A, uint32_t* n, uint32_t* nnz) {
+    API_BEGIN
+    if (!A) MLP_THROW(ERR_ARG, "null matrix");
+    if (n) *n = A->A.nrow;
+    if (nnz) *nnz = A->A.nnz;
+    API_END
+}
+
+int mlp_matrix_download(const mlp_matrix* A, uint32_t* ia, uint32_t* ja, double* a) {
+    API_BEGIN
+    if (!A) MLP_THROW(ERR_ARG, "null matrix");
+    const DCSR& m = A->A;
+    if (ia) CK(cudaMemcpyAsync(ia, m.ia.p, ((size_t)m.nrow + 1) * 4, cudaMemcpyDeviceToHost, A->s));
+    if (ja) CK(cudaMemcpyAsync(ja, m.ja.p, (size_t)m.nnz * 4, cudaMemcpyDeviceToHost, A->s));
+    if (a) CK(cudaMemcpyAsync(a, m.a.p, (size_t)m.nnz * 8, cudaMemcpyDeviceToHost, A->s));
+    CK(cudaStreamSynchronize(A->s));
+    API_END
+}
+
+int mlp_spmv(const mlp_matrix* A, const double* x, double* y, void* stream) {
+    API_BEGIN
+    if (!A || !x || !y) MLP_THROW(ERR_ARG, "null pointer");
+    cudaStream_t s = stream ? (cudaStream_t)stream : A->s;
+    spmv(A->A, x, y, s);
+    if (!stream) CK(cudaStreamSynchronize(s));
+    API_END
+}
+
+int mlp_prec_create(const mlp_matrix* A, const mlp_prec_cfg* c, mlp_prec** out) {
+    API_BEGIN
+    if (!A || !c || !out) MLP_THROW(ERR_ARG, "null pointer");
+    BuildCfg cfg;
+    cfg.kind = c->kind;
+    if (c->kind != MLP_PREC_MSPLIT && c->kind != MLP_PREC_CHEB) MLP_THROW(ERR_CONFIG, "unknown preconditioner kind");
+    if (c->kind == MLP_PREC_MSPLIT) {
+        if (!c->nq || !c->q) MLP_THROW(ERR_CONFIG, "q list is empty");
+        if (!c->nniter || !c->niter) MLP_THROW(ERR_CONFIG, "level_niter list is empty");
+        cfg.q.assign(c->q, c->q + c->nq);
+        cfg.niter.assign(c->niter, c->niter + c->nniter);
+        for (double q : cfg.q)
+            if (!(q >= 0 && q < 1)) MLP_THROW(ERR_CONFIG, "q must lie in [0, 1)");
+        cfg.coarse_n = c->coarse_n;
+        cfg.max_levels = c->max_levels;
+        cfg.degree_max = c->degree_max;
+        cfg.order = c->order;
+        if (cfg.max_levels == 0) MLP_THROW(ERR_CONFIG, "max_levels must be positive");
+    } else {
+        if (!c->nsigma || !c->sigma) MLP_THROW(ERR_CONFIG, "sigma list is empty");
+        if (!c->nncheb || !c->ncheb) MLP_THROW(ERR_CONFIG, "niters list is empty");
+        cfg.sigma.assign(c->sigma, c->sigma + c->nsigma);
+        cfg.ncheb.assign(c->ncheb, c->ncheb + c->nncheb);
+        for (double s : cfg.sigma)
+            if (!(s > 1)) MLP_THROW(ERR_CONFIG, "All sigmas must be > 1");  // main_helper.cc:235-238
+        cfg.use_tails = c->use_tails;
+    }
+    auto* H = new mlp_prec();
+    try {
+        H->s = new_stream();
+        cudaEvent_t e0, e1;
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        CK(cudaEventRecord(e0, H->s));
+        H->P = make_prec(A->A, cfg, c->fp32 != 0, H->s);
+        CK(cudaEventRecord(e1, H->s));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        H->setup_ms = ms;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    } catch (...) {
+        delete H;
+        throw;
+    }
+    *out = H;
+    API_END
+}
+
+int mlp_prec_destroy(mlp_prec* P) {
+    API_BEGIN
+    delete P;
+    API_END
+}
+
+static void apply_natural(mlp_prec* P, const double* f, double* x, cudaStream_t s) {
+    Prec& Q = *P->P;
+    const Level& L0 = *Q.H->lv[0];
+    gather(L0.N, L0.phi.p, f, Q.fin_buf.p, s);
+    prec_apply_frame(Q, s);
+    scatter(L0.N, L0.phi.p, Q.fout_buf.p, x, s);
+}
+
+int mlp_prec_apply(mlp_prec* P, const double* f, double* x, void* stream) {
+    API_BEGIN
+    if (!P || !f || !x) MLP_THROW(ERR_ARG, "null pointer");
+    cudaStream_t s = stream ? (cudaStream_t)stream : P->s;
+    apply_natural(P, f, x, s);
+    if (!stream) CK(cudaStreamSynchronize(s));
+    API_END
+}
+
+int mlp_prec_apply_host(mlp_prec* P, const double* f, double* x) {
+    API_BEGIN
+    if (!P || !f || !x) MLP_THROW(ERR_ARG, "null pointer");
+    uint32_t n = P->P->H->lv[0]->N;
+    P->tmp_in.alloc(n);
+    P->tmp_out.alloc(n);
+    CK(cudaMemcpyAsync(P->tmp_in.p, f, (size_t)n * 8, cudaMemcpyHostToDevice, P->s));
+    apply_natural(P, P->tmp_in.p, P->tmp_out.p, P->s);
+    CK(cudaMemcpyAsync(x, P->tmp_out.p, (size_t)n * 8, cudaMemcpyDeviceToHost, P->s));
+    CK(cudaStreamSynchronize(P->s));
+    API_END
+}
+
+int mlp_prec_nlevels(const mlp_prec* P, uint32_t* nl) {
+    API_BEGIN
+    if (!P || !nl) MLP_THROW(ERR_ARG, "null pointer");
+    *nl = P->P->H->nlevels;
+    API_END
+}
+
+int mlp_prec_level_info(const mlp_prec* P, uint32_t level, mlp_level_info* info) {
+    API_BEGIN
+    if (!P || !info) MLP_THROW(ERR_ARG, "null pointer");
+    const Hierarchy& H = *P->P->H;
+    if (level >= H.nlevels) MLP_THROW(ERR_ARG, "level out of range");
+    const Level& L = *H.lv[level];
+    memset(info, 0, sizeof *info);
+    info->N = L.N; info->nnz = L.nnz; info->M = L.M; info->Md = L.Md; info->n = L.n;
+    info->niter = L.niter; info->ncheb = L.ncheb; info->direct = L.direct;
+    info->q = L.q; info->alpha = L.alpha; info->beta = L.beta; info->lmin = L.lmin; info->lmax = L.lmax;
+    info->L_nnz = L.L.nnz; info->U_nnz = L.U.nnz;
+    info->nwave_l = L.lw_off.empty() ? 0 : (uint32_t)L.lw_off.size() - 1;
+    info->nwave_u = L.uw_off.empty() ? 0 : (uint32_t)L.uw_off.size() - 1;
+    API_END
+}
+
+int mlp_prec_level_export(const mlp_prec* P, uint32_t level, uint32_t* map, uint32_t* L_ia, uint32_t* L_ja,
+                          double* L_a, uint32_t* U_ia, uint32_t* U_ja, double* U_a, uint32_t* A_ia,
+                          uint32_t* A_ja, double* A_a, double* dval) {
+    API_BEGIN
+    if (!P) MLP_THROW(ERR_ARG, "null pointer");
+    const Hierarchy& H = *P->P->H;
+    if (level >= H.nlevels) MLP_THROW(ERR_ARG, "level out of range");
+    const Level& L = *H.lv[level];
+    cudaStream_t s = P->s;
+    auto cp = [&](void* dst, const void* src, size_t bytes) {
+        if (dst && bytes && src) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+    };
+    if (!L.direct) {
+        cp(map, L.map.p, (size_t)L.N * 4);
+        cp(L_ia, L.L.ia.p, ((size_t)L.L.nrow + 1) * 4);
+        cp(L_ja, L.L.ja.p, (size_t)L.L.nnz * 4);
+        cp(L_a, L.L.a.p, (size_t)L.L.nnz * 8);
+        cp(U_ia, L.U.ia.p, ((size_t)L.U.nrow + 1) * 4);
+        cp(U_ja, L.U.ja.p, (size_t)L.U.nnz * 4);
+        cp(U_a, L.U.a.p, (size_t)L.U.nnz * 8);
+        cp(dval, L.dval.p, (size_t)L.Md * 8);
+    }
+    cp(A_ia, L.A.ia.p, ((size_t)L.A.nrow + 1) * 4);
+    cp(A_ja, L.A.ja.p, (size_t)L.A.nnz * 4);
+    cp(A_a, L.A.a.p, (size_t)L.A.nnz * 8);
+    CK(cudaStreamSynchronize(s));
+    API_END
+}
+
+int mlp_prec_bytes_per_apply(const mlp_prec* P, uint64_t* bytes) {
+    API_BEGIN
+    if (!P || !bytes) MLP_THROW(ERR_ARG, "null pointer");
+    *bytes = P->P->bytes_per_apply;
+    API_END
+}
+
+static int pcg_common(const mlp_matrix* A, const double* b_dev, mlp_prec* P, double* x_dev, double eps,
+                      uint32_t maxit, int32_t flexible, mlp_stats* stats, cudaStream_t s) {
+    PcgStats st;
+    int rc = pcg_solve(A->A, b_dev, *P->P, x_dev, eps, maxit, flexible != 0, st, s);
+    if (stats) {
+        stats->niter = st.niter;
+        stats->napply = st.napply;
+        stats->init_norm = st.init_norm;
+        stats->final_norm = st.final_norm;
+        stats->final_rel = st.final_rel;
+        stats->t_solve_ms = st.t_total_ms;
+        stats->t_setup_ms = P->setup_ms;
+    }
+    return rc;
+}
+
+int mlp_pcg(const mlp_matrix* A, const double* b_host, mlp_prec* P, double* x_host, double eps, uint32_t maxit,
+            int32_t flexible, mlp_stats* stats) {
+    API_BEGIN
+    if (!A || !b_host || !P || !x_host) MLP_THROW(ERR_ARG, "null pointer");
+    uint32_t n = A->A.nrow;
+    cudaStream_t s = P->s;
+    DBuf<double> b(n), x(n);
+    CK(cudaMemcpyAsync(b.p, b_host, (size_t)n * 8, cudaMemcpyHostToDevice, s));
+    int rc = pcg_common(A, b.p, P, x.p, eps, maxit, flexible, stats, s);
+    CK(cudaMemcpyAsync(x_host, x.p, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return rc;
+    API_END
+}
+
+int mlp_pcg_device(const mlp_matrix* A, const double* b_dev, mlp_prec* P, double* x_dev, double eps,
+                   uint32_t maxit, int32_t flexible, mlp_stats* stats, void* stream) {
+    API_BEGIN
+    if (!A || !b_dev || !P || !x_dev) MLP_THROW(ERR_ARG, "null pointer");
+    cudaStream_t s = stream ? (cudaStream_t)stream : P->s;
+    return pcg_common(A, b_dev, P, x_dev, eps, maxit, flexible, stats, s);
+    API_END
+}
+
+int mlp_generate_x0(double* x, uint32_t n) {
+    API_BEGIN
+    if (!x && n) MLP_THROW(ERR_ARG, "null pointer");
+    struct random_data rd;
+    memset(&rd, 0, sizeof rd);
+    char state[128];
+    initstate_r(3, state, sizeof state, &rd);
+    srandom_r(3, &rd);
+    for (uint32_t i = 0; i < n; i++) {
+        int32_t v;
+        random_r(&rd, &v);
+        x[i] = 20. * (v - 0.5 * RAND_MAX) / RAND_MAX + 100;
+    }
+    API_END
+}
+
+}  // extern "C"

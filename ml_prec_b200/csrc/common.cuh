@@ -1,0 +1,124 @@
+// Shared infrastructure of the ml_prec_b200 CUDA library: error state, device
+// buffers, CSR containers and small launch helpers. Every entry point of the
+// C ABI returns an int status and records a message retrievable through
+// mlp_last_error() (include/mlp_b200.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace mlp {
+
+// Status codes of the C ABI (mirrored in include/mlp_b200.h).
+enum Status : int {
+    OK = 0,
+    ERR_ARG = 1,          // invalid argument / size
+    ERR_CONFIG = 2,       // bad preconditioner configuration
+    ERR_LEVELS = 3,       // "Too many levels"
+    ERR_CURVATURE = 4,    // <Ap, p> <= 0 in PCG
+    ERR_NOT_FINITE = 5,   // NaN / Inf in a scalar
+    ERR_MAXIT = 6,        // iteration cap reached
+    ERR_CUDA = 7,         // CUDA runtime error
+    ERR_NO_ITER = 8,      // "No need to iterate"
+    ERR_LIMIT = 9,        // a documented size limit was exceeded
+    ERR_INTERNAL = 10,    // a device-side consistency check failed
+};
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define MLP_THROW(code, msg)                                                     \
+    do {                                                                         \
+        throw ::mlp::Error((code), std::string(msg) + " (" + __FILE__ + ":" +    \
+                                       std::to_string(__LINE__) + ")");          \
+    } while (0)
+
+#define CK(call)                                                                 \
+    do {                                                                         \
+        cudaError_t e_ = (call);                                                 \
+        if (e_ != cudaSuccess)                                                   \
+            MLP_THROW(::mlp::ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define CK_LAUNCH() CK(cudaGetLastError())
+
+void set_last_error(const std::string& s);
+const char* last_error();
+
+// Device buffer (RAII). Allocations go through cudaMallocAsync on the library's
+// stream so that repeated setups reuse the pool.
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    explicit DBuf(size_t count) { alloc(count); }
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    DBuf(DBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DBuf& operator=(DBuf&& o) noexcept {
+        if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+        return *this;
+    }
+    ~DBuf() { release(); }
+    void alloc(size_t count) {
+        release();
+        n = count;
+        if (count) CK(cudaMalloc(&p, count * sizeof(T)));
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void zero(cudaStream_t s) { if (n) CK(cudaMemsetAsync(p, 0, n * sizeof(T), s)); }
+    void upload(const T* h, size_t count, cudaStream_t s) {
+        if (count > n) alloc(count);
+        if (count) CK(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+    std::vector<T> download(cudaStream_t s, size_t count = (size_t)-1) const {
+        if (count == (size_t)-1) count = n;
+        std::vector<T> h(count);
+        if (count) CK(cudaMemcpyAsync(h.data(), p, count * sizeof(T), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        return h;
+    }
+};
+
+// CSR matrix on the device: 32-bit indices, FP64 values (plus an optional FP32
+// copy of the values for the reduced-precision preconditioner).
+struct DCSR {
+    uint32_t nrow = 0, ncol = 0, nnz = 0;
+    DBuf<uint32_t> ia, ja;
+    DBuf<double> a;
+    DBuf<float> a32;
+    void alloc(uint32_t r, uint32_t c, uint32_t z) {
+        nrow = r; ncol = c; nnz = z;
+        ia.alloc((size_t)r + 1);
+        ja.alloc(z ? z : 1);
+        a.alloc(z ? z : 1);
+    }
+};
+
+inline unsigned grid_for(size_t n, unsigned block) {
+    size_t g = (n + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > 0x7fffffff) g = 0x7fffffff;
+    return (unsigned)g;
+}
+
+int num_sms();
+
+// Exclusive scan of 32-bit counts on the device; returns the total (synchronises).
+uint32_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n, cudaStream_t s);
+// Same, total left on the device at out[n] (no host synchronisation).
+void exclusive_scan_u32_async(const uint32_t* in, uint32_t* out, uint32_t n, cudaStream_t s);
+
+}  // namespace mlp

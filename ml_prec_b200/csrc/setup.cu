@@ -1,0 +1,1130 @@
+// Hierarchy construction kernels (marking, ordering, sparse Schur elimination,
+// matrix assembly). Compiled with -fmad=false: every floating-point expression
+// rounds exactly as the reference's x86-64 SSE2 build does (no contraction into
+// FMA), so every integer decision taken on a floating-point comparison (which
+// link is dropped, the node ordering, the coarse sparsity pattern) and every
+// factor value come out bit-identical to the reference.
+#include "setup.cuh"
+
+namespace mlp {
+
+// ---------------------------------------------------------------------------
+// SPE 7-point assembly (spe.cc:69-131, XYZ order). Row i = (x, y, z) has the
+// diagonal first (initialised to c) followed by the existing neighbours in the
+// order -z, -y, -x, +x, +y, +z; each link value v = 2/(1/k_i + 1/k_j)/(h*h) is
+// stored as -v and added to the diagonal in that order. The permeability field
+// is addressed like SPEMesh::index_k (mesh.h:57-59), i.e. modulo 60x220x85.
+// Dirichlet x-faces (benchmark problem): diag += 2*kx/hx^2 at x = 0 and
+// x = nx-1 (in that order), b = that value at x = 0 (p = 1), 0 elsewhere.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t kidx(uint32_t i, uint32_t j, uint32_t k) {
+    return (k * 13200u + j * 60u + i) % 1122000u;
+}
+
+__global__ void k_spe_rowlen(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t* len) {
+    uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t N = nx * ny * nz;
+    if (r >= N) return;
+    uint32_t i = r % nx, j = (r / nx) % ny, k = r / (nx * ny);
+    len[r] = 1 + (k > 0) + (j > 0) + (i > 0) + (i + 1 < nx) + (j + 1 < ny) + (k + 1 < nz);
+}
+
+__device__ __forceinline__ double spe_link(const double* K, uint32_t a, uint32_t b, double h) {
+    return 2 / (1 / K[a] + 1 / K[b]) / (h * h);
+}
+
+__global__ void k_spe_fill(uint32_t nx, uint32_t ny, uint32_t nz, const double* __restrict__ kx,
+                           const double* __restrict__ ky, const double* __restrict__ kz, double c,
+                           int dirichlet, const uint32_t* __restrict__ ia, uint32_t* __restrict__ ja,
+                           double* __restrict__ a, double* __restrict__ b) {
+    uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t N = nx * ny * nz;
+    if (r >= N) return;
+    const double hx = 20, hy = 10, hz = 2;
+    uint32_t i = r % nx, j = (r / nx) % ny, k = r / (nx * ny);
+    uint32_t p = ia[r];
+    uint32_t dind = p;
+    uint32_t me = kidx(i, j, k);
+    double diag = c;
+    ja[p++] = r;
+    if (k) { double v = spe_link(kz, me, kidx(i, j, k - 1), hz); ja[p] = r - nx * ny; a[p++] = -v; diag += v; }
+    if (j) { double v = spe_link(ky, me, kidx(i, j - 1, k), hy); ja[p] = r - nx; a[p++] = -v; diag += v; }
+    if (i) { double v = spe_link(kx, me, kidx(i - 1, j, k), hx); ja[p] = r - 1; a[p++] = -v; diag += v; }
+    if (i + 1 < nx) { double v = spe_link(kx, me, kidx(i + 1, j, k), hx); ja[p] = r + 1; a[p++] = -v; diag += v; }
+    if (j + 1 < ny) { double v = spe_link(ky, me, kidx(i, j + 1, k), hy); ja[p] = r + nx; a[p++] = -v; diag += v; }
+    if (k + 1 < nz) { double v = spe_link(kz, me, kidx(i, j, k + 1), hz); ja[p] = r + nx * ny; a[p++] = -v; diag += v; }
+    double bb = 0;
+    if (dirichlet) {
+        double tD = 2 * kx[me] / (hx * hx);
+        if (i == 0) { diag += tD; bb += tD * 1.0; }
+        if (i == nx - 1) diag += tD;
+    }
+    a[dind] = diag;
+    if (b) b[r] = bb;
+}
+
+void spe_assemble(uint32_t nx, uint32_t ny, uint32_t nz, const double* kx, const double* ky,
+                  const double* kz, double c, int dirichlet, DCSR& A, double* b, cudaStream_t s) {
+    uint32_t N = nx * ny * nz;
+    DBuf<uint32_t> len(N);
+    k_spe_rowlen<<<grid_for(N, 256), 256, 0, s>>>(nx, ny, nz, len.p);
+    CK_LAUNCH();
+    A.ia.alloc((size_t)N + 1);
+    uint32_t nnz = exclusive_scan_u32(len.p, A.ia.p, N, s);
+    A.nrow = A.ncol = N;
+    A.nnz = nnz;
+    A.ja.alloc(nnz);
+    A.a.alloc(nnz);
+    k_spe_fill<<<grid_for(N, 256), 256, 0, s>>>(nx, ny, nz, kx, ky, kz, c, dirichlet, A.ia.p, A.ja.p,
+                                               A.a.p, b);
+    CK_LAUNCH();
+}
+
+// ---------------------------------------------------------------------------
+// Marking.
+// Stable ascending order of a row's off-diagonals by |a| (the insertion sort of
+// multi_split_constr.cc:26-36 / cheb_constr.cc:155-165: strict '>' keeps equal
+// magnitudes in ja order). Rows are short (7-point stencil and its Schur
+// complements), so each thread sorts its row in a local array of MAXR entries;
+// longer rows set the overflow flag and the host reports ERR_LIMIT.
+// ---------------------------------------------------------------------------
+static constexpr int MAXR = 64;
+
+__device__ __forceinline__ int sort_row(const double* __restrict__ a, uint32_t rs, uint32_t nrz,
+                                        uint8_t* idx) {
+    if (nrz > MAXR) return -1;
+    for (uint32_t t = 0; t < nrz; t++) {
+        double v = fabs(a[rs + 1 + t]);
+        int j = (int)t - 1;
+        while (j >= 0 && fabs(a[rs + 1 + idx[j]]) > v) { idx[j + 1] = idx[j]; j--; }
+        idx[j + 1] = (uint8_t)t;
+    }
+    return 0;
+}
+
+// Multi-split q-threshold link dropping (multi_split_constr.cc:65-113):
+// aux = a_ii + sum_j a_ij (ja order); s = q/(1-q)*aux; walk the off-diagonals by
+// increasing |a|, dropping link (i,j) while -a_ij <= s (s -= -a_ij); then
+// aux *= 1/(1-q). keep[j_] = 0 for dropped links; nout = kept links of the row;
+// nin[j] = number of kept links pointing to j.
+__global__ void k_mark_msplit(uint32_t N, const uint32_t* __restrict__ ia, const uint32_t* __restrict__ ja,
+                              const double* __restrict__ a, double q, uint8_t* __restrict__ keep,
+                              int* __restrict__ nout, int* __restrict__ nin, double* __restrict__ aux,
+                              int* __restrict__ err) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    uint32_t rs = ia[i], re = ia[i + 1], nrz = re - rs - 1;
+    double ax = a[rs];
+    for (uint32_t j_ = rs + 1; j_ < re; j_++) ax += a[j_];
+    uint8_t idx[MAXR];
+    if (sort_row(a, rs, nrz, idx)) { atomicOr(err, 1); return; }
+    uint64_t drop = 0;
+    int no = (int)nrz;
+    double s = q / (1 - q) * ax;
+    for (uint32_t t = 0; t < nrz; t++) {
+        uint32_t j_ = rs + 1 + idx[t];
+        double aij = -a[j_];
+        if (aij <= s) {
+            drop |= 1ull << idx[t];
+            no--;
+            s -= aij;
+        } else
+            break;
+    }
+    keep[rs] = 1;
+    for (uint32_t t = 0; t < nrz; t++) {
+        uint32_t j_ = rs + 1 + t;
+        bool kp = !((drop >> t) & 1ull);
+        keep[j_] = kp;
+        if (kp) atomicAdd(&nin[ja[j_]], 1);
+    }
+    nout[i] = no;
+    aux[i] = ax * (1. / (1 - q));
+}
+
+// uh_cheb two-ended marking (cheb_constr.cc:191-232 with to_remove,
+// cheb_prec.h:57-85): aux = sum of the row (diagonal first, ja order); walk the
+// off-diagonals by increasing |a| accumulating t = -2v/(aux*(beta-1)) while
+// s + t <= 1; each such link is marked from this end (want[j_] = 1). A link is
+// removed when both of its ends marked it (LinkTypeCheb::mark, cheb_misc.h:73).
+__global__ void k_mark_cheb(uint32_t N, const uint32_t* __restrict__ ia, const double* __restrict__ a,
+                            double beta, uint8_t* __restrict__ want, double* __restrict__ aux,
+                            int* __restrict__ err) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    uint32_t rs = ia[i], re = ia[i + 1], nrz = re - rs - 1;
+    double ax = 0.0;
+    for (uint32_t j_ = rs; j_ < re; j_++) ax += a[j_];
+    uint8_t idx[MAXR];
+    if (sort_row(a, rs, nrz, idx)) { atomicOr(err, 1); return; }
+    for (uint32_t j_ = rs; j_ < re; j_++) want[j_] = 0;
+    double s = 0.;
+    for (uint32_t t = 0; t < nrz; t++) {
+        double v = a[rs + 1 + idx[t]];
+        double tt = -2 * v / (ax * (beta - 1));
+        if (s + tt > 1) break;
+        s += tt;
+        want[rs + 1 + idx[t]] = 1;
+    }
+    aux[i] = ax;
+}
+
+// Transpose position of every off-diagonal: tpos[j_] = position of (j, i) in
+// row j (binary search over the sorted off-diagonal part, skyline.cc:15-28).
+__global__ void k_transpose_pos(uint32_t N, const uint32_t* __restrict__ ia, const uint32_t* __restrict__ ja,
+                                uint32_t* __restrict__ tpos, int* __restrict__ err) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    for (uint32_t j_ = ia[i] + 1; j_ < ia[i + 1]; j_++) {
+        uint32_t j = ja[j_];
+        uint32_t lo = ia[j] + 1, hi = ia[j + 1];
+        while (lo < hi) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (ja[mid] < i) lo = mid + 1; else hi = mid;
+        }
+        if (lo < ia[j + 1] && ja[lo] == i) tpos[j_] = lo;
+        else { tpos[j_] = 0xffffffffu; atomicOr(err, 2); }
+    }
+}
+
+// Link state after the two-ended marking: keep = not marked from both ends;
+// nlinks = kept links of the row; slot[j_] = upper-triangle position of the link
+// (where LinkTypeCheb keeps its counter).
+__global__ void k_cheb_links(uint32_t N, const uint32_t* __restrict__ ia, const uint32_t* __restrict__ ja,
+                             const uint8_t* __restrict__ want, const uint32_t* __restrict__ tpos,
+                             uint8_t* __restrict__ keep, int* __restrict__ nlinks, uint32_t* __restrict__ slot) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    int nl = 0;
+    keep[ia[i]] = 1;
+    for (uint32_t j_ = ia[i] + 1; j_ < ia[i + 1]; j_++) {
+        uint32_t t = tpos[j_];
+        bool removed = want[j_] && want[t];
+        keep[j_] = !removed;
+        nl += !removed;
+        slot[j_] = ja[j_] > i ? j_ : t;
+    }
+    nlinks[i] = nl;
+}
+
+// ---------------------------------------------------------------------------
+// Stable bucket partition (the node orderings). Every node gets a bucket id
+// (< NB, or NONE to skip it); nodes are written bucket by bucket, keeping index
+// order inside a bucket, or reversed order for buckets flagged in rev_mask
+// (the reference fills the diagonal group from the end: map[eind--]).
+// ---------------------------------------------------------------------------
+static constexpr int PT = 1024;  // nodes per partition tile
+
+__global__ void k_part_count(uint32_t N, const uint8_t* __restrict__ bucket, int NB, uint32_t ntile,
+                             uint32_t* __restrict__ counts) {
+    __shared__ uint32_t c[8];
+    if (threadIdx.x < 8) c[threadIdx.x] = 0;
+    __syncthreads();
+    uint32_t i = blockIdx.x * PT + threadIdx.x;
+    if (i < N && bucket[i] < NB) atomicAdd(&c[bucket[i]], 1u);
+    __syncthreads();
+    if (threadIdx.x < (unsigned)NB) counts[threadIdx.x * ntile + blockIdx.x] = c[threadIdx.x];
+}
+
+__global__ void k_part_scatter(uint32_t N, const uint8_t* __restrict__ bucket, int NB, uint32_t ntile,
+                               const uint32_t* __restrict__ offs, uint32_t base, uint32_t rev_mask,
+                               const uint32_t* __restrict__ bucket_total_start, uint32_t* __restrict__ map) {
+    __shared__ uint32_t wcnt[8][PT / 32];
+    uint32_t i = blockIdx.x * PT + threadIdx.x;
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int b = (i < N) ? bucket[i] : 255;
+    uint32_t myrank = 0;
+    for (int v = 0; v < NB; v++) {
+        unsigned m = __ballot_sync(0xffffffffu, b == v);
+        if (b == v) myrank = __popc(m & ((1u << lane) - 1));
+        if (lane == 0) wcnt[v][w] = __popc(m);
+    }
+    __syncthreads();
+    if (b < NB) {
+        uint32_t before = 0;
+        for (int ww = 0; ww < w; ww++) before += wcnt[b][ww];
+        uint32_t r = offs[b * ntile + blockIdx.x] + before + myrank;  // rank over all nodes
+        uint32_t bstart = bucket_total_start[b];                       // start of bucket b
+        uint32_t bend = bucket_total_start[b + 1];
+        uint32_t inb = r - bstart;
+        uint32_t pos = ((rev_mask >> b) & 1u) ? (bend - 1 - inb) : r;
+        map[base + pos] = i;
+    }
+}
+
+__global__ void k_bucket_starts(const uint32_t* offs, uint32_t ntile, int NB, uint32_t total, uint32_t* starts) {
+    if (threadIdx.x == 0) {
+        for (int v = 0; v < NB; v++) starts[v] = offs[v * ntile];
+        starts[NB] = total;
+    }
+}
+
+// Writes map[base + ...] for every node whose bucket < NB; returns the count of
+// each bucket (host side, synchronises).
+std::vector<uint32_t> stable_partition(uint32_t N, const uint8_t* bucket, int NB, uint32_t rev_mask,
+                                       uint32_t* map, uint32_t base, cudaStream_t s) {
+    uint32_t ntile = (N + PT - 1) / PT;
+    if (!ntile) ntile = 1;
+    DBuf<uint32_t> counts((size_t)NB * ntile + 1), offs((size_t)NB * ntile + 1), starts(NB + 1);
+    counts.zero(s);
+    k_part_count<<<ntile, PT, 0, s>>>(N, bucket, NB, ntile, counts.p);
+    CK_LAUNCH();
+    uint32_t total = exclusive_scan_u32(counts.p, offs.p, NB * ntile, s);
+    k_bucket_starts<<<1, 32, 0, s>>>(offs.p, ntile, NB, total, starts.p);
+    CK_LAUNCH();
+    k_part_scatter<<<ntile, PT, 0, s>>>(N, bucket, NB, ntile, offs.p, base, rev_mask, starts.p, map);
+    CK_LAUNCH();
+    std::vector<uint32_t> st = starts.download(s);
+    std::vector<uint32_t> cnt(NB);
+    for (int v = 0; v < NB; v++) cnt[v] = st[v + 1] - st[v];
+    return cnt;
+}
+
+// Bucket ids of order_simple_1 (multi_split_mark.cc:156-191):
+// 0: out = 0 and in != 0, 1: out = 1, 2: out = 2, 3: out > 2, 4: out = 0 and in = 0.
+__global__ void k_bucket_simple1(uint32_t N, const int* __restrict__ nout, const int* __restrict__ nin,
+                                 uint8_t* __restrict__ bucket) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    int o = nout[i];
+    uint8_t b;
+    if (o == 0) b = nin[i] != 0 ? 0 : 4;
+    else b = o <= 2 ? (uint8_t)o : 3;
+    bucket[i] = b;
+}
+
+// Bucket ids of order_none (multi_split_mark.cc:8-25): 0 linked, 1 isolated.
+__global__ void k_bucket_none(uint32_t N, const int* __restrict__ nout, const int* __restrict__ nin,
+                              uint8_t* __restrict__ bucket) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    bucket[i] = (nin[i] == 0 && nout[i] == 0) ? 1 : 0;
+}
+
+// Remaining nodes after the uh_cheb tail group (cheb_mark.cc:177-189):
+// 0 = still linked (coarse, index order), 1 = no links (diagonal, reversed),
+// marked nodes are skipped.
+__global__ void k_bucket_cheb_rest(uint32_t N, const int* __restrict__ nlinks, const uint8_t* __restrict__ marked,
+                                   uint8_t* __restrict__ bucket) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    bucket[i] = marked[i] ? 255 : (nlinks[i] == 0 ? 1 : 0);
+}
+
+__global__ void k_bucket_deg1(uint32_t N, const int* __restrict__ nlinks, uint8_t* __restrict__ bucket) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    bucket[i] = nlinks[i] == 1 ? 0 : 255;
+}
+
+// uh_cheb tail group (cheb_mark.cc:121-162). A tail starts at a node with one
+// remaining link and follows it while the next node is left with exactly one
+// link. Only nodes that start with one link can ever be found with exactly one
+// link by the outer scan (a walk that leaves a node with one link continues
+// through it), so the scan runs over that candidate list in index order. The
+// walk is a sequential greedy process and runs on one thread.
+__global__ void k_cheb_tails(const uint32_t* __restrict__ ia, const uint32_t* __restrict__ ja,
+                             const uint32_t* __restrict__ slot, uint8_t* __restrict__ state,
+                             int* __restrict__ nlinks, const uint32_t* __restrict__ cand, uint32_t ncand,
+                             uint8_t* __restrict__ marked, uint32_t* __restrict__ map, uint32_t* __restrict__ out,
+                             int* __restrict__ err) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    uint32_t pind = 0;
+    for (uint32_t c = 0; c < ncand; c++) {
+        uint32_t i0 = cand[c];
+        if (nlinks[i0] != 1) continue;
+        do {
+            map[pind++] = i0;
+            marked[i0] = 1;
+            uint32_t j_ = ia[i0] + 1, e = ia[i0 + 1];
+            for (; j_ < e; j_++)
+                if (state[slot[j_]]) break;
+            if (j_ == e) { atomicOr(err, 4); out[0] = pind; return; }
+            uint32_t i1 = ja[j_];
+            state[slot[j_]] = 0;
+            nlinks[i0] = -1;
+            nlinks[i1]--;
+            i0 = i1;
+        } while (nlinks[i0] == 1);
+        if (nlinks[i0] == 0) {
+            map[pind++] = i0;
+            marked[i0] = 1;
+            nlinks[i0] = -1;
+        }
+    }
+    out[0] = pind;
+}
+
+__global__ void k_rmap(uint32_t N, const uint32_t* __restrict__ map, uint32_t* __restrict__ rmap) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) rmap[map[i]] = i;
+}
+
+// ---------------------------------------------------------------------------
+// Sparse Schur elimination (construct_sparse_lu, sparse_lu.cc:6-133).
+// Each permuted row i < N-Md is processed by one thread in its own slot of
+// `cap` (column, value) pairs kept sorted by column. The row is loaded as the
+// diagonal aux[map[i]] minus the kept links scaled by 1/beta (ja order), then
+// the slot's columns k < min(i, M) are eliminated in increasing order with
+// l_ik = w_k / U_kk and the k-th U row's updates, fill allowed. l_ik overwrites
+// the value of column k; after the loop the slot holds the L entries first and
+// the U row (i < M) or next-level row (i >= M) after them.
+// Rows i < M depend on the U rows of the columns they eliminate, so they are
+// processed in rounds: a row is finished in round r only if every U row it
+// reads finished in an earlier round, otherwise it records the blocking column
+// and retries. done[i] (the round number) is therefore one plus the largest
+// round among its dependencies: the level schedule of the L solve. Rows >= M
+// depend on U rows only and are processed in one pass afterwards.
+// ---------------------------------------------------------------------------
+struct LUArgs {
+    const uint32_t* Aia;
+    const uint32_t* Aja;
+    const double* Aa;
+    const uint8_t* keep;
+    const double* aux;
+    const uint32_t* map;
+    const uint32_t* rmap;
+    uint32_t M, R;  // R = N - Md rows are factored
+    double beta;
+    uint32_t cap;
+    uint32_t* scol;
+    double* sval;
+    uint32_t* slen;
+    uint32_t* sldiv;
+    int* done;
+    uint32_t* wait;
+    int* flags;  // bit 0: overflow
+};
+
+// 1 = finished, 0 = blocked, -1 = slot overflow
+__device__ int lu_row(const LUArgs& g, uint32_t i, int round) {
+    const uint32_t cap = g.cap;
+    uint32_t* wc = g.scol + (size_t)i * cap;
+    double* wv = g.sval + (size_t)i * cap;
+    uint32_t arow = g.map[i];
+    uint32_t wn = 1;
+    wc[0] = i;
+    double diag = g.aux[arow];
+    for (uint32_t j_ = g.Aia[arow] + 1; j_ < g.Aia[arow + 1]; j_++) {
+        if (!g.keep[j_]) continue;
+        uint32_t nj = g.rmap[g.Aja[j_]];
+        double z = g.Aa[j_] / g.beta;
+        if (wn == cap) return -1;
+        uint32_t p = wn;
+        while (p > 0 && wc[p - 1] > nj) { wc[p] = wc[p - 1]; wv[p] = wv[p - 1]; p--; }
+        wc[p] = nj; wv[p] = z; wn++;
+        diag -= z;
+    }
+    for (uint32_t t = 0; t < wn; t++)
+        if (wc[t] == i) { wv[t] = diag; break; }
+    uint32_t m = i < g.M ? i : g.M;
+    uint32_t t = 0;
+    for (; t < wn && wc[t] < m; t++) {
+        uint32_t k = wc[t];
+        int dk = g.done[k];
+        if (dk == 0 || dk >= round) { g.wait[i] = k; return 0; }
+        const uint32_t* kc = g.scol + (size_t)k * cap;
+        const double* kv = g.sval + (size_t)k * cap;
+        uint32_t ks = g.sldiv[k], ke = g.slen[k];
+        double lik = wv[t] / kv[ks];
+        wv[t] = lik;
+        uint32_t pos = t + 1;  // columns of U row k are > k and sorted: merge forward
+        for (uint32_t u = ks + 1; u < ke; u++) {
+            uint32_t j = kc[u];
+            double uv = kv[u];
+            while (pos < wn && wc[pos] < j) pos++;
+            if (pos < wn && wc[pos] == j) {
+                wv[pos] = wv[pos] - lik * uv;
+            } else {
+                if (wn == cap) return -1;
+                for (uint32_t q = wn; q > pos; q--) { wc[q] = wc[q - 1]; wv[q] = wv[q - 1]; }
+                wc[pos] = j;
+                wv[pos] = -lik * uv;
+                wn++;
+            }
+            pos++;
+        }
+    }
+    g.slen[i] = wn;
+    g.sldiv[i] = t;
+    return 1;
+}
+
+__global__ void k_lu_round(LUArgs g, const uint32_t* __restrict__ pin, const uint32_t* __restrict__ npin,
+                           uint32_t* __restrict__ pout, uint32_t* __restrict__ npout, int round) {
+    uint32_t n = *npin;
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+        uint32_t i = pin[idx];
+        uint32_t k = g.wait[i];
+        if (k != 0xffffffffu) {
+            int dk = g.done[k];
+            if (dk == 0 || dk >= round) { pout[atomicAdd(npout, 1u)] = i; continue; }
+        }
+        int r = lu_row(g, i, round);
+        if (r == 1) g.done[i] = round;
+        else if (r == 0) pout[atomicAdd(npout, 1u)] = i;
+        else atomicOr(g.flags, 1);
+    }
+}
+
+__global__ void k_lu_coarse(LUArgs g) {
+    uint32_t i = g.M + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.R) return;
+    int r = lu_row(g, i, 0x7fffffff);
+    if (r != 1) atomicOr(g.flags, r < 0 ? 1 : 8);
+}
+
+__global__ void k_iota(uint32_t n, uint32_t* __restrict__ v) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = i;
+}
+
+// counts for the compaction: L (R rows), U (M rows), next-level (R-M rows)
+__global__ void k_lu_counts(uint32_t R, uint32_t M, const uint32_t* __restrict__ slen,
+                            const uint32_t* __restrict__ sldiv, uint32_t* __restrict__ lc,
+                            uint32_t* __restrict__ uc, uint32_t* __restrict__ nc) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= R) return;
+    lc[i] = sldiv[i];
+    if (i < M) uc[i] = slen[i] - sldiv[i];
+    else nc[i - M] = slen[i] - sldiv[i];
+}
+
+__global__ void k_lu_emit(uint32_t R, uint32_t M, uint32_t cap, const uint32_t* __restrict__ scol,
+                          const double* __restrict__ sval, const uint32_t* __restrict__ slen,
+                          const uint32_t* __restrict__ sldiv, const uint32_t* __restrict__ Lia,
+                          uint32_t* __restrict__ Lja, double* __restrict__ La, const uint32_t* __restrict__ Uia,
+                          uint32_t* __restrict__ Uja, double* __restrict__ Ua, const uint32_t* __restrict__ nia,
+                          uint32_t* __restrict__ nja, double* __restrict__ na) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= R) return;
+    const uint32_t* c = scol + (size_t)i * cap;
+    const double* v = sval + (size_t)i * cap;
+    uint32_t ld = sldiv[i], wn = slen[i];
+    uint32_t p = Lia[i];
+    for (uint32_t t = 0; t < ld; t++) { Lja[p] = c[t]; La[p] = v[t]; p++; }
+    if (i < M) {
+        p = Uia[i];
+        for (uint32_t t = ld; t < wn; t++) { Uja[p] = c[t]; Ua[p] = v[t]; p++; }
+    } else {
+        p = nia[i - M];
+        for (uint32_t t = ld; t < wn; t++)
+            if (c[t] == i) { nja[p] = i - M; na[p] = v[t]; p++; break; }
+        for (uint32_t t = ld; t < wn; t++)
+            if (c[t] != i) { nja[p] = c[t] - M; na[p] = v[t]; p++; }
+    }
+}
+
+__global__ void k_dval(uint32_t Md, uint32_t base, const uint32_t* __restrict__ map, const double* __restrict__ aux,
+                       double* __restrict__ dval) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < Md) dval[i] = 1. / aux[map[base + i]];
+}
+
+}  // namespace mlp
+
+// ===========================================================================
+// Host orchestration of the hierarchy build.
+// ===========================================================================
+namespace mlp {
+
+double cheb_poly(double x, uint32_t k) {  // misc.cc:232-242
+    switch (k) {
+        case 0: return 1;
+        case 1: return x;
+        case 2: return 2 * x * x - 1;
+        case 3: return x * (4 * x * x - 3);
+        default: return cosh(k * acosh(x));
+    }
+}
+
+static int read_flag(const int* d, cudaStream_t s) {
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, d, 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return h;
+}
+static uint32_t read_u32(const uint32_t* d, cudaStream_t s) {
+    uint32_t h = 0;
+    CK(cudaMemcpyAsync(&h, d, 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return h;
+}
+
+// ---- frame construction kernels -----------------------------------------
+// pi(q): frame position -> permuted index; phi(q) = map[pi(q)].
+__global__ void k_frame_phi(uint32_t N, uint32_t M, uint32_t n, const uint32_t* __restrict__ eperm,
+                            const uint32_t* __restrict__ phi_next, const uint32_t* __restrict__ map,
+                            uint32_t* __restrict__ pi, uint32_t* __restrict__ phi) {
+    uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= N) return;
+    uint32_t p;
+    if (q < M) p = eperm[q];
+    else if (q < M + n) p = M + phi_next[q - M];
+    else p = q;
+    pi[q] = p;
+    phi[q] = map[p];
+}
+
+__global__ void k_invert(uint32_t N, const uint32_t* __restrict__ perm, uint32_t* __restrict__ inv) {
+    uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < N) inv[perm[q]] = q;
+}
+
+__global__ void k_row_len_perm(uint32_t R, const uint32_t* __restrict__ src_row, const uint32_t* __restrict__ ia,
+                               uint32_t* __restrict__ len) {
+    uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= R) return;
+    uint32_t r = src_row ? src_row[q] : q;
+    len[q] = ia[r + 1] - ia[r];
+}
+
+// Copies rows src_row[q] of (ia, ja, a) to row q of the output, relabelling the
+// columns through colmap (identity when null).
+__global__ void k_gather_rows(uint32_t R, const uint32_t* __restrict__ src_row, const uint32_t* __restrict__ ia,
+                              const uint32_t* __restrict__ ja, const double* __restrict__ a,
+                              const uint32_t* __restrict__ colmap, const uint32_t* __restrict__ oia,
+                              uint32_t* __restrict__ oja, double* __restrict__ oa) {
+    uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= R) return;
+    uint32_t r = src_row ? src_row[q] : q;
+    uint32_t o = oia[q];
+    for (uint32_t j = ia[r]; j < ia[r + 1]; j++, o++) {
+        oja[o] = colmap ? colmap[ja[j]] : ja[j];
+        oa[o] = a[j];
+    }
+}
+
+// Relabel map for U/L columns given in permuted indexing: E columns go through
+// einv, coarse columns through M + iphi_next, diagonal columns stay.
+__global__ void k_perm_to_frame(uint32_t N, uint32_t M, uint32_t n, const uint32_t* __restrict__ einv,
+                                const uint32_t* __restrict__ iphi_next, uint32_t* __restrict__ out) {
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= N) return;
+    if (p < M) out[p] = einv[p];
+    else if (p < M + n) out[p] = M + iphi_next[p - M];
+    else out[p] = p;
+}
+
+// uh_cheb sym_multiply operator (skyline.cc:115-155) as a full matrix: entries
+// on and below the diagonal come from the row itself, entries above it from the
+// mirrored lower entry of the other row.
+__global__ void k_sym_values(uint32_t N, const uint32_t* __restrict__ ia, const uint32_t* __restrict__ ja,
+                             const double* __restrict__ a, const uint32_t* __restrict__ tpos,
+                             double* __restrict__ out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    out[ia[i]] = a[ia[i]];
+    for (uint32_t j_ = ia[i] + 1; j_ < ia[i + 1]; j_++) out[j_] = ja[j_] < i ? a[j_] : a[tpos[j_]];
+}
+
+// Level schedule of a triangular DAG given as CSR dependencies (diagonal entry
+// skipped when it equals the row): level[i] = 1 + max level of its
+// dependencies, computed in rounds like the elimination.
+__global__ void k_dag_round(uint32_t R, const uint32_t* __restrict__ ia, const uint32_t* __restrict__ ja,
+                            uint32_t depmax, int* __restrict__ lev, const uint32_t* __restrict__ pin,
+                            const uint32_t* __restrict__ npin, uint32_t* __restrict__ pout,
+                            uint32_t* __restrict__ npout, int round) {
+    uint32_t n = *npin;
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+        uint32_t i = pin[idx];
+        bool ok = true;
+        for (uint32_t j = ia[i]; j < ia[i + 1]; j++) {
+            uint32_t k = ja[j];
+            if (k == i || k >= depmax) continue;
+            int lk = lev[k];
+            if (lk == 0 || lk >= round) { ok = false; break; }
+        }
+        if (ok) lev[i] = round;
+        else pout[atomicAdd(npout, 1u)] = i;
+    }
+}
+
+// ---- dense inverse of the coarsest level (Gauss-Jordan, no pivoting) -----
+__global__ void k_dense_from_csr(uint32_t n, const uint32_t* __restrict__ ia, const uint32_t* __restrict__ ja,
+                                 const double* __restrict__ a, double* __restrict__ D) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (uint32_t j = ia[i]; j < ia[i + 1]; j++) D[(size_t)i * n + ja[j]] = a[j];
+}
+__global__ void k_gj_pivot(uint32_t n, uint32_t k, double* __restrict__ D, double* __restrict__ col,
+                           int* __restrict__ err) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    double p = D[(size_t)k * n + k];
+    if (p == 0.0) { if (t == 0) atomicOr(err, 16); return; }
+    if (t < n) col[t] = D[(size_t)t * n + k];  // column k before the update
+}
+__global__ void k_gj_update(uint32_t n, uint32_t k, double* __restrict__ D, const double* __restrict__ col) {
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t i = blockIdx.y;
+    if (j >= n) return;
+    double piv = 1 / col[k];
+    double rkj = (j == k) ? piv : D[(size_t)k * n + j] * piv;
+    if (i == k) return;
+    double f = col[i];
+    double v = (j == k) ? 0.0 : D[(size_t)i * n + j];
+    D[(size_t)i * n + j] = v - f * rkj;
+}
+__global__ void k_gj_rowk(uint32_t n, uint32_t k, double* __restrict__ D, const double* __restrict__ col) {
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    double piv = 1 / col[k];
+    D[(size_t)k * n + j] = (j == k) ? piv : D[(size_t)k * n + j] * piv;
+}
+
+// ---- per-level construction ------------------------------------------------
+
+struct Scratch {
+    DBuf<uint8_t> keep, want, bucket, marked, state;
+    DBuf<int> nout, nin, nlinks, flag;
+    DBuf<double> aux;
+    DBuf<uint32_t> rmap, tpos, slot, cand, cnt;
+};
+
+static void sparse_lu_level(Level& li, Level& ln, const uint8_t* keep, const double* aux, const uint32_t* rmap,
+                            double beta, cudaStream_t s) {
+    const DCSR& A = li.A;
+    uint32_t N = li.N, M = li.M, Md = li.Md, R = N - Md;
+    li.done.alloc(M ? M : 1);
+    li.done.zero(s);
+    DBuf<uint32_t> slen(R ? R : 1), sldiv(R ? R : 1), wait(R ? R : 1);
+    DBuf<int> flags(1);
+    uint32_t cap = 32;
+    for (int attempt = 0;; attempt++) {
+        DBuf<uint32_t> scol((size_t)R * cap + 1);
+        DBuf<double> sval((size_t)R * cap + 1);
+        flags.zero(s);
+        li.done.zero(s);
+        CK(cudaMemsetAsync(wait.p, 0xff, wait.n * 4, s));
+        LUArgs g{A.ia.p, A.ja.p, A.a.p, keep, aux, li.map.p, rmap, M, R, beta, cap,
+                 scol.p, sval.p, slen.p, sldiv.p, li.done.p, wait.p, flags.p};
+        // E rows in rounds
+        int rounds = 0;
+        if (M) {
+            DBuf<uint32_t> pa(M), pb(M), cnt(2);
+            k_iota<<<grid_for(M, 256), 256, 0, s>>>(M, pa.p);
+            CK_LAUNCH();
+            CK(cudaMemcpyAsync(cnt.p, &M, 4, cudaMemcpyHostToDevice, s));
+            uint32_t* pin = pa.p; uint32_t* pout = pb.p;
+            uint32_t* cin = cnt.p; uint32_t* cout = cnt.p + 1;
+            unsigned grid = (unsigned)std::min<size_t>(grid_for(M, 256), (size_t)num_sms() * 8);
+            uint32_t prev_left = M;
+            for (;;) {
+                for (int b = 0; b < 4; b++) {
+                    rounds++;
+                    CK(cudaMemsetAsync(cout, 0, 4, s));
+                    k_lu_round<<<grid, 256, 0, s>>>(g, pin, cin, pout, cout, rounds);
+                    CK_LAUNCH();
+                    std::swap(pin, pout);
+                    std::swap(cin, cout);
+                }
+                uint32_t left = read_u32(cin, s);
+                if ((read_flag(flags.p, s) & 1) || left == 0) break;
+                // every round finishes at least the rows whose dependencies are
+                // done; no progress over four rounds means a cycle
+                if (left >= prev_left) MLP_THROW(ERR_INTERNAL, "elimination makes no progress");
+                prev_left = left;
+            }
+        }
+        if (!(read_flag(flags.p, s) & 1) && R > M) {
+            k_lu_coarse<<<grid_for(R - M, 128), 128, 0, s>>>(g);
+            CK_LAUNCH();
+        }
+        int fl = read_flag(flags.p, s);
+        if (fl & 8) MLP_THROW(ERR_INTERNAL, "coarse row met an unfinished U row");
+        if (fl & 1) {
+            if (cap >= 4096) MLP_THROW(ERR_LIMIT, "elimination row exceeds 4096 entries");
+            cap *= 2;
+            continue;
+        }
+        // compaction
+        DBuf<uint32_t> lc(R + 1), uc(M + 1), nc(R - M + 1);
+        k_lu_counts<<<grid_for(R, 256), 256, 0, s>>>(R, M, slen.p, sldiv.p, lc.p, uc.p, nc.p);
+        CK_LAUNCH();
+        li.L.ia.alloc((size_t)R + 1);
+        uint32_t lnnz = exclusive_scan_u32(lc.p, li.L.ia.p, R, s);
+        li.U.ia.alloc((size_t)M + 1);
+        uint32_t unnz = exclusive_scan_u32(uc.p, li.U.ia.p, M, s);
+        ln.A.ia.alloc((size_t)(R - M) + 1);
+        uint32_t nnnz = exclusive_scan_u32(nc.p, ln.A.ia.p, R - M, s);
+        li.L.nrow = li.L.ncol = R; li.L.nnz = lnnz;
+        li.L.ja.alloc(lnnz ? lnnz : 1); li.L.a.alloc(lnnz ? lnnz : 1);
+        li.U.nrow = M; li.U.ncol = R; li.U.nnz = unnz;
+        li.U.ja.alloc(unnz ? unnz : 1); li.U.a.alloc(unnz ? unnz : 1);
+        ln.A.nrow = ln.A.ncol = R - M; ln.A.nnz = nnnz;
+        ln.A.ja.alloc(nnnz ? nnnz : 1); ln.A.a.alloc(nnnz ? nnnz : 1);
+        if (R) {
+            k_lu_emit<<<grid_for(R, 128), 128, 0, s>>>(R, M, cap, scol.p, sval.p, slen.p, sldiv.p, li.L.ia.p,
+                                                      li.L.ja.p, li.L.a.p, li.U.ia.p, li.U.ja.p, li.U.a.p,
+                                                      ln.A.ia.p, ln.A.ja.p, ln.A.a.p);
+            CK_LAUNCH();
+        }
+        li.nwave_l = (uint32_t)rounds;  // upper bound, refined by the frame build
+        CK(cudaStreamSynchronize(s));
+        break;
+    }
+}
+
+static void build_level_msplit(Hierarchy& H, const BuildCfg& cfg, uint32_t level, Scratch& S, cudaStream_t s) {
+    Level& li = *H.lv[level];
+    const DCSR& A = li.A;
+    li.N = A.nrow;
+    li.nnz = A.nnz;
+    if (li.N <= H.coarse_n || level == H.nlevels - 1) {
+        H.nlevels = level + 1;
+        H.coarse_n = li.N;
+        li.direct = true;
+        return;
+    }
+    uint32_t N = li.N;
+    S.keep.alloc(A.nnz ? A.nnz : 1);
+    S.nout.alloc(N); S.nin.alloc(N); S.aux.alloc(N); S.flag.alloc(1);
+    S.nin.zero(s); S.flag.zero(s);
+    k_mark_msplit<<<grid_for(N, 128), 128, 0, s>>>(N, A.ia.p, A.ja.p, A.a.p, li.q, S.keep.p, S.nout.p, S.nin.p,
+                                                  S.aux.p, S.flag.p);
+    CK_LAUNCH();
+    if (read_flag(S.flag.p, s)) MLP_THROW(ERR_LIMIT, "a row has more than 64 off-diagonal entries");
+    li.map.alloc(N);
+    S.bucket.alloc(N);
+    li.M = 0;
+    if (cfg.order == ORDER_SIMPLE_1) {
+        k_bucket_simple1<<<grid_for(N, 256), 256, 0, s>>>(N, S.nout.p, S.nin.p, S.bucket.p);
+        CK_LAUNCH();
+        std::vector<uint32_t> cnt = stable_partition(N, S.bucket.p, 5, 0, li.map.p, 0, s);
+        uint32_t acc = cnt[0];
+        for (uint32_t d = 1; d <= 3; d++) {
+            acc += cnt[d];
+            if (d == cfg.degree_max) li.M = acc;
+        }
+        li.Md = cnt[4];
+    } else if (cfg.order == ORDER_NONE) {
+        k_bucket_none<<<grid_for(N, 256), 256, 0, s>>>(N, S.nout.p, S.nin.p, S.bucket.p);
+        CK_LAUNCH();
+        std::vector<uint32_t> cnt = stable_partition(N, S.bucket.p, 2, 2u, li.map.p, 0, s);
+        li.M = 0;
+        li.Md = cnt[1];
+    } else {
+        MLP_THROW(ERR_CONFIG, "elim_order must be simple_1 or none");
+    }
+    S.rmap.alloc(N);
+    k_rmap<<<grid_for(N, 256), 256, 0, s>>>(N, li.map.p, S.rmap.p);
+    CK_LAUNCH();
+    H.lv.emplace_back(new Level());
+    Level& ln = *H.lv[level + 1];
+    Level& lc = *H.lv[level];  // re-fetch: emplace_back may move unique_ptrs (not the objects)
+    sparse_lu_level(lc, ln, S.keep.p, S.aux.p, S.rmap.p, 1.0, s);
+    lc.n = N - lc.M - lc.Md;
+    lc.dval.alloc(lc.Md ? lc.Md : 1);
+    if (lc.Md) {
+        k_dval<<<grid_for(lc.Md, 256), 256, 0, s>>>(lc.Md, N - lc.Md, lc.map.p, S.aux.p, lc.dval.p);
+        CK_LAUNCH();
+    }
+    if (lc.n) {
+        ln.q = level + 1 < cfg.q.size() ? cfg.q[level + 1] : cfg.q.back();
+        ln.niter = level + 1 < cfg.niter.size() ? cfg.niter[level + 1] : cfg.niter.back();
+        build_level_msplit(H, cfg, level + 1, S, s);
+    } else {
+        H.lv.pop_back();
+        H.nlevels = level + 1;
+    }
+}
+
+static void build_level_cheb(Hierarchy& H, const BuildCfg& cfg, uint32_t level, Scratch& S, cudaStream_t s) {
+    Level& li = *H.lv[level];
+    const DCSR& A = li.A;
+    uint32_t N = A.nrow, nnz = A.nnz;
+    li.N = N;
+    li.nnz = nnz;
+    S.want.alloc(nnz ? nnz : 1); S.keep.alloc(nnz ? nnz : 1); S.aux.alloc(N); S.flag.alloc(1);
+    S.tpos.alloc(nnz ? nnz : 1); S.slot.alloc(nnz ? nnz : 1); S.nlinks.alloc(N);
+    S.flag.zero(s);
+    k_mark_cheb<<<grid_for(N, 128), 128, 0, s>>>(N, A.ia.p, A.a.p, li.beta, S.want.p, S.aux.p, S.flag.p);
+    CK_LAUNCH();
+    k_transpose_pos<<<grid_for(N, 128), 128, 0, s>>>(N, A.ia.p, A.ja.p, S.tpos.p, S.flag.p);
+    CK_LAUNCH();
+    int fl = read_flag(S.flag.p, s);
+    if (fl & 1) MLP_THROW(ERR_LIMIT, "a row has more than 64 off-diagonal entries");
+    if (fl & 2) MLP_THROW(ERR_ARG, "uh_cheb needs a structurally symmetric matrix");
+    k_cheb_links<<<grid_for(N, 128), 128, 0, s>>>(N, A.ia.p, A.ja.p, S.want.p, S.tpos.p, S.keep.p, S.nlinks.p,
+                                                 S.slot.p);
+    CK_LAUNCH();
+    // sym operator values for the Chebyshev steps that use this level's matrix
+    if (level > 0) {
+        li.As.nrow = li.As.ncol = N; li.As.nnz = nnz;
+        li.As.a.alloc(nnz ? nnz : 1);
+        k_sym_values<<<grid_for(N, 128), 128, 0, s>>>(N, A.ia.p, A.ja.p, A.a.p, S.tpos.p, li.As.a.p);
+        CK_LAUNCH();
+    }
+    li.map.alloc(N);
+    S.marked.alloc(N);
+    S.marked.zero(s);
+    uint32_t M = 0;
+    if (cfg.use_tails) {
+        S.state.alloc(nnz ? nnz : 1);
+        CK(cudaMemcpyAsync(S.state.p, S.keep.p, nnz, cudaMemcpyDeviceToDevice, s));
+        S.bucket.alloc(N);
+        S.cand.alloc(N ? N : 1);
+        k_bucket_deg1<<<grid_for(N, 256), 256, 0, s>>>(N, S.nlinks.p, S.bucket.p);
+        CK_LAUNCH();
+        std::vector<uint32_t> c1 = stable_partition(N, S.bucket.p, 1, 0, S.cand.p, 0, s);
+        S.cnt.alloc(1);
+        k_cheb_tails<<<1, 1, 0, s>>>(A.ia.p, A.ja.p, S.slot.p, S.state.p, S.nlinks.p, S.cand.p, c1[0], S.marked.p,
+                                     li.map.p, S.cnt.p, S.flag.p);
+        CK_LAUNCH();
+        M = read_u32(S.cnt.p, s);
+        if (read_flag(S.flag.p, s) & 4) MLP_THROW(ERR_INTERNAL, "Could not find remaining link");
+    }
+    S.bucket.alloc(N);
+    k_bucket_cheb_rest<<<grid_for(N, 256), 256, 0, s>>>(N, S.nlinks.p, S.marked.p, S.bucket.p);
+    CK_LAUNCH();
+    std::vector<uint32_t> cnt = stable_partition(N, S.bucket.p, 2, 2u, li.map.p, M, s);
+    li.M = M;
+    li.Md = cnt[1];
+    S.rmap.alloc(N);
+    k_rmap<<<grid_for(N, 256), 256, 0, s>>>(N, li.map.p, S.rmap.p);
+    CK_LAUNCH();
+    H.lv.emplace_back(new Level());
+    Level& ln = *H.lv[level + 1];
+    Level& lc = *H.lv[level];
+    sparse_lu_level(lc, ln, S.keep.p, S.aux.p, S.rmap.p, lc.beta, s);
+    lc.n = N - lc.M - lc.Md;
+    lc.dval.alloc(lc.Md ? lc.Md : 1);
+    if (lc.Md) {
+        k_dval<<<grid_for(lc.Md, 256), 256, 0, s>>>(lc.Md, N - lc.Md, lc.map.p, S.aux.p, lc.dval.p);
+        CK_LAUNCH();
+    }
+    if (lc.n) {
+        if (level + 1 >= H.nlevels) MLP_THROW(ERR_LEVELS, "Too many levels: " + std::to_string(level + 1));
+        ln.alpha = 1.0;
+        ln.beta = level + 1 < cfg.sigma.size() ? cfg.sigma[level + 1] : cfg.sigma.back();
+        build_level_cheb(H, cfg, level + 1, S, s);
+    } else {
+        H.lv.pop_back();
+        H.nlevels = level + 1;
+    }
+}
+
+// Host counting sort of rows by level value (1-based), stable in row index.
+static void counting_sort(const std::vector<int>& lev, uint32_t nrows, std::vector<uint32_t>& off,
+                          std::vector<uint32_t>& rows) {
+    int maxl = 0;
+    for (uint32_t i = 0; i < nrows; i++) maxl = std::max(maxl, lev[i]);
+    off.assign((size_t)maxl + 1, 0);
+    for (uint32_t i = 0; i < nrows; i++) off[lev[i]]++;  // lev >= 1
+    uint32_t acc = 0;
+    for (int d = 0; d <= maxl; d++) { uint32_t c = off[d]; off[d] = acc; acc += c; }
+    std::vector<uint32_t> pos(off);
+    rows.resize(nrows);
+    for (uint32_t i = 0; i < nrows; i++) rows[pos[lev[i]]++] = i;
+    // off[d] is the start of level d (levels start at 1); drop level 0 slot
+    off.erase(off.begin());
+    off.push_back(nrows);
+}
+
+// Builds the frame-order operators of every level, bottom-up.
+static void build_frames(Hierarchy& H, cudaStream_t s) {
+    for (int l = (int)H.nlevels - 1; l >= 0; l--) {
+        Level& li = *H.lv[l];
+        uint32_t N = li.N;
+        li.phi.alloc(N ? N : 1);
+        li.iphi.alloc(N ? N : 1);
+        if (li.direct) {
+            k_iota<<<grid_for(N, 256), 256, 0, s>>>(N, li.phi.p);
+            CK_LAUNCH();
+            k_iota<<<grid_for(N, 256), 256, 0, s>>>(N, li.iphi.p);
+            CK_LAUNCH();
+        }
+        uint32_t M = li.M, n = li.n, R = N - li.Md;
+        if (!li.direct) {
+        // E block order: by L wavefront (elimination round), then permuted index
+        std::vector<int> done = li.done.download(s, M);
+        std::vector<uint32_t> off, rows;
+        counting_sort(done, M, off, rows);
+        li.lw_off = off;
+        li.nwave_l = (uint32_t)off.size() - 1;
+        li.eperm.alloc(M ? M : 1);
+        if (M) li.eperm.upload(rows.data(), M, s);
+        DBuf<uint32_t> pi(N), einv(M ? M : 1), p2f(N);
+        const uint32_t* phi_next = (l + 1 < (int)H.nlevels) ? H.lv[l + 1]->phi.p : nullptr;
+        const uint32_t* iphi_next = (l + 1 < (int)H.nlevels) ? H.lv[l + 1]->iphi.p : nullptr;
+        k_frame_phi<<<grid_for(N, 256), 256, 0, s>>>(N, M, n, li.eperm.p, phi_next, li.map.p, pi.p, li.phi.p);
+        CK_LAUNCH();
+        k_invert<<<grid_for(N, 256), 256, 0, s>>>(N, li.phi.p, li.iphi.p);
+        CK_LAUNCH();
+        if (M) {
+            k_invert<<<grid_for(M, 256), 256, 0, s>>>(M, li.eperm.p, einv.p);
+            CK_LAUNCH();
+        }
+        k_perm_to_frame<<<grid_for(N, 256), 256, 0, s>>>(N, M, n, einv.p, iphi_next, p2f.p);
+        CK_LAUNCH();
+        // Lf: rows pi(q), q < R; columns (E, permuted) -> frame
+        {
+            DBuf<uint32_t> len(R + 1);
+            k_row_len_perm<<<grid_for(R, 256), 256, 0, s>>>(R, pi.p, li.L.ia.p, len.p);
+            CK_LAUNCH();
+            li.Lf.ia.alloc((size_t)R + 1);
+            uint32_t z = exclusive_scan_u32(len.p, li.Lf.ia.p, R, s);
+            li.Lf.nrow = R; li.Lf.ncol = M; li.Lf.nnz = z;
+            li.Lf.ja.alloc(z ? z : 1); li.Lf.a.alloc(z ? z : 1);
+            k_gather_rows<<<grid_for(R, 256), 256, 0, s>>>(R, pi.p, li.L.ia.p, li.L.ja.p, li.L.a.p, p2f.p,
+                                                         li.Lf.ia.p, li.Lf.ja.p, li.Lf.a.p);
+            CK_LAUNCH();
+        }
+        // Uf: rows eperm[q], columns -> frame
+        if (M) {
+            DBuf<uint32_t> len(M + 1);
+            k_row_len_perm<<<grid_for(M, 256), 256, 0, s>>>(M, li.eperm.p, li.U.ia.p, len.p);
+            CK_LAUNCH();
+            li.Uf.ia.alloc((size_t)M + 1);
+            uint32_t z = exclusive_scan_u32(len.p, li.Uf.ia.p, M, s);
+            li.Uf.nrow = M; li.Uf.ncol = R; li.Uf.nnz = z;
+            li.Uf.ja.alloc(z ? z : 1); li.Uf.a.alloc(z ? z : 1);
+            k_gather_rows<<<grid_for(M, 256), 256, 0, s>>>(M, li.eperm.p, li.U.ia.p, li.U.ja.p, li.U.a.p, p2f.p,
+                                                         li.Uf.ia.p, li.Uf.ja.p, li.Uf.a.p);
+            CK_LAUNCH();
+            // U-solve wavefronts: row q depends on the E columns of its row
+            DBuf<int> lev(M);
+            lev.zero(s);
+            DBuf<uint32_t> pa(M), pb(M), cnt(2);
+            k_iota<<<grid_for(M, 256), 256, 0, s>>>(M, pa.p);
+            CK_LAUNCH();
+            CK(cudaMemcpyAsync(cnt.p, &M, 4, cudaMemcpyHostToDevice, s));
+            uint32_t *pin = pa.p, *pout = pb.p, *cin = cnt.p, *cout = cnt.p + 1;
+            int round = 0;
+            uint32_t prev_left = M;
+            unsigned grid = (unsigned)std::min<size_t>(grid_for(M, 256), (size_t)num_sms() * 8);
+            for (;;) {
+                for (int b = 0; b < 4; b++) {
+                    round++;
+                    CK(cudaMemsetAsync(cout, 0, 4, s));
+                    k_dag_round<<<grid, 256, 0, s>>>(M, li.Uf.ia.p, li.Uf.ja.p, M, lev.p, pin, cin, pout, cout,
+                                                     round);
+                    CK_LAUNCH();
+                    std::swap(pin, pout);
+                    std::swap(cin, cout);
+                }
+                uint32_t left = read_u32(cin, s);
+                if (left == 0) break;
+                if (left >= prev_left) MLP_THROW(ERR_INTERNAL, "U schedule makes no progress");
+                prev_left = left;
+            }
+            std::vector<int> ul = lev.download(s, M);
+            std::vector<uint32_t> uoff, urows;
+            counting_sort(ul, M, uoff, urows);
+            li.uw_off = uoff;
+            li.uw_rows.alloc(M);
+            li.uw_rows.upload(urows.data(), M, s);
+        }
+        }  // !direct
+        // Af: rows phi(q), columns -> iphi
+        {
+            const DCSR& A = li.A;
+            DBuf<uint32_t> len(N + 1);
+            k_row_len_perm<<<grid_for(N, 256), 256, 0, s>>>(N, li.phi.p, A.ia.p, len.p);
+            CK_LAUNCH();
+            li.Af.ia.alloc((size_t)N + 1);
+            uint32_t z = exclusive_scan_u32(len.p, li.Af.ia.p, N, s);
+            li.Af.nrow = li.Af.ncol = N; li.Af.nnz = z;
+            li.Af.ja.alloc(z ? z : 1); li.Af.a.alloc(z ? z : 1);
+            k_gather_rows<<<grid_for(N, 256), 256, 0, s>>>(N, li.phi.p, A.ia.p, A.ja.p, A.a.p, li.iphi.p,
+                                                         li.Af.ia.p, li.Af.ja.p, li.Af.a.p);
+            CK_LAUNCH();
+            if (H.kind == PREC_CHEB && l > 0) {
+                // symmetric operator with the same pattern, frame order
+                li.As.ia.alloc((size_t)N + 1);
+                CK(cudaMemcpyAsync(li.As.ia.p, li.Af.ia.p, ((size_t)N + 1) * 4, cudaMemcpyDeviceToDevice, s));
+                DBuf<double> av(z ? z : 1);
+                DBuf<uint32_t> jv(z ? z : 1);
+                k_gather_rows<<<grid_for(N, 256), 256, 0, s>>>(N, li.phi.p, A.ia.p, A.ja.p, li.As.a.p, li.iphi.p,
+                                                             li.As.ia.p, jv.p, av.p);
+                CK_LAUNCH();
+                li.As.ja = std::move(jv);
+                li.As.a = std::move(av);
+                li.As.nrow = li.As.ncol = N; li.As.nnz = z;
+            }
+        }
+    }
+}
+
+static void build_direct(Level& li, cudaStream_t s) {
+    uint32_t n = li.N;
+    li.cinv.alloc((size_t)n * n + 1);
+    li.cinv.zero(s);
+    if (!n) return;
+    k_dense_from_csr<<<grid_for(n, 128), 128, 0, s>>>(n, li.A.ia.p, li.A.ja.p, li.A.a.p, li.cinv.p);
+    CK_LAUNCH();
+    DBuf<double> col(n);
+    DBuf<int> err(1);
+    err.zero(s);
+    dim3 g2(grid_for(n, 256), n);
+    for (uint32_t k = 0; k < n; k++) {
+        k_gj_pivot<<<grid_for(n, 256), 256, 0, s>>>(n, k, li.cinv.p, col.p, err.p);
+        k_gj_update<<<g2, 256, 0, s>>>(n, k, li.cinv.p, col.p);
+        k_gj_rowk<<<grid_for(n, 256), 256, 0, s>>>(n, k, li.cinv.p, col.p);
+    }
+    CK_LAUNCH();
+    if (read_flag(err.p, s)) MLP_THROW(ERR_INTERNAL, "zero pivot in the coarse-level inverse");
+}
+
+std::unique_ptr<Hierarchy> build_hierarchy(const DCSR& A0, const BuildCfg& cfg, cudaStream_t s) {
+    auto H = std::unique_ptr<Hierarchy>(new Hierarchy());
+    H->kind = cfg.kind;
+    H->lv.emplace_back(new Level());
+    Level& l0 = *H->lv[0];
+    // level 0 keeps its own copy of A (the caller may release its matrix)
+    l0.A.alloc(A0.nrow, A0.ncol, A0.nnz);
+    CK(cudaMemcpyAsync(l0.A.ia.p, A0.ia.p, ((size_t)A0.nrow + 1) * 4, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(l0.A.ja.p, A0.ja.p, (size_t)A0.nnz * 4, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(l0.A.a.p, A0.a.p, (size_t)A0.nnz * 8, cudaMemcpyDeviceToDevice, s));
+    Scratch S;
+    if (cfg.kind == PREC_MSPLIT) {
+        // multi_split_constr.cc:252-275
+        if (cfg.max_levels == 0 || cfg.q.empty() || cfg.niter.empty())
+            MLP_THROW(ERR_CONFIG, "max_levels, q and level_niter must be non-empty");
+        H->nlevels = cfg.max_levels;
+        H->coarse_n = cfg.coarse_n;
+        l0.q = cfg.q[0];
+        l0.niter = 1;
+        build_level_msplit(*H, cfg, 0, S, s);
+        Level& last = *H->lv[H->nlevels - 1];
+        if (last.M == 0) { last.niter = 0; last.q = 0; }
+    } else {
+        // cheb_constr.cc:292-365
+        if (cfg.sigma.empty() || cfg.ncheb.empty()) MLP_THROW(ERR_CONFIG, "sigmas and niters must be non-empty");
+        H->nlevels = 30;
+        l0.alpha = 1.0;
+        l0.beta = cfg.sigma[0];
+        build_level_cheb(*H, cfg, 0, S, s);
+        for (uint32_t l = 0; l < H->nlevels; l++)
+            H->lv[l]->ncheb = l < cfg.ncheb.size() ? cfg.ncheb[l] : cfg.ncheb.back();
+        Level& last = *H->lv[H->nlevels - 1];
+        last.lmin = last.alpha;
+        last.lmax = last.beta;
+        for (int l = (int)H->nlevels - 2; l >= 0; l--) {
+            Level& a = *H->lv[l];
+            Level& b = *H->lv[l + 1];
+            double cs = cheb_poly((b.lmax + b.lmin) / (b.lmax - b.lmin), a.ncheb);
+            a.lmin = a.alpha * (1 - 1 / cs);
+            a.lmax = a.beta * (1 + 1 / cs);
+        }
+    }
+    H->lv.resize(H->nlevels);
+    Level& last = *H->lv[H->nlevels - 1];
+    if (H->kind == PREC_MSPLIT && H->coarse_n && !last.direct) {
+        // a configured coarse_n makes the last level a direct solve even when
+        // the hierarchy ended on its own (multi_split_solve.cc:77-83)
+        last.direct = true;
+    }
+    if (last.direct) {
+        if (last.N > cfg.dense_max)
+            MLP_THROW(ERR_LIMIT, "coarsest level has " + std::to_string(last.N) +
+                                     " unknowns, more than the dense direct solve allows (" +
+                                     std::to_string(cfg.dense_max) + ")");
+        build_direct(last, s);
+    }
+    build_frames(*H, s);
+    CK(cudaStreamSynchronize(s));
+    return H;
+}
+
+}  // namespace mlp

@@ -1,0 +1,728 @@
+// Solve phase: CSR SpMV, the level-scheduled triangular solves, the recursive
+// multi-split / Chebyshev apply recorded as a launch plan (replayed as one CUDA
+// graph), and the device-resident PCG loop.
+//
+// Every vector of level l lives in the level's frame order (setup.cuh): the
+// next level's vectors are slices [M, M+n) of this level's, so the recursion
+// moves no data between levels.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+
+#include "solve.cuh"
+
+namespace mlp {
+
+// ---------------------------------------------------------------------------
+// Kernels
+// ---------------------------------------------------------------------------
+
+// y = A x  (or y = f - A x when f != null). LPR lanes cooperate on one row and
+// reduce with shuffles; rows of a 7-point stencil use 8 lanes.
+template <class T, int LPR>
+__global__ void __launch_bounds__(256) k_spmv(uint32_t n, const uint32_t* __restrict__ ia,
+                                              const uint32_t* __restrict__ ja, const T* __restrict__ a,
+                                              const T* __restrict__ x, T* __restrict__ y,
+                                              const T* __restrict__ f) {
+    uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t row = gid / LPR;
+    int lane = gid % LPR;
+    bool active = row < n;
+    T s = 0;
+    if (active) {
+        uint32_t e = ia[row + 1];
+        for (uint32_t j = ia[row] + lane; j < e; j += LPR) s += a[j] * x[ja[j]];
+    }
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (active && lane == 0) y[row] = f ? f[row] - s : s;
+}
+
+template <class T>
+static void launch_spmv(uint32_t n, uint32_t nnz, const uint32_t* ia, const uint32_t* ja, const T* a, const T* x,
+                        T* y, const T* f, cudaStream_t s) {
+    if (!n) return;
+    double avg = (double)nnz / n;
+    int lpr = avg <= 1.5 ? 1 : avg <= 3 ? 2 : avg <= 6 ? 4 : avg <= 12 ? 8 : avg <= 24 ? 16 : 32;
+    unsigned blocks = grid_for((size_t)n * lpr, 256);
+    switch (lpr) {
+        case 1: k_spmv<T, 1><<<blocks, 256, 0, s>>>(n, ia, ja, a, x, y, f); break;
+        case 2: k_spmv<T, 2><<<blocks, 256, 0, s>>>(n, ia, ja, a, x, y, f); break;
+        case 4: k_spmv<T, 4><<<blocks, 256, 0, s>>>(n, ia, ja, a, x, y, f); break;
+        case 8: k_spmv<T, 8><<<blocks, 256, 0, s>>>(n, ia, ja, a, x, y, f); break;
+        case 16: k_spmv<T, 16><<<blocks, 256, 0, s>>>(n, ia, ja, a, x, y, f); break;
+        default: k_spmv<T, 32><<<blocks, 256, 0, s>>>(n, ia, ja, a, x, y, f); break;
+    }
+}
+
+void spmv(const DCSR& A, const double* x, double* y, cudaStream_t s) {
+    launch_spmv<double>(A.nrow, A.nnz, A.ia.p, A.ja.p, A.a.p, x, y, nullptr, s);
+    CK_LAUNCH();
+}
+
+// One wavefront of the L solve (solve_L, multi_split_solve.cc:25-36) over
+// contiguous frame rows [r0, r1): w_q = src_q - sum_k L_qk w_k.
+template <class T>
+__global__ void k_lwave(uint32_t r0, uint32_t r1, const uint32_t* __restrict__ ia, const uint32_t* __restrict__ ja,
+                        const T* __restrict__ a, const T* __restrict__ src, T* __restrict__ w) {
+    uint32_t q = r0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= r1) return;
+    T s = src[q];
+    for (uint32_t j = ia[q]; j < ia[q + 1]; j++) s -= a[j] * w[ja[j]];
+    w[q] = s;
+}
+
+// Coarse rows of the L solve (they read eliminated rows only) fused with the
+// diagonal block (solve_diagonal, multi_split_solve.cc:12-22): rows [M, R)
+// write w, rows [R, N) write out = dval * src.
+template <class T>
+__global__ void k_lcoarse_diag(uint32_t M, uint32_t R, uint32_t N, const uint32_t* __restrict__ ia,
+                               const uint32_t* __restrict__ ja, const T* __restrict__ a, const T* __restrict__ src,
+                               T* __restrict__ w, const T* __restrict__ dval, T* __restrict__ out) {
+    uint32_t q = M + blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= N) return;
+    if (q < R) {
+        T s = src[q];
+        for (uint32_t j = ia[q]; j < ia[q + 1]; j++) s -= a[j] * w[ja[j]];
+        w[q] = s;
+    } else {
+        out[q] = dval[q - R] * src[q];
+    }
+}
+
+// One wavefront of the U solve (solve_U, multi_split_solve.cc:39-53):
+// out_q = (w_q - sum_{j != q} U_qj out_j) / U_qq, rows given by a list.
+template <class T>
+__global__ void k_uwave(uint32_t cnt, const uint32_t* __restrict__ rows, const uint32_t* __restrict__ ia,
+                        const uint32_t* __restrict__ ja, const T* __restrict__ a, const T* __restrict__ w,
+                        T* __restrict__ out) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= cnt) return;
+    uint32_t q = rows[t];
+    uint32_t rs = ia[q];
+    T z = w[q];
+    for (uint32_t j = rs + 1; j < ia[q + 1]; j++) z -= a[j] * out[ja[j]];
+    out[q] = z / a[rs];
+}
+
+template <class T>
+__global__ void k_axpy1(uint32_t n, T* __restrict__ x, const T* __restrict__ u) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] += u[i];
+}
+
+template <class T>
+__global__ void k_scale(uint32_t n, T* __restrict__ x, T alpha) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] *= alpha;
+}
+
+template <class T>
+__global__ void k_copy(uint32_t n, const T* __restrict__ src, T* __restrict__ dst) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[i];
+}
+
+// Chebyshev step 2 (cheb_solve.cc:70-72): x2 = -alpha*x2 + c*u1
+template <class T>
+__global__ void k_cheb2(uint32_t n, T* __restrict__ x2, const T* __restrict__ u1, T malpha, T c) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x2[i] = x2[i] * malpha + c * u1[i];
+}
+// Chebyshev step k >= 3 (cheb_solve.cc:98-99): x2 = u1 - alpha*x2 + beta*(u1-u0)
+template <class T>
+__global__ void k_chebk(uint32_t n, T* __restrict__ x2, const T* __restrict__ u1, const T* __restrict__ u0,
+                        T alpha, T beta) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x2[i] = u1[i] - alpha * x2[i] + beta * (u1[i] - u0[i]);
+}
+
+// Dense coarsest level: x = C^{-1} f, one warp per row.
+template <class T>
+__global__ void k_dense_gemv(uint32_t n, const T* __restrict__ C, const T* __restrict__ f, T* __restrict__ x) {
+    uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const T* c = C + (size_t)row * n;
+    T s = 0;
+    for (uint32_t j = lane; j < n; j += 32) s += c[j] * f[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) x[row] = s;
+}
+
+__global__ void k_to_f32(uint32_t n, const double* __restrict__ a, float* __restrict__ b) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (float)a[i];
+}
+__global__ void k_to_f64(uint32_t n, const float* __restrict__ a, double* __restrict__ b) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (double)a[i];
+}
+__global__ void k_gather(uint32_t n, const uint32_t* __restrict__ idx, const double* __restrict__ src,
+                         double* __restrict__ dst) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[idx[i]];
+}
+__global__ void k_scatter(uint32_t n, const uint32_t* __restrict__ idx, const double* __restrict__ src,
+                          double* __restrict__ dst) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[idx[i]] = src[i];
+}
+
+void gather(uint32_t n, const uint32_t* idx, const double* src, double* dst, cudaStream_t s) {
+    if (!n) return;
+    k_gather<<<grid_for(n, 256), 256, 0, s>>>(n, idx, src, dst);
+    CK_LAUNCH();
+}
+void scatter(uint32_t n, const uint32_t* idx, const double* src, double* dst, cudaStream_t s) {
+    if (!n) return;
+    k_scatter<<<grid_for(n, 256), 256, 0, s>>>(n, idx, src, dst);
+    CK_LAUNCH();
+}
+
+// ---------------------------------------------------------------------------
+// Plan builder: replays the reference's recursion once on the host and records
+// the launches.
+// ---------------------------------------------------------------------------
+static bool is_equal1(double a) { return std::fabs(a - 1.0) <= 2.220446049250313e-16; }
+
+template <class T>
+static const T* vals(const DCSR& m);
+template <>
+const double* vals<double>(const DCSR& m) { return m.a.p; }
+template <>
+const float* vals<float>(const DCSR& m) { return m.a32.p; }
+template <class T>
+static const T* dvals(const Level& l);
+template <>
+const double* dvals<double>(const Level& l) { return l.dval.p; }
+template <>
+const float* dvals<float>(const Level& l) { return l.dval32.p; }
+template <class T>
+static const T* cinv(const Level& l);
+template <>
+const double* cinv<double>(const Level& l) { return l.cinv.p; }
+template <>
+const float* cinv<float>(const Level& l) { return l.cinv32.p; }
+
+template <class T>
+struct Builder {
+    Hierarchy& H;
+    std::vector<LevelWork<T>>& W;
+    Plan& plan;
+    uint64_t bytes = 0;
+
+    void op(std::function<void(cudaStream_t)> f) {
+        plan.ops.push_back(std::move(f));
+        plan.launches++;
+    }
+
+    void lsolve(const Level& L, const T* src, T* w) {
+        const uint32_t* ia = L.Lf.ia.p;
+        const uint32_t* ja = L.Lf.ja.p;
+        const T* a = vals<T>(L.Lf);
+        for (size_t d = 0; d + 1 < L.lw_off.size(); d++) {
+            uint32_t r0 = L.lw_off[d], r1 = L.lw_off[d + 1];
+            if (r1 <= r0) continue;
+            op([=](cudaStream_t s) { k_lwave<T><<<grid_for(r1 - r0, 128), 128, 0, s>>>(r0, r1, ia, ja, a, src, w); });
+        }
+    }
+    void coarse_diag(const Level& L, const T* src, T* w, T* out) {
+        uint32_t M = L.M, R = L.N - L.Md, N = L.N;
+        if (N <= M) return;
+        const uint32_t* ia = L.Lf.ia.p;
+        const uint32_t* ja = L.Lf.ja.p;
+        const T* a = vals<T>(L.Lf);
+        const T* dv = dvals<T>(L);
+        op([=](cudaStream_t s) {
+            k_lcoarse_diag<T><<<grid_for(N - M, 128), 128, 0, s>>>(M, R, N, ia, ja, a, src, w, dv, out);
+        });
+    }
+    void usolve(const Level& L, const T* w, T* out) {
+        const uint32_t* ia = L.Uf.ia.p;
+        const uint32_t* ja = L.Uf.ja.p;
+        const T* a = vals<T>(L.Uf);
+        const uint32_t* rows = L.uw_rows.p;
+        for (size_t d = 0; d + 1 < L.uw_off.size(); d++) {
+            uint32_t o0 = L.uw_off[d], o1 = L.uw_off[d + 1];
+            if (o1 <= o0) continue;
+            op([=](cudaStream_t s) {
+                k_uwave<T><<<grid_for(o1 - o0, 128), 128, 0, s>>>(o1 - o0, rows + o0, ia, ja, a, w, out);
+            });
+        }
+    }
+    void direct(const Level& L, const T* f, T* x) {
+        uint32_t n = L.N;
+        const T* C = cinv<T>(L);
+        op([=](cudaStream_t s) { k_dense_gemv<T><<<grid_for((size_t)n * 32, 256), 256, 0, s>>>(n, C, f, x); });
+        bytes += (uint64_t)n * n * sizeof(T) + 2ull * n * sizeof(T);
+    }
+    uint64_t sweep_bytes(const Level& L) const {
+        // L (E and coarse rows), U, dval, src/w/out vectors
+        uint64_t b = (uint64_t)L.Lf.nnz * (4 + sizeof(T)) + 4ull * (L.N - L.Md + 1);
+        b += (uint64_t)L.Uf.nnz * (4 + sizeof(T)) + 4ull * (L.M + 1) + 4ull * L.M;
+        b += (uint64_t)L.Md * sizeof(T);
+        b += sizeof(T) * (uint64_t)(L.N + 2ull * (L.N - L.Md) + L.N);
+        return b;
+    }
+    uint64_t spmv_bytes(const DCSR& A) const {
+        return (uint64_t)A.nnz * (4 + sizeof(T)) + 4ull * (A.nrow + 1) + 3ull * sizeof(T) * A.nrow;
+    }
+
+    // MultiSplitPrec::solve(level, f, x) (multi_split_solve.cc:59-157)
+    void ms(uint32_t l, const T* f, T* x) {
+        Level& L = *H.lv[l];
+        if (L.direct) { direct(L, f, x); return; }
+        LevelWork<T>& w = W[l];
+        uint32_t N = L.N, M = L.M;
+        bool has_next = l + 1 < H.nlevels;
+        // step 1, x0 = 0: r = f
+        lsolve(L, f, w.w.p);
+        coarse_diag(L, f, w.w.p, x);
+        if (has_next && L.n) ms(l + 1, w.w.p + M, x + M);
+        usolve(L, w.w.p, x);
+        bytes += sweep_bytes(L);
+        // steps 2..niter: x += B_l (f - A_l x)
+        for (uint32_t it = 2; it <= L.niter; it++) {
+            const uint32_t* ia = L.Af.ia.p;
+            const uint32_t* ja = L.Af.ja.p;
+            const T* a = vals<T>(L.Af);
+            uint32_t nnz = L.Af.nnz;
+            T* r = w.r.p;
+            op([=](cudaStream_t s) { launch_spmv<T>(N, nnz, ia, ja, a, x, r, f, s); });
+            lsolve(L, r, w.w.p);
+            coarse_diag(L, r, w.w.p, w.u0.p);
+            if (has_next && L.n) ms(l + 1, w.w.p + M, w.u0.p + M);
+            usolve(L, w.w.p, w.u0.p);
+            T* u0 = w.u0.p;
+            op([=](cudaStream_t s) { k_axpy1<T><<<grid_for(N, 256), 256, 0, s>>>(N, x, u0); });
+            bytes += sweep_bytes(L) + spmv_bytes(L.Af) + 3ull * sizeof(T) * N;
+        }
+    }
+
+    // Prec::solve(level, f, x) (cheb_solve.cc:13-123)
+    void ch(uint32_t l, const T* f, T* x) {
+        Level& L = *H.lv[l];
+        LevelWork<T>& w = W[l];
+        uint32_t M = L.M;
+        lsolve(L, f, w.w.p);
+        coarse_diag(L, f, w.w.p, x);
+        bytes += sweep_bytes(L);
+        if (l + 1 < H.nlevels) {
+            Level& Ln = *H.lv[l + 1];
+            uint32_t n = Ln.N, nch = L.ncheb;
+            const T* F = w.w.p + M;
+            double lmin = Ln.lmin, lmax = Ln.lmax;
+            double eta = (lmax + lmin) / (lmax - lmin);
+            T *u0 = w.cu0.p, *u1 = w.cu1.p, *x2 = w.cx2.p, *tmp = w.ctmp.p;
+            const uint32_t* sia = Ln.As.ia.p;
+            const uint32_t* sja = Ln.As.ja.p;
+            const T* sa = vals<T>(Ln.As);
+            uint32_t snnz = Ln.As.nnz;
+            double alpha = 2 / (lmax + lmin), beta;
+            auto scale = [&](T* v, double al) {
+                if (is_equal1(al)) return;
+                T a = (T)al;
+                op([=](cudaStream_t s) { k_scale<T><<<grid_for(n, 256), 256, 0, s>>>(n, v, a); });
+            };
+            if (nch > 1) { ch(l + 1, F, u1); scale(u1, alpha); }
+            else { ch(l + 1, F, x2); scale(x2, alpha); }
+            if (nch > 1) {
+                alpha = 4 / (lmax - lmin) * cheb_poly(eta, 1) / cheb_poly(eta, 2);
+                beta = cheb_poly(eta, 0) / cheb_poly(eta, 2);
+                op([=](cudaStream_t s) { launch_spmv<T>(n, snnz, sia, sja, sa, u1, tmp, F, s); });
+                // tmp = F - A u1 above; the reference forms A u1 - F: negate via the scalars
+                ch(l + 1, tmp, x2);
+                // x2 := -alpha * solve(A u1 - F) + (1+beta) u1 = alpha * solve(F - A u1) + (1+beta) u1
+                double c = is_equal1(1 + beta) ? 1.0 : 1 + beta;
+                T ma = (T)alpha, cc = (T)c;
+                op([=](cudaStream_t s) { k_cheb2<T><<<grid_for(n, 256), 256, 0, s>>>(n, x2, u1, ma, cc); });
+                bytes += spmv_bytes(Ln.As) + 3ull * sizeof(T) * n;
+            }
+            for (uint32_t i = 3; i <= nch; i++) {
+                T* t = u0; u0 = u1; u1 = x2; x2 = t;  // cheb_solve.cc:87-89
+                alpha = 4 / (lmax - lmin) * cheb_poly(eta, i - 1) / cheb_poly(eta, i);
+                beta = cheb_poly(eta, i - 2) / cheb_poly(eta, i);
+                op([=](cudaStream_t s) { launch_spmv<T>(n, snnz, sia, sja, sa, u1, tmp, F, s); });
+                ch(l + 1, tmp, x2);
+                // x2 = u1 - alpha*solve(A u1 - F) + beta*(u1-u0) = u1 + alpha*solve(F - A u1) + ...
+                T ma = (T)(-alpha), bb = (T)beta;
+                T* u0c = u0; T* u1c = u1; T* x2c = x2;
+                op([=](cudaStream_t s) { k_chebk<T><<<grid_for(n, 256), 256, 0, s>>>(n, x2c, u1c, u0c, ma, bb); });
+                bytes += spmv_bytes(Ln.As) + 4ull * sizeof(T) * n;
+            }
+            T* xo = x + M;
+            T* fin = x2;
+            op([=](cudaStream_t s) { k_copy<T><<<grid_for(n, 256), 256, 0, s>>>(n, fin, xo); });
+        }
+        usolve(L, w.w.p, x);
+    }
+};
+
+// Chebyshev sign convention: the reference solves with (A u1 - F); the plan
+// solves with (F - A u1) (one fused residual kernel) and flips the sign of the
+// coefficient that multiplies that solve. The preconditioner is linear, so the
+// two forms are the same operator.
+
+template <class T>
+static void alloc_work(Hierarchy& H, std::vector<LevelWork<T>>& W) {
+    W.clear();
+    W.resize(H.nlevels);
+    for (uint32_t l = 0; l < H.nlevels; l++) {
+        Level& L = *H.lv[l];
+        if (L.direct) continue;
+        W[l].w.alloc(L.N - L.Md + 1);
+        if (H.kind == PREC_MSPLIT) {
+            if (L.niter >= 2) { W[l].r.alloc(L.N); W[l].u0.alloc(L.N); }
+        } else if (l + 1 < H.nlevels) {
+            uint32_t n = H.lv[l + 1]->N;
+            W[l].cu0.alloc(n); W[l].cu1.alloc(n); W[l].cx2.alloc(n); W[l].ctmp.alloc(n);
+        }
+    }
+}
+
+__global__ void k_d2f(size_t n, const double* __restrict__ a, float* __restrict__ b) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (float)a[i];
+}
+static void make_f32(const DBuf<double>& src, DBuf<float>& dst, size_t n, cudaStream_t s) {
+    dst.alloc(n ? n : 1);
+    if (n) { k_d2f<<<grid_for(n, 256), 256, 0, s>>>(n, src.p, dst.p); CK_LAUNCH(); }
+}
+static void make_f32(DCSR& m, cudaStream_t s) { make_f32(m.a, m.a32, m.nnz, s); }
+
+Prec::~Prec() {
+    if (graph) cudaGraphExecDestroy(graph);
+}
+
+std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, cudaStream_t s) {
+    auto P = std::unique_ptr<Prec>(new Prec());
+    P->stream = s;
+    P->fp32 = fp32;
+    P->H = build_hierarchy(A, cfg, s);
+    Hierarchy& H = *P->H;
+    uint32_t N0 = H.lv[0]->N;
+    P->fin_buf.alloc(N0);
+    P->fout_buf.alloc(N0);
+    P->fin = P->fin_buf.p;
+    P->fout = P->fout_buf.p;
+    if (!fp32) {
+        alloc_work<double>(H, P->w64);
+        Builder<double> B{H, P->w64, P->plan};
+        if (H.kind == PREC_MSPLIT) B.ms(0, P->fin, P->fout);
+        else B.ch(0, P->fin, P->fout);
+        P->bytes_per_apply = B.bytes;
+    } else {
+        for (uint32_t l = 0; l < H.nlevels; l++) {
+            Level& L = *H.lv[l];
+            make_f32(L.Lf, s); make_f32(L.Uf, s); make_f32(L.Af, s);
+            if (H.kind == PREC_CHEB && l > 0) make_f32(L.As, s);
+            make_f32(L.dval, L.dval32, L.Md, s);
+            if (L.direct) make_f32(L.cinv, L.cinv32, (size_t)L.N * L.N, s);
+        }
+        alloc_work<float>(H, P->w32);
+        P->f32.alloc(N0);
+        P->z32.alloc(N0);
+        Builder<float> B{H, P->w32, P->plan};
+        const double* fin = P->fin;
+        float* f32 = P->f32.p;
+        B.op([=](cudaStream_t st) { k_to_f32<<<grid_for(N0, 256), 256, 0, st>>>(N0, fin, f32); });
+        if (H.kind == PREC_MSPLIT) B.ms(0, P->f32.p, P->z32.p);
+        else B.ch(0, P->f32.p, P->z32.p);
+        float* z32 = P->z32.p;
+        double* fout = P->fout;
+        B.op([=](cudaStream_t st) { k_to_f64<<<grid_for(N0, 256), 256, 0, st>>>(N0, z32, fout); });
+        P->bytes_per_apply = B.bytes + 12ull * N0 * 2;
+    }
+    CK(cudaStreamSynchronize(s));
+    // capture the apply once as a graph
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    P->plan.run(s);
+    cudaError_t le = cudaGetLastError();
+    CK(cudaStreamEndCapture(s, &g));
+    if (le != cudaSuccess) { cudaGraphDestroy(g); MLP_THROW(ERR_CUDA, cudaGetErrorString(le)); }
+    cudaError_t ie = cudaGraphInstantiate(&P->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) MLP_THROW(ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+    return P;
+}
+
+void prec_apply_frame(Prec& P, cudaStream_t s) {
+    if (P.graph) CK(cudaGraphLaunch(P.graph, s));
+    else P.plan.run(s);
+}
+
+// ---------------------------------------------------------------------------
+// PCG
+// ---------------------------------------------------------------------------
+static constexpr int RB = 256;  // reduction block
+
+struct PcgDev {
+    double rz0, rz1, app, alpha, beta, rr, rz_prev;
+    unsigned ticket[4];
+    int status;  // 1: <Ap,p> <= 0, 2: not finite
+};
+
+__device__ __forceinline__ double block_sum(double v) {
+    __shared__ double sh[32];
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double t = 0;
+    if (w == 0) {
+        t = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    }
+    __syncthreads();
+    return t;  // valid in thread 0
+}
+
+// Deterministic grid reduction: block partials in fixed slots, the last block
+// to arrive sums them in slot order.
+__device__ __forceinline__ bool finish_reduce(double part, double* partials, unsigned* ticket, double* total) {
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = part;
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    double v = 0;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) v += ((volatile double*)partials)[b];
+    v = block_sum(v);
+    if (threadIdx.x == 0) { *total = v; *ticket = 0; }
+    return true;
+}
+
+// Ap = A p, app = (Ap, p), alpha = rz0 / app.
+template <int LPR>
+__global__ void __launch_bounds__(RB) k_pcg_spmv_dot(uint32_t n, const uint32_t* __restrict__ ia,
+                                                     const uint32_t* __restrict__ ja, const double* __restrict__ a,
+                                                     const double* __restrict__ p, double* __restrict__ Ap,
+                                                     double* partials, PcgDev* d) {
+    double part = 0;
+    const uint32_t groups = gridDim.x * (RB / LPR);
+    int lane = threadIdx.x % LPR;
+    for (uint32_t row = blockIdx.x * (RB / LPR) + threadIdx.x / LPR;; row += groups) {
+        bool active = row < n;
+        if (__all_sync(0xffffffffu, !active)) break;
+        double s = 0;
+        if (active) {
+            uint32_t e = ia[row + 1];
+            for (uint32_t j = ia[row] + lane; j < e; j += LPR) s += a[j] * p[ja[j]];
+        }
+#pragma unroll
+        for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (active && lane == 0) {
+            Ap[row] = s;
+            part += s * p[row];
+        }
+    }
+    part = block_sum(part);
+    double tot;
+    if (finish_reduce(part, partials, &d->ticket[0], &tot) && threadIdx.x == 0) {
+        d->app = tot;
+        if (!(tot > 0)) d->status |= (tot != tot) ? 2 : 1;
+        d->alpha = d->rz0 / tot;
+    }
+}
+
+// x += alpha p; r -= alpha Ap; rr = (r, r)
+__global__ void __launch_bounds__(RB) k_pcg_update(uint32_t n, double* __restrict__ x, double* __restrict__ r,
+                                                   const double* __restrict__ p, const double* __restrict__ Ap,
+                                                   double* partials, PcgDev* d) {
+    double alpha = d->alpha;
+    double part = 0;
+    for (uint32_t i = blockIdx.x * RB + threadIdx.x; i < n; i += gridDim.x * RB) {
+        x[i] += alpha * p[i];
+        double ri = r[i] - alpha * Ap[i];
+        r[i] = ri;
+        part += ri * ri;
+    }
+    part = block_sum(part);
+    double tot;
+    if (finish_reduce(part, partials, &d->ticket[1], &tot) && threadIdx.x == 0) {
+        d->rr = tot;
+        if (tot != tot || tot > 1e308) d->status |= 2;
+    }
+}
+
+// rz1 = (r, z); beta = rz1/rz0 (or Polak-Ribiere (r - r_prev, z)/rz0); rz0 = rz1.
+__global__ void __launch_bounds__(RB) k_pcg_dot_rz(uint32_t n, const double* __restrict__ r,
+                                                   const double* __restrict__ z, const double* __restrict__ rprev,
+                                                   double* partials, PcgDev* d, int flexible) {
+    double part = 0, part2 = 0;
+    for (uint32_t i = blockIdx.x * RB + threadIdx.x; i < n; i += gridDim.x * RB) {
+        part += r[i] * z[i];
+        if (flexible) part2 += rprev[i] * z[i];
+    }
+    part = block_sum(part);
+    double tot;
+    bool last = finish_reduce(part, partials, &d->ticket[2], &tot);
+    if (flexible) {
+        __syncthreads();
+        part2 = block_sum(part2);
+        double tot2;
+        bool last2 = finish_reduce(part2, partials + gridDim.x, &d->ticket[3], &tot2);
+        if (last2 && threadIdx.x == 0) d->rz_prev = tot2;
+        (void)last;
+    }
+    if (last && threadIdx.x == 0) d->rz1 = tot;
+}
+
+__global__ void k_pcg_beta(PcgDev* d, int flexible) {
+    double num = flexible ? d->rz1 - d->rz_prev : d->rz1;
+    d->beta = num / d->rz0;
+    d->rz0 = d->rz1;
+    if (d->beta != d->beta) d->status |= 2;
+}
+
+// p = beta p + z (dscal then daxpy, pcg.cc:71-72)
+__global__ void k_pcg_p(uint32_t n, double* __restrict__ p, const double* __restrict__ z, const PcgDev* d) {
+    double beta = d->beta;
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = beta * p[i] + z[i];
+}
+
+__global__ void k_dot_simple(uint32_t n, const double* __restrict__ a, const double* __restrict__ b,
+                             double* partials, unsigned* ticket, double* out) {
+    double part = 0;
+    for (uint32_t i = blockIdx.x * RB + threadIdx.x; i < n; i += gridDim.x * RB) part += a[i] * b[i];
+    part = block_sum(part);
+    double tot;
+    if (finish_reduce(part, partials, ticket, &tot) && threadIdx.x == 0) *out = tot;
+}
+
+const double* x0_device(uint32_t n, cudaStream_t s) {
+    static std::mutex mu;
+    static std::map<std::pair<int, uint32_t>, double*> cache;
+    std::lock_guard<std::mutex> lk(mu);
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    auto key = std::make_pair(dev, n);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    // generate_x0 (solvers.cc:9-21): srandom(3); 20*(random()-0.5*RAND_MAX)/RAND_MAX + 100.
+    // random_r keeps glibc's generator without touching the process-wide state.
+    std::vector<double> h(n);
+    struct random_data rd;
+    memset(&rd, 0, sizeof rd);
+    char state[128];
+    initstate_r(3, state, sizeof state, &rd);
+    srandom_r(3, &rd);
+    for (uint32_t i = 0; i < n; i++) {
+        int32_t v;
+        random_r(&rd, &v);
+        h[i] = 20. * (v - 0.5 * RAND_MAX) / RAND_MAX + 100;
+    }
+    double* d = nullptr;
+    CK(cudaMalloc(&d, (size_t)(n ? n : 1) * 8));
+    CK(cudaMemcpyAsync(d, h.data(), (size_t)n * 8, cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    cache[key] = d;
+    return d;
+}
+
+int pcg_solve(const DCSR& A, const double* b, Prec& P, double* x, double eps, uint32_t maxit, bool flexible,
+              PcgStats& st, cudaStream_t s) {
+    Hierarchy& H = *P.H;
+    const Level& L0 = *H.lv[0];
+    const DCSR& Af = L0.Af;
+    uint32_t n = A.nrow;
+    if (n != L0.N) MLP_THROW(ERR_ARG, "matrix and preconditioner sizes differ");
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, s));
+    DBuf<double> xf(n), bf(n), p(n), Ap(n), rprev(flexible ? n : 1);
+    double* r = P.fin_buf.p;
+    double* z = P.fout_buf.p;
+    unsigned G = (unsigned)std::max(1, std::min<int>((int)grid_for(n, RB), num_sms() * 4));
+    DBuf<double> partials(2 * (size_t)G);
+    DBuf<PcgDev> dd(1);
+    dd.zero(s);
+    PcgDev* d = dd.p;
+    gather(n, L0.phi.p, b, bf.p, s);
+    gather(n, L0.phi.p, x0_device(n, s), xf.p, s);
+    // r = b - A x
+    launch_spmv<double>(n, Af.nnz, Af.ia.p, Af.ja.p, Af.a.p, xf.p, r, bf.p, s);
+    CK_LAUNCH();
+    double* hpin = nullptr;
+    CK(cudaMallocHost(&hpin, sizeof(PcgDev)));
+    auto fetch = [&]() -> PcgDev {
+        CK(cudaMemcpyAsync(hpin, d, sizeof(PcgDev), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        PcgDev h;
+        memcpy(&h, hpin, sizeof h);
+        return h;
+    };
+    k_dot_simple<<<G, RB, 0, s>>>(n, r, r, partials.p, &d->ticket[1], &d->rr);
+    CK_LAUNCH();
+    prec_apply_frame(P, s);
+    CK(cudaMemcpyAsync(p.p, z, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
+    k_dot_simple<<<G, RB, 0, s>>>(n, r, z, partials.p, &d->ticket[2], &d->rz0);
+    CK_LAUNCH();
+    if (flexible) CK(cudaMemcpyAsync(rprev.p, r, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
+    PcgDev h = fetch();
+    double norm = std::sqrt(h.rr), init = norm;
+    st.init_norm = init;
+    if (init * eps < 1e-14) eps = 1e-14 / init;  // check_and_replace_eps, solvers.cc:49-58
+    uint32_t it = 0;
+    uint32_t napply = 1;
+    double avg = (double)Af.nnz / n;
+    int lpr = avg <= 3 ? 2 : avg <= 6 ? 4 : avg <= 12 ? 8 : avg <= 24 ? 16 : 32;
+    int rc = OK;
+    std::string msg;
+    while (norm / init > eps) {
+        if (maxit && it >= maxit) { rc = ERR_MAXIT; msg = "iteration cap reached"; break; }
+        switch (lpr) {
+            case 2: k_pcg_spmv_dot<2><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p.p, Ap.p, partials.p, d); break;
+            case 4: k_pcg_spmv_dot<4><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p.p, Ap.p, partials.p, d); break;
+            case 8: k_pcg_spmv_dot<8><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p.p, Ap.p, partials.p, d); break;
+            case 16: k_pcg_spmv_dot<16><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p.p, Ap.p, partials.p, d); break;
+            default: k_pcg_spmv_dot<32><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p.p, Ap.p, partials.p, d); break;
+        }
+        k_pcg_update<<<G, RB, 0, s>>>(n, xf.p, r, p.p, Ap.p, partials.p, d);
+        CK_LAUNCH();
+        h = fetch();
+        if (h.status & 1) { rc = ERR_CURVATURE; msg = "<Ap, p> = " + std::to_string(h.app); break; }
+        if (h.status & 2) { rc = ERR_NOT_FINITE; msg = "non-finite value in PCG scalars"; break; }
+        norm = std::sqrt(h.rr);
+        it++;
+        if (!(norm / init > eps)) break;  // the reference's last apply cannot change x
+        prec_apply_frame(P, s);
+        napply++;
+        k_pcg_dot_rz<<<G, RB, 0, s>>>(n, r, z, rprev.p, partials.p, d, flexible ? 1 : 0);
+        k_pcg_beta<<<1, 1, 0, s>>>(d, flexible ? 1 : 0);
+        k_pcg_p<<<grid_for(n, 256), 256, 0, s>>>(n, p.p, z, d);
+        if (flexible) CK(cudaMemcpyAsync(rprev.p, r, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
+        CK_LAUNCH();
+    }
+    scatter(n, L0.phi.p, xf.p, x, s);
+    CK(cudaEventRecord(e1, s));
+    CK(cudaStreamSynchronize(s));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFreeHost(hpin);
+    st.niter = it;
+    st.final_norm = norm;
+    st.final_rel = norm / init;
+    st.t_total_ms = ms;
+    st.napply = napply;
+    if (rc == OK && it == 0) { rc = ERR_NO_ITER; msg = "No need to iterate"; }
+    if (rc != OK) set_last_error(msg);
+    return rc;
+}
+
+}  // namespace mlp

@@ -1,0 +1,70 @@
+// Solve-phase objects: the preconditioner apply plan and the PCG driver.
+#pragma once
+
+#include <functional>
+
+#include "setup.cuh"
+
+namespace mlp {
+
+// Work vectors of one level for the apply (typed by the preconditioner's
+// arithmetic: double for the plain path, float for the reduced-precision form).
+template <class T>
+struct LevelWork {
+    DBuf<T> r, w, u0;            // multi-split: residual, L-solve output, correction
+    DBuf<T> cu0, cu1, cx2, ctmp; // uh_cheb: Chebyshev vectors on the coarse slice
+};
+
+// A recorded sequence of launches. Replaying it (directly or as a CUDA graph)
+// applies the preconditioner z = B r, both vectors in level-0 frame order.
+struct Plan {
+    std::vector<std::function<void(cudaStream_t)>> ops;
+    size_t launches = 0;
+    void run(cudaStream_t s) const {
+        for (auto& f : ops) f(s);
+    }
+};
+
+struct Prec {
+    std::unique_ptr<Hierarchy> H;
+    bool fp32 = false;  // hierarchy stored and applied in FP32
+    std::vector<LevelWork<double>> w64;
+    std::vector<LevelWork<float>> w32;
+    DBuf<float> f32, z32;  // FP32 staging of the level-0 input/output
+    DBuf<double> zin, zout; // frame-order staging for the natural-order apply entry point
+    Plan plan;              // z = B r, frame order, on fin -> fout
+    const double* fin = nullptr;
+    double* fout = nullptr;
+    DBuf<double> fin_buf, fout_buf;
+    cudaGraphExec_t graph = nullptr;
+    cudaStream_t stream = nullptr;
+    uint64_t bytes_per_apply = 0;  // algorithmic bytes of one apply
+    ~Prec();
+};
+
+std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, cudaStream_t s);
+void prec_apply_frame(Prec& P, cudaStream_t s);  // fout = B fin
+
+// y = A x for a CSR matrix (any level, frame or natural order).
+void spmv(const DCSR& A, const double* x, double* y, cudaStream_t s);
+
+void gather(uint32_t n, const uint32_t* idx, const double* src, double* dst, cudaStream_t s);
+void scatter(uint32_t n, const uint32_t* idx, const double* src, double* dst, cudaStream_t s);
+
+struct PcgStats {
+    uint32_t niter = 0;
+    double init_norm = 0, final_norm = 0, final_rel = 0;
+    double t_total_ms = 0, t_prec_ms = 0, t_spmv_ms = 0;
+    uint32_t napply = 0;
+};
+
+// PCGSolver (pcg.cc:8-102) with x0 of generate_x0; b and x are device
+// vectors in natural order. flexible = Polak-Ribiere beta (needed when the
+// preconditioner is applied in reduced precision).
+int pcg_solve(const DCSR& A, const double* b, Prec& P, double* x, double eps, uint32_t maxit, bool flexible,
+              PcgStats& st, cudaStream_t s);
+
+// Cached x0 (generate_x0 depends only on n).
+const double* x0_device(uint32_t n, cudaStream_t s);
+
+}  // namespace mlp

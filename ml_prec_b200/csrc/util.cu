@@ -1,0 +1,121 @@
+// Library-wide utilities: error string, SM count, device exclusive scan.
+#include "common.cuh"
+
+#include <mutex>
+
+namespace mlp {
+
+static thread_local std::string g_last_error;
+
+void set_last_error(const std::string& s) { g_last_error = s; }
+const char* last_error() { return g_last_error.c_str(); }
+
+int num_sms() {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    return sms;
+}
+
+// ---- exclusive scan -------------------------------------------------------
+// Three passes: per-tile sums, a single-block scan of the tile sums, then the
+// per-tile scan with its offset. A tile is 1024 threads x 4 items.
+static constexpr int SCAN_T = 1024;
+static constexpr int SCAN_I = 4;
+static constexpr int SCAN_TILE = SCAN_T * SCAN_I;
+
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* total) {
+    __shared__ uint32_t warp_tot[32];
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_tot[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        uint32_t t = lane < (blockDim.x >> 5) ? warp_tot[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        warp_tot[lane] = t;  // inclusive
+    }
+    __syncthreads();
+    uint32_t base = wid ? warp_tot[wid - 1] : 0;
+    if (total) *total = warp_tot[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return base + x - v;
+}
+
+__global__ void k_tile_sums(const uint32_t* __restrict__ in, uint32_t n, uint32_t* __restrict__ sums) {
+    size_t base = (size_t)blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_I;
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_I; k++)
+        if (base + k < n) s += in[base + k];
+    uint32_t tot;
+    block_excl_scan(s, &tot);
+    if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+__global__ void k_scan_sums(uint32_t* sums, uint32_t nt, uint32_t* total_out) {
+    uint32_t carry = 0;
+    for (uint32_t base = 0; base < nt; base += blockDim.x) {
+        uint32_t i = base + threadIdx.x;
+        uint32_t v = i < nt ? sums[i] : 0;
+        uint32_t tot;
+        uint32_t ex = block_excl_scan(v, &tot);
+        if (i < nt) sums[i] = ex + carry;
+        carry += tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && total_out) *total_out = carry;
+}
+
+__global__ void k_tile_scan(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint32_t n,
+                            const uint32_t* __restrict__ sums) {
+    size_t base = (size_t)blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_I;
+    uint32_t v[SCAN_I];
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_I; k++) {
+        v[k] = base + k < n ? in[base + k] : 0;
+        s += v[k];
+    }
+    uint32_t ex = block_excl_scan(s, nullptr) + sums[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < SCAN_I; k++) {
+        if (base + k < n) out[base + k] = ex;
+        ex += v[k];
+    }
+}
+
+void exclusive_scan_u32_async(const uint32_t* in, uint32_t* out, uint32_t n, cudaStream_t s) {
+    uint32_t nt = (n + SCAN_TILE - 1) / SCAN_TILE;
+    if (nt == 0) nt = 1;
+    DBuf<uint32_t> sums(nt);
+    k_tile_sums<<<nt, SCAN_T, 0, s>>>(in, n, sums.p);
+    CK_LAUNCH();
+    k_scan_sums<<<1, SCAN_T, 0, s>>>(sums.p, nt, out + n);
+    CK_LAUNCH();
+    k_tile_scan<<<nt, SCAN_T, 0, s>>>(in, out, n, sums.p);
+    CK_LAUNCH();
+    CK(cudaStreamSynchronize(s));  // sums is released on return
+}
+
+uint32_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n, cudaStream_t s) {
+    exclusive_scan_u32_async(in, out, n, s);
+    uint32_t tot = 0;
+    CK(cudaMemcpyAsync(&tot, out + n, 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return tot;
+}
+
+}  // namespace mlp

@@ -1,0 +1,97 @@
+"""Writes the golden fixtures of tests/golden/ by running the reference itself.
+
+The reference (ml_prec) is compiled from its own sources by `make -C oracle ref`
+into oracle/_ref/ref_driver (a driver of this project linked against the
+unmodified reference objects). For each case below the driver builds the
+matrix with SPEMesh::construct_matrix from a seeded synthetic field, constructs
+the preconditioner, runs one preconditioner apply on a seeded vector and a PCG
+solve, and dumps the hierarchy. This script stores the inputs and those outputs
+as compressed .npz files. It needs the reference sources (REF below) and is run
+only when the fixtures are regenerated; the tests read the .npz files.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+from ml_prec_b200 import fields  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+REF = os.environ.get("MLP_REF_SRC", "/root/reference")
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+# name: (field model, field seed, nx, ny, nz, c, prec, options)
+CASES = {
+    "ms_iid_12x22x6": ("iid", 1, 12, 22, 6, 1.0, "msplit", {}),
+    "ms_layered_16x22x8_c01": ("layered", 2, 16, 22, 8, 0.1, "msplit", {}),
+    "ms_direct_20x22x6": ("iid", 3, 20, 22, 6, 1.0, "msplit", {"max_levels": 2}),
+    "ms_deg1_12x22x6": ("iid", 5, 12, 22, 6, 1.0, "msplit", {"degree_max": 1, "level_niter": "3 4"}),
+    "ms_tiny_1x1x1": ("iid", 1, 1, 1, 1, 1.0, "msplit", {}),
+    "ms_line_1x1x7": ("iid", 1, 1, 1, 7, 1.0, "msplit", {}),
+    "ch_layered_16x22x8": ("layered", 2, 16, 22, 8, 1.0, "cheb", {"sigmas": [3.0], "niters": [4]}),
+    "ch_iid_12x22x6": ("iid", 4, 12, 22, 6, 1.0, "cheb", {"sigmas": [3.0, 2.5], "niters": [2, 3]}),
+}
+
+
+def main():
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={REF}"], check=True)
+    with tempfile.TemporaryDirectory() as td:
+        perms = {}
+        for name, (model, seed, nx, ny, nz, c, prec, opt) in CASES.items():
+            key = (model, seed)
+            if key not in perms:
+                kx, ky, kz = fields.field(model, seed)
+                fn = os.path.join(td, f"perm_{model}_{seed}.bin")
+                fields.write_perm_bin(fn, kx, ky, kz)
+                perms[key] = fn
+            od = os.path.join(td, name)
+            os.makedirs(od)
+            N = nx * ny * nz
+            f = np.random.default_rng(1234).standard_normal(N)
+            f.tofile(os.path.join(od, "f_in.f64"))
+            kw = {}
+            if prec == "msplit":
+                cfg = os.path.join(od, "msplit.cfg")
+                with open(cfg, "w") as fh:
+                    fh.write(O.msplit_cfg_text(level_niter=opt.get("level_niter", "5"),
+                                               degree_max=opt.get("degree_max", 2),
+                                               max_levels=opt.get("max_levels", 15)))
+                kw["cfg"] = cfg
+            else:
+                kw["sigmas"] = opt["sigmas"]
+                kw["niters"] = opt["niters"]
+            res = O.run_ref(od, perm=perms[key], nx=nx, ny=ny, nz=nz, c=c, prec=prec, eps=1e-8, dump=True,
+                            apply=os.path.join(od, "f_in.f64"), **kw)
+            _, _, ia, ja, a = O.read_csr(os.path.join(od, "A0.csr"))
+            d = dict(nx=nx, ny=ny, nz=nz, c=c, model=model, seed=seed, prec=prec,
+                     options=json.dumps(opt), A_ia=ia, A_ja=ja, A_a=a,
+                     b=np.fromfile(os.path.join(od, "b.f64")), f_in=f,
+                     apply_out=np.fromfile(os.path.join(od, "apply_out.f64")),
+                     x=np.fromfile(os.path.join(od, "x.f64")), niter=res["niter"],
+                     nlevels=res["nlevels"], levels=json.dumps(res["levels"]))
+            for l in range(res["nlevels"]):
+                p = lambda s: os.path.join(od, f"l{l}_{s}")
+                if os.path.exists(p("map.u32")):
+                    d[f"l{l}_map"] = np.fromfile(p("map.u32"), np.uint32)
+                    d[f"l{l}_dval"] = np.fromfile(p("dval.f64"))
+                    for m in ("L", "U"):
+                        _, _, i2, j2, a2 = O.read_csr(p(f"{m}.csr"))
+                        d[f"l{l}_{m}_ia"], d[f"l{l}_{m}_ja"], d[f"l{l}_{m}_a"] = i2, j2, a2
+                if l > 0:
+                    _, _, i2, j2, a2 = O.read_csr(p("A.csr"))
+                    d[f"l{l}_A_ia"], d[f"l{l}_A_ja"], d[f"l{l}_A_a"] = i2, j2, a2
+            np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **d)
+            print(name, "N", N, "levels", res["nlevels"], "niter", res["niter"], flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,113 @@
+"""CUDA path against the reference's outputs (golden fixtures) and the oracle.
+
+Bar: integer work (hierarchy shape, node permutation, factor and coarse-matrix
+sparsity) bit-exact; factor and coarse-matrix values bit-exact too (the setup
+kernels are compiled without FMA contraction and keep the reference's operation
+order); preconditioner apply within 1e-12 relative (parallel reductions change
+the rounding); PCG iteration count within +-1 and solution within 1e-10
+relative of the reference's.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_cases
+from util import gpu_prec, load_golden, oracle_prec
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def M():
+    import ml_prec_b200 as M
+    return M
+
+
+def gpu_matrix(M, g):
+    return M.CSRMatrix.from_arrays(g["A_ia"], g["A_ja"], g["A_a"])
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_hierarchy_bit_exact(M, name):
+    g = load_golden(name)
+    A = gpu_matrix(M, g)
+    P = gpu_prec(A, g)
+    assert P.nlevels == int(g["nlevels"])
+    for l, ref in enumerate(g["levels"]):
+        lv = P.level(l)
+        for k in ("N", "nnz", "M", "Md"):
+            assert lv[k] == ref[k], (l, k, lv[k], ref[k])
+        if not lv["direct"] and f"l{l}_map" in g and g[f"l{l}_map"].size:
+            assert np.array_equal(lv["map"], g[f"l{l}_map"]), l
+            assert np.array_equal(lv["dval"], g[f"l{l}_dval"]), l
+            for m in ("L", "U"):
+                ia, ja, a = lv[m]
+                assert np.array_equal(ia, g[f"l{l}_{m}_ia"]), (l, m)
+                assert np.array_equal(ja, g[f"l{l}_{m}_ja"]), (l, m)
+                assert np.array_equal(a, g[f"l{l}_{m}_a"]), (l, m)
+        if l > 0:
+            ia, ja, a = lv["A"]
+            assert np.array_equal(ia, g[f"l{l}_A_ia"]), l
+            assert np.array_equal(ja, g[f"l{l}_A_ja"]), l
+            assert np.array_equal(a, g[f"l{l}_A_a"]), l
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_apply_matches_reference(M, name):
+    g = load_golden(name)
+    A = gpu_matrix(M, g)
+    P = gpu_prec(A, g)
+    z = P.solve(g["f_in"])
+    ref = g["apply_out"]
+    assert np.linalg.norm(z - ref) <= 1e-12 * np.linalg.norm(ref)
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_pcg_matches_reference(M, name):
+    g = load_golden(name)
+    A = gpu_matrix(M, g)
+    P = gpu_prec(A, g)
+    st = M.SolverStats()
+    x = M.PCGSolver(A, g["b"], P, stats=st, eps=1e-8)
+    assert abs(st.niter - int(g["niter"])) <= 1
+    assert np.linalg.norm(x - g["x"]) <= 1e-10 * np.linalg.norm(g["x"])
+
+
+@pytest.mark.parametrize("model,seed,dims,c", [("iid", 1, (12, 22, 6), 1.0), ("layered", 2, (60, 220, 85), 1.0),
+                                                ("layered", 7, (31, 17, 9), 0.1)])
+def test_assembly_bit_exact(M, model, seed, dims, c):
+    from ml_prec_b200 import fields
+    from oracle import oracle as O
+    kx, ky, kz = fields.field(model, seed)
+    A, b = M.CSRMatrix.spe(*dims, kx, ky, kz, c=c, dirichlet=True)
+    Ao, bo = O.assemble(*dims, kx, ky, kz, c, True)
+    ia, ja, a = A.arrays()
+    assert np.array_equal(ia, Ao.ia) and np.array_equal(ja, Ao.ja)
+    assert np.array_equal(a, Ao.a)
+    assert np.array_equal(b, bo)
+
+
+def test_full_size_hierarchy_and_pcg_against_oracle(M):
+    """60x220x85 layered field (1,122,000 cells): hierarchy bit-exact on every
+    level, PCG iterations within +-1 of the oracle's."""
+    from ml_prec_b200 import fields
+    from oracle import oracle as O
+    kx, ky, kz = fields.field("layered", 2)
+    A, b = M.CSRMatrix.spe(60, 220, 85, kx, ky, kz, c=1.0)
+    Ao, bo = O.assemble(60, 220, 85, kx, ky, kz, 1.0, True)
+    P = M.MultiSplitPrec(A, q=(0.8,), niter=(5,), max_levels=15, degree_max=2)
+    Po = O.Prec(Ao, "msplit", q=(0.8,), niter=(5,), max_levels=15, degree_max=2)
+    assert P.nlevels == Po.nlevels
+    for l in range(Po.nlevels):
+        lv, lo = P.level(l), Po.level(l)
+        for k in ("N", "nnz", "M", "Md"):
+            assert lv[k] == lo[k], (l, k)
+        if "map" in lo:
+            assert np.array_equal(lv["map"], lo["map"])
+            for m in ("L", "U"):
+                for t in range(3):
+                    assert np.array_equal(lv[m][t], lo[m][t]), (l, m, t)
+    st = M.SolverStats()
+    x = M.PCGSolver(A, b, P, stats=st, eps=1e-8)
+    xo, it, rel, rc = O.pcg(Ao, bo, Po, 1e-8)
+    assert rc == 0 and abs(st.niter - it) <= 1
+    assert np.linalg.norm(x - xo) <= 1e-9 * np.linalg.norm(xo)
