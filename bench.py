@@ -1,0 +1,336 @@
+"""Benchmark: seconds to relative residual 1e-8 on the 60x220x85 (1,122,000-cell)
+reservoir-pressure problem, multi-split preconditioned CG on one B200.
+
+Workload (one "step"): build the multi-split hierarchy on the device from the
+matrix already resident in HBM (marking, ordering, Schur elimination, solve
+schedules), then PCG from generate_x0's start vector to ||r||/||r0|| <= 1e-8.
+Problem: seeded synthetic layered permeability field (smooth layers 1-35,
+channelised layers 36-85, ky = kx, kz = 0.1 kx) standing in for SPE10, the
+reference stencil with c = 1 and Dirichlet x-faces; msplit.cfg parameters
+(q = 0.8, simple_1, degree_max = 2, level_niter = 5, max_levels = 15).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line is printed by rank 0. `value` is the device-timed seconds per
+step of the FP64 path (max over ranks; every rank solves its own replica, no
+data-path collective, "weak" scaling). `e2e` is the same step through the C ABI
+with host buffers (matrix and right-hand side uploaded, solution downloaded,
+hierarchy built and freed) timed on the host. `forms.fp32_prec` reports the
+FP32-stored hierarchy inside flexible FP64 PCG. `roofline` is the level-0 SpMV
+of the PCG loop (the dominant streaming kernel), `cpu_baseline` the reference
+itself (oracle/_ref, single-threaded) on the same problem.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "s to rel-res 1e-8 @1.1M cells (multi-split PCG, 60x220x85)"
+UNIT = "s"
+NX, NY, NZ, C_REACT, SEED = 60, 220, 85, 1.0, 2
+EPS = 1e-8
+MSPLIT = dict(q=(0.8,), niter=(5,), max_levels=15, degree_max=2, order="simple_1")
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons while the timed region runs."""
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        try:
+            for line in open(self.path):
+                f = [t.strip() for t in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx = max(mx, float(f[2]))
+                except ValueError:
+                    continue
+                names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+                for nm, v in zip(names, f[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+            os.unlink(self.path)
+        except OSError:
+            pass
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def flush_l2(buf):
+    buf.fill_(1.0)  # 256 MB write, larger than the 126 MB L2
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    import ml_prec_b200 as M
+    from ml_prec_b200 import fields
+    from ml_prec_b200._capi import Stats, check, lib
+
+    torch.cuda.set_device(local)
+    check(lib().mlp_set_device(local))
+    kx, ky, kz = fields.field("layered", SEED)
+    A, b = M.CSRMatrix.spe(NX, NY, NZ, kx, ky, kz, c=C_REACT, dirichlet=True)
+    N = A.n
+    dev = torch.device("cuda", local)
+    b_d = torch.from_numpy(b).to(dev)
+    x_d = torch.empty(N, dtype=torch.float64, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step(fp32=False):
+        P = M.MultiSplitPrec(A, fp32=fp32, **MSPLIT)
+        st = Stats()
+        rc = lib().mlp_pcg_device(A.h, C.c_void_p(b_d.data_ptr()), P.h, C.c_void_p(x_d.data_ptr()), EPS, 0,
+                                  int(fp32), C.byref(st), C.c_void_p(stream.cuda_stream))
+        check(rc)
+        nb = P.bytes_per_apply
+        del P
+        return st, nb
+
+    def timed(fp32, K, W):
+        for _ in range(W):
+            step(fp32)
+        torch.cuda.synchronize()
+        tot, last = 0.0, None
+        for _ in range(K):
+            flush_l2(flush)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            last = step(fp32)
+            e1.record(stream)
+            e1.synchronize()
+            tot += e0.elapsed_time(e1) / 1e3
+        return tot, last
+
+    barrier = (lambda: torch.distributed.barrier()) if ws > 1 else (lambda: None)
+    barrier()
+    torch.cuda.synchronize()
+
+    def launches():
+        c = C.c_uint64()
+        check(lib().mlp_launch_count(C.byref(c)))
+        return c.value
+    for _ in range(args.warmup):
+        step(False)
+    torch.cuda.synchronize()
+    l0 = launches()
+    with Clocks(local) as clk:
+        t64, (st64, nb64) = timed(False, args.steps, 0)
+        torch.cuda.synchronize()
+    nlaunch = launches() - l0
+    barrier()
+    t32, (st32, nb32) = timed(True, max(1, args.steps // 2), 1)
+
+    # solution accuracy of the FP32 form against the FP64 path
+    x64 = M.PCGSolver(A, b, M.MultiSplitPrec(A, **MSPLIT), eps=EPS)
+    x32 = M.PCGSolver(A, b, M.MultiSplitPrec(A, fp32=True, **MSPLIT), eps=EPS)
+    err32 = float(np.linalg.norm(x32 - x64) / np.linalg.norm(x64))
+
+    # roofline: level-0 SpMV of the PCG loop, timed with events on its stream
+    ia, ja, a = A.arrays()
+    xs = torch.randn(N, dtype=torch.float64, device=dev)
+    ys = torch.empty_like(xs)
+    reps = 50
+    for _ in range(5):
+        check(lib().mlp_spmv(A.h, C.c_void_p(xs.data_ptr()), C.c_void_p(ys.data_ptr()),
+                             C.c_void_p(stream.cuda_stream)))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    spmv_ms = 0.0
+    for _ in range(reps):
+        flush_l2(flush)
+        e0.record(stream)
+        check(lib().mlp_spmv(A.h, C.c_void_p(xs.data_ptr()), C.c_void_p(ys.data_ptr()),
+                             C.c_void_p(stream.cuda_stream)))
+        e1.record(stream)
+        e1.synchronize()
+        spmv_ms += e0.elapsed_time(e1)
+    spmv_ms /= reps
+    nnz = A.nnz()
+    spmv_bytes = 12 * nnz + 4 * (N + 1) + 8 * N + 8 * N
+
+    # e2e through the C ABI with host buffers
+    e2e = None
+    if rank == 0 or True:
+        def e2e_step():
+            A2 = M.CSRMatrix.from_arrays(ia, ja, a)
+            P2 = M.MultiSplitPrec(A2, **MSPLIT)
+            x = M.PCGSolver(A2, b, P2, eps=EPS)
+            del P2, A2
+            return x
+        e2e_step()
+        t0 = time.perf_counter()
+        ke = max(1, min(args.steps, 5))
+        for _ in range(ke):
+            e2e_step()
+        e2e_t = (time.perf_counter() - t0) / ke
+        e2e = {"value": e2e_t, "unit": UNIT, "h2d_bytes_per_step": int(ia.nbytes + ja.nbytes + a.nbytes + b.nbytes),
+               "d2h_bytes_per_step": int(8 * N)}
+
+    res = dict(nlaunch=nlaunch, t64=t64, t32=t32, st64=st64, st32=st32, nb64=nb64, nb32=nb32, err32=err32, spmv_ms=spmv_ms,
+               spmv_bytes=spmv_bytes, e2e=e2e, clocks=clk.summary(), N=N, nnz=nnz)
+    return res
+
+
+def reference_cpu(steps, warmup, timeout=1800):
+    """The reference's own CPU build (oracle/_ref/ref_driver) on the same problem."""
+    from oracle import oracle as O
+    from ml_prec_b200 import fields
+    if not O.ref_available():
+        return None
+    kx, ky, kz = fields.field("layered", SEED)
+    with tempfile.TemporaryDirectory() as td:
+        perm = os.path.join(td, "perm.bin")
+        fields.write_perm_bin(perm, kx, ky, kz)
+        cfg = os.path.join(td, "msplit.cfg")
+        with open(cfg, "w") as f:
+            f.write(O.msplit_cfg_text())
+        r = O.run_ref(os.path.join(td, "out"), perm=perm, nx=NX, ny=NY, nz=NZ, c=C_REACT, prec="msplit",
+                      cfg=cfg, eps=EPS, reps=warmup + steps, timeout=timeout)
+    su = r["t_setup_all"][warmup:]
+    so = r["t_solve_all"][warmup:]
+    per = [a + b for a, b in zip(su, so)]
+    return dict(value=float(np.mean(per)), setup=float(np.mean(su)), solve=float(np.mean(so)),
+                niter=r["niter"], steps=len(per))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    ws, rank, local = dist_env()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        cores = 1
+        steps = max(1, min(args.steps, 5))
+        r = reference_cpu(steps, 1)
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_driver was not built"}))
+            return
+        line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": r["steps"],
+                "warmup": 1, "ms_per_step": r["value"] * 1e3, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "60x220x85 layered field, c=1, msplit.cfg, PCG to 1e-8",
+                           "parallelism": "single-threaded reference"},
+                "impl": "reference",
+                "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": cores, "kind": "reference",
+                                 "sample": f"{r['steps']} full setup+solve steps after 1 warm-up"},
+                "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "setup_s": r["setup"], "solve_s": r["solve"], "iters": r["niter"]}
+        print(json.dumps(line))
+        return
+
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("gloo", timeout=timedelta(seconds=600))
+    res = run_ours(args, ws, rank, local)
+    t_step = res["t64"] / args.steps
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([t_step], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_step = float(t.item())
+    if rank != 0:
+        if ws > 1:
+            torch.distributed.destroy_process_group()
+        return
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    achieved = res["spmv_bytes"] / (res["spmv_ms"] / 1e3) / 1e9
+    st64, st32 = res["st64"], res["st32"]
+    cpu = None
+    if not args.no_cpu_baseline:
+        r = reference_cpu(1, 0)
+        if r:
+            cpu = {"value": r["value"], "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": "one full setup+PCG solve of the same 60x220x85 problem (single-threaded reference)",
+                   "iters": r["niter"], "setup_s": r["setup"], "solve_s": r["solve"]}
+    line = {
+        "metric": METRIC, "value": t_step, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_step * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "60x220x85 layered field (seed 2), c=1, Dirichlet x-faces; multi-split "
+                               "q=0.8 simple_1 degree_max=2 level_niter=5; setup+PCG to rel-res 1e-8",
+                   "cells": res["N"], "nnz": res["nnz"], "l2": "flushed (256 MB write) between steps",
+                   "parallelism": f"replicas x{ws}"},
+        "iters": st64.niter, "setup_ms": st64.t_setup_ms, "solve_ms": st64.t_solve_ms,
+        "forms": {"fp32_prec": {"s_per_step": res["t32"] / max(1, args.steps // 2), "iters": st32.niter,
+                                "setup_ms": st32.t_setup_ms, "solve_ms": st32.t_solve_ms,
+                                "x_rel_err_vs_fp64": res["err32"]}},
+        "e2e": res["e2e"],
+        "gpu_launches": res["nlaunch"],
+        "roofline": {"bound": "hbm", "kernel": "level-0 CSR SpMV (k_spmv<double,8>)", "achieved": achieved,
+                     "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s",
+                     "bytes_per_launch": res["spmv_bytes"], "ms_per_launch": res["spmv_ms"], "traffic": None},
+        "prec_bytes_per_apply": res["nb64"],
+        "cpu_baseline": cpu,
+        "clocks": res["clocks"],
+    }
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

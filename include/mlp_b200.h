@@ -150,6 +150,10 @@ int mlp_pcg(const mlp_matrix* A, const double* b_host, mlp_prec* P, double* x_ho
 int mlp_pcg_device(const mlp_matrix* A, const double* b_dev, mlp_prec* P, double* x_dev, double eps,
                    uint32_t maxit, int32_t flexible, mlp_stats* stats, void* stream);
 
+/* Number of kernels this library has launched in the process so far (graph
+ * kernel nodes included); no reference counterpart, used for accounting. */
+int mlp_launch_count(uint64_t* count);
+
 /* generate_x0 (solvers.cc:9-21) on the host: srandom(3), glibc random(). */
 int mlp_generate_x0(double* x_host, uint32_t n);
 

@@ -340,6 +340,13 @@ int mlp_pcg_device(const mlp_matrix* A, const double* b_dev, mlp_prec* P, double
     API_END
 }
 
+int mlp_launch_count(uint64_t* count) {
+    API_BEGIN
+    if (!count) MLP_THROW(ERR_ARG, "null pointer");
+    *count = launch_count();
+    API_END
+}
+
 int mlp_generate_x0(double* x, uint32_t n) {
     API_BEGIN
     if (!x && n) MLP_THROW(ERR_ARG, "null pointer");

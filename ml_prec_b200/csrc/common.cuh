@@ -47,7 +47,13 @@ struct Error : std::runtime_error {
             MLP_THROW(::mlp::ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
-#define CK_LAUNCH() CK(cudaGetLastError())
+void count_launches(uint64_t n);
+uint64_t launch_count();
+#define CK_LAUNCH()                 \
+    do {                            \
+        ::mlp::count_launches(1);   \
+        CK(cudaGetLastError());     \
+    } while (0)
 
 void set_last_error(const std::string& s);
 const char* last_error();

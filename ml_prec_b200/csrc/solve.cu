@@ -454,6 +454,7 @@ std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, c
 void prec_apply_frame(Prec& P, cudaStream_t s) {
     if (P.graph) CK(cudaGraphLaunch(P.graph, s));
     else P.plan.run(s);
+    count_launches(P.plan.launches);
 }
 
 // ---------------------------------------------------------------------------
@@ -692,6 +693,7 @@ int pcg_solve(const DCSR& A, const double* b, Prec& P, double* x, double eps, ui
             default: k_pcg_spmv_dot<32><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p.p, Ap.p, partials.p, d); break;
         }
         k_pcg_update<<<G, RB, 0, s>>>(n, xf.p, r, p.p, Ap.p, partials.p, d);
+        count_launches(1);
         CK_LAUNCH();
         h = fetch();
         if (h.status & 1) { rc = ERR_CURVATURE; msg = "<Ap, p> = " + std::to_string(h.app); break; }
@@ -704,6 +706,7 @@ int pcg_solve(const DCSR& A, const double* b, Prec& P, double* x, double eps, ui
         k_pcg_dot_rz<<<G, RB, 0, s>>>(n, r, z, rprev.p, partials.p, d, flexible ? 1 : 0);
         k_pcg_beta<<<1, 1, 0, s>>>(d, flexible ? 1 : 0);
         k_pcg_p<<<grid_for(n, 256), 256, 0, s>>>(n, p.p, z, d);
+        count_launches(2);
         if (flexible) CK(cudaMemcpyAsync(rprev.p, r, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
         CK_LAUNCH();
     }

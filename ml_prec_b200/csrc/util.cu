@@ -1,11 +1,16 @@
 // Library-wide utilities: error string, SM count, device exclusive scan.
 #include "common.cuh"
 
+#include <atomic>
 #include <mutex>
 
 namespace mlp {
 
 static thread_local std::string g_last_error;
+static std::atomic<uint64_t> g_launches{0};
+
+void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 void set_last_error(const std::string& s) { g_last_error = s; }
 const char* last_error() { return g_last_error.c_str(); }

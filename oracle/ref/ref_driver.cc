@@ -222,6 +222,7 @@ int main(int argc, char** argv) {
 
     PrecBase* B = 0;
     double t_setup = 0;
+    std::vector<double> setups, solves;
     for (int r = 0; r < a.reps; r++) {
         delete B;
         double ts = now();
@@ -237,9 +238,13 @@ int main(int argc, char** argv) {
             return 2;
         }
         double te = now() - ts;
+        setups.push_back(te);
         if (r == 0 || te < t_setup) t_setup = te;
     }
     js << ",\n  \"t_setup\": " << t_setup;
+    js << ",\n  \"t_setup_all\": [";
+    for (size_t r = 0; r < setups.size(); r++) js << (r ? ", " : "") << setups[r];
+    js << "]";
 
     // Hierarchy dump.
     std::vector<uint> lvN;
@@ -298,8 +303,12 @@ int main(int argc, char** argv) {
             double ts = now();
             PCGSolver(A, b, *B, x, stats, a.eps, NORM_L2, true);
             double te = now() - ts;
+            solves.push_back(te);
             if (r == 0 || te < best) best = te;
         }
+        js << ",\n  \"t_solve_all\": [";
+        for (size_t r = 0; r < solves.size(); r++) js << (r ? ", " : "") << solves[r];
+        js << "]";
         js << ",\n  \"niter\": " << stats.niter << ",\n  \"t_solve\": " << best
            << ",\n  \"t_prec_avg\": " << stats.t_prec << ",\n  \"t_resid_avg\": " << stats.t_resid;
         write_raw("x.f64", &x[0], 8 * (size_t)x.size());
