@@ -942,6 +942,8 @@ static void build_frames(Hierarchy& H, cudaStream_t s) {
         counting_sort(done, M, off, rows);
         li.lw_off = off;
         li.nwave_l = (uint32_t)off.size() - 1;
+        li.lw_off_d.alloc(off.size());
+        li.lw_off_d.upload(off.data(), off.size(), s);
         li.eperm.alloc(M ? M : 1);
         if (M) li.eperm.upload(rows.data(), M, s);
         DBuf<uint32_t> pi(N), einv(M ? M : 1), p2f(N);
@@ -1012,6 +1014,8 @@ static void build_frames(Hierarchy& H, cudaStream_t s) {
             std::vector<uint32_t> uoff, urows;
             counting_sort(ul, M, uoff, urows);
             li.uw_off = uoff;
+            li.uw_off_d.alloc(uoff.size());
+            li.uw_off_d.upload(uoff.data(), uoff.size(), s);
             li.uw_rows.alloc(M);
             li.uw_rows.upload(urows.data(), M, s);
         }

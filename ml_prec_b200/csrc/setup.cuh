@@ -59,6 +59,7 @@ struct Level {
     std::vector<uint32_t> lw_off;  // L wavefront d covers E rows [lw_off[d], lw_off[d+1])
     std::vector<uint32_t> uw_off;  // U wavefront d covers uw_rows[uw_off[d] .. uw_off[d+1])
     DBuf<uint32_t> uw_rows;
+    DBuf<uint32_t> lw_off_d, uw_off_d;  // device copies of the wavefront offsets
     // direct coarsest level
     DBuf<double> cinv;      // dense inverse, row-major N x N
     DBuf<float> cinv32;

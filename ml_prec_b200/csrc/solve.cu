@@ -11,6 +11,7 @@
 #include <map>
 #include <mutex>
 
+#include "small.cuh"
 #include "solve.cuh"
 
 namespace mlp {
@@ -105,6 +106,54 @@ __global__ void k_uwave(uint32_t cnt, const uint32_t* __restrict__ rows, const u
     T z = w[q];
     for (uint32_t j = rs + 1; j < ia[q + 1]; j++) z -= a[j] * out[ja[j]];
     out[q] = z / a[rs];
+}
+
+// The deep wavefronts of a level hold few rows each: one CTA runs all of them
+// with a barrier between wavefronts instead of one launch per wavefront.
+static constexpr uint32_t TAIL_ROWS = 1024;
+static constexpr uint32_t TAIL_THREADS = 1024;
+
+template <class T>
+__global__ void __launch_bounds__(TAIL_THREADS) k_lwave_tail(uint32_t d0, uint32_t d1, const uint32_t* __restrict__ off,
+                                                             const uint32_t* __restrict__ ia,
+                                                             const uint32_t* __restrict__ ja, const T* __restrict__ a,
+                                                             const T* __restrict__ src, T* w) {
+    for (uint32_t d = d0; d < d1; d++) {
+        uint32_t r0 = off[d], r1 = off[d + 1];
+        for (uint32_t q = r0 + threadIdx.x; q < r1; q += blockDim.x) {
+            T s = src[q];
+            for (uint32_t j = ia[q]; j < ia[q + 1]; j++) s -= a[j] * w[ja[j]];
+            w[q] = s;
+        }
+        __syncthreads();
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(TAIL_THREADS) k_uwave_tail(uint32_t d0, uint32_t d1, const uint32_t* __restrict__ off,
+                                                             const uint32_t* __restrict__ rows,
+                                                             const uint32_t* __restrict__ ia,
+                                                             const uint32_t* __restrict__ ja, const T* __restrict__ a,
+                                                             const T* __restrict__ w, T* out) {
+    for (uint32_t d = d0; d < d1; d++) {
+        uint32_t o0 = off[d], o1 = off[d + 1];
+        for (uint32_t t = o0 + threadIdx.x; t < o1; t += blockDim.x) {
+            uint32_t q = rows[t];
+            uint32_t rs = ia[q];
+            T z = w[q];
+            for (uint32_t j = rs + 1; j < ia[q + 1]; j++) z -= a[j] * out[ja[j]];
+            out[q] = z / a[rs];
+        }
+        __syncthreads();
+    }
+}
+
+// First wavefront from which every remaining wavefront is small.
+static size_t tail_start(const std::vector<uint32_t>& off) {
+    size_t nw = off.empty() ? 0 : off.size() - 1;
+    size_t d = nw;
+    while (d > 0 && off[d] - off[d - 1] <= TAIL_ROWS) d--;
+    return (nw - d >= 2) ? d : nw;
 }
 
 template <class T>
@@ -213,7 +262,16 @@ struct Builder {
     Hierarchy& H;
     std::vector<LevelWork<T>>& W;
     Plan& plan;
+    const SmallPlan<T>* small = nullptr;
     uint64_t bytes = 0;
+
+    bool small_call(uint32_t l, const T* f, T* x) {
+        if (!small || !small->valid() || l != small->first) return false;
+        const SmallPlan<T>* sp = small;
+        op([=](cudaStream_t s) { launch_small<T>(*sp, f, x, s); });
+        bytes += sp->h.bytes_static + 2ull * sizeof(T) * sp->N0;
+        return true;
+    }
 
     void op(std::function<void(cudaStream_t)> f) {
         plan.ops.push_back(std::move(f));
@@ -224,10 +282,19 @@ struct Builder {
         const uint32_t* ia = L.Lf.ia.p;
         const uint32_t* ja = L.Lf.ja.p;
         const T* a = vals<T>(L.Lf);
-        for (size_t d = 0; d + 1 < L.lw_off.size(); d++) {
+        size_t nw = L.lw_off.empty() ? 0 : L.lw_off.size() - 1;
+        size_t dt = tail_start(L.lw_off);
+        for (size_t d = 0; d < dt; d++) {
             uint32_t r0 = L.lw_off[d], r1 = L.lw_off[d + 1];
             if (r1 <= r0) continue;
             op([=](cudaStream_t s) { k_lwave<T><<<grid_for(r1 - r0, 128), 128, 0, s>>>(r0, r1, ia, ja, a, src, w); });
+        }
+        if (dt < nw) {
+            const uint32_t* off = L.lw_off_d.p;
+            uint32_t d0 = (uint32_t)dt, d1 = (uint32_t)nw;
+            op([=](cudaStream_t s) {
+                k_lwave_tail<T><<<1, TAIL_THREADS, 0, s>>>(d0, d1, off, ia, ja, a, src, w);
+            });
         }
     }
     void coarse_diag(const Level& L, const T* src, T* w, T* out) {
@@ -246,11 +313,20 @@ struct Builder {
         const uint32_t* ja = L.Uf.ja.p;
         const T* a = vals<T>(L.Uf);
         const uint32_t* rows = L.uw_rows.p;
-        for (size_t d = 0; d + 1 < L.uw_off.size(); d++) {
+        size_t nw = L.uw_off.empty() ? 0 : L.uw_off.size() - 1;
+        size_t dt = tail_start(L.uw_off);
+        for (size_t d = 0; d < dt; d++) {
             uint32_t o0 = L.uw_off[d], o1 = L.uw_off[d + 1];
             if (o1 <= o0) continue;
             op([=](cudaStream_t s) {
                 k_uwave<T><<<grid_for(o1 - o0, 128), 128, 0, s>>>(o1 - o0, rows + o0, ia, ja, a, w, out);
+            });
+        }
+        if (dt < nw) {
+            const uint32_t* off = L.uw_off_d.p;
+            uint32_t d0 = (uint32_t)dt, d1 = (uint32_t)nw;
+            op([=](cudaStream_t s) {
+                k_uwave_tail<T><<<1, TAIL_THREADS, 0, s>>>(d0, d1, off, rows, ia, ja, a, w, out);
             });
         }
     }
@@ -274,6 +350,7 @@ struct Builder {
 
     // MultiSplitPrec::solve(level, f, x) (multi_split_solve.cc:59-157)
     void ms(uint32_t l, const T* f, T* x) {
+        if (small_call(l, f, x)) return;
         Level& L = *H.lv[l];
         if (L.direct) { direct(L, f, x); return; }
         LevelWork<T>& w = W[l];
@@ -305,6 +382,7 @@ struct Builder {
 
     // Prec::solve(level, f, x) (cheb_solve.cc:13-123)
     void ch(uint32_t l, const T* f, T* x) {
+        if (small_call(l, f, x)) return;
         Level& L = *H.lv[l];
         LevelWork<T>& w = W[l];
         uint32_t M = L.M;
@@ -397,6 +475,15 @@ static void make_f32(DCSR& m, cudaStream_t s) { make_f32(m.a, m.a32, m.nnz, s); 
 Prec::~Prec() {
     if (graph) cudaGraphExecDestroy(graph);
 }
+Prec::Prec() = default;
+
+// Shared-memory budget of the small-level kernel; MLP_SMALL_BUDGET (bytes, 0 =
+// off) overrides it, which the tests use to exercise both apply paths.
+static uint32_t small_budget() {
+    const char* e = getenv("MLP_SMALL_BUDGET");
+    if (e && *e) return (uint32_t)strtoul(e, nullptr, 10);
+    return 200 * 1024;
+}
 
 std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, cudaStream_t s) {
     auto P = std::unique_ptr<Prec>(new Prec());
@@ -411,7 +498,9 @@ std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, c
     P->fout = P->fout_buf.p;
     if (!fp32) {
         alloc_work<double>(H, P->w64);
-        Builder<double> B{H, P->w64, P->plan};
+        P->sp64.reset(new SmallPlan<double>());
+        if (small_budget()) build_small<double>(H, *P->sp64, small_budget(), s);
+        Builder<double> B{H, P->w64, P->plan, P->sp64.get()};
         if (H.kind == PREC_MSPLIT) B.ms(0, P->fin, P->fout);
         else B.ch(0, P->fin, P->fout);
         P->bytes_per_apply = B.bytes;
@@ -424,9 +513,11 @@ std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, c
             if (L.direct) make_f32(L.cinv, L.cinv32, (size_t)L.N * L.N, s);
         }
         alloc_work<float>(H, P->w32);
+        P->sp32.reset(new SmallPlan<float>());
+        if (small_budget()) build_small<float>(H, *P->sp32, small_budget(), s);
         P->f32.alloc(N0);
         P->z32.alloc(N0);
-        Builder<float> B{H, P->w32, P->plan};
+        Builder<float> B{H, P->w32, P->plan, P->sp32.get()};
         const double* fin = P->fin;
         float* f32 = P->f32.p;
         B.op([=](cudaStream_t st) { k_to_f32<<<grid_for(N0, 256), 256, 0, st>>>(N0, fin, f32); });

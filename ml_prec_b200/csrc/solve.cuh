@@ -25,8 +25,13 @@ struct Plan {
     }
 };
 
+template <class T>
+struct SmallPlan;
+
 struct Prec {
     std::unique_ptr<Hierarchy> H;
+    std::unique_ptr<SmallPlan<double>> sp64;
+    std::unique_ptr<SmallPlan<float>> sp32;
     bool fp32 = false;  // hierarchy stored and applied in FP32
     std::vector<LevelWork<double>> w64;
     std::vector<LevelWork<float>> w32;
@@ -39,6 +44,7 @@ struct Prec {
     cudaGraphExec_t graph = nullptr;
     cudaStream_t stream = nullptr;
     uint64_t bytes_per_apply = 0;  // algorithmic bytes of one apply
+    Prec();
     ~Prec();
 };
 

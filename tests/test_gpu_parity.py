@@ -22,6 +22,15 @@ def M():
     return M
 
 
+@pytest.fixture(params=["small", "launch"])
+def apply_path(request, monkeypatch):
+    """Run each case through the shared-memory small-level kernel (default)
+    and through the per-wavefront launch path (small kernel disabled)."""
+    if request.param == "launch":
+        monkeypatch.setenv("MLP_SMALL_BUDGET", "0")
+    return request.param
+
+
 def gpu_matrix(M, g):
     return M.CSRMatrix.from_arrays(g["A_ia"], g["A_ja"], g["A_a"])
 
@@ -52,7 +61,7 @@ def test_hierarchy_bit_exact(M, name):
 
 
 @pytest.mark.parametrize("name", golden_cases())
-def test_apply_matches_reference(M, name):
+def test_apply_matches_reference(M, name, apply_path):
     g = load_golden(name)
     A = gpu_matrix(M, g)
     P = gpu_prec(A, g)
@@ -62,7 +71,7 @@ def test_apply_matches_reference(M, name):
 
 
 @pytest.mark.parametrize("name", golden_cases())
-def test_pcg_matches_reference(M, name):
+def test_pcg_matches_reference(M, name, apply_path):
     g = load_golden(name)
     A = gpu_matrix(M, g)
     P = gpu_prec(A, g)
