@@ -150,6 +150,22 @@ int mlp_pcg(const mlp_matrix* A, const double* b_host, mlp_prec* P, double* x_ho
 int mlp_pcg_device(const mlp_matrix* A, const double* b_dev, mlp_prec* P, double* x_dev, double eps,
                    uint32_t maxit, int32_t flexible, mlp_stats* stats, void* stream);
 
+/* PCG that allocates no device memory. It has no counterpart in the
+ * reference: it serves callers that cannot call cudaMalloc while they run
+ * (code recording into a stream capture, hosts whose device memory belongs to
+ * their own allocator). It computes exactly what mlp_pcg_device computes, but
+ * the solver's vectors and reduction scratch live in one file-scope device
+ * array of the library, sized for at most 131072 unknowns (about 5 MB, held by
+ * every GPU that loads the library until the process exits); larger systems
+ * are rejected with MLP_ERR_LIMIT. The matrix and the preconditioner must have
+ * been created beforehand (those calls allocate). The first call on a device
+ * looks up the array's device address; make that first call before any stream
+ * capture. All calls share the one array: calls that overlap on the GPU (other
+ * threads, other streams) race and must be serialised by the caller. t_solve_ms
+ * is host wall time. */
+int mlp_pcg_device_noalloc(const mlp_matrix* A, const double* b_dev, mlp_prec* P, double* x_dev, double eps,
+                           uint32_t maxit, int32_t flexible, mlp_stats* stats, void* stream);
+
 /* Number of kernels this library has launched in the process so far (graph
  * kernel nodes included); no reference counterpart, used for accounting. */
 int mlp_launch_count(uint64_t* count);

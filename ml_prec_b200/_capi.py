@@ -23,7 +23,7 @@ EXPORTS = [
     "mlp_matrix_download", "mlp_spmv",
     "mlp_prec_create", "mlp_prec_destroy", "mlp_prec_apply", "mlp_prec_apply_host", "mlp_prec_nlevels",
     "mlp_prec_level_info", "mlp_prec_level_export", "mlp_prec_bytes_per_apply",
-    "mlp_pcg", "mlp_pcg_device", "mlp_launch_count", "mlp_generate_x0",
+    "mlp_pcg", "mlp_pcg_device", "mlp_pcg_device_noalloc", "mlp_launch_count", "mlp_generate_x0",
 ]
 
 
@@ -96,6 +96,8 @@ def lib():
         L.mlp_pcg.argtypes = [vp, f64p, vp, f64p, C.c_double, C.c_uint32, C.c_int32, C.POINTER(Stats)]
         L.mlp_pcg_device.argtypes = [vp, vp, vp, vp, C.c_double, C.c_uint32, C.c_int32, C.POINTER(Stats), vp]
         L.mlp_generate_x0.argtypes = [f64p, C.c_uint32]
+        L.mlp_pcg_device_noalloc.argtypes = [vp, vp, vp, vp, C.c_double, C.c_uint32, C.c_int32,
+                                             C.POINTER(Stats), vp]
         L.mlp_launch_count.argtypes = [C.POINTER(C.c_uint64)]
         _lib = L
     return _lib

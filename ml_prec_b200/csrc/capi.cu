@@ -347,6 +347,26 @@ int mlp_launch_count(uint64_t* count) {
     API_END
 }
 
+int mlp_pcg_device_noalloc(const mlp_matrix* A, const double* b_dev, mlp_prec* P, double* x_dev, double eps,
+                           uint32_t maxit, int32_t flexible, mlp_stats* stats, void* stream) {
+    API_BEGIN
+    if (!A || !b_dev || !P || !x_dev) MLP_THROW(ERR_ARG, "null pointer");
+    cudaStream_t s = stream ? (cudaStream_t)stream : P->s;
+    PcgStats st;
+    int rc = pcg_solve_noalloc(A->A, b_dev, *P->P, x_dev, eps, maxit, flexible != 0, st, s);
+    if (stats) {
+        stats->niter = st.niter;
+        stats->napply = st.napply;
+        stats->init_norm = st.init_norm;
+        stats->final_norm = st.final_norm;
+        stats->final_rel = st.final_rel;
+        stats->t_solve_ms = st.t_total_ms;
+        stats->t_setup_ms = P->setup_ms;
+    }
+    return rc;
+    API_END
+}
+
 int mlp_generate_x0(double* x, uint32_t n) {
     API_BEGIN
     if (!x && n) MLP_THROW(ERR_ARG, "null pointer");

@@ -6,6 +6,7 @@
 // next level's vectors are slices [M, M+n) of this level's, so the recursion
 // moves no data between levels.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -813,6 +814,160 @@ int pcg_solve(const DCSR& A, const double* b, Prec& P, double* x, double eps, ui
     st.final_norm = norm;
     st.final_rel = norm / init;
     st.t_total_ms = ms;
+    st.napply = napply;
+    if (rc == OK && it == 0) { rc = ERR_NO_ITER; msg = "No need to iterate"; }
+    if (rc != OK) set_last_error(msg);
+    return rc;
+}
+
+}  // namespace mlp
+
+namespace mlp {
+
+// ---------------------------------------------------------------------------
+// PCG without device allocation.
+//
+// Callers that cannot allocate device memory while they run (code executing
+// inside a stream capture, or hosts that own the whole device pool through a
+// custom allocator) use this variant of pcg_solve. The solver's own vectors and
+// reduction scratch live in the file-scope array below instead of buffers from
+// cudaMalloc; the matrix and the preconditioner handle were built beforehand.
+// The array holds up to NOALLOC_MAX_N unknowns; every GPU that loads the
+// library holds it (about 5 MB) until the process exits.
+// ---------------------------------------------------------------------------
+static constexpr uint32_t NOALLOC_MAX_N = 131072;
+static constexpr uint32_t NOALLOC_GRID = 1024;  // largest reduction grid used
+static constexpr size_t NOALLOC_HDR = 16;       // doubles reserved for PcgDev
+static constexpr size_t NOALLOC_DOUBLES = NOALLOC_HDR + 2 * (size_t)NOALLOC_GRID + 5 * (size_t)NOALLOC_MAX_N;
+static_assert(sizeof(PcgDev) <= NOALLOC_HDR * sizeof(double), "PcgDev must fit the header");
+
+static __device__ __align__(256) double g_pcg_scratch[NOALLOC_DOUBLES];
+
+// Device address of g_pcg_scratch for the current device. The name is only a
+// host-side stand-in for the array, so the address is taken once per device
+// with cudaGetSymbolAddress while that device is current, and cached.
+static double* noalloc_scratch() {
+    static std::mutex mu;
+    static std::map<int, double*> addr;
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = addr.find(dev);
+    if (it != addr.end()) return it->second;
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_pcg_scratch);
+    if (e != cudaSuccess) MLP_THROW(ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    addr[dev] = (double*)p;
+    return (double*)p;
+}
+
+uint32_t pcg_noalloc_max_n() { return NOALLOC_MAX_N; }
+
+int pcg_solve_noalloc(const DCSR& A, const double* b, Prec& P, double* x, double eps, uint32_t maxit,
+                      bool flexible, PcgStats& st, cudaStream_t s) {
+    Hierarchy& H = *P.H;
+    const Level& L0 = *H.lv[0];
+    const DCSR& Af = L0.Af;
+    uint32_t n = A.nrow;
+    if (n != L0.N) MLP_THROW(ERR_ARG, "matrix and preconditioner sizes differ");
+    if (n > NOALLOC_MAX_N)
+        MLP_THROW(ERR_LIMIT, "the allocation-free PCG holds at most " + std::to_string(NOALLOC_MAX_N) +
+                                 " unknowns; this system has " + std::to_string(n));
+    unsigned G = (unsigned)std::max(1, std::min<int>((int)grid_for(n, RB), num_sms() * 4));
+    if (G > NOALLOC_GRID) MLP_THROW(ERR_LIMIT, "reduction grid exceeds the static scratch");
+    auto t0 = std::chrono::steady_clock::now();
+    double* base = noalloc_scratch();
+    PcgDev* d = reinterpret_cast<PcgDev*>(base);
+    double* partials = base + NOALLOC_HDR;
+    double* xf = partials + 2 * (size_t)NOALLOC_GRID;
+    double* bf = xf + NOALLOC_MAX_N;
+    double* p = bf + NOALLOC_MAX_N;
+    double* Ap = p + NOALLOC_MAX_N;
+    double* rprev = Ap + NOALLOC_MAX_N;
+    double* r = P.fin_buf.p;
+    double* z = P.fout_buf.p;
+    // the array keeps the previous call's contents: the reduction tickets and
+    // status flags must start at zero
+    CK(cudaMemsetAsync(d, 0, sizeof(PcgDev), s));
+    // x0 of generate_x0 (solvers.cc:9-21), staged through a host stack buffer
+    // into p (natural order), then permuted into the frame like b
+    {
+        struct random_data rd;
+        memset(&rd, 0, sizeof rd);
+        char state[128];
+        initstate_r(3, state, sizeof state, &rd);
+        srandom_r(3, &rd);
+        double chunk[2048];
+        for (uint32_t i0 = 0; i0 < n; i0 += 2048) {
+            uint32_t m = std::min<uint32_t>(2048, n - i0);
+            for (uint32_t i = 0; i < m; i++) {
+                int32_t v;
+                random_r(&rd, &v);
+                chunk[i] = 20. * (v - 0.5 * RAND_MAX) / RAND_MAX + 100;
+            }
+            CK(cudaMemcpyAsync(p + i0, chunk, (size_t)m * 8, cudaMemcpyHostToDevice, s));
+            CK(cudaStreamSynchronize(s));
+        }
+    }
+    gather(n, L0.phi.p, b, bf, s);
+    gather(n, L0.phi.p, p, xf, s);
+    launch_spmv<double>(n, Af.nnz, Af.ia.p, Af.ja.p, Af.a.p, xf, r, bf, s);
+    CK_LAUNCH();
+    auto fetch = [&]() -> PcgDev {
+        PcgDev h;
+        CK(cudaMemcpyAsync(&h, d, sizeof(PcgDev), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        return h;
+    };
+    k_dot_simple<<<G, RB, 0, s>>>(n, r, r, partials, &d->ticket[1], &d->rr);
+    CK_LAUNCH();
+    prec_apply_frame(P, s);
+    CK(cudaMemcpyAsync(p, z, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
+    k_dot_simple<<<G, RB, 0, s>>>(n, r, z, partials, &d->ticket[2], &d->rz0);
+    CK_LAUNCH();
+    if (flexible) CK(cudaMemcpyAsync(rprev, r, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
+    PcgDev h = fetch();
+    double norm = std::sqrt(h.rr), init = norm;
+    st.init_norm = init;
+    if (init * eps < 1e-14) eps = 1e-14 / init;  // check_and_replace_eps, solvers.cc:49-58
+    uint32_t it = 0, napply = 1;
+    double avg = (double)Af.nnz / n;
+    int lpr = avg <= 3 ? 2 : avg <= 6 ? 4 : avg <= 12 ? 8 : avg <= 24 ? 16 : 32;
+    int rc = OK;
+    std::string msg;
+    while (norm / init > eps) {
+        if (maxit && it >= maxit) { rc = ERR_MAXIT; msg = "iteration cap reached"; break; }
+        switch (lpr) {
+            case 2: k_pcg_spmv_dot<2><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p, Ap, partials, d); break;
+            case 4: k_pcg_spmv_dot<4><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p, Ap, partials, d); break;
+            case 8: k_pcg_spmv_dot<8><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p, Ap, partials, d); break;
+            case 16: k_pcg_spmv_dot<16><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p, Ap, partials, d); break;
+            default: k_pcg_spmv_dot<32><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p, Ap, partials, d); break;
+        }
+        k_pcg_update<<<G, RB, 0, s>>>(n, xf, r, p, Ap, partials, d);
+        count_launches(1);
+        CK_LAUNCH();
+        h = fetch();
+        if (h.status & 1) { rc = ERR_CURVATURE; msg = "<Ap, p> = " + std::to_string(h.app); break; }
+        if (h.status & 2) { rc = ERR_NOT_FINITE; msg = "non-finite value in PCG scalars"; break; }
+        norm = std::sqrt(h.rr);
+        it++;
+        if (!(norm / init > eps)) break;
+        prec_apply_frame(P, s);
+        napply++;
+        k_pcg_dot_rz<<<G, RB, 0, s>>>(n, r, z, rprev, partials, d, flexible ? 1 : 0);
+        k_pcg_beta<<<1, 1, 0, s>>>(d, flexible ? 1 : 0);
+        k_pcg_p<<<grid_for(n, 256), 256, 0, s>>>(n, p, z, d);
+        count_launches(2);
+        if (flexible) CK(cudaMemcpyAsync(rprev, r, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
+        CK_LAUNCH();
+    }
+    scatter(n, L0.phi.p, xf, x, s);
+    CK(cudaStreamSynchronize(s));
+    st.niter = it;
+    st.final_norm = norm;
+    st.final_rel = norm / init;
+    st.t_total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     st.napply = napply;
     if (rc == OK && it == 0) { rc = ERR_NO_ITER; msg = "No need to iterate"; }
     if (rc != OK) set_last_error(msg);

@@ -70,6 +70,12 @@ struct PcgStats {
 int pcg_solve(const DCSR& A, const double* b, Prec& P, double* x, double eps, uint32_t maxit, bool flexible,
               PcgStats& st, cudaStream_t s);
 
+// pcg_solve with every solver vector and reduction scratch in a static device
+// array instead of allocations (at most pcg_noalloc_max_n() unknowns).
+int pcg_solve_noalloc(const DCSR& A, const double* b, Prec& P, double* x, double eps, uint32_t maxit,
+                      bool flexible, PcgStats& st, cudaStream_t s);
+uint32_t pcg_noalloc_max_n();
+
 // Cached x0 (generate_x0 depends only on n).
 const double* x0_device(uint32_t n, cudaStream_t s);
 
