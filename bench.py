@@ -137,14 +137,20 @@ def run_ours(args, ws, rank, local):
             step(fp32)
         torch.cuda.synchronize()
         tot, last = 0.0, None
-        for _ in range(K):
+        for k in range(K):
             flush_l2(flush)
             torch.cuda.synchronize()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
+            # the first timed FP64 step is the range an ncu launch list filters on
+            tag = (k == 0 and not fp32)
+            if tag:
+                torch.cuda.nvtx.range_push("bench_step")
             e0.record(stream)
             last = step(fp32)
             e1.record(stream)
+            if tag:
+                torch.cuda.nvtx.range_pop()
             e1.synchronize()
             tot += e0.elapsed_time(e1) / 1e3
         return tot, last
@@ -162,6 +168,7 @@ def run_ours(args, ws, rank, local):
     torch.cuda.synchronize()
     l0 = launches()
     with Clocks(local) as clk:
+        time.sleep(2.0)  # let the sampler start before the timed region
         t64, (st64, nb64) = timed(False, args.steps, 0)
         torch.cuda.synchronize()
     nlaunch = launches() - l0

@@ -85,6 +85,7 @@ int mlp_matrix_create(uint32_t n, const uint32_t* ia, const uint32_t* ja, const 
         M->A.ia.upload(ia, (size_t)n + 1, M->s);
         M->A.ja.upload(ja, nnz, M->s);
         M->A.a.upload(a, nnz, M->s);
+        csr_tile_stats(M->A, M->s);
         CK(cudaStreamSynchronize(M->s));
     } catch (...) {
         delete M;
@@ -112,6 +113,7 @@ int mlp_matrix_create_spe(uint32_t nx, uint32_t ny, uint32_t nz, const double* k
         DBuf<double> b(b_host ? N : 0);
         spe_assemble(nx, ny, nz, dk.p, dk.p + KN, dk.p + 2 * KN, c, dirichlet, M->A, b_host ? b.p : nullptr, M->s);
         if (b_host) CK(cudaMemcpyAsync(b_host, b.p, (size_t)N * 8, cudaMemcpyDeviceToHost, M->s));
+        csr_tile_stats(M->A, M->s);
         CK(cudaStreamSynchronize(M->s));
     } catch (...) {
         delete M;

@@ -8,6 +8,7 @@
 #include <stdint.h>
 
 #include <cstdio>
+#include <utility>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -74,10 +75,12 @@ struct DBuf {
         return *this;
     }
     ~DBuf() { release(); }
+    // 16 bytes of slack past the end: kernels that stage a row range with
+    // 16-byte vector loads may read (never use) up to 15 bytes beyond it.
     void alloc(size_t count) {
         release();
         n = count;
-        if (count) CK(cudaMalloc(&p, count * sizeof(T)));
+        if (count) CK(cudaMalloc(&p, count * sizeof(T) + 16));
     }
     void release() {
         if (p) cudaFree(p);
@@ -102,6 +105,7 @@ struct DBuf {
 // copy of the values for the reduced-precision preconditioner).
 struct DCSR {
     uint32_t nrow = 0, ncol = 0, nnz = 0;
+    uint32_t tile_max = 0;  // largest nnz of a 256-row tile (0 = not computed)
     DBuf<uint32_t> ia, ja;
     DBuf<double> a;
     DBuf<float> a32;
@@ -112,6 +116,32 @@ struct DCSR {
         a.alloc(z ? z : 1);
     }
 };
+
+// Programmatic dependent launch. Kernels of the apply plan start with
+// pdl_wait() (returns once the preceding kernel in the stream has finished and
+// its writes are visible; a no-op when launched without the attribute) and
+// then pdl_trigger() (lets the next kernel be scheduled while this one runs),
+// so the launch latency of each kernel overlaps its predecessor.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+
+bool pdl_enabled();
+
+template <typename... KArgs, typename... Args>
+inline void launch_k(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                     Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
 
 inline unsigned grid_for(size_t n, unsigned block) {
     size_t g = (n + block - 1) / block;

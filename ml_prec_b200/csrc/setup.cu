@@ -5,6 +5,7 @@
 // link is dropped, the node ordering, the coarse sparsity pattern) and every
 // factor value come out bit-identical to the reference.
 #include "setup.cuh"
+#include "solve.cuh"
 
 namespace mlp {
 
@@ -672,6 +673,98 @@ __global__ void k_gj_rowk(uint32_t n, uint32_t k, double* __restrict__ D, const 
     D[(size_t)k * n + j] = (j == k) ? piv : D[(size_t)k * n + j] * piv;
 }
 
+
+// ---- explicit triangular solves ------------------------------------------
+// Rows are built as Row(q) = base(q) + sum_k c_qk Row(k) with the rows k
+// finished in an earlier wavefront. Each row is a sorted (column, value) list
+// in its own slot of `cap` pairs.
+__device__ __forceinline__ bool slot_merge(uint32_t* wc, double* wv, uint32_t& wn, uint32_t cap,
+                                           const uint32_t* kc, const double* kv, uint32_t kn, double c) {
+    uint32_t pos = 0;
+    for (uint32_t u = 0; u < kn; u++) {
+        uint32_t j = kc[u];
+        while (pos < wn && wc[pos] < j) pos++;
+        if (pos < wn && wc[pos] == j) {
+            wv[pos] += c * kv[u];
+        } else {
+            if (wn == cap) return false;
+            for (uint32_t t = wn; t > pos; t--) { wc[t] = wc[t - 1]; wv[t] = wv[t - 1]; }
+            wc[pos] = j;
+            wv[pos] = c * kv[u];
+            wn++;
+        }
+        pos++;
+    }
+    return true;
+}
+
+// P1 rows q in [r0, r1): Row(q) = e_q - sum_k l_qk Row(k).
+__global__ void k_p1_rows(uint32_t r0, uint32_t r1, const uint32_t* __restrict__ ia, const uint32_t* __restrict__ ja,
+                          const double* __restrict__ a, uint32_t cap, uint32_t* scol, double* sval,
+                          uint32_t* slen, int* flags) {
+    uint32_t q = r0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= r1) return;
+    uint32_t* wc = scol + (size_t)q * cap;
+    double* wv = sval + (size_t)q * cap;
+    uint32_t wn = 1;
+    wc[0] = q;
+    wv[0] = 1.0;
+    for (uint32_t j = ia[q]; j < ia[q + 1]; j++) {
+        uint32_t k = ja[j];
+        if (!slot_merge(wc, wv, wn, cap, scol + (size_t)k * cap, sval + (size_t)k * cap, slen[k], -a[j])) {
+            atomicOr(flags, 1);
+            return;
+        }
+    }
+    slen[q] = wn;
+}
+
+// G rows (E rows listed by U wavefront): Row(q) = (e_q - sum_C u_qc e_c
+// - sum_E u_qj Row(j)) / u_qq.
+__global__ void k_g_rows(uint32_t cnt, const uint32_t* __restrict__ rows, uint32_t M,
+                         const uint32_t* __restrict__ ia, const uint32_t* __restrict__ ja,
+                         const double* __restrict__ a, uint32_t cap, uint32_t* scol, double* sval, uint32_t* slen,
+                         int* flags) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= cnt) return;
+    uint32_t q = rows[t];
+    uint32_t rs = ia[q], re = ia[q + 1];
+    double inv = 1 / a[rs];
+    uint32_t* wc = scol + (size_t)q * cap;
+    double* wv = sval + (size_t)q * cap;
+    uint32_t wn = 1;
+    wc[0] = q;
+    wv[0] = inv;
+    for (uint32_t j = rs + 1; j < re; j++) {
+        uint32_t c = ja[j];
+        if (c < M) continue;
+        uint32_t one = c;
+        double v = 1.0;
+        if (!slot_merge(wc, wv, wn, cap, &one, &v, 1, -a[j] * inv)) { atomicOr(flags, 1); return; }
+    }
+    for (uint32_t j = rs + 1; j < re; j++) {
+        uint32_t k = ja[j];
+        if (k >= M) continue;
+        if (!slot_merge(wc, wv, wn, cap, scol + (size_t)k * cap, sval + (size_t)k * cap, slen[k], -a[j] * inv)) {
+            atomicOr(flags, 1);
+            return;
+        }
+    }
+    slen[q] = wn;
+}
+
+__global__ void k_slots_emit(uint32_t R, uint32_t cap, const uint32_t* __restrict__ scol,
+                             const double* __restrict__ sval, const uint32_t* __restrict__ ia,
+                             uint32_t* __restrict__ ja, double* __restrict__ a) {
+    uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= R) return;
+    uint32_t o = ia[q], n = ia[q + 1] - o;
+    for (uint32_t t = 0; t < n; t++) {
+        ja[o + t] = scol[(size_t)q * cap + t];
+        a[o + t] = sval[(size_t)q * cap + t];
+    }
+}
+
 // ---- per-level construction ------------------------------------------------
 
 struct Scratch {
@@ -921,6 +1014,63 @@ static void counting_sort(const std::vector<int>& lev, uint32_t nrows, std::vect
     off.push_back(nrows);
 }
 
+
+// Explicit forms of the level's triangular solves (P1 and G, setup.cuh).
+static void build_explicit(Level& li, cudaStream_t s) {
+    uint32_t M = li.M, R = li.N - li.Md;
+    DBuf<int> flags(1);
+    // P1
+    for (uint32_t cap = 16;; cap *= 2) {
+        if (cap > 65536) MLP_THROW(ERR_LIMIT, "explicit L solve row exceeds 65536 entries");
+        DBuf<uint32_t> scol((size_t)R * cap + 1), slen(R + 1);
+        DBuf<double> sval((size_t)R * cap + 1);
+        flags.zero(s);
+        for (size_t d = 0; d + 1 < li.lw_off.size(); d++) {
+            uint32_t r0 = li.lw_off[d], r1 = li.lw_off[d + 1];
+            if (r1 > r0) k_p1_rows<<<grid_for(r1 - r0, 128), 128, 0, s>>>(r0, r1, li.Lf.ia.p, li.Lf.ja.p, li.Lf.a.p,
+                                                                         cap, scol.p, sval.p, slen.p, flags.p);
+        }
+        if (R > M)
+            k_p1_rows<<<grid_for(R - M, 128), 128, 0, s>>>(M, R, li.Lf.ia.p, li.Lf.ja.p, li.Lf.a.p, cap, scol.p,
+                                                         sval.p, slen.p, flags.p);
+        CK_LAUNCH();
+        if (read_flag(flags.p, s)) continue;
+        li.P1.ia.alloc((size_t)R + 1);
+        uint32_t z = exclusive_scan_u32(slen.p, li.P1.ia.p, R, s);
+        li.P1.nrow = R; li.P1.ncol = R; li.P1.nnz = z;
+        li.P1.ja.alloc(z ? z : 1); li.P1.a.alloc(z ? z : 1);
+        if (R) k_slots_emit<<<grid_for(R, 128), 128, 0, s>>>(R, cap, scol.p, sval.p, li.P1.ia.p, li.P1.ja.p, li.P1.a.p);
+        CK_LAUNCH();
+        CK(cudaStreamSynchronize(s));
+        break;
+    }
+    // G
+    li.G.nrow = M; li.G.ncol = R; li.G.nnz = 0;
+    if (!M) { li.G.ia.alloc(1); li.G.ia.zero(s); li.G.ja.alloc(1); li.G.a.alloc(1); return; }
+    for (uint32_t cap = 16;; cap *= 2) {
+        if (cap > 65536) MLP_THROW(ERR_LIMIT, "explicit U solve row exceeds 65536 entries");
+        DBuf<uint32_t> scol((size_t)M * cap + 1), slen(M + 1);
+        DBuf<double> sval((size_t)M * cap + 1);
+        flags.zero(s);
+        for (size_t d = 0; d + 1 < li.uw_off.size(); d++) {
+            uint32_t o0 = li.uw_off[d], o1 = li.uw_off[d + 1];
+            if (o1 > o0) k_g_rows<<<grid_for(o1 - o0, 128), 128, 0, s>>>(o1 - o0, li.uw_rows.p + o0, M, li.Uf.ia.p,
+                                                                        li.Uf.ja.p, li.Uf.a.p, cap, scol.p, sval.p,
+                                                                        slen.p, flags.p);
+        }
+        CK_LAUNCH();
+        if (read_flag(flags.p, s)) continue;
+        li.G.ia.alloc((size_t)M + 1);
+        uint32_t z = exclusive_scan_u32(slen.p, li.G.ia.p, M, s);
+        li.G.nnz = z;
+        li.G.ja.alloc(z ? z : 1); li.G.a.alloc(z ? z : 1);
+        k_slots_emit<<<grid_for(M, 128), 128, 0, s>>>(M, cap, scol.p, sval.p, li.G.ia.p, li.G.ja.p, li.G.a.p);
+        CK_LAUNCH();
+        CK(cudaStreamSynchronize(s));
+        break;
+    }
+}
+
 // Builds the frame-order operators of every level, bottom-up.
 static void build_frames(Hierarchy& H, cudaStream_t s) {
     for (int l = (int)H.nlevels - 1; l >= 0; l--) {
@@ -1047,6 +1197,9 @@ static void build_frames(Hierarchy& H, cudaStream_t s) {
                 li.As.nrow = li.As.ncol = N; li.As.nnz = z;
             }
         }
+        csr_tile_stats(li.Af, s);
+        if (H.kind == PREC_CHEB && l > 0) csr_tile_stats(li.As, s);
+        if (!li.direct) build_explicit(li, s);
     }
 }
 

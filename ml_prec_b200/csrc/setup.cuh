@@ -56,6 +56,11 @@ struct Level {
     DCSR Lf;                // L rows in frame order (R = N-Md rows, columns < M)
     DCSR Uf;                // U rows (M) with frame columns
     DCSR As;                // uh_cheb: full matrix mirrored from the lower half, frame order
+    // Triangular solves in explicit form (frame order):
+    //  P1 (rows [0, R), columns [0, R)): w = P1 s solves the L system of the
+    //     eliminated and coarse rows at once, P1 = (I + L)^{-1} restricted to them;
+    //  G  (rows [0, M), columns [0, M+n)): x_E = G [w_E; x_C] solves the U system.
+    DCSR P1, G;
     std::vector<uint32_t> lw_off;  // L wavefront d covers E rows [lw_off[d], lw_off[d+1])
     std::vector<uint32_t> uw_off;  // U wavefront d covers uw_rows[uw_off[d] .. uw_off[d+1])
     DBuf<uint32_t> uw_rows;

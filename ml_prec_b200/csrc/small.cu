@@ -1,5 +1,6 @@
 // Shared-memory-resident solve of the small coarse levels (small.cuh).
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "small.cuh"
@@ -171,6 +172,8 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_small(const SBlob* __restrict
                                                          const T* __restrict__ f, T* __restrict__ x) {
     extern __shared__ __align__(16) uint8_t sm[];
     __shared__ __align__(16) SBlob D;
+    pdl_wait();
+    pdl_trigger();
     {
         const int4* src = reinterpret_cast<const int4*>(gdesc);
         int4* dst = reinterpret_cast<int4*>(&D);
@@ -190,6 +193,36 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_small(const SBlob* __restrict
     if (D.kind == PREC_MSPLIT) s_ms<T>(D, sm, 0, at<T>(sm, D.o_f), sx);
     else s_ch<T>(D, sm, 0, at<T>(sm, D.o_f), sx);
     for (uint32_t i = threadIdx.x; i < D.lv[0].N; i += blockDim.x) x[i] = sx[i];
+}
+
+// Tabulates the small solve: block j solves with e_j and writes column j of
+// the N0 x N0 row-major operator.
+template <class T>
+__global__ void __launch_bounds__(SMALL_THREADS) k_small_columns(const SBlob* __restrict__ gdesc,
+                                                                 const uint8_t* __restrict__ gblob,
+                                                                 T* __restrict__ S) {
+    extern __shared__ __align__(16) uint8_t sm[];
+    __shared__ __align__(16) SBlob D;
+    {
+        const int4* src = reinterpret_cast<const int4*>(gdesc);
+        int4* dst = reinterpret_cast<int4*>(&D);
+        for (uint32_t i = threadIdx.x; i < sizeof(SBlob) / 16; i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+    uint32_t n = D.lv[0].N, col = blockIdx.x;
+    {
+        const int4* src = reinterpret_cast<const int4*>(gblob);
+        int4* dst = reinterpret_cast<int4*>(sm);
+        uint32_t n16 = D.bytes_static / 16;
+        for (uint32_t i = threadIdx.x; i < n16; i += blockDim.x) dst[i] = src[i];
+        T* sf = at<T>(sm, D.o_f);
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sf[i] = (i == col) ? T(1) : T(0);
+    }
+    __syncthreads();
+    T* sx = at<T>(sm, D.o_x);
+    if (D.kind == PREC_MSPLIT) s_ms<T>(D, sm, 0, at<T>(sm, D.o_f), sx);
+    else s_ch<T>(D, sm, 0, at<T>(sm, D.o_f), sx);
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) S[(size_t)i * n + col] = sx[i];
 }
 
 // ---------------------------------------------------------------------------
@@ -363,16 +396,28 @@ void build_small(Hierarchy& H, SmallPlan<T>& sp, uint32_t budget, cudaStream_t s
     if (best < 0) return;
     if (!pack<T>(H, (uint32_t)best, sp, budget, false, keep, s)) return;
     CK(cudaFuncSetAttribute(k_small<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.h.bytes_total));
+    CK(cudaFuncSetAttribute(k_small_columns<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.h.bytes_total));
     // The recursive solve nests one call per level (about 150 bytes of stack
     // each); raise the per-thread stack limit when the default is too small.
     size_t need = 256 + (size_t)(sp.h.nlev + 2) * 256, cur = 0;
     CK(cudaDeviceGetLimit(&cur, cudaLimitStackSize));
     if (cur < need) CK(cudaDeviceSetLimit(cudaLimitStackSize, need));
+    // tabulate the operator when it is small (MLP_DENSE_OP_MAX overrides the
+    // largest size, 0 turns tabulation off)
+    uint32_t dmax = 2048;
+    if (const char* e = getenv("MLP_DENSE_OP_MAX")) dmax = (uint32_t)strtoul(e, nullptr, 10);
+    if (sp.N0 && sp.N0 <= dmax) {
+        sp.dense.alloc((size_t)sp.N0 * sp.N0);
+        k_small_columns<T><<<sp.N0, SMALL_THREADS, sp.h.bytes_total, s>>>(sp.desc.p, sp.blob.p, sp.dense.p);
+        CK_LAUNCH();
+        CK(cudaStreamSynchronize(s));
+    }
 }
 
 template <class T>
 void launch_small(const SmallPlan<T>& sp, const T* f, T* x, cudaStream_t s) {
-    k_small<T><<<1, SMALL_THREADS, sp.h.bytes_total, s>>>(sp.desc.p, sp.blob.p, f, x);
+    launch_k(k_small<T>, 1, SMALL_THREADS, sp.h.bytes_total, s, (const SBlob*)sp.desc.p,
+             (const uint8_t*)sp.blob.p, f, x);
 }
 
 template void build_small<double>(Hierarchy&, SmallPlan<double>&, uint32_t, cudaStream_t);

@@ -50,6 +50,10 @@ struct SmallPlan {
     SBlob h{};
     uint32_t first = 0xffffffffu;  // level where the small solve starts
     uint32_t N0 = 0;
+    // The level solve is a fixed linear operator; when it is small enough it is
+    // tabulated once (column j = the solve applied to e_j) and every later call
+    // is one dense matrix-vector product.
+    DBuf<T> dense;                  // N0 x N0, row-major; empty if not tabulated
     bool valid() const { return first != 0xffffffffu; }
 };
 

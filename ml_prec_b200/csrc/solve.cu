@@ -28,6 +28,8 @@ __global__ void __launch_bounds__(256) k_spmv(uint32_t n, const uint32_t* __rest
                                               const uint32_t* __restrict__ ja, const T* __restrict__ a,
                                               const T* __restrict__ x, T* __restrict__ y,
                                               const T* __restrict__ f) {
+    pdl_wait();
+    pdl_trigger();
     uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t row = gid / LPR;
     int lane = gid % LPR;
@@ -42,25 +44,96 @@ __global__ void __launch_bounds__(256) k_spmv(uint32_t n, const uint32_t* __rest
     if (active && lane == 0) y[row] = f ? f[row] - s : s;
 }
 
+// Staged CSR SpMV: a CTA takes tiles of ST_ROWS consecutive rows; the tile's
+// column indices and values are copied into shared memory with 16-byte vector
+// loads (coalesced, independent of the row structure), then each thread
+// reduces one row from shared memory, gathering x through L2.
+static constexpr uint32_t ST_ROWS = 256;
+static constexpr uint32_t ST_MAX_NNZ = 3072;
+
+template <class T, int MODE>  // MODE 0: y = A x, 1: y = f - A x
+__global__ void __launch_bounds__(ST_ROWS) k_spmv_staged(uint32_t n, const uint32_t* __restrict__ ia,
+                                                         const uint32_t* __restrict__ ja, const T* __restrict__ a,
+                                                         const T* __restrict__ x, T* __restrict__ y,
+                                                         const T* __restrict__ f) {
+    pdl_wait();
+    pdl_trigger();
+    __shared__ uint32_t s_ia[ST_ROWS + 1];
+    __shared__ __align__(16) uint32_t s_ja[ST_MAX_NNZ + 8];
+    __shared__ __align__(16) T s_a[ST_MAX_NNZ + 8];
+    constexpr uint32_t VA = 16 / sizeof(T);
+    uint32_t ntiles = (n + ST_ROWS - 1) / ST_ROWS;
+    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        uint32_t r0 = t * ST_ROWS, nr = min(ST_ROWS, n - r0);
+        for (uint32_t i = threadIdx.x; i <= nr; i += blockDim.x) s_ia[i] = ia[r0 + i];
+        __syncthreads();
+        uint32_t e0 = s_ia[0], e1 = s_ia[nr];
+        uint32_t bj = e0 & ~3u, nvj = (e1 - bj + 3) / 4;
+        uint32_t ba = e0 & ~(VA - 1), nva = (e1 - ba + VA - 1) / VA;
+        const uint4* gj = reinterpret_cast<const uint4*>(ja + bj);
+        const uint4* ga = reinterpret_cast<const uint4*>(a + ba);
+        for (uint32_t v = threadIdx.x; v < nvj; v += blockDim.x) reinterpret_cast<uint4*>(s_ja)[v] = gj[v];
+        for (uint32_t v = threadIdx.x; v < nva; v += blockDim.x) reinterpret_cast<uint4*>(s_a)[v] = ga[v];
+        __syncthreads();
+        if (threadIdx.x < nr) {
+            T acc = 0;
+            uint32_t je = s_ia[threadIdx.x + 1];
+            for (uint32_t j = s_ia[threadIdx.x]; j < je; j++) acc += s_a[j - ba] * x[s_ja[j - bj]];
+            uint32_t row = r0 + threadIdx.x;
+            y[row] = MODE ? f[row] - acc : acc;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_tile_max(uint32_t n, const uint32_t* __restrict__ ia, uint32_t* __restrict__ out) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t r0 = t * ST_ROWS;
+    if (r0 >= n) return;
+    uint32_t r1 = min(n, r0 + ST_ROWS);
+    atomicMax(out, ia[r1] - ia[r0]);
+}
+
+void csr_tile_stats(DCSR& m, cudaStream_t s) {
+    if (!m.nrow) { m.tile_max = 0; return; }
+    DBuf<uint32_t> d(1);
+    d.zero(s);
+    uint32_t nt = (m.nrow + ST_ROWS - 1) / ST_ROWS;
+    k_tile_max<<<grid_for(nt, 256), 256, 0, s>>>(m.nrow, m.ia.p, d.p);
+    CK_LAUNCH();
+    CK(cudaMemcpyAsync(&m.tile_max, d.p, 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+}
+
+static unsigned staged_grid(uint32_t n) {
+    uint32_t nt = (n + ST_ROWS - 1) / ST_ROWS;
+    return (unsigned)std::max<uint32_t>(1, std::min<uint32_t>(nt, (uint32_t)num_sms() * 5));
+}
+
 template <class T>
 static void launch_spmv(uint32_t n, uint32_t nnz, const uint32_t* ia, const uint32_t* ja, const T* a, const T* x,
-                        T* y, const T* f, cudaStream_t s) {
+                        T* y, const T* f, cudaStream_t s, uint32_t tile_max = 0) {
     if (!n) return;
+    if (tile_max && tile_max <= ST_MAX_NNZ && n >= 4 * ST_ROWS) {
+        if (f) launch_k(k_spmv_staged<T, 1>, staged_grid(n), ST_ROWS, 0, s, n, ia, ja, a, x, y, f);
+        else launch_k(k_spmv_staged<T, 0>, staged_grid(n), ST_ROWS, 0, s, n, ia, ja, a, x, y, f);
+        return;
+    }
     double avg = (double)nnz / n;
     int lpr = avg <= 1.5 ? 1 : avg <= 3 ? 2 : avg <= 6 ? 4 : avg <= 12 ? 8 : avg <= 24 ? 16 : 32;
     unsigned blocks = grid_for((size_t)n * lpr, 256);
     switch (lpr) {
-        case 1: k_spmv<T, 1><<<blocks, 256, 0, s>>>(n, ia, ja, a, x, y, f); break;
-        case 2: k_spmv<T, 2><<<blocks, 256, 0, s>>>(n, ia, ja, a, x, y, f); break;
-        case 4: k_spmv<T, 4><<<blocks, 256, 0, s>>>(n, ia, ja, a, x, y, f); break;
-        case 8: k_spmv<T, 8><<<blocks, 256, 0, s>>>(n, ia, ja, a, x, y, f); break;
-        case 16: k_spmv<T, 16><<<blocks, 256, 0, s>>>(n, ia, ja, a, x, y, f); break;
-        default: k_spmv<T, 32><<<blocks, 256, 0, s>>>(n, ia, ja, a, x, y, f); break;
+        case 1: launch_k(k_spmv<T, 1>, blocks, 256, 0, s, n, ia, ja, a, x, y, f); break;
+        case 2: launch_k(k_spmv<T, 2>, blocks, 256, 0, s, n, ia, ja, a, x, y, f); break;
+        case 4: launch_k(k_spmv<T, 4>, blocks, 256, 0, s, n, ia, ja, a, x, y, f); break;
+        case 8: launch_k(k_spmv<T, 8>, blocks, 256, 0, s, n, ia, ja, a, x, y, f); break;
+        case 16: launch_k(k_spmv<T, 16>, blocks, 256, 0, s, n, ia, ja, a, x, y, f); break;
+        default: launch_k(k_spmv<T, 32>, blocks, 256, 0, s, n, ia, ja, a, x, y, f); break;
     }
 }
 
 void spmv(const DCSR& A, const double* x, double* y, cudaStream_t s) {
-    launch_spmv<double>(A.nrow, A.nnz, A.ia.p, A.ja.p, A.a.p, x, y, nullptr, s);
+    launch_spmv<double>(A.nrow, A.nnz, A.ia.p, A.ja.p, A.a.p, x, y, nullptr, s, A.tile_max);
     CK_LAUNCH();
 }
 
@@ -69,6 +142,8 @@ void spmv(const DCSR& A, const double* x, double* y, cudaStream_t s) {
 template <class T>
 __global__ void k_lwave(uint32_t r0, uint32_t r1, const uint32_t* __restrict__ ia, const uint32_t* __restrict__ ja,
                         const T* __restrict__ a, const T* __restrict__ src, T* __restrict__ w) {
+    pdl_wait();
+    pdl_trigger();
     uint32_t q = r0 + blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= r1) return;
     T s = src[q];
@@ -83,6 +158,8 @@ template <class T>
 __global__ void k_lcoarse_diag(uint32_t M, uint32_t R, uint32_t N, const uint32_t* __restrict__ ia,
                                const uint32_t* __restrict__ ja, const T* __restrict__ a, const T* __restrict__ src,
                                T* __restrict__ w, const T* __restrict__ dval, T* __restrict__ out) {
+    pdl_wait();
+    pdl_trigger();
     uint32_t q = M + blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= N) return;
     if (q < R) {
@@ -100,6 +177,8 @@ template <class T>
 __global__ void k_uwave(uint32_t cnt, const uint32_t* __restrict__ rows, const uint32_t* __restrict__ ia,
                         const uint32_t* __restrict__ ja, const T* __restrict__ a, const T* __restrict__ w,
                         T* __restrict__ out) {
+    pdl_wait();
+    pdl_trigger();
     uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= cnt) return;
     uint32_t q = rows[t];
@@ -119,6 +198,8 @@ __global__ void __launch_bounds__(TAIL_THREADS) k_lwave_tail(uint32_t d0, uint32
                                                              const uint32_t* __restrict__ ia,
                                                              const uint32_t* __restrict__ ja, const T* __restrict__ a,
                                                              const T* __restrict__ src, T* w) {
+    pdl_wait();
+    pdl_trigger();
     for (uint32_t d = d0; d < d1; d++) {
         uint32_t r0 = off[d], r1 = off[d + 1];
         for (uint32_t q = r0 + threadIdx.x; q < r1; q += blockDim.x) {
@@ -136,6 +217,8 @@ __global__ void __launch_bounds__(TAIL_THREADS) k_uwave_tail(uint32_t d0, uint32
                                                              const uint32_t* __restrict__ ia,
                                                              const uint32_t* __restrict__ ja, const T* __restrict__ a,
                                                              const T* __restrict__ w, T* out) {
+    pdl_wait();
+    pdl_trigger();
     for (uint32_t d = d0; d < d1; d++) {
         uint32_t o0 = off[d], o1 = off[d + 1];
         for (uint32_t t = o0 + threadIdx.x; t < o1; t += blockDim.x) {
@@ -159,18 +242,24 @@ static size_t tail_start(const std::vector<uint32_t>& off) {
 
 template <class T>
 __global__ void k_axpy1(uint32_t n, T* __restrict__ x, const T* __restrict__ u) {
+    pdl_wait();
+    pdl_trigger();
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) x[i] += u[i];
 }
 
 template <class T>
 __global__ void k_scale(uint32_t n, T* __restrict__ x, T alpha) {
+    pdl_wait();
+    pdl_trigger();
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) x[i] *= alpha;
 }
 
 template <class T>
 __global__ void k_copy(uint32_t n, const T* __restrict__ src, T* __restrict__ dst) {
+    pdl_wait();
+    pdl_trigger();
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) dst[i] = src[i];
 }
@@ -178,6 +267,8 @@ __global__ void k_copy(uint32_t n, const T* __restrict__ src, T* __restrict__ ds
 // Chebyshev step 2 (cheb_solve.cc:70-72): x2 = -alpha*x2 + c*u1
 template <class T>
 __global__ void k_cheb2(uint32_t n, T* __restrict__ x2, const T* __restrict__ u1, T malpha, T c) {
+    pdl_wait();
+    pdl_trigger();
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) x2[i] = x2[i] * malpha + c * u1[i];
 }
@@ -185,6 +276,8 @@ __global__ void k_cheb2(uint32_t n, T* __restrict__ x2, const T* __restrict__ u1
 template <class T>
 __global__ void k_chebk(uint32_t n, T* __restrict__ x2, const T* __restrict__ u1, const T* __restrict__ u0,
                         T alpha, T beta) {
+    pdl_wait();
+    pdl_trigger();
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) x2[i] = u1[i] - alpha * x2[i] + beta * (u1[i] - u0[i]);
 }
@@ -192,6 +285,8 @@ __global__ void k_chebk(uint32_t n, T* __restrict__ x2, const T* __restrict__ u1
 // Dense coarsest level: x = C^{-1} f, one warp per row.
 template <class T>
 __global__ void k_dense_gemv(uint32_t n, const T* __restrict__ C, const T* __restrict__ f, T* __restrict__ x) {
+    pdl_wait();
+    pdl_trigger();
     uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
     if (row >= n) return;
@@ -204,10 +299,14 @@ __global__ void k_dense_gemv(uint32_t n, const T* __restrict__ C, const T* __res
 }
 
 __global__ void k_to_f32(uint32_t n, const double* __restrict__ a, float* __restrict__ b) {
+    pdl_wait();
+    pdl_trigger();
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) b[i] = (float)a[i];
 }
 __global__ void k_to_f64(uint32_t n, const float* __restrict__ a, double* __restrict__ b) {
+    pdl_wait();
+    pdl_trigger();
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) b[i] = (double)a[i];
 }
@@ -232,6 +331,105 @@ void scatter(uint32_t n, const uint32_t* idx, const double* src, double* dst, cu
     k_scatter<<<grid_for(n, 256), 256, 0, s>>>(n, idx, src, dst);
     CK_LAUNCH();
 }
+
+
+// ---- explicit-form sweep kernels -------------------------------------------
+// Phase 1 of a level solve: w = P1 src on rows [0, R) (the L solve of the
+// eliminated and coarse rows) and out = dval * src on the diagonal rows
+// [R, N). The first nb1 blocks take the P1 rows with LPR lanes per row, the
+// rest one diagonal row per thread.
+template <class T, int LPR>
+__global__ void __launch_bounds__(256) k_phase1(uint32_t R, uint32_t N, uint32_t nb1, const uint32_t* __restrict__ ia,
+                                                const uint32_t* __restrict__ ja, const T* __restrict__ a,
+                                                const T* __restrict__ dval, const T* __restrict__ src,
+                                                T* __restrict__ w, T* __restrict__ out) {
+    pdl_wait();
+    pdl_trigger();
+    if (blockIdx.x < nb1) {
+        uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+        uint32_t row = gid / LPR;
+        int lane = gid % LPR;
+        bool active = row < R;
+        T s = 0;
+        if (active) {
+            uint32_t e = ia[row + 1];
+            for (uint32_t j = ia[row] + lane; j < e; j += LPR) s += a[j] * src[ja[j]];
+        }
+#pragma unroll
+        for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (active && lane == 0) w[row] = s;
+    } else {
+        uint32_t q = R + (blockIdx.x - nb1) * blockDim.x + threadIdx.x;
+        if (q < N) out[q] = dval[q - R] * src[q];
+    }
+}
+
+// Phase 2: out_q = sum_j G_qj y_j on the eliminated rows q < M, where
+// y_j = w_j for eliminated columns (j < M) and out_j (the coarse solution the
+// recursion wrote) for coarse columns.
+template <class T, int LPR>
+__global__ void __launch_bounds__(256) k_phase2(uint32_t M, const uint32_t* __restrict__ ia,
+                                                const uint32_t* __restrict__ ja, const T* __restrict__ a,
+                                                const T* __restrict__ w, T* out) {
+    pdl_wait();
+    pdl_trigger();
+    uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t row = gid / LPR;
+    int lane = gid % LPR;
+    bool active = row < M;
+    T s = 0;
+    if (active) {
+        uint32_t e = ia[row + 1];
+        for (uint32_t j = ia[row] + lane; j < e; j += LPR) {
+            uint32_t c = ja[j];
+            s += a[j] * (c < M ? w[c] : out[c]);
+        }
+    }
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (active && lane == 0) out[row] = s;
+}
+
+// Correction step of a level sweep: x += u0 and, when more sweeps follow,
+// r -= A u0 (the residual f - A x updated in place of recomputing it).
+template <class T, int LPR>
+__global__ void __launch_bounds__(256) k_update(uint32_t n, const uint32_t* __restrict__ ia,
+                                                const uint32_t* __restrict__ ja, const T* __restrict__ a,
+                                                const T* __restrict__ u0, T* __restrict__ x, T* __restrict__ r,
+                                                int do_r) {
+    pdl_wait();
+    pdl_trigger();
+    uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t row = gid / LPR;
+    int lane = gid % LPR;
+    bool active = row < n;
+    T s = 0;
+    if (active && do_r) {
+        uint32_t e = ia[row + 1];
+        for (uint32_t j = ia[row] + lane; j < e; j += LPR) s += a[j] * u0[ja[j]];
+    }
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (active && lane == 0) {
+        x[row] += u0[row];
+        if (do_r) r[row] -= s;
+    }
+}
+
+static int pick_lpr(uint32_t n, uint32_t nnz) {
+    double avg = n ? (double)nnz / n : 1;
+    return avg <= 1.5 ? 1 : avg <= 3 ? 2 : avg <= 6 ? 4 : avg <= 12 ? 8 : avg <= 24 ? 16 : 32;
+}
+
+#define LPR_SWITCH(lpr, KERNEL, ...)                                      \
+    switch (lpr) {                                                        \
+        case 1: launch_k(KERNEL<T, 1>, __VA_ARGS__); break;               \
+        case 2: launch_k(KERNEL<T, 2>, __VA_ARGS__); break;               \
+        case 4: launch_k(KERNEL<T, 4>, __VA_ARGS__); break;               \
+        case 8: launch_k(KERNEL<T, 8>, __VA_ARGS__); break;               \
+        case 16: launch_k(KERNEL<T, 16>, __VA_ARGS__); break;             \
+        default: launch_k(KERNEL<T, 32>, __VA_ARGS__); break;             \
+    }
 
 // ---------------------------------------------------------------------------
 // Plan builder: replays the reference's recursion once on the host and records
@@ -269,6 +467,15 @@ struct Builder {
     bool small_call(uint32_t l, const T* f, T* x) {
         if (!small || !small->valid() || l != small->first) return false;
         const SmallPlan<T>* sp = small;
+        if (sp->dense.p) {
+            uint32_t n = sp->N0;
+            const T* C = sp->dense.p;
+            op([=](cudaStream_t s) {
+                launch_k(k_dense_gemv<T>, grid_for((size_t)n * 32, 256), 256, 0, s, n, C, f, x);
+            });
+            bytes += (uint64_t)n * n * sizeof(T) + 2ull * n * sizeof(T);
+            return true;
+        }
         op([=](cudaStream_t s) { launch_small<T>(*sp, f, x, s); });
         bytes += sp->h.bytes_static + 2ull * sizeof(T) * sp->N0;
         return true;
@@ -288,13 +495,13 @@ struct Builder {
         for (size_t d = 0; d < dt; d++) {
             uint32_t r0 = L.lw_off[d], r1 = L.lw_off[d + 1];
             if (r1 <= r0) continue;
-            op([=](cudaStream_t s) { k_lwave<T><<<grid_for(r1 - r0, 128), 128, 0, s>>>(r0, r1, ia, ja, a, src, w); });
+            op([=](cudaStream_t s) { launch_k(k_lwave<T>, grid_for(r1 - r0, 128), 128, 0, s, r0, r1, ia, ja, a, src, w); });
         }
         if (dt < nw) {
             const uint32_t* off = L.lw_off_d.p;
             uint32_t d0 = (uint32_t)dt, d1 = (uint32_t)nw;
             op([=](cudaStream_t s) {
-                k_lwave_tail<T><<<1, TAIL_THREADS, 0, s>>>(d0, d1, off, ia, ja, a, src, w);
+                launch_k(k_lwave_tail<T>, 1, TAIL_THREADS, 0, s, d0, d1, off, ia, ja, a, src, w);
             });
         }
     }
@@ -306,7 +513,7 @@ struct Builder {
         const T* a = vals<T>(L.Lf);
         const T* dv = dvals<T>(L);
         op([=](cudaStream_t s) {
-            k_lcoarse_diag<T><<<grid_for(N - M, 128), 128, 0, s>>>(M, R, N, ia, ja, a, src, w, dv, out);
+            launch_k(k_lcoarse_diag<T>, grid_for(N - M, 128), 128, 0, s, M, R, N, ia, ja, a, src, w, dv, out);
         });
     }
     void usolve(const Level& L, const T* w, T* out) {
@@ -320,23 +527,65 @@ struct Builder {
             uint32_t o0 = L.uw_off[d], o1 = L.uw_off[d + 1];
             if (o1 <= o0) continue;
             op([=](cudaStream_t s) {
-                k_uwave<T><<<grid_for(o1 - o0, 128), 128, 0, s>>>(o1 - o0, rows + o0, ia, ja, a, w, out);
+                launch_k(k_uwave<T>, grid_for(o1 - o0, 128), 128, 0, s, o1 - o0, rows + o0, ia, ja, a, w, out);
             });
         }
         if (dt < nw) {
             const uint32_t* off = L.uw_off_d.p;
             uint32_t d0 = (uint32_t)dt, d1 = (uint32_t)nw;
             op([=](cudaStream_t s) {
-                k_uwave_tail<T><<<1, TAIL_THREADS, 0, s>>>(d0, d1, off, rows, ia, ja, a, w, out);
+                launch_k(k_uwave_tail<T>, 1, TAIL_THREADS, 0, s, d0, d1, off, rows, ia, ja, a, w, out);
             });
         }
     }
     void direct(const Level& L, const T* f, T* x) {
         uint32_t n = L.N;
         const T* C = cinv<T>(L);
-        op([=](cudaStream_t s) { k_dense_gemv<T><<<grid_for((size_t)n * 32, 256), 256, 0, s>>>(n, C, f, x); });
+        op([=](cudaStream_t s) { launch_k(k_dense_gemv<T>, grid_for((size_t)n * 32, 256), 256, 0, s, n, C, f, x); });
         bytes += (uint64_t)n * n * sizeof(T) + 2ull * n * sizeof(T);
     }
+    // One application of the level's split operator on src: phase 1 (L solve
+    // and diagonal block), the recursion on the coarse slice, phase 2 (U solve).
+    void phase1(const Level& L, const T* src, T* w, T* out) {
+        uint32_t R = L.N - L.Md, N = L.N;
+        int lpr = pick_lpr(R, L.P1.nnz);
+        uint32_t nb1 = R ? grid_for((size_t)R * lpr, 256) : 0;
+        uint32_t nb2 = N > R ? grid_for(N - R, 256) : 0;
+        if (!nb1 && !nb2) return;
+        const uint32_t* ia = L.P1.ia.p;
+        const uint32_t* ja = L.P1.ja.p;
+        const T* a = vals<T>(L.P1);
+        const T* dv = dvals<T>(L);
+        op([=](cudaStream_t s) {
+            LPR_SWITCH(lpr, k_phase1, nb1 + nb2, 256, 0, s, R, N, nb1, ia, ja, a, dv, src, w, out);
+        });
+        bytes += (uint64_t)L.P1.nnz * (4 + sizeof(T)) + 4ull * (R + 1) + sizeof(T) * (2ull * N + L.Md) ;
+    }
+    void phase2(const Level& L, const T* w, T* out) {
+        uint32_t M = L.M;
+        if (!M) return;
+        int lpr = pick_lpr(M, L.G.nnz);
+        const uint32_t* ia = L.G.ia.p;
+        const uint32_t* ja = L.G.ja.p;
+        const T* a = vals<T>(L.G);
+        op([=](cudaStream_t s) {
+            LPR_SWITCH(lpr, k_phase2, grid_for((size_t)M * lpr, 256), 256, 0, s, M, ia, ja, a, w, out);
+        });
+        bytes += (uint64_t)L.G.nnz * (4 + sizeof(T)) + 4ull * (M + 1) + sizeof(T) * (M + L.n + M);
+    }
+    void update(const Level& L, const T* u0, T* x, T* r, bool do_r) {
+        uint32_t N = L.N;
+        int lpr = do_r ? pick_lpr(N, L.Af.nnz) : 1;
+        const uint32_t* ia = L.Af.ia.p;
+        const uint32_t* ja = L.Af.ja.p;
+        const T* a = vals<T>(L.Af);
+        int dr = do_r ? 1 : 0;
+        op([=](cudaStream_t s) {
+            LPR_SWITCH(lpr, k_update, grid_for((size_t)N * lpr, 256), 256, 0, s, N, ia, ja, a, u0, x, r, dr);
+        });
+        bytes += sizeof(T) * 3ull * N + (do_r ? spmv_bytes(L.Af) : 0);
+    }
+
     uint64_t sweep_bytes(const Level& L) const {
         // L (E and coarse rows), U, dval, src/w/out vectors
         uint64_t b = (uint64_t)L.Lf.nnz * (4 + sizeof(T)) + 4ull * (L.N - L.Md + 1);
@@ -349,11 +598,43 @@ struct Builder {
         return (uint64_t)A.nnz * (4 + sizeof(T)) + 4ull * (A.nrow + 1) + 3ull * sizeof(T) * A.nrow;
     }
 
-    // MultiSplitPrec::solve(level, f, x) (multi_split_solve.cc:59-157)
+    // MultiSplitPrec::solve(level, f, x) (multi_split_solve.cc:59-157) with the
+    // triangular solves in explicit form: each sweep is phase 1, the recursion
+    // and phase 2; the correction sweeps update the residual in place.
     void ms(uint32_t l, const T* f, T* x) {
         if (small_call(l, f, x)) return;
         Level& L = *H.lv[l];
         if (L.direct) { direct(L, f, x); return; }
+        if (!explicit_solves) { ms_waves(l, f, x); return; }
+        LevelWork<T>& w = W[l];
+        uint32_t N = L.N, M = L.M;
+        bool next = l + 1 < H.nlevels && L.n;
+        phase1(L, f, w.w.p, x);
+        if (next) ms(l + 1, w.w.p + M, x + M);
+        phase2(L, w.w.p, x);
+        if (L.niter < 2) return;
+        {
+            const uint32_t* ia = L.Af.ia.p;
+            const uint32_t* ja = L.Af.ja.p;
+            const T* a = vals<T>(L.Af);
+            uint32_t nnz = L.Af.nnz, tm = L.Af.tile_max;
+            T* r = w.r.p;
+            op([=](cudaStream_t s) { launch_spmv<T>(N, nnz, ia, ja, a, x, r, f, s, tm); });
+            bytes += spmv_bytes(L.Af);
+        }
+        for (uint32_t it = 2; it <= L.niter; it++) {
+            phase1(L, w.r.p, w.w.p, w.u0.p);
+            if (next) ms(l + 1, w.w.p + M, w.u0.p + M);
+            phase2(L, w.w.p, w.u0.p);
+            update(L, w.u0.p, x, w.r.p, it < L.niter);
+        }
+    }
+
+    bool explicit_solves = true;
+
+    // Wavefront form of ms (the L and U solves one wavefront at a time).
+    void ms_waves(uint32_t l, const T* f, T* x) {
+        Level& L = *H.lv[l];
         LevelWork<T>& w = W[l];
         uint32_t N = L.N, M = L.M;
         bool has_next = l + 1 < H.nlevels;
@@ -376,7 +657,7 @@ struct Builder {
             if (has_next && L.n) ms(l + 1, w.w.p + M, w.u0.p + M);
             usolve(L, w.w.p, w.u0.p);
             T* u0 = w.u0.p;
-            op([=](cudaStream_t s) { k_axpy1<T><<<grid_for(N, 256), 256, 0, s>>>(N, x, u0); });
+            op([=](cudaStream_t s) { launch_k(k_axpy1<T>, grid_for(N, 256), 256, 0, s, N, x, (const T*)u0); });
             bytes += sweep_bytes(L) + spmv_bytes(L.Af) + 3ull * sizeof(T) * N;
         }
     }
@@ -387,9 +668,13 @@ struct Builder {
         Level& L = *H.lv[l];
         LevelWork<T>& w = W[l];
         uint32_t M = L.M;
-        lsolve(L, f, w.w.p);
-        coarse_diag(L, f, w.w.p, x);
-        bytes += sweep_bytes(L);
+        if (explicit_solves) {
+            phase1(L, f, w.w.p, x);
+        } else {
+            lsolve(L, f, w.w.p);
+            coarse_diag(L, f, w.w.p, x);
+            bytes += sweep_bytes(L);
+        }
         if (l + 1 < H.nlevels) {
             Level& Ln = *H.lv[l + 1];
             uint32_t n = Ln.N, nch = L.ncheb;
@@ -400,44 +685,45 @@ struct Builder {
             const uint32_t* sia = Ln.As.ia.p;
             const uint32_t* sja = Ln.As.ja.p;
             const T* sa = vals<T>(Ln.As);
-            uint32_t snnz = Ln.As.nnz;
+            uint32_t snnz = Ln.As.nnz, stm = Ln.As.tile_max;
             double alpha = 2 / (lmax + lmin), beta;
             auto scale = [&](T* v, double al) {
                 if (is_equal1(al)) return;
                 T a = (T)al;
-                op([=](cudaStream_t s) { k_scale<T><<<grid_for(n, 256), 256, 0, s>>>(n, v, a); });
+                op([=](cudaStream_t s) { launch_k(k_scale<T>, grid_for(n, 256), 256, 0, s, n, v, a); });
             };
             if (nch > 1) { ch(l + 1, F, u1); scale(u1, alpha); }
             else { ch(l + 1, F, x2); scale(x2, alpha); }
             if (nch > 1) {
                 alpha = 4 / (lmax - lmin) * cheb_poly(eta, 1) / cheb_poly(eta, 2);
                 beta = cheb_poly(eta, 0) / cheb_poly(eta, 2);
-                op([=](cudaStream_t s) { launch_spmv<T>(n, snnz, sia, sja, sa, u1, tmp, F, s); });
+                op([=](cudaStream_t s) { launch_spmv<T>(n, snnz, sia, sja, sa, u1, tmp, F, s, stm); });
                 // tmp = F - A u1 above; the reference forms A u1 - F: negate via the scalars
                 ch(l + 1, tmp, x2);
                 // x2 := -alpha * solve(A u1 - F) + (1+beta) u1 = alpha * solve(F - A u1) + (1+beta) u1
                 double c = is_equal1(1 + beta) ? 1.0 : 1 + beta;
                 T ma = (T)alpha, cc = (T)c;
-                op([=](cudaStream_t s) { k_cheb2<T><<<grid_for(n, 256), 256, 0, s>>>(n, x2, u1, ma, cc); });
+                op([=](cudaStream_t s) { launch_k(k_cheb2<T>, grid_for(n, 256), 256, 0, s, n, x2, (const T*)u1, ma, cc); });
                 bytes += spmv_bytes(Ln.As) + 3ull * sizeof(T) * n;
             }
             for (uint32_t i = 3; i <= nch; i++) {
                 T* t = u0; u0 = u1; u1 = x2; x2 = t;  // cheb_solve.cc:87-89
                 alpha = 4 / (lmax - lmin) * cheb_poly(eta, i - 1) / cheb_poly(eta, i);
                 beta = cheb_poly(eta, i - 2) / cheb_poly(eta, i);
-                op([=](cudaStream_t s) { launch_spmv<T>(n, snnz, sia, sja, sa, u1, tmp, F, s); });
+                op([=](cudaStream_t s) { launch_spmv<T>(n, snnz, sia, sja, sa, u1, tmp, F, s, stm); });
                 ch(l + 1, tmp, x2);
                 // x2 = u1 - alpha*solve(A u1 - F) + beta*(u1-u0) = u1 + alpha*solve(F - A u1) + ...
                 T ma = (T)(-alpha), bb = (T)beta;
                 T* u0c = u0; T* u1c = u1; T* x2c = x2;
-                op([=](cudaStream_t s) { k_chebk<T><<<grid_for(n, 256), 256, 0, s>>>(n, x2c, u1c, u0c, ma, bb); });
+                op([=](cudaStream_t s) { launch_k(k_chebk<T>, grid_for(n, 256), 256, 0, s, n, x2c, (const T*)u1c, (const T*)u0c, ma, bb); });
                 bytes += spmv_bytes(Ln.As) + 4ull * sizeof(T) * n;
             }
             T* xo = x + M;
             T* fin = x2;
-            op([=](cudaStream_t s) { k_copy<T><<<grid_for(n, 256), 256, 0, s>>>(n, fin, xo); });
+            op([=](cudaStream_t s) { launch_k(k_copy<T>, grid_for(n, 256), 256, 0, s, n, (const T*)fin, xo); });
         }
-        usolve(L, w.w.p, x);
+        if (explicit_solves) phase2(L, w.w.p, x);
+        else usolve(L, w.w.p, x);
     }
 };
 
@@ -497,11 +783,14 @@ std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, c
     P->fout_buf.alloc(N0);
     P->fin = P->fin_buf.p;
     P->fout = P->fout_buf.p;
+    const char* ex = getenv("MLP_EXPLICIT");
+    bool explicit_solves = !(ex && ex[0] == '0');
     if (!fp32) {
         alloc_work<double>(H, P->w64);
         P->sp64.reset(new SmallPlan<double>());
         if (small_budget()) build_small<double>(H, *P->sp64, small_budget(), s);
         Builder<double> B{H, P->w64, P->plan, P->sp64.get()};
+        B.explicit_solves = explicit_solves;
         if (H.kind == PREC_MSPLIT) B.ms(0, P->fin, P->fout);
         else B.ch(0, P->fin, P->fout);
         P->bytes_per_apply = B.bytes;
@@ -509,6 +798,7 @@ std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, c
         for (uint32_t l = 0; l < H.nlevels; l++) {
             Level& L = *H.lv[l];
             make_f32(L.Lf, s); make_f32(L.Uf, s); make_f32(L.Af, s);
+            if (!L.direct) { make_f32(L.P1, s); make_f32(L.G, s); }
             if (H.kind == PREC_CHEB && l > 0) make_f32(L.As, s);
             make_f32(L.dval, L.dval32, L.Md, s);
             if (L.direct) make_f32(L.cinv, L.cinv32, (size_t)L.N * L.N, s);
@@ -519,14 +809,15 @@ std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, c
         P->f32.alloc(N0);
         P->z32.alloc(N0);
         Builder<float> B{H, P->w32, P->plan, P->sp32.get()};
+        B.explicit_solves = explicit_solves;
         const double* fin = P->fin;
         float* f32 = P->f32.p;
-        B.op([=](cudaStream_t st) { k_to_f32<<<grid_for(N0, 256), 256, 0, st>>>(N0, fin, f32); });
+        B.op([=](cudaStream_t st) { launch_k(k_to_f32, grid_for(N0, 256), 256, 0, st, N0, fin, f32); });
         if (H.kind == PREC_MSPLIT) B.ms(0, P->f32.p, P->z32.p);
         else B.ch(0, P->f32.p, P->z32.p);
         float* z32 = P->z32.p;
         double* fout = P->fout;
-        B.op([=](cudaStream_t st) { k_to_f64<<<grid_for(N0, 256), 256, 0, st>>>(N0, z32, fout); });
+        B.op([=](cudaStream_t st) { launch_k(k_to_f64, grid_for(N0, 256), 256, 0, st, N0, (const float*)z32, fout); });
         P->bytes_per_apply = B.bytes + 12ull * N0 * 2;
     }
     CK(cudaStreamSynchronize(s));
@@ -619,6 +910,49 @@ __global__ void __launch_bounds__(RB) k_pcg_spmv_dot(uint32_t n, const uint32_t*
             Ap[row] = s;
             part += s * p[row];
         }
+    }
+    part = block_sum(part);
+    double tot;
+    if (finish_reduce(part, partials, &d->ticket[0], &tot) && threadIdx.x == 0) {
+        d->app = tot;
+        if (!(tot > 0)) d->status |= (tot != tot) ? 2 : 1;
+        d->alpha = d->rz0 / tot;
+    }
+}
+
+// Staged form of k_pcg_spmv_dot (same tiles as k_spmv_staged).
+__global__ void __launch_bounds__(ST_ROWS) k_pcg_spmv_dot_staged(uint32_t n, const uint32_t* __restrict__ ia,
+                                                                 const uint32_t* __restrict__ ja,
+                                                                 const double* __restrict__ a,
+                                                                 const double* __restrict__ p,
+                                                                 double* __restrict__ Ap, double* partials,
+                                                                 PcgDev* d) {
+    __shared__ uint32_t s_ia[ST_ROWS + 1];
+    __shared__ __align__(16) uint32_t s_ja[ST_MAX_NNZ + 8];
+    __shared__ __align__(16) double s_a[ST_MAX_NNZ + 8];
+    double part = 0;
+    uint32_t ntiles = (n + ST_ROWS - 1) / ST_ROWS;
+    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        uint32_t r0 = t * ST_ROWS, nr = min(ST_ROWS, n - r0);
+        for (uint32_t i = threadIdx.x; i <= nr; i += blockDim.x) s_ia[i] = ia[r0 + i];
+        __syncthreads();
+        uint32_t e0 = s_ia[0], e1 = s_ia[nr];
+        uint32_t bj = e0 & ~3u, nvj = (e1 - bj + 3) / 4;
+        uint32_t ba = e0 & ~1u, nva = (e1 - ba + 1) / 2;
+        const uint4* gj = reinterpret_cast<const uint4*>(ja + bj);
+        const uint4* ga = reinterpret_cast<const uint4*>(a + ba);
+        for (uint32_t v = threadIdx.x; v < nvj; v += blockDim.x) reinterpret_cast<uint4*>(s_ja)[v] = gj[v];
+        for (uint32_t v = threadIdx.x; v < nva; v += blockDim.x) reinterpret_cast<uint4*>(s_a)[v] = ga[v];
+        __syncthreads();
+        if (threadIdx.x < nr) {
+            double acc = 0;
+            uint32_t je = s_ia[threadIdx.x + 1];
+            for (uint32_t j = s_ia[threadIdx.x]; j < je; j++) acc += s_a[j - ba] * p[s_ja[j - bj]];
+            uint32_t row = r0 + threadIdx.x;
+            Ap[row] = acc;
+            part += acc * p[row];
+        }
+        __syncthreads();
     }
     part = block_sum(part);
     double tot;
@@ -747,7 +1081,7 @@ int pcg_solve(const DCSR& A, const double* b, Prec& P, double* x, double eps, ui
     gather(n, L0.phi.p, b, bf.p, s);
     gather(n, L0.phi.p, x0_device(n, s), xf.p, s);
     // r = b - A x
-    launch_spmv<double>(n, Af.nnz, Af.ia.p, Af.ja.p, Af.a.p, xf.p, r, bf.p, s);
+    launch_spmv<double>(n, Af.nnz, Af.ia.p, Af.ja.p, Af.a.p, xf.p, r, bf.p, s, Af.tile_max);
     CK_LAUNCH();
     double* hpin = nullptr;
     CK(cudaMallocHost(&hpin, sizeof(PcgDev)));
@@ -775,9 +1109,14 @@ int pcg_solve(const DCSR& A, const double* b, Prec& P, double* x, double eps, ui
     int lpr = avg <= 3 ? 2 : avg <= 6 ? 4 : avg <= 12 ? 8 : avg <= 24 ? 16 : 32;
     int rc = OK;
     std::string msg;
+    bool staged = Af.tile_max && Af.tile_max <= ST_MAX_NNZ && n >= 4 * ST_ROWS;
+    unsigned Gs = staged_grid(n);
+    if (staged && 2 * (size_t)Gs > partials.n) partials.alloc(2 * (size_t)Gs);
     while (norm / init > eps) {
         if (maxit && it >= maxit) { rc = ERR_MAXIT; msg = "iteration cap reached"; break; }
-        switch (lpr) {
+        if (staged) {
+            k_pcg_spmv_dot_staged<<<Gs, ST_ROWS, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p.p, Ap.p, partials.p, d);
+        } else switch (lpr) {
             case 2: k_pcg_spmv_dot<2><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p.p, Ap.p, partials.p, d); break;
             case 4: k_pcg_spmv_dot<4><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p.p, Ap.p, partials.p, d); break;
             case 8: k_pcg_spmv_dot<8><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p.p, Ap.p, partials.p, d); break;
@@ -911,7 +1250,7 @@ int pcg_solve_noalloc(const DCSR& A, const double* b, Prec& P, double* x, double
     }
     gather(n, L0.phi.p, b, bf, s);
     gather(n, L0.phi.p, p, xf, s);
-    launch_spmv<double>(n, Af.nnz, Af.ia.p, Af.ja.p, Af.a.p, xf, r, bf, s);
+    launch_spmv<double>(n, Af.nnz, Af.ia.p, Af.ja.p, Af.a.p, xf, r, bf, s, Af.tile_max);
     CK_LAUNCH();
     auto fetch = [&]() -> PcgDev {
         PcgDev h;
@@ -935,9 +1274,14 @@ int pcg_solve_noalloc(const DCSR& A, const double* b, Prec& P, double* x, double
     int lpr = avg <= 3 ? 2 : avg <= 6 ? 4 : avg <= 12 ? 8 : avg <= 24 ? 16 : 32;
     int rc = OK;
     std::string msg;
+    bool staged = Af.tile_max && Af.tile_max <= ST_MAX_NNZ && n >= 4 * ST_ROWS;
+    unsigned Gs = staged_grid(n);
+    if (staged && Gs > 2 * NOALLOC_GRID) MLP_THROW(ERR_LIMIT, "reduction grid exceeds the static scratch");
     while (norm / init > eps) {
         if (maxit && it >= maxit) { rc = ERR_MAXIT; msg = "iteration cap reached"; break; }
-        switch (lpr) {
+        if (staged) {
+            k_pcg_spmv_dot_staged<<<Gs, ST_ROWS, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p, Ap, partials, d);
+        } else switch (lpr) {
             case 2: k_pcg_spmv_dot<2><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p, Ap, partials, d); break;
             case 4: k_pcg_spmv_dot<4><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p, Ap, partials, d); break;
             case 8: k_pcg_spmv_dot<8><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p, Ap, partials, d); break;

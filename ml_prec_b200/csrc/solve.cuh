@@ -51,6 +51,9 @@ struct Prec {
 std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, cudaStream_t s);
 void prec_apply_frame(Prec& P, cudaStream_t s);  // fout = B fin
 
+// Records the largest nnz of a 256-row tile (decides the staged SpMV).
+void csr_tile_stats(DCSR& m, cudaStream_t s);
+
 // y = A x for a CSR matrix (any level, frame or natural order).
 void spmv(const DCSR& A, const double* x, double* y, cudaStream_t s);
 

@@ -2,6 +2,7 @@
 #include "common.cuh"
 
 #include <atomic>
+#include <cstdlib>
 #include <mutex>
 
 namespace mlp {
@@ -14,6 +15,15 @@ uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 void set_last_error(const std::string& s) { g_last_error = s; }
 const char* last_error() { return g_last_error.c_str(); }
+
+bool pdl_enabled() {
+    static int on = -1;
+    if (on < 0) {
+        const char* e = getenv("MLP_PDL");
+        on = (e && e[0] == '0') ? 0 : 1;
+    }
+    return on == 1;
+}
 
 int num_sms() {
     static int sms = 0;

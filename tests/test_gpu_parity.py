@@ -22,12 +22,18 @@ def M():
     return M
 
 
-@pytest.fixture(params=["small", "launch"])
+@pytest.fixture(params=["dense", "small", "explicit", "waves"])
 def apply_path(request, monkeypatch):
-    """Run each case through the shared-memory small-level kernel (default)
-    and through the per-wavefront launch path (small kernel disabled)."""
-    if request.param == "launch":
+    """Run each case through every apply path: the tabulated small-level
+    operator (default), the shared-memory small-level kernel (tabulation off),
+    the launch path with explicit triangular solves (small kernel off), and the
+    launch path with wavefront triangular solves."""
+    if request.param == "small":
+        monkeypatch.setenv("MLP_DENSE_OP_MAX", "0")
+    if request.param in ("explicit", "waves"):
         monkeypatch.setenv("MLP_SMALL_BUDGET", "0")
+    if request.param == "waves":
+        monkeypatch.setenv("MLP_EXPLICIT", "0")
     return request.param
 
 
