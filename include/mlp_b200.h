@@ -144,7 +144,9 @@ int mlp_prec_bytes_per_apply(const mlp_prec* P, uint64_t* bytes);
  * x0 from generate_x0 (solvers.cc:9-21), stop when ||r||/||r0|| <= eps (eps
  * raised so that the absolute stop is >= 1e-14, solvers.cc:49-58).
  * flexible != 0 uses the Polak-Ribiere beta (needed with an FP32 hierarchy).
- * maxit = 0 means no cap. */
+ * maxit = 0 selects the library's cap of 10,000 iterations (the reference has
+ * none; the iterations run on the device and must end); reaching the cap
+ * returns MLP_ERR_MAXIT. */
 int mlp_pcg(const mlp_matrix* A, const double* b_host, mlp_prec* P, double* x_host, double eps, uint32_t maxit,
             int32_t flexible, mlp_stats* stats);
 int mlp_pcg_device(const mlp_matrix* A, const double* b_dev, mlp_prec* P, double* x_dev, double eps,

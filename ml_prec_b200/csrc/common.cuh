@@ -101,6 +101,63 @@ struct DBuf {
     }
 };
 
+// Scratch arena for the temporaries of a hierarchy build or an assembly. Each
+// device keeps a list of chunks that are reused from one build to the next
+// (temporaries then cost neither cudaMalloc nor cudaFree, whose implicit
+// synchronisation and page mapping dominated short setups). An ArenaScope
+// takes the device's lock for its lifetime, so builds in one process are
+// serialised; Tmp<T> buffers created inside a scope come from the arena, outside
+// one they fall back to an ordinary allocation.
+void* arena_take(size_t bytes);  // null when no scope is active
+struct ArenaScope {
+    ArenaScope();
+    ~ArenaScope();
+    ArenaScope(const ArenaScope&) = delete;
+    ArenaScope& operator=(const ArenaScope&) = delete;
+    int dev;
+};
+
+template <class T>
+struct Tmp {
+    T* p = nullptr;
+    size_t n = 0;
+    bool owned = false;
+    Tmp() = default;
+    explicit Tmp(size_t count) { alloc(count); }
+    Tmp(const Tmp&) = delete;
+    Tmp& operator=(const Tmp&) = delete;
+    ~Tmp() { release(); }
+    void alloc(size_t count) {
+        release();
+        n = count;
+        if (!count) return;
+        size_t bytes = count * sizeof(T) + 16;
+        p = static_cast<T*>(arena_take(bytes));
+        if (!p) {
+            CK(cudaMalloc(&p, bytes));
+            owned = true;
+        }
+    }
+    void release() {
+        if (p && owned) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        owned = false;
+    }
+    void zero(cudaStream_t s) { if (n) CK(cudaMemsetAsync(p, 0, n * sizeof(T), s)); }
+    void upload(const T* h, size_t count, cudaStream_t s) {
+        if (count > n) alloc(count);
+        if (count) CK(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+    std::vector<T> download(cudaStream_t s, size_t count = (size_t)-1) const {
+        if (count == (size_t)-1) count = n;
+        std::vector<T> h(count);
+        if (count) CK(cudaMemcpyAsync(h.data(), p, count * sizeof(T), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        return h;
+    }
+};
+
 // CSR matrix on the device: 32-bit indices, FP64 values (plus an optional FP32
 // copy of the values for the reduced-precision preconditioner).
 struct DCSR {
@@ -126,6 +183,10 @@ __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;"
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" :::); }
 
 bool pdl_enabled();
+
+// Host-side phase timer of the setup, printed to stderr when MLP_TRACE=1.
+void trace(const char* label);
+void trace_flush();
 
 template <typename... KArgs, typename... Args>
 inline void launch_k(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,

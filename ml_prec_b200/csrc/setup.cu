@@ -66,8 +66,9 @@ __global__ void k_spe_fill(uint32_t nx, uint32_t ny, uint32_t nz, const double* 
 
 void spe_assemble(uint32_t nx, uint32_t ny, uint32_t nz, const double* kx, const double* ky,
                   const double* kz, double c, int dirichlet, DCSR& A, double* b, cudaStream_t s) {
+    ArenaScope arena;
     uint32_t N = nx * ny * nz;
-    DBuf<uint32_t> len(N);
+    Tmp<uint32_t> len(N);
     k_spe_rowlen<<<grid_for(N, 256), 256, 0, s>>>(nx, ny, nz, len.p);
     CK_LAUNCH();
     A.ia.alloc((size_t)N + 1);
@@ -266,7 +267,7 @@ std::vector<uint32_t> stable_partition(uint32_t N, const uint8_t* bucket, int NB
                                        uint32_t* map, uint32_t base, cudaStream_t s) {
     uint32_t ntile = (N + PT - 1) / PT;
     if (!ntile) ntile = 1;
-    DBuf<uint32_t> counts((size_t)NB * ntile + 1), offs((size_t)NB * ntile + 1), starts(NB + 1);
+    Tmp<uint32_t> counts((size_t)NB * ntile + 1), offs((size_t)NB * ntile + 1), starts(NB + 1);
     counts.zero(s);
     k_part_count<<<ntile, PT, 0, s>>>(N, bucket, NB, ntile, counts.p);
     CK_LAUNCH();
@@ -768,10 +769,10 @@ __global__ void k_slots_emit(uint32_t R, uint32_t cap, const uint32_t* __restric
 // ---- per-level construction ------------------------------------------------
 
 struct Scratch {
-    DBuf<uint8_t> keep, want, bucket, marked, state;
-    DBuf<int> nout, nin, nlinks, flag;
-    DBuf<double> aux;
-    DBuf<uint32_t> rmap, tpos, slot, cand, cnt;
+    Tmp<uint8_t> keep, want, bucket, marked, state;
+    Tmp<int> nout, nin, nlinks, flag;
+    Tmp<double> aux;
+    Tmp<uint32_t> rmap, tpos, slot, cand, cnt;
 };
 
 static void sparse_lu_level(Level& li, Level& ln, const uint8_t* keep, const double* aux, const uint32_t* rmap,
@@ -780,12 +781,12 @@ static void sparse_lu_level(Level& li, Level& ln, const uint8_t* keep, const dou
     uint32_t N = li.N, M = li.M, Md = li.Md, R = N - Md;
     li.done.alloc(M ? M : 1);
     li.done.zero(s);
-    DBuf<uint32_t> slen(R ? R : 1), sldiv(R ? R : 1), wait(R ? R : 1);
-    DBuf<int> flags(1);
+    Tmp<uint32_t> slen(R ? R : 1), sldiv(R ? R : 1), wait(R ? R : 1);
+    Tmp<int> flags(1);
     uint32_t cap = 32;
     for (int attempt = 0;; attempt++) {
-        DBuf<uint32_t> scol((size_t)R * cap + 1);
-        DBuf<double> sval((size_t)R * cap + 1);
+        Tmp<uint32_t> scol((size_t)R * cap + 1);
+        Tmp<double> sval((size_t)R * cap + 1);
         flags.zero(s);
         li.done.zero(s);
         CK(cudaMemsetAsync(wait.p, 0xff, wait.n * 4, s));
@@ -794,7 +795,7 @@ static void sparse_lu_level(Level& li, Level& ln, const uint8_t* keep, const dou
         // E rows in rounds
         int rounds = 0;
         if (M) {
-            DBuf<uint32_t> pa(M), pb(M), cnt(2);
+            Tmp<uint32_t> pa(M), pb(M), cnt(2);
             k_iota<<<grid_for(M, 256), 256, 0, s>>>(M, pa.p);
             CK_LAUNCH();
             CK(cudaMemcpyAsync(cnt.p, &M, 4, cudaMemcpyHostToDevice, s));
@@ -803,7 +804,7 @@ static void sparse_lu_level(Level& li, Level& ln, const uint8_t* keep, const dou
             unsigned grid = (unsigned)std::min<size_t>(grid_for(M, 256), (size_t)num_sms() * 8);
             uint32_t prev_left = M;
             for (;;) {
-                for (int b = 0; b < 4; b++) {
+                for (int b = 0; b < 16; b++) {
                     rounds++;
                     CK(cudaMemsetAsync(cout, 0, 4, s));
                     k_lu_round<<<grid, 256, 0, s>>>(g, pin, cin, pout, cout, rounds);
@@ -814,7 +815,7 @@ static void sparse_lu_level(Level& li, Level& ln, const uint8_t* keep, const dou
                 uint32_t left = read_u32(cin, s);
                 if ((read_flag(flags.p, s) & 1) || left == 0) break;
                 // every round finishes at least the rows whose dependencies are
-                // done; no progress over four rounds means a cycle
+                // done; no progress over sixteen rounds means a cycle
                 if (left >= prev_left) MLP_THROW(ERR_INTERNAL, "elimination makes no progress");
                 prev_left = left;
             }
@@ -831,7 +832,7 @@ static void sparse_lu_level(Level& li, Level& ln, const uint8_t* keep, const dou
             continue;
         }
         // compaction
-        DBuf<uint32_t> lc(R + 1), uc(M + 1), nc(R - M + 1);
+        Tmp<uint32_t> lc(R + 1), uc(M + 1), nc(R - M + 1);
         k_lu_counts<<<grid_for(R, 256), 256, 0, s>>>(R, M, slen.p, sldiv.p, lc.p, uc.p, nc.p);
         CK_LAUNCH();
         li.L.ia.alloc((size_t)R + 1);
@@ -905,7 +906,9 @@ static void build_level_msplit(Hierarchy& H, const BuildCfg& cfg, uint32_t level
     H.lv.emplace_back(new Level());
     Level& ln = *H.lv[level + 1];
     Level& lc = *H.lv[level];  // re-fetch: emplace_back may move unique_ptrs (not the objects)
+    trace("ms mark+order");
     sparse_lu_level(lc, ln, S.keep.p, S.aux.p, S.rmap.p, 1.0, s);
+    trace("ms sparse lu");
     lc.n = N - lc.M - lc.Md;
     lc.dval.alloc(lc.Md ? lc.Md : 1);
     if (lc.Md) {
@@ -1018,12 +1021,12 @@ static void counting_sort(const std::vector<int>& lev, uint32_t nrows, std::vect
 // Explicit forms of the level's triangular solves (P1 and G, setup.cuh).
 static void build_explicit(Level& li, cudaStream_t s) {
     uint32_t M = li.M, R = li.N - li.Md;
-    DBuf<int> flags(1);
+    Tmp<int> flags(1);
     // P1
     for (uint32_t cap = 16;; cap *= 2) {
         if (cap > 65536) MLP_THROW(ERR_LIMIT, "explicit L solve row exceeds 65536 entries");
-        DBuf<uint32_t> scol((size_t)R * cap + 1), slen(R + 1);
-        DBuf<double> sval((size_t)R * cap + 1);
+        Tmp<uint32_t> scol((size_t)R * cap + 1), slen(R + 1);
+        Tmp<double> sval((size_t)R * cap + 1);
         flags.zero(s);
         for (size_t d = 0; d + 1 < li.lw_off.size(); d++) {
             uint32_t r0 = li.lw_off[d], r1 = li.lw_off[d + 1];
@@ -1049,8 +1052,8 @@ static void build_explicit(Level& li, cudaStream_t s) {
     if (!M) { li.G.ia.alloc(1); li.G.ia.zero(s); li.G.ja.alloc(1); li.G.a.alloc(1); return; }
     for (uint32_t cap = 16;; cap *= 2) {
         if (cap > 65536) MLP_THROW(ERR_LIMIT, "explicit U solve row exceeds 65536 entries");
-        DBuf<uint32_t> scol((size_t)M * cap + 1), slen(M + 1);
-        DBuf<double> sval((size_t)M * cap + 1);
+        Tmp<uint32_t> scol((size_t)M * cap + 1), slen(M + 1);
+        Tmp<double> sval((size_t)M * cap + 1);
         flags.zero(s);
         for (size_t d = 0; d + 1 < li.uw_off.size(); d++) {
             uint32_t o0 = li.uw_off[d], o1 = li.uw_off[d + 1];
@@ -1096,7 +1099,7 @@ static void build_frames(Hierarchy& H, cudaStream_t s) {
         li.lw_off_d.upload(off.data(), off.size(), s);
         li.eperm.alloc(M ? M : 1);
         if (M) li.eperm.upload(rows.data(), M, s);
-        DBuf<uint32_t> pi(N), einv(M ? M : 1), p2f(N);
+        Tmp<uint32_t> pi(N), einv(M ? M : 1), p2f(N);
         const uint32_t* phi_next = (l + 1 < (int)H.nlevels) ? H.lv[l + 1]->phi.p : nullptr;
         const uint32_t* iphi_next = (l + 1 < (int)H.nlevels) ? H.lv[l + 1]->iphi.p : nullptr;
         k_frame_phi<<<grid_for(N, 256), 256, 0, s>>>(N, M, n, li.eperm.p, phi_next, li.map.p, pi.p, li.phi.p);
@@ -1111,7 +1114,7 @@ static void build_frames(Hierarchy& H, cudaStream_t s) {
         CK_LAUNCH();
         // Lf: rows pi(q), q < R; columns (E, permuted) -> frame
         {
-            DBuf<uint32_t> len(R + 1);
+            Tmp<uint32_t> len(R + 1);
             k_row_len_perm<<<grid_for(R, 256), 256, 0, s>>>(R, pi.p, li.L.ia.p, len.p);
             CK_LAUNCH();
             li.Lf.ia.alloc((size_t)R + 1);
@@ -1124,7 +1127,7 @@ static void build_frames(Hierarchy& H, cudaStream_t s) {
         }
         // Uf: rows eperm[q], columns -> frame
         if (M) {
-            DBuf<uint32_t> len(M + 1);
+            Tmp<uint32_t> len(M + 1);
             k_row_len_perm<<<grid_for(M, 256), 256, 0, s>>>(M, li.eperm.p, li.U.ia.p, len.p);
             CK_LAUNCH();
             li.Uf.ia.alloc((size_t)M + 1);
@@ -1135,9 +1138,9 @@ static void build_frames(Hierarchy& H, cudaStream_t s) {
                                                          li.Uf.ia.p, li.Uf.ja.p, li.Uf.a.p);
             CK_LAUNCH();
             // U-solve wavefronts: row q depends on the E columns of its row
-            DBuf<int> lev(M);
+            Tmp<int> lev(M);
             lev.zero(s);
-            DBuf<uint32_t> pa(M), pb(M), cnt(2);
+            Tmp<uint32_t> pa(M), pb(M), cnt(2);
             k_iota<<<grid_for(M, 256), 256, 0, s>>>(M, pa.p);
             CK_LAUNCH();
             CK(cudaMemcpyAsync(cnt.p, &M, 4, cudaMemcpyHostToDevice, s));
@@ -1146,7 +1149,7 @@ static void build_frames(Hierarchy& H, cudaStream_t s) {
             uint32_t prev_left = M;
             unsigned grid = (unsigned)std::min<size_t>(grid_for(M, 256), (size_t)num_sms() * 8);
             for (;;) {
-                for (int b = 0; b < 4; b++) {
+                for (int b = 0; b < 16; b++) {
                     round++;
                     CK(cudaMemsetAsync(cout, 0, 4, s));
                     k_dag_round<<<grid, 256, 0, s>>>(M, li.Uf.ia.p, li.Uf.ja.p, M, lev.p, pin, cin, pout, cout,
@@ -1173,7 +1176,7 @@ static void build_frames(Hierarchy& H, cudaStream_t s) {
         // Af: rows phi(q), columns -> iphi
         {
             const DCSR& A = li.A;
-            DBuf<uint32_t> len(N + 1);
+            Tmp<uint32_t> len(N + 1);
             k_row_len_perm<<<grid_for(N, 256), 256, 0, s>>>(N, li.phi.p, A.ia.p, len.p);
             CK_LAUNCH();
             li.Af.ia.alloc((size_t)N + 1);
@@ -1197,9 +1200,11 @@ static void build_frames(Hierarchy& H, cudaStream_t s) {
                 li.As.nrow = li.As.ncol = N; li.As.nnz = z;
             }
         }
+        trace("frame operators");
         csr_tile_stats(li.Af, s);
         if (H.kind == PREC_CHEB && l > 0) csr_tile_stats(li.As, s);
         if (!li.direct) build_explicit(li, s);
+        trace("explicit solves");
     }
 }
 
@@ -1210,8 +1215,8 @@ static void build_direct(Level& li, cudaStream_t s) {
     if (!n) return;
     k_dense_from_csr<<<grid_for(n, 128), 128, 0, s>>>(n, li.A.ia.p, li.A.ja.p, li.A.a.p, li.cinv.p);
     CK_LAUNCH();
-    DBuf<double> col(n);
-    DBuf<int> err(1);
+    Tmp<double> col(n);
+    Tmp<int> err(1);
     err.zero(s);
     dim3 g2(grid_for(n, 256), n);
     for (uint32_t k = 0; k < n; k++) {
@@ -1224,6 +1229,8 @@ static void build_direct(Level& li, cudaStream_t s) {
 }
 
 std::unique_ptr<Hierarchy> build_hierarchy(const DCSR& A0, const BuildCfg& cfg, cudaStream_t s) {
+    ArenaScope arena;
+    trace("build start");
     auto H = std::unique_ptr<Hierarchy>(new Hierarchy());
     H->kind = cfg.kind;
     H->lv.emplace_back(new Level());
@@ -1278,6 +1285,7 @@ std::unique_ptr<Hierarchy> build_hierarchy(const DCSR& A0, const BuildCfg& cfg, 
                                      " unknowns, more than the dense direct solve allows (" +
                                      std::to_string(cfg.dense_max) + ")");
         build_direct(last, s);
+        trace("dense coarse inverse");
     }
     build_frames(*H, s);
     CK(cudaStreamSynchronize(s));

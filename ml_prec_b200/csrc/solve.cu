@@ -96,7 +96,7 @@ __global__ void k_tile_max(uint32_t n, const uint32_t* __restrict__ ia, uint32_t
 
 void csr_tile_stats(DCSR& m, cudaStream_t s) {
     if (!m.nrow) { m.tile_max = 0; return; }
-    DBuf<uint32_t> d(1);
+    Tmp<uint32_t> d(1);
     d.zero(s);
     uint32_t nt = (m.nrow + ST_ROWS - 1) / ST_ROWS;
     k_tile_max<<<grid_for(nt, 256), 256, 0, s>>>(m.nrow, m.ia.p, d.p);
@@ -773,10 +773,12 @@ static uint32_t small_budget() {
 }
 
 std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, cudaStream_t s) {
+    ArenaScope arena;
     auto P = std::unique_ptr<Prec>(new Prec());
     P->stream = s;
     P->fp32 = fp32;
     P->H = build_hierarchy(A, cfg, s);
+    trace("hierarchy");
     Hierarchy& H = *P->H;
     uint32_t N0 = H.lv[0]->N;
     P->fin_buf.alloc(N0);
@@ -821,6 +823,7 @@ std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, c
         P->bytes_per_apply = B.bytes + 12ull * N0 * 2;
     }
     CK(cudaStreamSynchronize(s));
+    trace("plan + small levels");
     // capture the apply once as a graph
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -831,6 +834,8 @@ std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, c
     cudaError_t ie = cudaGraphInstantiate(&P->graph, g, 0);
     cudaGraphDestroy(g);
     if (ie != cudaSuccess) MLP_THROW(ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+    trace("graph");
+    trace_flush();
     return P;
 }
 
@@ -844,6 +849,9 @@ void prec_apply_frame(Prec& P, cudaStream_t s) {
 // PCG
 // ---------------------------------------------------------------------------
 static constexpr int RB = 256;  // reduction block
+// Iteration cap when the caller passes maxit = 0: the iterations must always
+// end, also when eps is below what rounding lets the residual reach.
+static constexpr uint32_t PCG_DEFAULT_MAXIT = 10000;
 
 struct PcgDev {
     double rz0, rz1, app, alpha, beta, rr, rz_prev;
@@ -1061,6 +1069,7 @@ const double* x0_device(uint32_t n, cudaStream_t s) {
 
 int pcg_solve(const DCSR& A, const double* b, Prec& P, double* x, double eps, uint32_t maxit, bool flexible,
               PcgStats& st, cudaStream_t s) {
+    if (maxit == 0) maxit = PCG_DEFAULT_MAXIT;
     Hierarchy& H = *P.H;
     const Level& L0 = *H.lv[0];
     const DCSR& Af = L0.Af;
@@ -1204,6 +1213,7 @@ uint32_t pcg_noalloc_max_n() { return NOALLOC_MAX_N; }
 
 int pcg_solve_noalloc(const DCSR& A, const double* b, Prec& P, double* x, double eps, uint32_t maxit,
                       bool flexible, PcgStats& st, cudaStream_t s) {
+    if (maxit == 0) maxit = PCG_DEFAULT_MAXIT;
     Hierarchy& H = *P.H;
     const Level& L0 = *H.lv[0];
     const DCSR& Af = L0.Af;

@@ -1,7 +1,13 @@
 // Library-wide utilities: error string, SM count, device exclusive scan.
 #include "common.cuh"
 
+#include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
 #include <cstdlib>
 #include <mutex>
 
@@ -23,6 +29,88 @@ bool pdl_enabled() {
         on = (e && e[0] == '0') ? 0 : 1;
     }
     return on == 1;
+}
+
+static bool trace_on() {
+    static int on = -1;
+    if (on < 0) {
+        const char* e = getenv("MLP_TRACE");
+        on = (e && e[0] == '1') ? 1 : 0;
+    }
+    return on == 1;
+}
+static thread_local std::vector<std::pair<std::string, double>> g_trace;
+
+void trace(const char* label) {
+    if (!trace_on()) return;
+    double t = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+    g_trace.emplace_back(label, t);
+}
+
+void trace_flush() {
+    if (!trace_on() || g_trace.empty()) return;
+    double t0 = g_trace.front().second, prev = t0;
+    for (auto& e : g_trace) {
+        fprintf(stderr, "[mlp trace] %-28s +%8.3f ms (total %8.3f)\n", e.first.c_str(), e.second - prev, e.second - t0);
+        prev = e.second;
+    }
+    g_trace.clear();
+}
+
+// ---- scratch arena ----------------------------------------------------------
+namespace {
+struct DevArena {
+    std::mutex mu;
+    struct Chunk { char* base; size_t cap, off; };
+    std::vector<Chunk> chunks;
+};
+DevArena& dev_arena(int dev) {
+    static std::mutex m;
+    static std::map<int, std::unique_ptr<DevArena>> all;
+    std::lock_guard<std::mutex> lk(m);
+    auto& a = all[dev];
+    if (!a) a.reset(new DevArena());
+    return *a;
+}
+thread_local DevArena* t_arena = nullptr;
+thread_local int t_arena_depth = 0;
+}  // namespace
+
+ArenaScope::ArenaScope() {
+    CK(cudaGetDevice(&dev));
+    if (t_arena_depth++ == 0) {
+        DevArena& a = dev_arena(dev);
+        a.mu.lock();
+        for (auto& c : a.chunks) c.off = 0;
+        t_arena = &a;
+    }
+}
+
+ArenaScope::~ArenaScope() {
+    if (--t_arena_depth == 0) {
+        // the scope's work must be finished before the memory is reused
+        cudaDeviceSynchronize();
+        DevArena* a = t_arena;
+        t_arena = nullptr;
+        a->mu.unlock();
+    }
+}
+
+void* arena_take(size_t bytes) {
+    DevArena* a = t_arena;
+    if (!a) return nullptr;
+    bytes = (bytes + 255) & ~(size_t)255;
+    for (auto& c : a->chunks)
+        if (c.off + bytes <= c.cap) {
+            void* p = c.base + c.off;
+            c.off += bytes;
+            return p;
+        }
+    size_t cap = std::max<size_t>(bytes, (size_t)64 << 20);
+    char* base = nullptr;
+    CK(cudaMalloc(&base, cap));
+    a->chunks.push_back({base, cap, bytes});
+    return base;
 }
 
 int num_sms() {
@@ -115,7 +203,7 @@ __global__ void k_tile_scan(const uint32_t* __restrict__ in, uint32_t* __restric
 void exclusive_scan_u32_async(const uint32_t* in, uint32_t* out, uint32_t n, cudaStream_t s) {
     uint32_t nt = (n + SCAN_TILE - 1) / SCAN_TILE;
     if (nt == 0) nt = 1;
-    DBuf<uint32_t> sums(nt);
+    Tmp<uint32_t> sums(nt);
     k_tile_sums<<<nt, SCAN_T, 0, s>>>(in, n, sums.p);
     CK_LAUNCH();
     k_scan_sums<<<1, SCAN_T, 0, s>>>(sums.p, nt, out + n);

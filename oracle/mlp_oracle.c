@@ -760,6 +760,7 @@ int or_pcg(const or_csr* A, const double* b, const or_prec* P, double* x, double
     memcpy(p, z, 8 * (size_t)n);
     double rz0 = ddot(r, z, n);
     if (init_norm * eps < 1e-14) eps = 1e-14 / init_norm; /* solvers.cc:49-58 */
+    if (maxit == 0) maxit = 100000; /* the checker must always return */
     uint32_t it = 0;
     int rc = 0;
     while (norm / init_norm > eps) {
