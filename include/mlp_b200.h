@@ -152,6 +152,39 @@ int mlp_pcg(const mlp_matrix* A, const double* b_host, mlp_prec* P, double* x_ho
 int mlp_pcg_device(const mlp_matrix* A, const double* b_dev, mlp_prec* P, double* x_dev, double eps,
                    uint32_t maxit, int32_t flexible, mlp_stats* stats, void* stream);
 
+/* mlp_pcg_device with a choice of start vector: x0_mode 0 = generate_x0 (the
+ * reference's start, solvers.cc:9-21), 1 = zero, 2 = the values already in
+ * x_dev. The zero start serves the adjoint solve of the differentiation form,
+ * whose right-hand side is small next to A x0. */
+int mlp_pcg_device_x0(const mlp_matrix* A, const double* b_dev, mlp_prec* P, double* x_dev, double eps,
+                      uint32_t maxit, int32_t flexible, int32_t x0_mode, mlp_stats* stats, void* stream);
+
+/* Differentiation form (no reference counterpart: the reference has no
+ * gradients). For a matrix made by mlp_matrix_create_spe, writes
+ * grad[c] = dJ/d(ln K_c) = -lambda^T (dA/dtheta_c p - db/dtheta_c) per mesh cell,
+ * where p solves A p = b and lambda solves A lambda = dJ/dp (A is symmetric);
+ * K scales kx, ky and kz of the cell (kz = 0.1 K in the benchmark fields).
+ * Uses the harmonic-mean transmissibility derivatives of the stencil of
+ * spe.cc:81-87 plus the Dirichlet x-face terms. Device vectors of N entries. */
+int mlp_matrix_grad_logk(const mlp_matrix* A, const double* p_dev, const double* lam_dev, double* grad_dev,
+                         void* stream);
+
+/* ---- ensemble form ----------------------------------------------------------
+ * Independent PCG solves of several (matrix, preconditioner) pairs, e.g. an
+ * ensemble of permeability realizations on meshes of different sizes, recorded
+ * as parallel branches of ONE CUDA graph (each branch: start, a conditional
+ * WHILE loop of iterations, scatter) and run with one launch. No reference
+ * counterpart (the reference solves one system per process run). A handle may
+ * belong to one ensemble at a time; the ensemble uses the handles' solver
+ * vectors, so the handles must outlive it. */
+typedef struct mlp_ensemble mlp_ensemble;
+int mlp_ensemble_create(uint32_t count, mlp_prec* const* P, int32_t flexible, int32_t x0_mode, mlp_ensemble** out);
+/* b_dev[i], x_dev[i]: member i's vectors (natural order); stats: count entries;
+ * t_ms: device time of the launch. */
+int mlp_ensemble_solve(mlp_ensemble* E, const double* const* b_dev, double* const* x_dev, double eps, uint32_t maxit,
+                       mlp_stats* stats, double* t_ms, void* stream);
+int mlp_ensemble_destroy(mlp_ensemble* E);
+
 /* PCG that allocates no device memory. It has no counterpart in the
  * reference: it serves callers that cannot call cudaMalloc while they run
  * (code recording into a stream capture, hosts whose device memory belongs to

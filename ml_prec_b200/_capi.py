@@ -23,7 +23,8 @@ EXPORTS = [
     "mlp_matrix_download", "mlp_spmv",
     "mlp_prec_create", "mlp_prec_destroy", "mlp_prec_apply", "mlp_prec_apply_host", "mlp_prec_nlevels",
     "mlp_prec_level_info", "mlp_prec_level_export", "mlp_prec_bytes_per_apply",
-    "mlp_pcg", "mlp_pcg_device", "mlp_pcg_device_noalloc", "mlp_launch_count", "mlp_generate_x0",
+    "mlp_pcg", "mlp_pcg_device", "mlp_pcg_device_x0", "mlp_matrix_grad_logk", "mlp_pcg_device_noalloc",
+    "mlp_launch_count", "mlp_generate_x0", "mlp_ensemble_create", "mlp_ensemble_solve", "mlp_ensemble_destroy",
 ]
 
 
@@ -99,6 +100,13 @@ def lib():
         L.mlp_pcg_device_noalloc.argtypes = [vp, vp, vp, vp, C.c_double, C.c_uint32, C.c_int32,
                                              C.POINTER(Stats), vp]
         L.mlp_launch_count.argtypes = [C.POINTER(C.c_uint64)]
+        L.mlp_pcg_device_x0.argtypes = [vp, vp, vp, vp, C.c_double, C.c_uint32, C.c_int32, C.c_int32,
+                                        C.POINTER(Stats), vp]
+        L.mlp_matrix_grad_logk.argtypes = [vp, vp, vp, vp, vp]
+        L.mlp_ensemble_create.argtypes = [C.c_uint32, C.POINTER(vp), C.c_int32, C.c_int32, C.POINTER(vp)]
+        L.mlp_ensemble_solve.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.c_double, C.c_uint32,
+                                         C.POINTER(Stats), C.POINTER(C.c_double), vp]
+        L.mlp_ensemble_destroy.argtypes = [vp]
         _lib = L
     return _lib
 

@@ -10,6 +10,10 @@ using namespace mlp;
 struct mlp_matrix {
     DCSR A;
     cudaStream_t s = nullptr;
+    // set by mlp_matrix_create_spe: the field and mesh the matrix came from
+    DBuf<double> field;  // kx, ky, kz blocks (3 x 1,122,000)
+    uint32_t nx = 0, ny = 0, nz = 0;
+    int32_t dirichlet = 0;
     ~mlp_matrix() {
         if (s) cudaStreamDestroy(s);
     }
@@ -105,7 +109,9 @@ int mlp_matrix_create_spe(uint32_t nx, uint32_t ny, uint32_t nz, const double* k
     auto* M = new mlp_matrix();
     try {
         M->s = new_stream();
-        DBuf<double> dk(3 * KN);
+        DBuf<double>& dk = M->field;
+        dk.alloc(3 * KN);
+        M->nx = nx; M->ny = ny; M->nz = nz; M->dirichlet = dirichlet;
         CK(cudaMemcpyAsync(dk.p, kx, KN * 8, cudaMemcpyHostToDevice, M->s));
         CK(cudaMemcpyAsync(dk.p + KN, ky, KN * 8, cudaMemcpyHostToDevice, M->s));
         CK(cudaMemcpyAsync(dk.p + 2 * KN, kz, KN * 8, cudaMemcpyHostToDevice, M->s));
@@ -305,7 +311,11 @@ int mlp_prec_bytes_per_apply(const mlp_prec* P, uint64_t* bytes) {
 static int pcg_common(const mlp_matrix* A, const double* b_dev, mlp_prec* P, double* x_dev, double eps,
                       uint32_t maxit, int32_t flexible, mlp_stats* stats, cudaStream_t s) {
     PcgStats st;
-    int rc = pcg_solve(A->A, b_dev, *P->P, x_dev, eps, maxit, flexible != 0, st, s);
+    // MLP_PCG_HOSTLOOP=1 selects the host-driven loop (the tests check the
+    // device-resident solve against it)
+    const char* hl = getenv("MLP_PCG_HOSTLOOP");
+    int rc = (hl && hl[0] == '1') ? pcg_solve_hostloop(A->A, b_dev, *P->P, x_dev, eps, maxit, flexible != 0, st, s)
+                                  : pcg_solve(A->A, b_dev, *P->P, x_dev, eps, maxit, flexible != 0, st, s);
     if (stats) {
         stats->niter = st.niter;
         stats->napply = st.napply;
@@ -366,6 +376,101 @@ int mlp_pcg_device_noalloc(const mlp_matrix* A, const double* b_dev, mlp_prec* P
         stats->t_setup_ms = P->setup_ms;
     }
     return rc;
+    API_END
+}
+
+int mlp_pcg_device_x0(const mlp_matrix* A, const double* b_dev, mlp_prec* P, double* x_dev, double eps,
+                      uint32_t maxit, int32_t flexible, int32_t x0_mode, mlp_stats* stats, void* stream) {
+    API_BEGIN
+    if (!A || !b_dev || !P || !x_dev) MLP_THROW(ERR_ARG, "null pointer");
+    if (x0_mode < 0 || x0_mode > 2) MLP_THROW(ERR_ARG, "x0_mode must be 0, 1 or 2");
+    cudaStream_t s = stream ? (cudaStream_t)stream : P->s;
+    set_pcg_x0_mode(x0_mode);
+    return pcg_common(A, b_dev, P, x_dev, eps, maxit, flexible, stats, s);
+    API_END
+}
+
+int mlp_matrix_grad_logk(const mlp_matrix* A, const double* p_dev, const double* lam_dev, double* grad_dev,
+                         void* stream) {
+    API_BEGIN
+    if (!A || !p_dev || !lam_dev || !grad_dev) MLP_THROW(ERR_ARG, "null pointer");
+    if (!A->field.p) MLP_THROW(ERR_ARG, "the matrix was not assembled from a permeability field");
+    cudaStream_t s = stream ? (cudaStream_t)stream : A->s;
+    const size_t KN = 1122000;
+    spe_grad_logk(A->nx, A->ny, A->nz, A->field.p, A->field.p + KN, A->field.p + 2 * KN, A->dirichlet, p_dev,
+                  lam_dev, grad_dev, s);
+    if (!stream) CK(cudaStreamSynchronize(s));
+    API_END
+}
+
+}  // extern "C"
+
+struct mlp_ensemble {
+    std::unique_ptr<Ensemble> E;
+    std::vector<mlp_prec*> handles;
+    cudaStream_t s = nullptr;
+    ~mlp_ensemble() {
+        E.reset();
+        if (s) cudaStreamDestroy(s);
+    }
+};
+
+extern "C" {
+
+int mlp_ensemble_create(uint32_t count, mlp_prec* const* P, int32_t flexible, int32_t x0_mode, mlp_ensemble** out) {
+    API_BEGIN
+    if (!P || !out || !count) MLP_THROW(ERR_ARG, "empty ensemble");
+    if (x0_mode < 0 || x0_mode > 2) MLP_THROW(ERR_ARG, "x0_mode must be 0, 1 or 2");
+    std::vector<Prec*> members;
+    for (uint32_t i = 0; i < count; i++) {
+        if (!P[i]) MLP_THROW(ERR_ARG, "null member handle");
+        for (uint32_t j = 0; j < i; j++)
+            if (P[j] == P[i]) MLP_THROW(ERR_ARG, "a handle appears twice in the ensemble");
+        members.push_back(P[i]->P.get());
+    }
+    auto* H = new mlp_ensemble();
+    try {
+        H->s = new_stream();
+        H->handles.assign(P, P + count);
+        H->E = make_ensemble(members, flexible != 0, x0_mode, H->s);
+        CK(cudaStreamSynchronize(H->s));
+    } catch (...) {
+        delete H;
+        throw;
+    }
+    *out = H;
+    API_END
+}
+
+int mlp_ensemble_solve(mlp_ensemble* E, const double* const* b_dev, double* const* x_dev, double eps, uint32_t maxit,
+                       mlp_stats* stats, double* t_ms, void* stream) {
+    API_BEGIN
+    if (!E || !b_dev || !x_dev) MLP_THROW(ERR_ARG, "null pointer");
+    size_t K = E->handles.size();
+    std::vector<const double*> b(b_dev, b_dev + K);
+    std::vector<double*> x(x_dev, x_dev + K);
+    cudaStream_t s = stream ? (cudaStream_t)stream : E->s;
+    std::vector<PcgStats> st;
+    double ms = 0;
+    int rc = ensemble_solve(*E->E, b, x, eps, maxit, st, ms, s);
+    if (t_ms) *t_ms = ms;
+    if (stats)
+        for (size_t i = 0; i < K; i++) {
+            stats[i].niter = st[i].niter;
+            stats[i].napply = st[i].napply;
+            stats[i].init_norm = st[i].init_norm;
+            stats[i].final_norm = st[i].final_norm;
+            stats[i].final_rel = st[i].final_rel;
+            stats[i].t_solve_ms = ms;
+            stats[i].t_setup_ms = E->handles[i]->setup_ms;
+        }
+    return rc;
+    API_END
+}
+
+int mlp_ensemble_destroy(mlp_ensemble* E) {
+    API_BEGIN
+    delete E;
     API_END
 }
 

@@ -857,7 +857,10 @@ struct PcgDev {
     double rz0, rz1, app, alpha, beta, rr, rz_prev;
     unsigned ticket[4];
     int status;  // 1: <Ap,p> <= 0, 2: not finite
+    uint32_t it, maxit;
+    double init, eps;
 };
+static int take_x0_mode();
 
 __device__ __forceinline__ double block_sum(double v) {
     __shared__ double sh[32];
@@ -1067,8 +1070,331 @@ const double* x0_device(uint32_t n, cudaStream_t s) {
     return d;
 }
 
+// ---------------------------------------------------------------------------
+// Device-resident PCG: one solve is one graph launch.
+// ---------------------------------------------------------------------------
+// End-of-iteration test: counts the iteration and keeps looping while
+// ||r||/||r0|| > eps (pcg.cc:42), no error was flagged and the cap is not hit.
+__global__ void k_pcg_check(PcgDev* d, cudaGraphConditionalHandle h) {
+    d->it++;
+    double norm = sqrt(d->rr);
+    bool go = norm / d->init > d->eps && d->status == 0 && (d->maxit == 0 || d->it < d->maxit);
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+__global__ void k_copy_d(uint32_t n, const double* __restrict__ a, double* __restrict__ b) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = a[i];
+}
+
+__global__ void k_fill_d(uint32_t n, double* __restrict__ a, double v) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = v;
+}
+
+// Clears the PCG scalars (reduction tickets, status) at the start of a solve.
+__global__ void k_zero_dev(PcgDev* d) {
+    uint32_t* w = reinterpret_cast<uint32_t*>(d);
+    for (uint32_t i = threadIdx.x; i < sizeof(PcgDev) / 4; i += blockDim.x) w[i] = 0;
+}
+
+// Start of the solve on the device: init = ||r0||, eps raised so that the
+// absolute stop is >= 1e-14 (check_and_replace_eps, solvers.cc:49-58); no
+// iteration when ||r0||/||r0|| > eps fails (the reference then throws "No need
+// to iterate").
+__global__ void k_pcg_start(PcgDev* d, const PcgParams* prm, cudaGraphConditionalHandle h) {
+    double init = sqrt(d->rr);
+    double eps = prm->eps;
+    if (init * eps < 1e-14) eps = 1e-14 / init;
+    d->init = init;
+    d->eps = eps;
+    d->it = 0;
+    d->maxit = prm->maxit;
+    d->status = 0;
+    if (!(init / init > eps)) cudaGraphSetConditional(h, 0u);
+}
+
+PcgWork::~PcgWork() {
+    for (auto& g : full)
+        if (g) cudaGraphExecDestroy(g);
+}
+
+static void pcg_work_alloc(Prec& P, uint32_t n) {
+    PcgWork& W = P.pcg;
+    if (W.n == n) return;
+    for (auto& g : W.full)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    W.n = n;
+    W.xf.alloc(n); W.bf.alloc(n); W.p.alloc(n); W.Ap.alloc(n); W.rprev.alloc(n);
+    W.bnat.alloc(n); W.xnat.alloc(n);
+    unsigned G = (unsigned)std::max(1, std::min<int>((int)grid_for(n, RB), num_sms() * 4));
+    W.partials.alloc(2 * (size_t)std::max<unsigned>(G, staged_grid(n)));
+    W.d.alloc(1);
+    W.prm.alloc(1);
+}
+
+// Records one PCG iteration (pcg.cc:46-75) on stream s.
+static void record_iteration(Prec& P, const DCSR& Af, uint32_t n, bool flexible, cudaGraphConditionalHandle h,
+                             cudaStream_t s) {
+    PcgWork& W = P.pcg;
+    PcgDev* d = W.d.p;
+    double* r = P.fin_buf.p;
+    double* z = P.fout_buf.p;
+    unsigned G = (unsigned)std::max(1, std::min<int>((int)grid_for(n, RB), num_sms() * 4));
+    bool staged = Af.tile_max && Af.tile_max <= ST_MAX_NNZ && n >= 4 * ST_ROWS;
+    double avg = (double)Af.nnz / n;
+    int lpr = avg <= 3 ? 2 : avg <= 6 ? 4 : avg <= 12 ? 8 : avg <= 24 ? 16 : 32;
+    if (staged) {
+        k_pcg_spmv_dot_staged<<<staged_grid(n), ST_ROWS, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, W.p.p, W.Ap.p,
+                                                                 W.partials.p, d);
+    } else switch (lpr) {
+        case 2: k_pcg_spmv_dot<2><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, W.p.p, W.Ap.p, W.partials.p, d); break;
+        case 4: k_pcg_spmv_dot<4><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, W.p.p, W.Ap.p, W.partials.p, d); break;
+        case 8: k_pcg_spmv_dot<8><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, W.p.p, W.Ap.p, W.partials.p, d); break;
+        case 16: k_pcg_spmv_dot<16><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, W.p.p, W.Ap.p, W.partials.p, d); break;
+        default: k_pcg_spmv_dot<32><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, W.p.p, W.Ap.p, W.partials.p, d); break;
+    }
+    k_pcg_update<<<G, RB, 0, s>>>(n, W.xf.p, r, W.p.p, W.Ap.p, W.partials.p, d);
+    k_pcg_check<<<1, 1, 0, s>>>(d, h);
+    P.plan.run(s);
+    k_pcg_dot_rz<<<G, RB, 0, s>>>(n, r, z, W.rprev.p, W.partials.p, d, flexible ? 1 : 0);
+    k_pcg_beta<<<1, 1, 0, s>>>(d, flexible ? 1 : 0);
+    k_pcg_p<<<grid_for(n, 256), 256, 0, s>>>(n, W.p.p, z, d);
+    if (flexible) k_copy_d<<<grid_for(n, 256), 256, 0, s>>>(n, r, W.rprev.p);
+}
+
+// Launches per loop iteration and per start (launch accounting).
+static uint64_t iteration_launches(const Prec& P, bool flexible) {
+    return 3 + P.plan.launches + 3 + (flexible ? 1 : 0);
+}
+static uint64_t start_launches(const Prec& P, bool flexible) {
+    return 6 + P.plan.launches + 2 + (flexible ? 1 : 0) + 1;
+}
+
+// Appends one complete PCG solve (pcg.cc:8-102) of handle P to graph g:
+// gather b and x0 into the frame, r = b - A x, the first apply, a conditional
+// WHILE node whose body is one iteration, and the scatter of x back. The
+// vectors live in P's PcgWork (b comes in through bnat, x leaves through xnat).
+static void append_pcg(cudaGraph_t g, Prec& P, uint32_t n, bool flexible, int x0m, cudaStream_t s) {
+    const Level& L0 = *P.H->lv[0];
+    const DCSR& Af = L0.Af;
+    PcgWork& W = P.pcg;
+    PcgDev* d = W.d.p;
+    double* r = P.fin_buf.p;
+    double* z = P.fout_buf.p;
+    unsigned G = (unsigned)std::max(1, std::min<int>((int)grid_for(n, RB), num_sms() * 4));
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+    const double* x0 = x0m == X0_GENERATE ? x0_device(n, s) : nullptr;
+    // start
+    CK(cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    k_zero_dev<<<1, 32, 0, s>>>(d);
+    gather(n, L0.phi.p, W.bnat.p, W.bf.p, s);
+    if (x0m == X0_ZERO) k_fill_d<<<grid_for(n, 256), 256, 0, s>>>(n, W.xf.p, 0.0);
+    else gather(n, L0.phi.p, x0m == X0_GIVEN ? W.xnat.p : x0, W.xf.p, s);
+    launch_spmv<double>(n, Af.nnz, Af.ia.p, Af.ja.p, Af.a.p, W.xf.p, r, W.bf.p, s, Af.tile_max);
+    k_dot_simple<<<G, RB, 0, s>>>(n, r, r, W.partials.p, &d->ticket[1], &d->rr);
+    P.plan.run(s);
+    k_copy_d<<<grid_for(n, 256), 256, 0, s>>>(n, z, W.p.p);
+    k_dot_simple<<<G, RB, 0, s>>>(n, r, z, W.partials.p, &d->ticket[2], &d->rz0);
+    if (flexible) k_copy_d<<<grid_for(n, 256), 256, 0, s>>>(n, r, W.rprev.p);
+    k_pcg_start<<<1, 1, 0, s>>>(d, W.prm.p, h);
+    cudaError_t le = cudaGetLastError();
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    CK(cudaStreamGetCaptureInfo(s, &cs, nullptr, nullptr, &deps, &ndeps));
+    std::vector<cudaGraphNode_t> dv(deps, deps + ndeps);
+    cudaGraph_t got;
+    CK(cudaStreamEndCapture(s, &got));
+    if (le != cudaSuccess) MLP_THROW(ERR_CUDA, cudaGetErrorString(le));
+    // loop
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    CK(cudaGraphAddNode(&cnode, g, dv.data(), dv.size(), &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CK(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    record_iteration(P, Af, n, flexible, h, s);
+    le = cudaGetLastError();
+    CK(cudaStreamEndCapture(s, &got));
+    if (le != cudaSuccess) MLP_THROW(ERR_CUDA, cudaGetErrorString(le));
+    // tail
+    CK(cudaStreamBeginCaptureToGraph(s, g, &cnode, nullptr, 1, cudaStreamCaptureModeThreadLocal));
+    scatter(n, L0.phi.p, W.xf.p, W.xnat.p, s);
+    le = cudaGetLastError();
+    CK(cudaStreamEndCapture(s, &got));
+    if (le != cudaSuccess) MLP_THROW(ERR_CUDA, cudaGetErrorString(le));
+}
+
+static cudaGraphExec_t instantiate(cudaGraph_t g) {
+    cudaGraphExec_t ex = nullptr;
+    cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) MLP_THROW(ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+    return ex;
+}
+
+static cudaGraphExec_t full_graph(Prec& P, uint32_t n, bool flexible, int x0m, cudaStream_t s) {
+    cudaGraphExec_t& ex = P.pcg.full[(flexible ? 1 : 0) * 3 + x0m];
+    if (ex) return ex;
+    cudaGraph_t g;
+    CK(cudaGraphCreate(&g, 0));
+    try {
+        append_pcg(g, P, n, flexible, x0m, s);
+    } catch (...) {
+        cudaGraphDestroy(g);
+        throw;
+    }
+    ex = instantiate(g);
+    return ex;
+}
+
+static void read_stats(const PcgDev& h, PcgStats& st, int& rc, std::string& msg) {
+    st.niter = h.it;
+    st.init_norm = h.init;
+    st.final_norm = std::sqrt(h.rr);
+    st.final_rel = st.final_norm / h.init;
+    st.napply = h.it + 1;
+    rc = OK;
+    if (h.status & 1) { rc = ERR_CURVATURE; msg = "<Ap, p> = " + std::to_string(h.app); }
+    else if (h.status & 2) { rc = ERR_NOT_FINITE; msg = "non-finite value in PCG scalars"; }
+    else if (h.maxit && h.it >= h.maxit && st.final_rel > h.eps) { rc = ERR_MAXIT; msg = "iteration cap reached"; }
+    else if (h.it == 0) { rc = ERR_NO_ITER; msg = "No need to iterate"; }
+}
+
+static thread_local int t_x0_mode = X0_GENERATE;
+void set_pcg_x0_mode(int mode) { t_x0_mode = mode; }
+static int take_x0_mode() {
+    int m = t_x0_mode;
+    t_x0_mode = X0_GENERATE;
+    return m;
+}
+
+// PCGSolver (pcg.cc:8-102) as one graph launch: start, loop and scatter run on
+// the device; the host waits once, for the statistics.
 int pcg_solve(const DCSR& A, const double* b, Prec& P, double* x, double eps, uint32_t maxit, bool flexible,
               PcgStats& st, cudaStream_t s) {
+    if (maxit == 0) maxit = PCG_DEFAULT_MAXIT;
+    const Level& L0 = *P.H->lv[0];
+    uint32_t n = A.nrow;
+    if (n != L0.N) MLP_THROW(ERR_ARG, "matrix and preconditioner sizes differ");
+    if (!n) MLP_THROW(ERR_ARG, "empty system");
+    int x0m = take_x0_mode();
+    pcg_work_alloc(P, n);
+    PcgWork& W = P.pcg;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    cudaGraphExec_t ex = full_graph(P, n, flexible, x0m, s);
+    CK(cudaEventRecord(e0, s));
+    PcgParams prm{eps, maxit};
+    CK(cudaMemcpyAsync(W.prm.p, &prm, sizeof prm, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(W.bnat.p, b, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
+    if (x0m == X0_GIVEN) CK(cudaMemcpyAsync(W.xnat.p, x, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
+    CK(cudaGraphLaunch(ex, s));
+    CK(cudaMemcpyAsync(x, W.xnat.p, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
+    CK(cudaEventRecord(e1, s));
+    PcgDev h;
+    CK(cudaMemcpyAsync(&h, W.d.p, sizeof(PcgDev), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    count_launches(start_launches(P, flexible) + (uint64_t)h.it * iteration_launches(P, flexible));
+    int rc;
+    std::string msg;
+    read_stats(h, st, rc, msg);
+    st.t_total_ms = ms;
+    if (rc != OK) set_last_error(msg);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Ensemble form: many independent solves (uneven sizes) as parallel branches
+// of one graph, launched once.
+// ---------------------------------------------------------------------------
+Ensemble::~Ensemble() {
+    if (exec) cudaGraphExecDestroy(exec);
+}
+
+std::unique_ptr<Ensemble> make_ensemble(const std::vector<Prec*>& members, bool flexible, int x0m,
+                                        cudaStream_t s) {
+    auto E = std::unique_ptr<Ensemble>(new Ensemble());
+    E->members = members;
+    E->flexible = flexible;
+    E->x0m = x0m;
+    cudaGraph_t g;
+    CK(cudaGraphCreate(&g, 0));
+    try {
+        for (Prec* P : members) {
+            uint32_t n = P->H->lv[0]->N;
+            pcg_work_alloc(*P, n);
+            append_pcg(g, *P, n, flexible, x0m, s);
+        }
+    } catch (...) {
+        cudaGraphDestroy(g);
+        throw;
+    }
+    E->exec = instantiate(g);
+    return E;
+}
+
+int ensemble_solve(Ensemble& E, const std::vector<const double*>& b, const std::vector<double*>& x, double eps,
+                   uint32_t maxit, std::vector<PcgStats>& st, double& ms_out, cudaStream_t s) {
+    if (maxit == 0) maxit = PCG_DEFAULT_MAXIT;
+    size_t K = E.members.size();
+    if (b.size() != K || x.size() != K) MLP_THROW(ERR_ARG, "one b and one x per ensemble member");
+    PcgParams prm{eps, maxit};
+    for (size_t i = 0; i < K; i++) {
+        Prec& P = *E.members[i];
+        uint32_t n = P.pcg.n;
+        CK(cudaMemcpyAsync(P.pcg.prm.p, &prm, sizeof prm, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(P.pcg.bnat.p, b[i], (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
+        if (E.x0m == X0_GIVEN) CK(cudaMemcpyAsync(P.pcg.xnat.p, x[i], (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
+    }
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, s));
+    CK(cudaGraphLaunch(E.exec, s));
+    CK(cudaEventRecord(e1, s));
+    std::vector<PcgDev> hs(K);
+    for (size_t i = 0; i < K; i++) {
+        Prec& P = *E.members[i];
+        CK(cudaMemcpyAsync(x[i], P.pcg.xnat.p, (size_t)P.pcg.n * 8, cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync(&hs[i], P.pcg.d.p, sizeof(PcgDev), cudaMemcpyDeviceToHost, s));
+    }
+    CK(cudaStreamSynchronize(s));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ms_out = ms;
+    st.resize(K);
+    int rc_all = OK;
+    std::string msg_all;
+    for (size_t i = 0; i < K; i++) {
+        int rc;
+        std::string msg;
+        read_stats(hs[i], st[i], rc, msg);
+        st[i].t_total_ms = ms;
+        count_launches(start_launches(*E.members[i], E.flexible) +
+                       (uint64_t)hs[i].it * iteration_launches(*E.members[i], E.flexible));
+        if (rc != OK && rc_all == OK) { rc_all = rc; msg_all = "member " + std::to_string(i) + ": " + msg; }
+    }
+    if (rc_all != OK) set_last_error(msg_all);
+    return rc_all;
+}
+
+// Host-driven form of pcg_solve (one host round trip per iteration), kept as
+// the reference point of the device loop in the tests.
+int pcg_solve_hostloop(const DCSR& A, const double* b, Prec& P, double* x, double eps, uint32_t maxit,
+                       bool flexible, PcgStats& st, cudaStream_t s) {
     if (maxit == 0) maxit = PCG_DEFAULT_MAXIT;
     Hierarchy& H = *P.H;
     const Level& L0 = *H.lv[0];
@@ -1088,7 +1414,9 @@ int pcg_solve(const DCSR& A, const double* b, Prec& P, double* x, double eps, ui
     dd.zero(s);
     PcgDev* d = dd.p;
     gather(n, L0.phi.p, b, bf.p, s);
-    gather(n, L0.phi.p, x0_device(n, s), xf.p, s);
+    int x0m = take_x0_mode();
+    if (x0m == X0_ZERO) xf.zero(s);
+    else gather(n, L0.phi.p, x0m == X0_GIVEN ? x : x0_device(n, s), xf.p, s);
     // r = b - A x
     launch_spmv<double>(n, Af.nnz, Af.ia.p, Af.ja.p, Af.a.p, xf.p, r, bf.p, s, Af.tile_max);
     CK_LAUNCH();

@@ -27,6 +27,24 @@ struct Plan {
 
 template <class T>
 struct SmallPlan;
+struct PcgDev;
+
+struct PcgParams {
+    double eps;
+    uint32_t maxit;
+};
+
+// Device-resident PCG state of one preconditioner handle: the solver vectors
+// and the whole-solve graphs (start, a conditional WHILE node whose body is one
+// iteration, scatter), kept between solves of the same size.
+struct PcgWork {
+    uint32_t n = 0;
+    DBuf<double> xf, bf, p, Ap, rprev, partials, bnat, xnat;
+    DBuf<PcgDev> d;
+    DBuf<PcgParams> prm;
+    cudaGraphExec_t full[6] = {};  // [flexible * 3 + x0 mode]
+    ~PcgWork();
+};
 
 struct Prec {
     std::unique_ptr<Hierarchy> H;
@@ -44,6 +62,7 @@ struct Prec {
     cudaGraphExec_t graph = nullptr;
     cudaStream_t stream = nullptr;
     uint64_t bytes_per_apply = 0;  // algorithmic bytes of one apply
+    PcgWork pcg;
     Prec();
     ~Prec();
 };
@@ -78,6 +97,30 @@ int pcg_solve(const DCSR& A, const double* b, Prec& P, double* x, double eps, ui
 int pcg_solve_noalloc(const DCSR& A, const double* b, Prec& P, double* x, double eps, uint32_t maxit,
                       bool flexible, PcgStats& st, cudaStream_t s);
 uint32_t pcg_noalloc_max_n();
+
+// Start vector of pcg_solve: the reference's generate_x0 (default), zero, or
+// the values already in x.
+enum X0Mode : int { X0_GENERATE = 0, X0_ZERO = 1, X0_GIVEN = 2 };
+void set_pcg_x0_mode(int mode);  // per thread, consumed by the next pcg_solve
+
+int pcg_solve_hostloop(const DCSR& A, const double* b, Prec& P, double* x, double eps, uint32_t maxit,
+                       bool flexible, PcgStats& st, cudaStream_t s);
+
+// Ensemble form: independent solves of several handles in one graph launch.
+struct Ensemble {
+    std::vector<Prec*> members;
+    bool flexible = false;
+    int x0m = 0;
+    cudaGraphExec_t exec = nullptr;
+    ~Ensemble();
+};
+std::unique_ptr<Ensemble> make_ensemble(const std::vector<Prec*>& members, bool flexible, int x0m, cudaStream_t s);
+int ensemble_solve(Ensemble& E, const std::vector<const double*>& b, const std::vector<double*>& x, double eps,
+                   uint32_t maxit, std::vector<PcgStats>& st, double& ms, cudaStream_t s);
+
+// Gradient of J with respect to ln K per cell (adjoint.cu).
+void spe_grad_logk(uint32_t nx, uint32_t ny, uint32_t nz, const double* kx, const double* ky, const double* kz,
+                   int dirichlet, const double* p, const double* lam, double* g, cudaStream_t s);
 
 // Cached x0 (generate_x0 depends only on n).
 const double* x0_device(uint32_t n, cudaStream_t s);

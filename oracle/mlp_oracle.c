@@ -747,12 +747,18 @@ void or_prec_apply(const or_prec* P, const double* f, double* x) {
 /* ---- PCG (pcg.cc:8-102) ---------------------------------------------------- */
 int or_pcg(const or_csr* A, const double* b, const or_prec* P, double* x, double eps,
            uint32_t* niter_out, double* final_rel, uint32_t maxit) {
+    return or_pcg_ex(A, b, P, x, eps, niter_out, final_rel, maxit, 0);
+}
+
+int or_pcg_ex(const or_csr* A, const double* b, const or_prec* P, double* x, double eps,
+              uint32_t* niter_out, double* final_rel, uint32_t maxit, int x0_mode) {
     uint32_t n = A->nrow;
     double* r = (double*)malloc(8 * (size_t)n);
     double* z = (double*)malloc(8 * (size_t)n);
     double* p = (double*)malloc(8 * (size_t)n);
     double* Ap = (double*)malloc(8 * (size_t)n);
-    or_generate_x0(x, n);
+    if (x0_mode == 1) memset(x, 0, 8 * (size_t)n);
+    else or_generate_x0(x, n);
     or_spmv(A, x, r);
     for (uint32_t i = 0; i < n; i++) r[i] = b[i] - r[i];
     double norm = sqrt(ddot(r, r, n)), init_norm = norm;
@@ -785,4 +791,41 @@ int or_pcg(const or_csr* A, const double* b, const or_prec* P, double* x, double
     *final_rel = norm / init_norm;
     free(r); free(z); free(p); free(Ap);
     return rc;
+}
+
+/* ---- differentiation form ------------------------------------------------
+ * dT/dtheta_i = 2 k_i k_j^2 / (h^2 (k_i + k_j)^2) for the harmonic-mean link of
+ * spe.cc:84 with k = K * (axis scale); dtD/dtheta = tD for the Dirichlet faces.
+ * g_c = -sum_j dT_cj (lam_c - lam_j)(p_c - p_j) - face: tD lam_c (p_c - p_D). */
+static double dT_dtheta(double ki, double kj, double h) {
+    double s = ki + kj;
+    return 2 * ki * kj * kj / (h * h * s * s);
+}
+
+void or_grad_logk(uint32_t nx, uint32_t ny, uint32_t nz, const double* kx, const double* ky, const double* kz,
+                  int dirichlet, const double* p, const double* lam, double* g) {
+    const double hx = 20, hy = 10, hz = 2;
+#define IDXK2(i, j, k) (((k) * KNY * KNX + (j) * KNX + (i)) % KN)
+#define TERM(cond, K, H, o, ii, jj, kk) \
+    if (cond) acc += dT_dtheta(K[me], K[IDXK2(ii, jj, kk)], H) * (lam[r] - lam[o]) * (p[r] - p[o]);
+    for (uint32_t k = 0; k < nz; k++)
+        for (uint32_t j = 0; j < ny; j++)
+            for (uint32_t i = 0; i < nx; i++) {
+                uint32_t r = (k * ny + j) * nx + i, me = IDXK2(i, j, k);
+                double acc = 0;
+                TERM(k > 0, kz, hz, r - nx * ny, i, j, k - 1)
+                TERM(j > 0, ky, hy, r - nx, i, j - 1, k)
+                TERM(i > 0, kx, hx, r - 1, i - 1, j, k)
+                TERM(i + 1 < nx, kx, hx, r + 1, i + 1, j, k)
+                TERM(j + 1 < ny, ky, hy, r + nx, i, j + 1, k)
+                TERM(k + 1 < nz, kz, hz, r + nx * ny, i, j, k + 1)
+                if (dirichlet) {
+                    double tD = 2 * kx[me] / (hx * hx);
+                    if (i == 0) acc += tD * lam[r] * (p[r] - 1.0);
+                    if (i == nx - 1) acc += tD * lam[r] * p[r];
+                }
+                g[r] = -acc;
+            }
+#undef TERM
+#undef IDXK2
 }

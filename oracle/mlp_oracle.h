@@ -98,6 +98,16 @@ const or_level* or_prec_level(const or_prec* P, uint32_t l);
 int or_pcg(const or_csr* A, const double* b, const or_prec* P, double* x, double eps,
            uint32_t* niter, double* final_rel, uint32_t maxit);
 
+/* or_pcg with a choice of start: x0_mode 0 = generate_x0, 1 = zero. */
+int or_pcg_ex(const or_csr* A, const double* b, const or_prec* P, double* x, double eps,
+              uint32_t* niter, double* final_rel, uint32_t maxit, int x0_mode);
+
+/* Differentiation form (no reference counterpart): dJ/d(ln K) per cell for
+ * the SPE matrix with Dirichlet x-faces, given p (A p = b) and lambda
+ * (A lambda = dJ/dp); the same formula as the CUDA kernel, in FP64 on the CPU. */
+void or_grad_logk(uint32_t nx, uint32_t ny, uint32_t nz, const double* kx, const double* ky, const double* kz,
+                  int dirichlet, const double* p, const double* lam, double* g);
+
 /* Dense LU without pivoting, in place (row-major n x n) and its solve. */
 int or_dense_lu(double* a, uint32_t n);
 void or_dense_lu_solve(const double* lu, uint32_t n, const double* b, double* x);

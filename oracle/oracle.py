@@ -75,6 +75,9 @@ def lib():
         L.or_pcg.argtypes = [C.POINTER(CSR), f64p, C.c_void_p, f64p, C.c_double,
                              C.POINTER(C.c_uint32), C.POINTER(C.c_double), C.c_uint32]
         L.or_csr_free.argtypes = [C.POINTER(CSR)]
+        L.or_pcg_ex.argtypes = [C.POINTER(CSR), f64p, C.c_void_p, f64p, C.c_double,
+                                C.POINTER(C.c_uint32), C.POINTER(C.c_double), C.c_uint32, C.c_int]
+        L.or_grad_logk.argtypes = [C.c_uint32] * 3 + [f64p] * 3 + [C.c_int, f64p, f64p, f64p]
         L.or_cheb.argtypes = [C.c_double, C.c_uint32]
         L.or_cheb.restype = C.c_double
         _lib = L
@@ -196,14 +199,24 @@ class Prec:
         return x
 
 
-def pcg(A: Matrix, b, P: Prec, eps=1e-8, maxit=0):
-    """PCGSolver restated; returns (x, niter, final_rel, rc)."""
+def pcg(A: Matrix, b, P: Prec, eps=1e-8, maxit=0, x0_zero=False):
+    """PCGSolver restated; returns (x, niter, final_rel, rc). rc -3: cap reached."""
     b = np.ascontiguousarray(b, np.float64)
     x = np.zeros(A.n)
     it = C.c_uint32(0)
     rel = C.c_double(0)
-    rc = lib().or_pcg(A.c, _p(b, f64p), P.h, _p(x, f64p), eps, C.byref(it), C.byref(rel), maxit)
+    rc = lib().or_pcg_ex(A.c, _p(b, f64p), P.h, _p(x, f64p), eps, C.byref(it), C.byref(rel), maxit,
+                         1 if x0_zero else 0)
     return x, it.value, rel.value, rc
+
+
+def grad_logk(nx, ny, nz, kx, ky, kz, p, lam, dirichlet=True):
+    """CPU FP64 dJ/d(ln K) per cell (differentiation form)."""
+    kx, ky, kz, p, lam = (np.ascontiguousarray(v, np.float64) for v in (kx, ky, kz, p, lam))
+    g = np.empty(nx * ny * nz)
+    lib().or_grad_logk(nx, ny, nz, _p(kx, f64p), _p(ky, f64p), _p(kz, f64p), int(dirichlet), _p(p, f64p),
+                       _p(lam, f64p), _p(g, f64p))
+    return g
 
 
 # ---- reference driver -------------------------------------------------------

@@ -126,3 +126,30 @@ def test_full_size_hierarchy_and_pcg_against_oracle(M):
     xo, it, rel, rc = O.pcg(Ao, bo, Po, 1e-8)
     assert rc == 0 and abs(st.niter - it) <= 1
     assert np.linalg.norm(x - xo) <= 1e-9 * np.linalg.norm(xo)
+
+
+@pytest.mark.parametrize("fp32", [False, True])
+def test_device_loop_matches_host_loop(M, fp32, monkeypatch):
+    """A solve runs as one graph launch (start, conditional WHILE loop,
+    scatter); the host-driven loop (one round trip per iteration) must give the
+    same iterates."""
+    g = load_golden("ms_layered_16x22x8_c01")
+    A = gpu_matrix(M, g)
+    P = gpu_prec(A, g, fp32=fp32)
+    st1 = M.SolverStats()
+    x1 = M.PCGSolver(A, g["b"], P, stats=st1, eps=1e-8)
+    monkeypatch.setenv("MLP_PCG_HOSTLOOP", "1")
+    st2 = M.SolverStats()
+    x2 = M.PCGSolver(A, g["b"], P, stats=st2, eps=1e-8)
+    assert st1.niter == st2.niter
+    assert np.array_equal(x1, x2)
+
+
+def test_iteration_cap_ends_the_device_loop(M):
+    """An unreachable tolerance stops at the cap with MLP_ERR_MAXIT."""
+    g = load_golden("ms_iid_12x22x6")
+    A = gpu_matrix(M, g)
+    P = gpu_prec(A, g)
+    with pytest.raises(M.MlpError) as e:
+        M.PCGSolver(A, g["b"], P, eps=1e-30, maxit=7)
+    assert e.value.code == 6
