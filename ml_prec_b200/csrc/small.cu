@@ -395,8 +395,17 @@ void build_small(Hierarchy& H, SmallPlan<T>& sp, uint32_t budget, cudaStream_t s
     }
     if (best < 0) return;
     if (!pack<T>(H, (uint32_t)best, sp, budget, false, keep, s)) return;
-    CK(cudaFuncSetAttribute(k_small<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.h.bytes_total));
-    CK(cudaFuncSetAttribute(k_small_columns<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.h.bytes_total));
+    // The attribute belongs to the kernel, not to this plan: several plans (of
+    // different sizes) live in one process, so it is set once to the largest
+    // size any plan may use and never lowered.
+    static int set_for[2] = {0, 0};
+    int& done = set_for[std::is_same<T, double>::value ? 0 : 1];
+    if (!done) {
+        int mx = (int)(limit - stat);
+        CK(cudaFuncSetAttribute(k_small<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+        CK(cudaFuncSetAttribute(k_small_columns<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+        done = 1;
+    }
     // The recursive solve nests one call per level (about 150 bytes of stack
     // each); raise the per-thread stack limit when the default is too small.
     size_t need = 256 + (size_t)(sp.h.nlev + 2) * 256, cur = 0;

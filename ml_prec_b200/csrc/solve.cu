@@ -321,6 +321,25 @@ __global__ void k_scatter(uint32_t n, const uint32_t* __restrict__ idx, const do
     if (i < n) dst[idx[i]] = src[i];
 }
 
+// Replays the recorded launches. With MLP_CAPTURE_DEBUG=1 every launch is
+// checked right away, so a failure names the launch that caused it.
+void Plan::run(cudaStream_t s) const {
+    static int dbg = -1;
+    if (dbg < 0) {
+        const char* e = getenv("MLP_CAPTURE_DEBUG");
+        dbg = (e && e[0] == '1') ? 1 : 0;
+    }
+    for (size_t i = 0; i < ops.size(); i++) {
+        ops[i](s);
+        if (dbg) {
+            cudaError_t e = cudaPeekAtLastError();
+            if (e != cudaSuccess)
+                MLP_THROW(ERR_CUDA, "plan op " + std::to_string(i) + " of " + std::to_string(ops.size()) + ": " +
+                                        cudaGetErrorString(e));
+        }
+    }
+}
+
 void gather(uint32_t n, const uint32_t* idx, const double* src, double* dst, cudaStream_t s) {
     if (!n) return;
     k_gather<<<grid_for(n, 256), 256, 0, s>>>(n, idx, src, dst);
@@ -1189,12 +1208,16 @@ static void append_pcg(cudaGraph_t g, Prec& P, uint32_t n, bool flexible, int x0
     // start
     CK(cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     k_zero_dev<<<1, 32, 0, s>>>(d);
+    CK(cudaPeekAtLastError());
     gather(n, L0.phi.p, W.bnat.p, W.bf.p, s);
     if (x0m == X0_ZERO) k_fill_d<<<grid_for(n, 256), 256, 0, s>>>(n, W.xf.p, 0.0);
     else gather(n, L0.phi.p, x0m == X0_GIVEN ? W.xnat.p : x0, W.xf.p, s);
     launch_spmv<double>(n, Af.nnz, Af.ia.p, Af.ja.p, Af.a.p, W.xf.p, r, W.bf.p, s, Af.tile_max);
+    CK(cudaPeekAtLastError());
     k_dot_simple<<<G, RB, 0, s>>>(n, r, r, W.partials.p, &d->ticket[1], &d->rr);
+    CK(cudaPeekAtLastError());
     P.plan.run(s);
+    CK(cudaPeekAtLastError());
     k_copy_d<<<grid_for(n, 256), 256, 0, s>>>(n, z, W.p.p);
     k_dot_simple<<<G, RB, 0, s>>>(n, r, z, W.partials.p, &d->ticket[2], &d->rz0);
     if (flexible) k_copy_d<<<grid_for(n, 256), 256, 0, s>>>(n, r, W.rprev.p);

@@ -20,9 +20,7 @@ struct LevelWork {
 struct Plan {
     std::vector<std::function<void(cudaStream_t)>> ops;
     size_t launches = 0;
-    void run(cudaStream_t s) const {
-        for (auto& f : ops) f(s);
-    }
+    void run(cudaStream_t s) const;
 };
 
 template <class T>
