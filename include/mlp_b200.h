@@ -115,6 +115,8 @@ int mlp_matrix_size(const mlp_matrix* A, uint32_t* n, uint32_t* nnz);
 int mlp_matrix_download(const mlp_matrix* A, uint32_t* ia_host, uint32_t* ja_host, double* a_host);
 /* y = A x (multiply(A, v, res, 'o'), csrmatrix.cc:260-274), device vectors. */
 int mlp_spmv(const mlp_matrix* A, const double* x_dev, double* y_dev, void* stream);
+/* Same with host vectors (copies in and out; the matrix's own stream). */
+int mlp_spmv_host(const mlp_matrix* A, const double* x_host, double* y_host);
 
 /* ---- preconditioners -------------------------------------------------------
  * mlp_prec_create replaces MultiSplitPrec(const SkylineMatrix&, const Config&)

@@ -20,7 +20,7 @@ f64p = C.POINTER(C.c_double)
 EXPORTS = [
     "mlp_last_error", "mlp_version", "mlp_device_count", "mlp_set_device",
     "mlp_matrix_create", "mlp_matrix_create_spe", "mlp_matrix_destroy", "mlp_matrix_size",
-    "mlp_matrix_download", "mlp_spmv",
+    "mlp_matrix_download", "mlp_spmv", "mlp_spmv_host",
     "mlp_prec_create", "mlp_prec_destroy", "mlp_prec_apply", "mlp_prec_apply_host", "mlp_prec_nlevels",
     "mlp_prec_level_info", "mlp_prec_level_export", "mlp_prec_bytes_per_apply",
     "mlp_pcg", "mlp_pcg_device", "mlp_pcg_device_x0", "mlp_matrix_grad_logk", "mlp_pcg_device_noalloc",
@@ -85,6 +85,7 @@ def lib():
         L.mlp_matrix_size.argtypes = [vp, u32p, u32p]
         L.mlp_matrix_download.argtypes = [vp, u32p, u32p, f64p]
         L.mlp_spmv.argtypes = [vp, vp, vp, vp]
+        L.mlp_spmv_host.argtypes = [vp, f64p, f64p]
         L.mlp_prec_create.argtypes = [vp, C.POINTER(PrecCfg), C.POINTER(vp)]
         L.mlp_prec_destroy.argtypes = [vp]
         L.mlp_prec_apply.argtypes = [vp, vp, vp, vp]

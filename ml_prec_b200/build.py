@@ -1,4 +1,6 @@
-"""Builds the CUDA library ml_prec_b200/lib/libmlp_b200.so for sm_100a.
+"""Builds the CUDA library ml_prec_b200/lib/libmlp_b200.so for sm_100a, the
+C++ host interface lib/libml_prec_host.so above it (host/ml_prec.h, the
+reference's types and calls) and the command-line driver lib/ml_prec_b200.
 
 Each .cu file under csrc/ is compiled with nvcc; setup.cu (the hierarchy
 construction) is compiled with -fmad=false so that its floating-point
@@ -15,6 +17,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "lib")
 LIB = os.path.join(OUT, "libmlp_b200.so")
+HOST = os.path.join(HERE, "host")
+HOST_LIB = os.path.join(OUT, "libml_prec_host.so")
+HOST_EXE = os.path.join(OUT, "ml_prec_b200")
+INCLUDE = os.path.join(HERE, "..", "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
@@ -58,7 +64,28 @@ def build(verbose: bool = False, force: bool = False) -> str:
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
+    build_host(verbose, force)
     return LIB
+
+
+def build_host(verbose: bool = False, force: bool = False):
+    """g++ build of the C++ host interface and driver, linked to the CUDA library."""
+    hdrs = [os.path.join(HOST, "ml_prec.h"), os.path.join(INCLUDE, "mlp_b200.h")]
+    flags = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-I" + HOST, "-I" + INCLUDE]
+    rpath = "-Wl,-rpath,$ORIGIN"
+    steps = [
+        (HOST_LIB, [os.path.join(HOST, "ml_prec.cc")] + hdrs + [LIB],
+         ["g++"] + flags + ["-shared", os.path.join(HOST, "ml_prec.cc"), "-o", HOST_LIB, "-L" + OUT, "-lmlp_b200",
+                            rpath]),
+        (HOST_EXE, [os.path.join(HOST, "main.cc"), HOST_LIB] + hdrs,
+         ["g++"] + flags + [os.path.join(HOST, "main.cc"), "-o", HOST_EXE, "-L" + OUT, "-lml_prec_host",
+                            "-lmlp_b200", rpath]),
+    ]
+    for target, deps, cmd in steps:
+        if force or _stale(target, deps):
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            subprocess.run(cmd, check=True)
 
 
 if __name__ == "__main__":

@@ -14,6 +14,7 @@ struct mlp_matrix {
     DBuf<double> field;  // kx, ky, kz blocks (3 x 1,122,000)
     uint32_t nx = 0, ny = 0, nz = 0;
     int32_t dirichlet = 0;
+    DBuf<double> tmp_x, tmp_y;  // staging of mlp_spmv_host
     ~mlp_matrix() {
         if (s) cudaStreamDestroy(s);
     }
@@ -160,6 +161,19 @@ int mlp_spmv(const mlp_matrix* A, const double* x, double* y, void* stream) {
     cudaStream_t s = stream ? (cudaStream_t)stream : A->s;
     spmv(A->A, x, y, s);
     if (!stream) CK(cudaStreamSynchronize(s));
+    API_END
+}
+
+int mlp_spmv_host(const mlp_matrix* A, const double* x, double* y) {
+    API_BEGIN
+    if (!A || !x || !y) MLP_THROW(ERR_ARG, "null pointer");
+    auto* M = const_cast<mlp_matrix*>(A);
+    M->tmp_x.alloc(A->A.ncol);
+    M->tmp_y.alloc(A->A.nrow);
+    CK(cudaMemcpyAsync(M->tmp_x.p, x, (size_t)A->A.ncol * 8, cudaMemcpyHostToDevice, A->s));
+    spmv(A->A, M->tmp_x.p, M->tmp_y.p, A->s);
+    CK(cudaMemcpyAsync(y, M->tmp_y.p, (size_t)A->A.nrow * 8, cudaMemcpyDeviceToHost, A->s));
+    CK(cudaStreamSynchronize(A->s));
     API_END
 }
 

@@ -2,8 +2,8 @@
 size, solved (forward and adjoint) as parallel branches of one CUDA graph.
 
 Each realization r gets its own mesh nx in [30, 60], ny in [110, 220],
-nz in [10, 85] (seeded) and its own i.i.d. log-normal field (the config-1
-model), its own matrix and FP32-stored multi-split hierarchy; the forward
+nz in [10, 85] (seeded) and its own i.i.d. log-normal field (the
+small-mesh model), its own matrix and FP32-stored multi-split hierarchy; the forward
 solves (right-hand side from the Dirichlet faces) and the adjoint solves
 (misfit gradient at 25 observation cells) of all realizations each run as one
 graph launch (mlp_ensemble_solve). Sharding the ensemble over several GPUs
