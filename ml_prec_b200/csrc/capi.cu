@@ -133,6 +133,7 @@ int mlp_matrix_create_spe(uint32_t nx, uint32_t ny, uint32_t nz, const double* k
 int mlp_matrix_destroy(mlp_matrix* A) {
     API_BEGIN
     delete A;
+    pool_sync_recycle();  // the released buffers become reusable once the device is idle
     API_END
 }
 
@@ -230,6 +231,7 @@ int mlp_prec_create(const mlp_matrix* A, const mlp_prec_cfg* c, mlp_prec** out) 
 int mlp_prec_destroy(mlp_prec* P) {
     API_BEGIN
     delete P;
+    pool_sync_recycle();  // the released buffers become reusable once the device is idle
     API_END
 }
 
@@ -485,6 +487,7 @@ int mlp_ensemble_solve(mlp_ensemble* E, const double* const* b_dev, double* cons
 int mlp_ensemble_destroy(mlp_ensemble* E) {
     API_BEGIN
     delete E;
+    pool_sync_recycle();  // the released buffers become reusable once the device is idle
     API_END
 }
 

@@ -59,8 +59,18 @@ uint64_t launch_count();
 void set_last_error(const std::string& s);
 const char* last_error();
 
-// Device buffer (RAII). Allocations go through cudaMallocAsync on the library's
-// stream so that repeated setups reuse the pool.
+// Device buffer pool. Released buffers are kept for reuse instead of being
+// given back with cudaFree (which synchronises the device and, with cudaMalloc,
+// dominated repeated setups). A released buffer may still be in use by queued
+// work, so it becomes reusable only at pool_recycle(dev), which callers invoke
+// right after a cudaDeviceSynchronize (the end of a build scope, the destroy
+// entry points); pool_sync_recycle() does both.
+void* pool_alloc(size_t bytes);
+void pool_release(void* p);
+void pool_recycle(int dev);
+void pool_sync_recycle();
+
+// Device buffer (RAII) on the pool.
 template <class T>
 struct DBuf {
     T* p = nullptr;
@@ -80,10 +90,10 @@ struct DBuf {
     void alloc(size_t count) {
         release();
         n = count;
-        if (count) CK(cudaMalloc(&p, count * sizeof(T) + 16));
+        if (count) p = static_cast<T*>(pool_alloc(count * sizeof(T) + 16));
     }
     void release() {
-        if (p) cudaFree(p);
+        if (p) pool_release(p);
         p = nullptr;
         n = 0;
     }
@@ -107,7 +117,7 @@ struct DBuf {
 // synchronisation and page mapping dominated short setups). An ArenaScope
 // takes the device's lock for its lifetime, so builds in one process are
 // serialised; Tmp<T> buffers created inside a scope come from the arena, outside
-// one they fall back to an ordinary allocation.
+// one they fall back to the buffer pool.
 void* arena_take(size_t bytes);  // null when no scope is active
 struct ArenaScope {
     ArenaScope();
@@ -134,12 +144,12 @@ struct Tmp {
         size_t bytes = count * sizeof(T) + 16;
         p = static_cast<T*>(arena_take(bytes));
         if (!p) {
-            CK(cudaMalloc(&p, bytes));
+            p = static_cast<T*>(pool_alloc(bytes));
             owned = true;
         }
     }
     void release() {
-        if (p && owned) cudaFree(p);
+        if (p && owned) pool_release(p);
         p = nullptr;
         n = 0;
         owned = false;

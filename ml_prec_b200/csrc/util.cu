@@ -90,6 +90,7 @@ ArenaScope::~ArenaScope() {
     if (--t_arena_depth == 0) {
         // the scope's work must be finished before the memory is reused
         cudaDeviceSynchronize();
+        pool_recycle(dev);
         DevArena* a = t_arena;
         t_arena = nullptr;
         a->mu.unlock();
@@ -111,6 +112,94 @@ void* arena_take(size_t bytes) {
     CK(cudaMalloc(&base, cap));
     a->chunks.push_back({base, cap, bytes});
     return base;
+}
+
+// ---- device buffer pool -------------------------------------------------------
+namespace {
+struct Pool {
+    std::mutex mu;
+    struct Block { int dev; size_t bytes; bool pending; };
+    std::map<void*, Block> live;                           // handed out or pending
+    std::map<int, std::multimap<size_t, void*>> free_;     // per device: reusable blocks by size
+    std::map<int, std::vector<void*>> pending;             // released, maybe still in use
+};
+Pool& pool() {
+    static Pool* p = new Pool();  // never destroyed: buffers may be released during exit
+    return *p;
+}
+// Size classes: four per octave above 4 KB (at most 25% slack).
+size_t size_class(size_t b) {
+    if (b <= 4096) return 4096;
+    int lg = 63 - __builtin_clzll((unsigned long long)(b - 1));
+    size_t step = (size_t)1 << (lg - 2);
+    return (b + step - 1) & ~(step - 1);
+}
+}  // namespace
+
+void* pool_alloc(size_t bytes) {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    size_t cls = size_class(bytes);
+    Pool& P = pool();
+    {
+        std::lock_guard<std::mutex> lk(P.mu);
+        auto& fl = P.free_[dev];
+        auto it = fl.find(cls);
+        if (it != fl.end()) {
+            void* p = it->second;
+            fl.erase(it);
+            P.live[p] = {dev, cls, false};
+            return p;
+        }
+    }
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, cls);
+    if (e != cudaSuccess) {
+        // out of memory: give the cached blocks back and try once more
+        cudaGetLastError();
+        CK(cudaDeviceSynchronize());
+        {
+            std::lock_guard<std::mutex> lk(P.mu);
+            for (void* q : P.pending[dev]) { P.free_[dev].emplace(P.live[q].bytes, q); P.live.erase(q); }
+            P.pending[dev].clear();
+            for (auto& kv : P.free_[dev]) cudaFree(kv.second);
+            P.free_[dev].clear();
+        }
+        CK(cudaMalloc(&p, cls));
+    }
+    std::lock_guard<std::mutex> lk(P.mu);
+    P.live[p] = {dev, cls, false};
+    return p;
+}
+
+void pool_release(void* p) {
+    if (!p) return;
+    Pool& P = pool();
+    std::lock_guard<std::mutex> lk(P.mu);
+    auto it = P.live.find(p);
+    if (it == P.live.end() || it->second.pending) return;
+    it->second.pending = true;
+    P.pending[it->second.dev].push_back(p);
+}
+
+void pool_recycle(int dev) {
+    Pool& P = pool();
+    std::lock_guard<std::mutex> lk(P.mu);
+    auto& pend = P.pending[dev];
+    for (void* q : pend) {
+        auto it = P.live.find(q);
+        if (it == P.live.end()) continue;
+        P.free_[dev].emplace(it->second.bytes, q);
+        P.live.erase(it);
+    }
+    pend.clear();
+}
+
+void pool_sync_recycle() {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceSynchronize());
+    pool_recycle(dev);
 }
 
 int num_sms() {
