@@ -435,6 +435,156 @@ __global__ void __launch_bounds__(256) k_update(uint32_t n, const uint32_t* __re
     }
 }
 
+// ---- fused level solve (one cluster) ------------------------------------------
+// A whole MultiSplitPrec::solve(l, f, x) call of a mid-size level whose coarse
+// sub-hierarchy is tabulated as one dense operator: all niter sweeps (phase 1,
+// the dense coarse product, phase 2, the residual / correction step) in ONE
+// launch of one thread-block cluster, with a cluster barrier between the
+// steps instead of a kernel boundary. The level's matrices and vectors are
+// read through L2 (they are a few MB); vectors written inside the kernel are
+// read with ld.global.cg so that no stale L1 line is used after a barrier.
+// Each step sums in the same order as the separate kernels (k_phase1,
+// k_dense_gemv, k_phase2, k_spmv_staged / k_spmv, k_update), so both paths give
+// identical results.
+template <class T>
+struct MidArgs {
+    uint32_t N, M, R, n, niter;
+    int lpr1, lpr2, lprr, lpru;  // lanes per row: P1, G, residual, correction
+    const uint32_t *p1_ia, *p1_ja, *g_ia, *g_ja, *af_ia, *af_ja;
+    const T *p1_a, *g_a, *af_a, *dval, *C;
+    const T* f;
+    T *x, *w, *r, *u0;
+};
+
+__device__ __forceinline__ void cluster_barrier() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+template <class T>
+__device__ __forceinline__ T ldcg(const T* p) { return __ldcg(p); }
+
+// Row-group loop: groups of lpr lanes take rows base + group; every lane of a
+// warp runs the same trip count, so the shuffles see full warps.
+template <class T, class Val, class Store>
+__device__ __forceinline__ void csr_rows(uint32_t nrows, int lpr, const uint32_t* __restrict__ ia,
+                                         const uint32_t* __restrict__ ja, const T* __restrict__ a, Val val,
+                                         Store store) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t nth = gridDim.x * blockDim.x;
+    const uint32_t groups = nth / lpr, g = tid / lpr;
+    const int lane = tid % lpr;
+    for (uint32_t base = 0; base < nrows; base += groups) {
+        uint32_t row = base + g;
+        bool act = row < nrows;
+        T s = 0;
+        if (act) {
+            uint32_t e = __ldg(ia + row + 1);
+            for (uint32_t j = __ldg(ia + row) + lane; j < e; j += lpr) s += __ldg(a + j) * val(__ldg(ja + j));
+        }
+        for (int o = lpr / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (act && lane == 0) store(row, s);
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(1024) k_mid_level(MidArgs<T> A) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t nth = gridDim.x * blockDim.x;
+    const uint32_t N = A.N, M = A.M, R = A.R, n = A.n;
+    T* w = A.w;
+    for (uint32_t it = 1; it <= A.niter; it++) {
+        const T* src = it == 1 ? A.f : A.r;
+        T* out = it == 1 ? A.x : A.u0;
+        // phase 1: w = P1 src (rows < R); out = dval * src (rows >= R)
+        csr_rows<T>(R, A.lpr1, A.p1_ia, A.p1_ja, A.p1_a, [&](uint32_t c) { return ldcg(src + c); },
+                    [&](uint32_t row, T v) { w[row] = v; });
+        for (uint32_t q = R + tid; q < N; q += nth) out[q] = __ldg(A.dval + (q - R)) * ldcg(src + q);
+        cluster_barrier();
+        // coarse slice: out[M + i] = sum_j C_ij w[M + j], one warp per row
+        {
+            const uint32_t warp = tid >> 5, nwarp = nth >> 5;
+            const int lane = threadIdx.x & 31;
+            for (uint32_t row = warp; row < n; row += nwarp) {
+                const T* c = A.C + (size_t)row * n;
+                T s = 0;
+                for (uint32_t j = lane; j < n; j += 32) s += __ldg(c + j) * ldcg(w + M + j);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+                if (lane == 0) out[M + row] = s;
+            }
+        }
+        cluster_barrier();
+        // phase 2: out_q = sum_j G_qj (j < M ? w_j : out_j), q < M
+        csr_rows<T>(M, A.lpr2, A.g_ia, A.g_ja, A.g_a, [&](uint32_t c) { return c < M ? ldcg(w + c) : ldcg(out + c); },
+                    [&](uint32_t row, T v) { out[row] = v; });
+        if (A.niter < 2) break;
+        cluster_barrier();
+        if (it == 1) {
+            // r = f - A x
+            csr_rows<T>(N, A.lprr, A.af_ia, A.af_ja, A.af_a, [&](uint32_t c) { return ldcg(A.x + c); },
+                        [&](uint32_t row, T v) { A.r[row] = ldcg(A.f + row) - v; });
+        } else if (it < A.niter) {
+            // x += u0; r -= A u0
+            csr_rows<T>(N, A.lpru, A.af_ia, A.af_ja, A.af_a, [&](uint32_t c) { return ldcg(A.u0 + c); },
+                        [&](uint32_t row, T v) {
+                            A.x[row] = ldcg(A.x + row) + ldcg(A.u0 + row);
+                            A.r[row] = ldcg(A.r + row) - v;
+                        });
+        } else {
+            for (uint32_t q = tid; q < N; q += nth) A.x[q] = ldcg(A.x + q) + ldcg(A.u0 + q);
+        }
+        if (it < A.niter) cluster_barrier();
+    }
+}
+
+// Cluster size of the fused level kernel: 16 CTAs of 1024 threads when the
+// device can co-schedule such a cluster, else 8; 0 disables the path
+// (MLP_MID=0 also disables it).
+template <class T>
+static int mid_cluster_size() {
+    const char* e = getenv("MLP_MID");
+    if (e && e[0] == '0') return 0;
+    static int cs = -1;
+    if (cs >= 0) return cs;
+    cs = 0;
+    cudaFuncSetAttribute(k_mid_level<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    for (int want : {16, 8}) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(want);
+        cfg.blockDim = dim3(1024);
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = want;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int nc = 0;
+        if (cudaOccupancyMaxActiveClusters(&nc, k_mid_level<T>, &cfg) == cudaSuccess && nc > 0) {
+            cs = want;
+            break;
+        }
+        cudaGetLastError();
+    }
+    return cs;
+}
+
+template <class T>
+static void launch_mid(const MidArgs<T>& a, int cs, cudaStream_t s) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cs);
+    cfg.blockDim = dim3(1024);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_mid_level<T>, a);
+}
+
 static int pick_lpr(uint32_t n, uint32_t nnz) {
     double avg = n ? (double)nnz / n : 1;
     return avg <= 1.5 ? 1 : avg <= 3 ? 2 : avg <= 6 ? 4 : avg <= 12 ? 8 : avg <= 24 ? 16 : 32;
@@ -625,6 +775,7 @@ struct Builder {
         Level& L = *H.lv[l];
         if (L.direct) { direct(L, f, x); return; }
         if (!explicit_solves) { ms_waves(l, f, x); return; }
+        if (mid_call(l, f, x)) return;
         LevelWork<T>& w = W[l];
         uint32_t N = L.N, M = L.M;
         bool next = l + 1 < H.nlevels && L.n;
@@ -650,6 +801,43 @@ struct Builder {
     }
 
     bool explicit_solves = true;
+
+    // The whole level-l call as one cluster launch (k_mid_level) when level
+    // l + 1 is the tabulated dense sub-hierarchy and level l is small enough
+    // for one cluster to sweep it.
+    static constexpr uint32_t MID_MAX_N = 1u << 17;
+    bool mid_call(uint32_t l, const T* f, T* x) {
+        Level& L = *H.lv[l];
+        if (!small || !small->valid() || !small->dense.p || small->first != l + 1) return false;
+        if (L.N > MID_MAX_N || !L.n || L.niter < 1) return false;
+        int cs = mid_cluster_size<T>();
+        if (!cs) return false;
+        LevelWork<T>& w = W[l];
+        MidArgs<T> a{};
+        a.N = L.N; a.M = L.M; a.R = L.N - L.Md; a.n = small->N0; a.niter = L.niter;
+        if (a.n != L.n) return false;
+        a.lpr1 = pick_lpr(a.R, L.P1.nnz);
+        a.lpr2 = pick_lpr(L.M, L.G.nnz);
+        bool staged = L.Af.tile_max && L.Af.tile_max <= ST_MAX_NNZ && L.N >= 4 * ST_ROWS;
+        a.lprr = staged ? 1 : pick_lpr(L.N, L.Af.nnz);
+        a.lpru = pick_lpr(L.N, L.Af.nnz);
+        a.p1_ia = L.P1.ia.p; a.p1_ja = L.P1.ja.p; a.p1_a = vals<T>(L.P1);
+        a.g_ia = L.G.ia.p; a.g_ja = L.G.ja.p; a.g_a = vals<T>(L.G);
+        a.af_ia = L.Af.ia.p; a.af_ja = L.Af.ja.p; a.af_a = vals<T>(L.Af);
+        a.dval = dvals<T>(L);
+        a.C = small->dense.p;
+        a.f = f; a.x = x; a.w = w.w.p; a.r = w.r.p; a.u0 = w.u0.p;
+        op([=](cudaStream_t s) { launch_mid<T>(a, cs, s); });
+        // bytes: the same as the separate steps
+        uint32_t R = a.R, N = L.N, M = L.M, n = a.n;
+        for (uint32_t it = 1; it <= L.niter; it++) {
+            bytes += (uint64_t)L.P1.nnz * (4 + sizeof(T)) + 4ull * (R + 1) + sizeof(T) * (2ull * N + L.Md);
+            bytes += (uint64_t)n * n * sizeof(T) + 2ull * n * sizeof(T);
+            if (M) bytes += (uint64_t)L.G.nnz * (4 + sizeof(T)) + 4ull * (M + 1) + sizeof(T) * (M + n + M);
+            if (L.niter >= 2) bytes += it == 1 ? spmv_bytes(L.Af) : sizeof(T) * 3ull * N + (it < L.niter ? spmv_bytes(L.Af) : 0);
+        }
+        return true;
+    }
 
     // Wavefront form of ms (the L and U solves one wavefront at a time).
     void ms_waves(uint32_t l, const T* f, T* x) {

@@ -22,12 +22,15 @@ def M():
     return M
 
 
-@pytest.fixture(params=["dense", "small", "explicit", "waves"])
+@pytest.fixture(params=["dense", "unfused", "small", "explicit", "waves"])
 def apply_path(request, monkeypatch):
     """Run each case through every apply path: the tabulated small-level
-    operator (default), the shared-memory small-level kernel (tabulation off),
-    the launch path with explicit triangular solves (small kernel off), and the
-    launch path with wavefront triangular solves."""
+    operator with the level above it fused into one cluster launch (default),
+    the same without the fused level kernel, the shared-memory small-level
+    kernel (tabulation off), the launch path with explicit triangular solves
+    (small kernel off), and the launch path with wavefront triangular solves."""
+    if request.param == "unfused":
+        monkeypatch.setenv("MLP_MID", "0")
     if request.param == "small":
         monkeypatch.setenv("MLP_DENSE_OP_MAX", "0")
     if request.param in ("explicit", "waves"):
@@ -153,3 +156,26 @@ def test_iteration_cap_ends_the_device_loop(M):
     with pytest.raises(M.MlpError) as e:
         M.PCGSolver(A, g["b"], P, eps=1e-30, maxit=7)
     assert e.value.code == 6
+
+
+@pytest.mark.parametrize("fp32", [False, True])
+def test_fused_level_kernel_is_identical_to_separate_launches(M, fp32, monkeypatch):
+    """60x220x85 layered field: the level above the tabulated sub-hierarchy
+    (26,907 rows) runs as one cluster launch; it sums in the same order as the
+    separate kernels, so the apply and the PCG iterates are bit-identical."""
+    from ml_prec_b200 import fields
+    kx, ky, kz = fields.field("layered", 2)
+    A, b = M.CSRMatrix.spe(60, 220, 85, kx, ky, kz, c=1.0)
+    f = np.random.default_rng(4).standard_normal(A.n)
+    kw = dict(q=(0.8,), niter=(5,), max_levels=15, degree_max=2, fp32=fp32)
+    P1 = M.MultiSplitPrec(A, **kw)
+    z1 = P1.solve(f)
+    st1 = M.SolverStats()
+    x1 = M.PCGSolver(A, b, P1, stats=st1, eps=1e-8)
+    monkeypatch.setenv("MLP_MID", "0")
+    P2 = M.MultiSplitPrec(A, **kw)
+    z2 = P2.solve(f)
+    st2 = M.SolverStats()
+    x2 = M.PCGSolver(A, b, P2, stats=st2, eps=1e-8)
+    assert np.array_equal(z1, z2)
+    assert st1.niter == st2.niter and np.array_equal(x1, x2)
