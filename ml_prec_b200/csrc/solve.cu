@@ -12,6 +12,8 @@
 #include <map>
 #include <mutex>
 
+#include <cooperative_groups.h>
+
 #include "small.cuh"
 #include "solve.cuh"
 
@@ -51,6 +53,26 @@ __global__ void __launch_bounds__(256) k_spmv(uint32_t n, const uint32_t* __rest
 static constexpr uint32_t ST_ROWS = 256;
 static constexpr uint32_t ST_MAX_NNZ = 3072;
 
+// Row sum of a staged tile: sum_j s_a[j - ba] * x[s_ja[j - bj]] over [j, je),
+// accumulated in column order; the column indices and x values of four
+// entries are loaded before their products are added, so the x gathers of a
+// row are in flight together instead of one after another.
+template <class T, class XF>
+__device__ __forceinline__ T staged_row(uint32_t j, uint32_t je, const uint32_t* s_ja, uint32_t bj, const T* s_a,
+                                        uint32_t ba, XF xv) {
+    T acc = 0;
+    for (; j + 4 <= je; j += 4) {
+        uint32_t c0 = s_ja[j - bj], c1 = s_ja[j + 1 - bj], c2 = s_ja[j + 2 - bj], c3 = s_ja[j + 3 - bj];
+        T x0 = xv(c0), x1 = xv(c1), x2 = xv(c2), x3 = xv(c3);
+        acc += s_a[j - ba] * x0;
+        acc += s_a[j + 1 - ba] * x1;
+        acc += s_a[j + 2 - ba] * x2;
+        acc += s_a[j + 3 - ba] * x3;
+    }
+    for (; j < je; j++) acc += s_a[j - ba] * xv(s_ja[j - bj]);
+    return acc;
+}
+
 template <class T, int MODE>  // MODE 0: y = A x, 1: y = f - A x
 __global__ void __launch_bounds__(ST_ROWS) k_spmv_staged(uint32_t n, const uint32_t* __restrict__ ia,
                                                          const uint32_t* __restrict__ ja, const T* __restrict__ a,
@@ -76,9 +98,8 @@ __global__ void __launch_bounds__(ST_ROWS) k_spmv_staged(uint32_t n, const uint3
         for (uint32_t v = threadIdx.x; v < nva; v += blockDim.x) reinterpret_cast<uint4*>(s_a)[v] = ga[v];
         __syncthreads();
         if (threadIdx.x < nr) {
-            T acc = 0;
-            uint32_t je = s_ia[threadIdx.x + 1];
-            for (uint32_t j = s_ia[threadIdx.x]; j < je; j++) acc += s_a[j - ba] * x[s_ja[j - bj]];
+            T acc = staged_row<T>(s_ia[threadIdx.x], s_ia[threadIdx.x + 1], s_ja, bj, s_a, ba,
+                                  [&](uint32_t c) { return x[c]; });
             uint32_t row = r0 + threadIdx.x;
             y[row] = MODE ? f[row] - acc : acc;
         }
@@ -285,14 +306,27 @@ __global__ void k_chebk(uint32_t n, T* __restrict__ x2, const T* __restrict__ u1
 // Dense coarsest level: x = C^{-1} f, one warp per row.
 template <class T>
 __global__ void k_dense_gemv(uint32_t n, const T* __restrict__ C, const T* __restrict__ f, T* __restrict__ x) {
-    pdl_wait();
-    pdl_trigger();
+    // the operator is constant: its row is loaded before the wait (see RowPre)
+    constexpr int CV = 16;
     uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
+    const T* c = C + (size_t)(row < n ? row : 0) * n;
+    T cv[CV];
+#pragma unroll
+    for (int k = 0; k < CV; k++) {
+        uint32_t j = lane + 32 * k;
+        cv[k] = (row < n && j < n) ? c[j] : T(0);
+    }
+    pdl_wait();
+    pdl_trigger();
     if (row >= n) return;
-    const T* c = C + (size_t)row * n;
     T s = 0;
-    for (uint32_t j = lane; j < n; j += 32) s += c[j] * f[j];
+#pragma unroll
+    for (int k = 0; k < CV; k++) {
+        uint32_t j = lane + 32 * k;
+        if (j < n) s += cv[k] * f[j];
+    }
+    for (uint32_t j = lane + 32 * CV; j < n; j += 32) s += c[j] * f[j];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0) x[row] = s;
@@ -353,6 +387,47 @@ void scatter(uint32_t n, const uint32_t* idx, const double* src, double* dst, cu
 
 
 // ---- explicit-form sweep kernels -------------------------------------------
+// The matrices of the apply are constant, so a row kernel loads its row's
+// first PRE_K entries (values and column indices) BEFORE griddepcontrol.wait:
+// under programmatic dependent launch those loads overlap the tail of the
+// previous kernel, and after the wait only the gathers of the vector the
+// previous kernel wrote remain on the critical path. The products are added in
+// the same order as a plain lane-strided loop.
+constexpr int PRE_K = 4;
+
+template <class T, int LPR>
+struct RowPre {
+    uint32_t jb = 0, je = 0;
+    T av[PRE_K];
+    uint32_t cv[PRE_K];
+    __device__ __forceinline__ void load(bool active, uint32_t row, int lane, const uint32_t* __restrict__ ia,
+                                         const uint32_t* __restrict__ ja, const T* __restrict__ a) {
+        if (active) {
+            jb = ia[row] + lane;
+            je = ia[row + 1];
+        }
+#pragma unroll
+        for (int k = 0; k < PRE_K; k++) {
+            uint32_t j = jb + k * LPR;
+            av[k] = 0;
+            cv[k] = 0;
+            if (j < je) {
+                av[k] = a[j];
+                cv[k] = ja[j];
+            }
+        }
+    }
+    template <class V>
+    __device__ __forceinline__ T sum(V val, const uint32_t* __restrict__ ja, const T* __restrict__ a) const {
+        T s = 0;
+#pragma unroll
+        for (int k = 0; k < PRE_K; k++)
+            if (jb + k * LPR < je) s += av[k] * val(cv[k]);
+        for (uint32_t j = jb + PRE_K * LPR; j < je; j += LPR) s += a[j] * val(ja[j]);
+        return s;
+    }
+};
+
 // Phase 1 of a level solve: w = P1 src on rows [0, R) (the L solve of the
 // eliminated and coarse rows) and out = dval * src on the diagonal rows
 // [R, N). The first nb1 blocks take the P1 rows with LPR lanes per row, the
@@ -362,24 +437,25 @@ __global__ void __launch_bounds__(256) k_phase1(uint32_t R, uint32_t N, uint32_t
                                                 const uint32_t* __restrict__ ja, const T* __restrict__ a,
                                                 const T* __restrict__ dval, const T* __restrict__ src,
                                                 T* __restrict__ w, T* __restrict__ out) {
-    pdl_wait();
-    pdl_trigger();
     if (blockIdx.x < nb1) {
         uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
         uint32_t row = gid / LPR;
         int lane = gid % LPR;
         bool active = row < R;
-        T s = 0;
-        if (active) {
-            uint32_t e = ia[row + 1];
-            for (uint32_t j = ia[row] + lane; j < e; j += LPR) s += a[j] * src[ja[j]];
-        }
+        RowPre<T, LPR> rp;
+        rp.load(active, row, lane, ia, ja, a);
+        pdl_wait();
+        pdl_trigger();
+        T s = rp.sum([&](uint32_t c) { return src[c]; }, ja, a);
 #pragma unroll
         for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (active && lane == 0) w[row] = s;
     } else {
         uint32_t q = R + (blockIdx.x - nb1) * blockDim.x + threadIdx.x;
-        if (q < N) out[q] = dval[q - R] * src[q];
+        T d = q < N ? dval[q - R] : T(0);
+        pdl_wait();
+        pdl_trigger();
+        if (q < N) out[q] = d * src[q];
     }
 }
 
@@ -390,20 +466,15 @@ template <class T, int LPR>
 __global__ void __launch_bounds__(256) k_phase2(uint32_t M, const uint32_t* __restrict__ ia,
                                                 const uint32_t* __restrict__ ja, const T* __restrict__ a,
                                                 const T* __restrict__ w, T* out) {
-    pdl_wait();
-    pdl_trigger();
     uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t row = gid / LPR;
     int lane = gid % LPR;
     bool active = row < M;
-    T s = 0;
-    if (active) {
-        uint32_t e = ia[row + 1];
-        for (uint32_t j = ia[row] + lane; j < e; j += LPR) {
-            uint32_t c = ja[j];
-            s += a[j] * (c < M ? w[c] : out[c]);
-        }
-    }
+    RowPre<T, LPR> rp;
+    rp.load(active, row, lane, ia, ja, a);
+    pdl_wait();
+    pdl_trigger();
+    T s = rp.sum([&](uint32_t c) { return c < M ? w[c] : out[c]; }, ja, a);
 #pragma unroll
     for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (active && lane == 0) out[row] = s;
@@ -416,17 +487,15 @@ __global__ void __launch_bounds__(256) k_update(uint32_t n, const uint32_t* __re
                                                 const uint32_t* __restrict__ ja, const T* __restrict__ a,
                                                 const T* __restrict__ u0, T* __restrict__ x, T* __restrict__ r,
                                                 int do_r) {
-    pdl_wait();
-    pdl_trigger();
     uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t row = gid / LPR;
     int lane = gid % LPR;
     bool active = row < n;
-    T s = 0;
-    if (active && do_r) {
-        uint32_t e = ia[row + 1];
-        for (uint32_t j = ia[row] + lane; j < e; j += LPR) s += a[j] * u0[ja[j]];
-    }
+    RowPre<T, LPR> rp;
+    rp.load(active && do_r, row, lane, ia, ja, a);
+    pdl_wait();
+    pdl_trigger();
+    T s = rp.sum([&](uint32_t c) { return u0[c]; }, ja, a);
 #pragma unroll
     for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (active && lane == 0) {
@@ -439,22 +508,35 @@ __global__ void __launch_bounds__(256) k_update(uint32_t n, const uint32_t* __re
 // A whole MultiSplitPrec::solve(l, f, x) call of a mid-size level whose coarse
 // sub-hierarchy is tabulated as one dense operator: all niter sweeps (phase 1,
 // the dense coarse product, phase 2, the residual / correction step) in ONE
-// launch of one thread-block cluster, with a cluster barrier between the
-// steps instead of a kernel boundary. The level's matrices and vectors are
-// read through L2 (they are a few MB); vectors written inside the kernel are
-// read with ld.global.cg so that no stale L1 line is used after a barrier.
-// Each step sums in the same order as the separate kernels (k_phase1,
-// k_dense_gemv, k_phase2, k_spmv_staged / k_spmv, k_update), so both paths give
-// identical results.
+// launch of one 16-CTA thread-block cluster, with a cluster barrier between
+// the steps instead of a kernel boundary.
+//
+// * The level's vectors (f, x, w, r, u0) live in the cluster's distributed
+//   shared memory: CTA o owns entries [o*chv, (o+1)*chv) of each, and any CTA
+//   reads or writes them through the owner's shared-memory window (DSMEM), so
+//   no step waits on a global-memory round trip. f is loaded at the start, x
+//   written back at the end.
+// * CTA c takes the same balanced slice of rows in every step (P1 rows,
+//   diagonal rows, dense-operator rows, G rows, level-matrix rows) and copies
+//   those matrix rows into its own shared memory once, with cp.async; the
+//   dense operator's rows are read from L2.
+// Rows are summed serially in column order (the separate kernels may split a
+// row over several lanes, so the two paths agree to rounding, not bit for bit).
 template <class T>
 struct MidArgs {
     uint32_t N, M, R, n, niter;
-    int lpr1, lpr2, lprr, lpru;  // lanes per row: P1, G, residual, correction
+    uint32_t trace;  // MLP_MID_TRACE=1: CTA 0 prints the time of every step (diagnostics)
     const uint32_t *p1_ia, *p1_ja, *g_ia, *g_ja, *af_ia, *af_ja;
     const T *p1_a, *g_a, *af_a, *dval, *C;
     const T* f;
-    T *x, *w, *r, *u0;
+    T* x;
 };
+
+__device__ __forceinline__ uint64_t gtimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 __device__ __forceinline__ void cluster_barrier() {
     asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
@@ -463,117 +545,342 @@ __device__ __forceinline__ void cluster_barrier() {
 template <class T>
 __device__ __forceinline__ T ldcg(const T* p) { return __ldcg(p); }
 
-// Row-group loop: groups of lpr lanes take rows base + group; every lane of a
-// warp runs the same trip count, so the shuffles see full warps.
+// Rows [c * ceil(rows / cs), ...) of CTA c.
+__host__ __device__ __forceinline__ void mid_slice(uint32_t rows, uint32_t cs, uint32_t c, uint32_t& r0,
+                                                    uint32_t& r1) {
+    uint32_t ch = (rows + cs - 1) / cs;
+    r0 = min(rows, c * ch);
+    r1 = min(rows, r0 + ch);
+}
+
+// Entries per CTA of each distributed vector (a multiple of 4, so every
+// owner's slice starts on a 16-byte boundary).
+__host__ __device__ __forceinline__ uint32_t mid_chunk(uint32_t N, uint32_t cs) {
+    return ((N + cs - 1) / cs + 3) & ~3u;
+}
+
+// Rows of CTA c in the three row steps: P1 (k = 0) and G (k = 1) rows in equal
+// slices; level-matrix rows (k = 2) by vector ownership, so that the
+// correction step updates x and r in the CTA's own shared memory.
+__host__ __device__ __forceinline__ void mid_rows(int k, uint32_t R, uint32_t M, uint32_t N, uint32_t cs, uint32_t c,
+                                                   uint32_t& r0, uint32_t& r1) {
+    if (k == 0) { mid_slice(R, cs, c, r0, r1); return; }
+    if (k == 1) { mid_slice(M, cs, c, r0, r1); return; }
+    uint32_t ch = mid_chunk(N, cs);
+    r0 = min(N, c * ch);
+    r1 = min(N, r0 + ch);
+}
+
+// Shared-memory layout of one CTA: the five vector slices (chv entries each:
+// f, x, w, r, u0), the staged coarse slice of w, then the matrix rows. Every
+// matrix array is copied from the 16-byte boundary at or below its first
+// element, so each region holds a few leading elements before the slice and
+// is indexed with that offset.
+struct MidLayout {
+    uint32_t r0[3], nr[3], e0[3], nnz[3];  // P1, G, level matrix
+    uint32_t c0, nc, d0, nd;                 // dense rows, diagonal rows
+    uint32_t chv;
+    size_t off_v, off_w, off_a[3], off_d;   // in units of T
+    size_t off_ia[3], off_ja[3];            // in units of uint32_t
+    size_t bytes;
+};
+
+template <class T>
+__host__ __device__ inline void mid_layout(MidLayout& L, uint32_t cs, uint32_t c, uint32_t R, uint32_t M, uint32_t N,
+                                           uint32_t n, const uint32_t* e_start, const uint32_t* e_end) {
+    constexpr size_t VT = 16 / sizeof(T);
+    auto pad_t = [](size_t cnt) { return (cnt + 2 * VT + VT - 1) / VT * VT; };
+    auto pad_u = [](size_t cnt) { return (cnt + 8 + 3) / 4 * 4; };
+    for (int k = 0; k < 3; k++) {
+        uint32_t a, b;
+        mid_rows(k, R, M, N, cs, c, a, b);
+        L.r0[k] = a;
+        L.nr[k] = b - a;
+        L.e0[k] = e_start[k];
+        L.nnz[k] = e_end[k] - e_start[k];
+    }
+    uint32_t a, b;
+    mid_slice(n, cs, c, a, b);
+    L.c0 = a; L.nc = b - a;
+    L.chv = mid_chunk(N, cs);
+    // diagonal rows [R, N): the ones this CTA owns
+    a = max(R, min(N, c * L.chv));
+    b = max(a, min(N, (c + 1) * L.chv));
+    L.d0 = a - R; L.nd = b - a;
+    size_t o = 0;
+    L.off_v = o; o += 5 * (size_t)L.chv;  // chv is a multiple of 4: each slice 16-byte aligned
+    L.off_w = o; o += pad_t(n);
+    for (int k = 0; k < 3; k++) { L.off_a[k] = o; o += pad_t(L.nnz[k]); }
+    L.off_d = o; o += pad_t(L.nd);
+    size_t u = o * sizeof(T) / 4;
+    for (int k = 0; k < 3; k++) {
+        L.off_ia[k] = u; u += pad_u(L.nr[k] + 1);
+        L.off_ja[k] = u; u += pad_u(L.nnz[k]);
+    }
+    L.bytes = u * 4;
+}
+
+// Starts the copy of src[i0, i1) into the 16-byte aligned region dst with
+// cp.async, from the 16-byte boundary at or below src + i0; returns the index
+// shift (element i lands at dst[i - shift]). The last vector may read up to 15
+// bytes past src + i1 (device buffers carry 16 bytes of slack). Completion:
+// cp_async_wait_all() then a barrier.
+template <class E>
+__device__ __forceinline__ size_t copy_async(E* dst, const E* src, size_t i0, size_t i1) {
+    constexpr size_t V = 16 / sizeof(E);
+    size_t b = i0 & ~(V - 1);
+    if (i1 <= i0) return b;
+    size_t nv = (i1 - b + V - 1) / V;
+    const char* s = reinterpret_cast<const char*>(src + b);
+    uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    for (size_t v = threadIdx.x; v < nv; v += blockDim.x)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d + (uint32_t)(v * 16)), "l"(s + v * 16)
+                     : "memory");
+    return b;
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Distributed vector: entry i lives in CTA i / chv at local index i % chv of
+// the same region; owner() divides with a precomputed reciprocal (exact for
+// i < 2^17 and chv < 2^14).
+template <class T>
+struct DVec {
+    T* local;       // this CTA's slice (same offset in every CTA)
+    uint32_t chv, inv, rank;
+    __device__ __forceinline__ T* at(uint32_t i) const {
+        uint32_t o = __umulhi(i, inv);
+        T* p = local + (i - o * chv);
+        if (o == rank) return p;  // own slice: plain shared-memory access
+        return cooperative_groups::this_cluster().map_shared_rank(p, o);
+    }
+    __device__ __forceinline__ T ld(uint32_t i) const { return *at(i); }
+    __device__ __forceinline__ void st(uint32_t i, T v) const { *at(i) = v; }
+};
+
+// One thread per row; a thread takes MID_U rows at once and first issues the
+// vector gathers of the first MID_K entries of each, so up to MID_U * MID_K
+// gathers are in flight together; the products are then added in row order
+// (the order of a serial loop over the row).
+constexpr int MID_U = 2, MID_K = 4, MID_CV = 16;
+
 template <class T, class Val, class Store>
-__device__ __forceinline__ void csr_rows(uint32_t nrows, int lpr, const uint32_t* __restrict__ ia,
-                                         const uint32_t* __restrict__ ja, const T* __restrict__ a, Val val,
-                                         Store store) {
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t nth = gridDim.x * blockDim.x;
-    const uint32_t groups = nth / lpr, g = tid / lpr;
-    const int lane = tid % lpr;
-    for (uint32_t base = 0; base < nrows; base += groups) {
-        uint32_t row = base + g;
-        bool act = row < nrows;
-        T s = 0;
-        if (act) {
-            uint32_t e = __ldg(ia + row + 1);
-            for (uint32_t j = __ldg(ia + row) + lane; j < e; j += lpr) s += __ldg(a + j) * val(__ldg(ja + j));
+__device__ __forceinline__ void smem_rows(uint32_t nrows, const uint32_t* ia, const uint32_t* ja, size_t bj,
+                                          const T* a, size_t ba, Val val, Store store) {
+    for (uint32_t base = 0; base < nrows; base += blockDim.x * MID_U) {
+        T av[MID_U][MID_K], xv[MID_U][MID_K];
+        uint32_t jb[MID_U], je[MID_U];
+#pragma unroll
+        for (int u = 0; u < MID_U; u++) {
+            uint32_t row = base + u * blockDim.x + threadIdx.x;
+            jb[u] = je[u] = 0;
+            if (row < nrows) {
+                jb[u] = ia[row];
+                je[u] = ia[row + 1];
+            }
+#pragma unroll
+            for (int k = 0; k < MID_K; k++) {
+                uint32_t j = jb[u] + k;
+                av[u][k] = 0;
+                xv[u][k] = 0;
+                if (j < je[u]) {
+                    av[u][k] = a[j - ba];
+                    xv[u][k] = val(ja[j - bj]);
+                }
+            }
         }
-        for (int o = lpr / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (act && lane == 0) store(row, s);
+#pragma unroll
+        for (int u = 0; u < MID_U; u++) {
+            uint32_t row = base + u * blockDim.x + threadIdx.x;
+            if (row >= nrows) continue;
+            T s = 0;
+#pragma unroll
+            for (int k = 0; k < MID_K; k++)
+                if (jb[u] + k < je[u]) s += av[u][k] * xv[u][k];
+            for (uint32_t j = jb[u] + MID_K; j < je[u]; j++) s += a[j - ba] * val(ja[j - bj]);
+            store(row, s);
+        }
     }
 }
 
 template <class T>
 __global__ void __launch_bounds__(1024) k_mid_level(MidArgs<T> A) {
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t nth = gridDim.x * blockDim.x;
+    extern __shared__ __align__(16) unsigned char mid_smem[];
+    const uint32_t c = blockIdx.x, cs = gridDim.x;
     const uint32_t N = A.N, M = A.M, R = A.R, n = A.n;
-    T* w = A.w;
+    const bool tr = A.trace && c == 0 && threadIdx.x == 0;
+    uint64_t ts[28];
+    int nts = 0;
+    if (tr) ts[nts++] = gtimer();
+    const uint32_t* gia[3] = {A.p1_ia, A.g_ia, A.af_ia};
+    const uint32_t* gja[3] = {A.p1_ja, A.g_ja, A.af_ja};
+    const T* ga[3] = {A.p1_a, A.g_a, A.af_a};
+    uint32_t es[3], ee[3];
+    for (int k = 0; k < 3; k++) {
+        uint32_t a, b;
+        mid_rows(k, R, M, N, cs, c, a, b);
+        es[k] = gia[k][a];
+        ee[k] = gia[k][b];
+    }
+    MidLayout L;
+    mid_layout<T>(L, cs, c, R, M, N, n, es, ee);
+    T* sv = reinterpret_cast<T*>(mid_smem);
+    uint32_t* su = reinterpret_cast<uint32_t*>(mid_smem);
+    const uint32_t chv = L.chv;
+    const uint32_t inv = (uint32_t)((0x100000000ull + chv - 1) / chv);
+    DVec<T> vf{sv + L.off_v, chv, inv, c}, vx{sv + L.off_v + chv, chv, inv, c},
+        vw{sv + L.off_v + 2 * chv, chv, inv, c}, vr{sv + L.off_v + 3 * chv, chv, inv, c},
+        vu{sv + L.off_v + 4 * chv, chv, inv, c};
+    // copy this CTA's matrix rows and its slice of f into shared memory
+    const uint32_t* ia_s[3];
+    const uint32_t* ja_s[3];
+    const T* a_s[3];
+    size_t bj[3], ba[3];
+    for (int k = 0; k < 3; k++) {
+        ba[k] = copy_async(sv + L.off_a[k], ga[k], L.e0[k], L.e0[k] + L.nnz[k]);
+        bj[k] = copy_async(su + L.off_ja[k], gja[k], L.e0[k], L.e0[k] + L.nnz[k]);
+        size_t bi = copy_async(su + L.off_ia[k], gia[k], L.r0[k], L.r0[k] + L.nr[k] + 1);
+        ia_s[k] = su + L.off_ia[k] + (L.r0[k] - bi);  // ia_s[k][row] = ia[r0 + row]
+        ja_s[k] = su + L.off_ja[k];
+        a_s[k] = sv + L.off_a[k];
+    }
+    size_t bd = copy_async(sv + L.off_d, A.dval, L.d0, L.d0 + L.nd);
+    const uint32_t v0 = min(N, c * chv), v1 = min(N, v0 + chv);
+    // f (a slice of the caller's vector, not necessarily 16-byte aligned): plain loads
+#pragma unroll 2
+    for (uint32_t i = v0 + threadIdx.x; i < v1; i += blockDim.x) vf.local[i - v0] = ldcg(A.f + i);
+    cp_async_wait_all();
+    __syncthreads();
+    cluster_barrier();  // every slice of f is in place before anyone reads it
+    if (tr) ts[nts++] = gtimer();
+    const T* dv = sv + L.off_d + (L.d0 - bd);  // dv[i] = dval[d0 + i]
+    T* wc = sv + L.off_w;
+    const uint32_t p0 = L.r0[0], g0 = L.r0[1], f0 = L.r0[2];
     for (uint32_t it = 1; it <= A.niter; it++) {
-        const T* src = it == 1 ? A.f : A.r;
-        T* out = it == 1 ? A.x : A.u0;
+        const DVec<T>& src = it == 1 ? vf : vr;
+        const DVec<T>& out = it == 1 ? vx : vu;
         // phase 1: w = P1 src (rows < R); out = dval * src (rows >= R)
-        csr_rows<T>(R, A.lpr1, A.p1_ia, A.p1_ja, A.p1_a, [&](uint32_t c) { return ldcg(src + c); },
-                    [&](uint32_t row, T v) { w[row] = v; });
-        for (uint32_t q = R + tid; q < N; q += nth) out[q] = __ldg(A.dval + (q - R)) * ldcg(src + q);
+        smem_rows<T>(L.nr[0], ia_s[0], ja_s[0], bj[0], a_s[0], ba[0], [&](uint32_t col) { return src.ld(col); },
+                     [&](uint32_t row, T v) { vw.st(p0 + row, v); });
+#pragma unroll 4
+        for (uint32_t i = threadIdx.x; i < L.nd; i += blockDim.x) {
+            uint32_t q = R + L.d0 + i;
+            out.st(q, dv[i] * src.ld(q));
+        }
         cluster_barrier();
-        // coarse slice: out[M + i] = sum_j C_ij w[M + j], one warp per row
+        if (tr && nts < 27) ts[nts++] = gtimer();
+        // coarse slice: out[M + i] = sum_j C_ij w[M + j], one warp per row;
+        // w's coarse slice is staged in shared memory first
+        for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) wc[j] = vw.ld(M + j);
+        __syncthreads();
         {
-            const uint32_t warp = tid >> 5, nwarp = nth >> 5;
+            const uint32_t warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
             const int lane = threadIdx.x & 31;
-            for (uint32_t row = warp; row < n; row += nwarp) {
-                const T* c = A.C + (size_t)row * n;
+            for (uint32_t i = warp; i < L.nc; i += nwarp) {
+                const T* crow = A.C + (size_t)(L.c0 + i) * n;
                 T s = 0;
-                for (uint32_t j = lane; j < n; j += 32) s += __ldg(c + j) * ldcg(w + M + j);
+                T cv[MID_CV];  // the lane's first MID_CV entries of the row, all loads in flight at once
+#pragma unroll
+                for (int k = 0; k < MID_CV; k++) {
+                    uint32_t j = lane + 32 * k;
+                    cv[k] = j < n ? __ldg(crow + j) : T(0);
+                }
+#pragma unroll
+                for (int k = 0; k < MID_CV; k++) {
+                    uint32_t j = lane + 32 * k;
+                    if (j < n) s += cv[k] * wc[j];
+                }
+                for (uint32_t j = lane + 32 * MID_CV; j < n; j += 32) s += __ldg(crow + j) * wc[j];
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-                if (lane == 0) out[M + row] = s;
+                if (lane == 0) out.st(M + L.c0 + i, s);
             }
         }
         cluster_barrier();
+        if (tr && nts < 27) ts[nts++] = gtimer();
         // phase 2: out_q = sum_j G_qj (j < M ? w_j : out_j), q < M
-        csr_rows<T>(M, A.lpr2, A.g_ia, A.g_ja, A.g_a, [&](uint32_t c) { return c < M ? ldcg(w + c) : ldcg(out + c); },
-                    [&](uint32_t row, T v) { out[row] = v; });
+        smem_rows<T>(L.nr[1], ia_s[1], ja_s[1], bj[1], a_s[1], ba[1],
+                     [&](uint32_t col) { return col < M ? vw.ld(col) : out.ld(col); },
+                     [&](uint32_t row, T v) { out.st(g0 + row, v); });
         if (A.niter < 2) break;
         cluster_barrier();
+        if (tr && nts < 27) ts[nts++] = gtimer();
         if (it == 1) {
             // r = f - A x
-            csr_rows<T>(N, A.lprr, A.af_ia, A.af_ja, A.af_a, [&](uint32_t c) { return ldcg(A.x + c); },
-                        [&](uint32_t row, T v) { A.r[row] = ldcg(A.f + row) - v; });
+            smem_rows<T>(L.nr[2], ia_s[2], ja_s[2], bj[2], a_s[2], ba[2], [&](uint32_t col) { return vx.ld(col); },
+                         [&](uint32_t row, T v) { vr.st(f0 + row, vf.ld(f0 + row) - v); });
         } else if (it < A.niter) {
             // x += u0; r -= A u0
-            csr_rows<T>(N, A.lpru, A.af_ia, A.af_ja, A.af_a, [&](uint32_t c) { return ldcg(A.u0 + c); },
-                        [&](uint32_t row, T v) {
-                            A.x[row] = ldcg(A.x + row) + ldcg(A.u0 + row);
-                            A.r[row] = ldcg(A.r + row) - v;
-                        });
+            smem_rows<T>(L.nr[2], ia_s[2], ja_s[2], bj[2], a_s[2], ba[2], [&](uint32_t col) { return vu.ld(col); },
+                         [&](uint32_t row, T v) {
+                             uint32_t q = f0 + row;
+                             vx.st(q, vx.ld(q) + vu.ld(q));
+                             vr.st(q, vr.ld(q) - v);
+                         });
         } else {
-            for (uint32_t q = tid; q < N; q += nth) A.x[q] = ldcg(A.x + q) + ldcg(A.u0 + q);
+#pragma unroll 4
+            for (uint32_t i = threadIdx.x; i < L.nr[2]; i += blockDim.x) {
+                uint32_t q = f0 + i;
+                vx.st(q, vx.ld(q) + vu.ld(q));
+            }
         }
-        if (it < A.niter) cluster_barrier();
+        if (it < A.niter) {
+            cluster_barrier();
+            if (tr && nts < 27) ts[nts++] = gtimer();
+        }
+    }
+    cluster_barrier();  // every update of x is done before the owners write it out
+    for (uint32_t i = v0 + threadIdx.x; i < v1; i += blockDim.x) A.x[i] = vx.local[i - v0];
+    if (tr) {
+        ts[nts++] = gtimer();
+        printf("[k_mid_level] N=%u steps=%d total %.2f us: copy-in %.2f", N, nts, (ts[nts - 1] - ts[0]) * 1e-3,
+               (ts[1] - ts[0]) * 1e-3);
+        for (int k = 2; k < nts; k++) printf(" %.2f", (ts[k] - ts[k - 1]) * 1e-3);
+        printf("\n");
     }
 }
 
-// Cluster size of the fused level kernel: 16 CTAs of 1024 threads when the
-// device can co-schedule such a cluster, else 8; 0 disables the path
-// (MLP_MID=0 also disables it).
+// Whether the fused level kernel can run as a 16-CTA cluster with this much
+// shared memory. The path is opt-in (MLP_MID=1): measured on B200 at 26,907
+// rows, one fused call (20 dependent steps) took 84 us against 55 us for the
+// same steps as separate graph-launched kernels with programmatic dependent
+// launch, because each step still waits on scattered gathers that one
+// cluster serves more slowly than the whole GPU.
 template <class T>
-static int mid_cluster_size() {
+static bool mid_cluster_ok(int cs, size_t smem) {
     const char* e = getenv("MLP_MID");
-    if (e && e[0] == '0') return 0;
-    static int cs = -1;
-    if (cs >= 0) return cs;
-    cs = 0;
-    cudaFuncSetAttribute(k_mid_level<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-    for (int want : {16, 8}) {
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(want);
-        cfg.blockDim = dim3(1024);
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = want;
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        int nc = 0;
-        if (cudaOccupancyMaxActiveClusters(&nc, k_mid_level<T>, &cfg) == cudaSuccess && nc > 0) {
-            cs = want;
-            break;
-        }
+    if (!(e && e[0] == '1')) return false;
+    static int attr_set = 0;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_mid_level<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        cudaFuncSetAttribute(k_mid_level<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)small_smem_limit());
         cudaGetLastError();
+        attr_set = 1;
     }
-    return cs;
-}
-
-template <class T>
-static void launch_mid(const MidArgs<T>& a, int cs, cudaStream_t s) {
+    if (smem > small_smem_limit()) return false;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(cs);
     cfg.blockDim = dim3(1024);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int nc = 0;
+    bool ok = cudaOccupancyMaxActiveClusters(&nc, k_mid_level<T>, &cfg) == cudaSuccess && nc > 0;
+    cudaGetLastError();
+    return ok;
+}
+
+template <class T>
+static void launch_mid(const MidArgs<T>& a, int cs, size_t smem, cudaStream_t s) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cs);
+    cfg.blockDim = dim3(1024);
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -806,28 +1113,51 @@ struct Builder {
     // l + 1 is the tabulated dense sub-hierarchy and level l is small enough
     // for one cluster to sweep it.
     static constexpr uint32_t MID_MAX_N = 1u << 17;
+    std::map<uint32_t, size_t> mid_smem;   // level -> shared memory of its fused kernel
+    cudaStream_t stream = nullptr;         // stream of the build (level data downloads)
+
+    // Shared memory of the largest CTA slice (row starts at the slice bounds).
+    size_t mid_smem_bytes(const Level& L, const MidArgs<T>& a, int cs) {
+        std::vector<uint32_t> ia1 = L.P1.ia.download(stream, (size_t)a.R + 1);
+        std::vector<uint32_t> ia2 = L.G.ia.download(stream, (size_t)a.M + 1);
+        std::vector<uint32_t> ia3 = L.Af.ia.download(stream, (size_t)a.N + 1);
+        const std::vector<uint32_t>* ias[3] = {&ia1, &ia2, &ia3};
+        size_t smem = 0;
+        for (int c = 0; c < cs; c++) {
+            uint32_t es[3], ee[3];
+            for (int k = 0; k < 3; k++) {
+                uint32_t r0, r1;
+                mid_rows(k, a.R, a.M, a.N, cs, c, r0, r1);
+                es[k] = (*ias[k])[r0];
+                ee[k] = (*ias[k])[r1];
+            }
+            MidLayout ml;
+            mid_layout<T>(ml, cs, c, a.R, a.M, a.N, a.n, es, ee);
+            smem = std::max(smem, ml.bytes);
+        }
+        return (smem + 15) & ~(size_t)15;
+    }
+
     bool mid_call(uint32_t l, const T* f, T* x) {
         Level& L = *H.lv[l];
         if (!small || !small->valid() || !small->dense.p || small->first != l + 1) return false;
-        if (L.N > MID_MAX_N || !L.n || L.niter < 1) return false;
-        int cs = mid_cluster_size<T>();
-        if (!cs) return false;
-        LevelWork<T>& w = W[l];
+        if (L.N > MID_MAX_N || !L.n || L.niter < 1 || small->N0 != L.n) return false;
+        const int cs = 16;
         MidArgs<T> a{};
         a.N = L.N; a.M = L.M; a.R = L.N - L.Md; a.n = small->N0; a.niter = L.niter;
-        if (a.n != L.n) return false;
-        a.lpr1 = pick_lpr(a.R, L.P1.nnz);
-        a.lpr2 = pick_lpr(L.M, L.G.nnz);
-        bool staged = L.Af.tile_max && L.Af.tile_max <= ST_MAX_NNZ && L.N >= 4 * ST_ROWS;
-        a.lprr = staged ? 1 : pick_lpr(L.N, L.Af.nnz);
-        a.lpru = pick_lpr(L.N, L.Af.nnz);
         a.p1_ia = L.P1.ia.p; a.p1_ja = L.P1.ja.p; a.p1_a = vals<T>(L.P1);
         a.g_ia = L.G.ia.p; a.g_ja = L.G.ja.p; a.g_a = vals<T>(L.G);
         a.af_ia = L.Af.ia.p; a.af_ja = L.Af.ja.p; a.af_a = vals<T>(L.Af);
         a.dval = dvals<T>(L);
         a.C = small->dense.p;
-        a.f = f; a.x = x; a.w = w.w.p; a.r = w.r.p; a.u0 = w.u0.p;
-        op([=](cudaStream_t s) { launch_mid<T>(a, cs, s); });
+        a.f = f; a.x = x;
+        const char* tre = getenv("MLP_MID_TRACE");
+        a.trace = (tre && tre[0] == '1') ? 1 : 0;
+        auto hit = mid_smem.find(l);
+        size_t smem = hit != mid_smem.end() ? hit->second : mid_smem_bytes(L, a, cs);
+        mid_smem[l] = smem;
+        if (!smem || !mid_cluster_ok<T>(cs, smem)) return false;
+        op([=](cudaStream_t s) { launch_mid<T>(a, cs, smem, s); });
         // bytes: the same as the separate steps
         uint32_t R = a.R, N = L.N, M = L.M, n = a.n;
         for (uint32_t it = 1; it <= L.niter; it++) {
@@ -1000,6 +1330,7 @@ std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, c
         if (small_budget()) build_small<double>(H, *P->sp64, small_budget(), s);
         Builder<double> B{H, P->w64, P->plan, P->sp64.get()};
         B.explicit_solves = explicit_solves;
+        B.stream = s;
         if (H.kind == PREC_MSPLIT) B.ms(0, P->fin, P->fout);
         else B.ch(0, P->fin, P->fout);
         P->bytes_per_apply = B.bytes;
@@ -1019,6 +1350,7 @@ std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, c
         P->z32.alloc(N0);
         Builder<float> B{H, P->w32, P->plan, P->sp32.get()};
         B.explicit_solves = explicit_solves;
+        B.stream = s;
         const double* fin = P->fin;
         float* f32 = P->f32.p;
         B.op([=](cudaStream_t st) { launch_k(k_to_f32, grid_for(N0, 256), 256, 0, st, N0, fin, f32); });
@@ -1163,9 +1495,8 @@ __global__ void __launch_bounds__(ST_ROWS) k_pcg_spmv_dot_staged(uint32_t n, con
         for (uint32_t v = threadIdx.x; v < nva; v += blockDim.x) reinterpret_cast<uint4*>(s_a)[v] = ga[v];
         __syncthreads();
         if (threadIdx.x < nr) {
-            double acc = 0;
-            uint32_t je = s_ia[threadIdx.x + 1];
-            for (uint32_t j = s_ia[threadIdx.x]; j < je; j++) acc += s_a[j - ba] * p[s_ja[j - bj]];
+            double acc = staged_row<double>(s_ia[threadIdx.x], s_ia[threadIdx.x + 1], s_ja, bj, s_a, ba,
+                                            [&](uint32_t c) { return p[c]; });
             uint32_t row = r0 + threadIdx.x;
             Ap[row] = acc;
             part += acc * p[row];

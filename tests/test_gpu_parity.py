@@ -159,10 +159,12 @@ def test_iteration_cap_ends_the_device_loop(M):
 
 
 @pytest.mark.parametrize("fp32", [False, True])
-def test_fused_level_kernel_is_identical_to_separate_launches(M, fp32, monkeypatch):
+def test_fused_level_kernel_matches_separate_launches(M, fp32, monkeypatch):
     """60x220x85 layered field: the level above the tabulated sub-hierarchy
-    (26,907 rows) runs as one cluster launch; it sums in the same order as the
-    separate kernels, so the apply and the PCG iterates are bit-identical."""
+    (26,907 rows) runs as one cluster launch. Its rows are summed serially, the
+    separate kernels may split a row over lanes, so the two agree to rounding:
+    the apply within 1e-13 (FP64) / 1e-5 (FP32) relative, the PCG iterations
+    within 1 and the solutions within 1e-10 (FP64) / 1e-6 (FP32)."""
     from ml_prec_b200 import fields
     kx, ky, kz = fields.field("layered", 2)
     A, b = M.CSRMatrix.spe(60, 220, 85, kx, ky, kz, c=1.0)
@@ -177,5 +179,7 @@ def test_fused_level_kernel_is_identical_to_separate_launches(M, fp32, monkeypat
     z2 = P2.solve(f)
     st2 = M.SolverStats()
     x2 = M.PCGSolver(A, b, P2, stats=st2, eps=1e-8)
-    assert np.array_equal(z1, z2)
-    assert st1.niter == st2.niter and np.array_equal(x1, x2)
+    tz, tx = (1e-5, 1e-6) if fp32 else (1e-13, 1e-10)
+    assert np.linalg.norm(z1 - z2) <= tz * np.linalg.norm(z2)
+    assert abs(st1.niter - st2.niter) <= 1
+    assert np.linalg.norm(x1 - x2) <= tx * np.linalg.norm(x2)
