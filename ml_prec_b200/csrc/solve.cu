@@ -23,6 +23,12 @@ namespace mlp {
 // Kernels
 // ---------------------------------------------------------------------------
 
+// a * b + c rounded once. Row sums that must agree bit for bit between
+// kernels (the separate and merged sweep steps) use it explicitly rather than
+// relying on the compiler's contraction of s += a * b.
+__device__ __forceinline__ double fmadd(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fmadd(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+
 // y = A x  (or y = f - A x when f != null). LPR lanes cooperate on one row and
 // reduce with shuffles; rows of a 7-point stencil use 8 lanes.
 template <class T, int LPR>
@@ -39,7 +45,7 @@ __global__ void __launch_bounds__(256) k_spmv(uint32_t n, const uint32_t* __rest
     T s = 0;
     if (active) {
         uint32_t e = ia[row + 1];
-        for (uint32_t j = ia[row] + lane; j < e; j += LPR) s += a[j] * x[ja[j]];
+        for (uint32_t j = ia[row] + lane; j < e; j += LPR) s = fmadd(a[j], x[ja[j]], s);
     }
 #pragma unroll
     for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
@@ -64,12 +70,12 @@ __device__ __forceinline__ T staged_row(uint32_t j, uint32_t je, const uint32_t*
     for (; j + 4 <= je; j += 4) {
         uint32_t c0 = s_ja[j - bj], c1 = s_ja[j + 1 - bj], c2 = s_ja[j + 2 - bj], c3 = s_ja[j + 3 - bj];
         T x0 = xv(c0), x1 = xv(c1), x2 = xv(c2), x3 = xv(c3);
-        acc += s_a[j - ba] * x0;
-        acc += s_a[j + 1 - ba] * x1;
-        acc += s_a[j + 2 - ba] * x2;
-        acc += s_a[j + 3 - ba] * x3;
+        acc = fmadd(s_a[j - ba], x0, acc);
+        acc = fmadd(s_a[j + 1 - ba], x1, acc);
+        acc = fmadd(s_a[j + 2 - ba], x2, acc);
+        acc = fmadd(s_a[j + 3 - ba], x3, acc);
     }
-    for (; j < je; j++) acc += s_a[j - ba] * xv(s_ja[j - bj]);
+    for (; j < je; j++) acc = fmadd(s_a[j - ba], xv(s_ja[j - bj]), acc);
     return acc;
 }
 
@@ -324,9 +330,9 @@ __global__ void k_dense_gemv(uint32_t n, const T* __restrict__ C, const T* __res
 #pragma unroll
     for (int k = 0; k < CV; k++) {
         uint32_t j = lane + 32 * k;
-        if (j < n) s += cv[k] * f[j];
+        if (j < n) s = fmadd(cv[k], f[j], s);
     }
-    for (uint32_t j = lane + 32 * CV; j < n; j += 32) s += c[j] * f[j];
+    for (uint32_t j = lane + 32 * CV; j < n; j += 32) s = fmadd(c[j], f[j], s);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0) x[row] = s;
@@ -422,8 +428,8 @@ struct RowPre {
         T s = 0;
 #pragma unroll
         for (int k = 0; k < PRE_K; k++)
-            if (jb + k * LPR < je) s += av[k] * val(cv[k]);
-        for (uint32_t j = jb + PRE_K * LPR; j < je; j += LPR) s += a[j] * val(ja[j]);
+            if (jb + k * LPR < je) s = fmadd(av[k], val(cv[k]), s);
+        for (uint32_t j = jb + PRE_K * LPR; j < je; j += LPR) s = fmadd(a[j], val(ja[j]), s);
         return s;
     }
 };
@@ -892,6 +898,169 @@ static void launch_mid(const MidArgs<T>& a, int cs, size_t smem, cudaStream_t s)
     cudaLaunchKernelEx(&cfg, k_mid_level<T>, a);
 }
 
+// ---- merged sweep steps --------------------------------------------------------
+// At a small level every kernel boundary costs more than the kernel's work, so
+// consecutive steps of the sweep are merged where the data allows, and each
+// merged kernel reproduces the separate kernels' arithmetic exactly (same
+// products, same lane-split partial sums, same butterfly order), so the merged
+// and separate paths give bit-identical results:
+//  * step A = correction of sweep it-1 + phase 1 of sweep it:
+//      x += u0;  r' = r - Af u0;  w = P1 r';  u0'_D = dval r'_D
+//    (or, for the second sweep, r' = f - Af x). A thread of a P1 row
+//    recomputes the entries r'_k it needs from Af row k instead of waiting for
+//    the whole of r' (r and u0 are double-buffered).
+//  * step B = the tabulated coarse product + phase 2:
+//      u0_C = C w_C;  u0_E = G [w_E; u0_C]
+//    a warp of an E row recomputes the entries of u0_C its G row needs.
+
+// Lane-split sum of a CSR row as LP cooperating lanes compute it (lane l adds
+// the entries l, l + LP, ... in order, then the xor butterfly of the lanes),
+// evaluated by one thread.
+template <class T, int LP, class V>
+__device__ __forceinline__ T lane_split_sum(uint32_t jb, uint32_t je, const uint32_t* __restrict__ ja,
+                                            const T* __restrict__ a, V val) {
+    T p[LP];
+#pragma unroll
+    for (int l = 0; l < LP; l++) p[l] = 0;
+    for (uint32_t j = jb; j < je; j++) {
+        // entry j belongs to lane (j - jb) % LP; LP is a power of two
+        T av = a[j], xv = val(ja[j]);
+        int l = (int)((j - jb) & (LP - 1));
+#pragma unroll
+        for (int m = 0; m < LP; m++)
+            if (m == l) p[m] = fmadd(av, xv, p[m]);
+    }
+#pragma unroll
+    for (int o = LP / 2; o > 0; o >>= 1) {
+        T q[LP];
+#pragma unroll
+        for (int l = 0; l < LP; l++) q[l] = p[l] + p[l ^ o];
+#pragma unroll
+        for (int l = 0; l < LP; l++) p[l] = q[l];
+    }
+    return p[0];
+}
+
+// Step A. Blocks [0, nbu): the rows of Af with LPU lanes per row (the
+// correction kernel's layout); blocks [nbu, ...): one thread per P1 row.
+// MODE 0: r' = f - Af x (second sweep); MODE 1: x += u0; r' = r - Af u0.
+template <class T, int LPU, int LPP, int MODE>
+__global__ void __launch_bounds__(256) k_merge_a(uint32_t N, uint32_t R, uint32_t nbu, const uint32_t* __restrict__ af_ia,
+                                                 const uint32_t* __restrict__ af_ja, const T* __restrict__ af_a,
+                                                 const uint32_t* __restrict__ p1_ia, const uint32_t* __restrict__ p1_ja,
+                                                 const T* __restrict__ p1_a, const T* __restrict__ dval,
+                                                 const T* __restrict__ f, T* __restrict__ x, const T* __restrict__ r_in,
+                                                 T* __restrict__ r_out, const T* __restrict__ u_in, T* __restrict__ u_out,
+                                                 T* __restrict__ w) {
+    const T* v = MODE == 0 ? x : u_in;  // the vector Af multiplies
+    if (blockIdx.x < nbu) {
+        uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+        uint32_t row = gid / LPU;
+        int lane = gid % LPU;
+        bool active = row < N;
+        RowPre<T, LPU> rp;
+        rp.load(active, row, lane, af_ia, af_ja, af_a);
+        T d = (active && row >= R) ? dval[row - R] : T(0);
+        pdl_wait();
+        pdl_trigger();
+        T s = rp.sum([&](uint32_t c) { return v[c]; }, af_ja, af_a);
+#pragma unroll
+        for (int o = LPU / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (active && lane == 0) {
+            T rn;
+            if (MODE == 0) {
+                rn = f[row] - s;
+            } else {
+                x[row] += u_in[row];
+                rn = r_in[row] - s;
+            }
+            r_out[row] = rn;
+            if (row >= R) u_out[row] = d * rn;
+        }
+    } else {
+        uint32_t q = (blockIdx.x - nbu) * blockDim.x + threadIdx.x;
+        uint32_t jb = 0, je = 0;
+        if (q < R) {
+            jb = p1_ia[q];
+            je = p1_ia[q + 1];
+        }
+        pdl_wait();
+        pdl_trigger();
+        if (q >= R) return;
+        T s = lane_split_sum<T, LPP>(jb, je, p1_ja, p1_a, [&](uint32_t k) {
+            T t = lane_split_sum<T, LPU>(af_ia[k], af_ia[k + 1], af_ja, af_a, [&](uint32_t c) { return v[c]; });
+            return MODE == 0 ? f[k] - t : r_in[k] - t;
+        });
+        w[q] = s;
+    }
+}
+
+// Step B with the coarse slice tabulated (C, n x n): warps [0, n) compute
+// u0_C = C w_C as k_dense_gemv does; warps [n, n + M) compute the E rows
+// u0_q = sum_j G_qj y_j (LPG-lane split), y_j = w_j (j < M) or the coarse
+// entry recomputed by the whole warp exactly as k_dense_gemv computes it.
+template <class T, int LPG>
+__global__ void __launch_bounds__(256) k_merge_b(uint32_t M, uint32_t n, const uint32_t* __restrict__ g_ia,
+                                                 const uint32_t* __restrict__ g_ja, const T* __restrict__ g_a,
+                                                 const T* __restrict__ C, const T* __restrict__ w, T* __restrict__ out) {
+    constexpr int CV = 16;
+    uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    const T* wc = w + M;
+    // the dense row of a coarse warp is constant: loaded before the wait
+    bool coarse = warp < n;
+    const T* crow = C + (size_t)(coarse ? warp : 0) * n;
+    T cv[CV];
+#pragma unroll
+    for (int k = 0; k < CV; k++) {
+        uint32_t j = lane + 32 * k;
+        cv[k] = (coarse && j < n) ? crow[j] : T(0);
+    }
+    pdl_wait();
+    pdl_trigger();
+    auto dense_dot = [&](const T* c, const T* pre) {
+        T s = 0;
+#pragma unroll
+        for (int k = 0; k < CV; k++) {
+            uint32_t j = lane + 32 * k;
+            if (j < n) s = fmadd(pre ? pre[k] : c[j], wc[j], s);
+        }
+        for (uint32_t j = lane + 32 * CV; j < n; j += 32) s = fmadd(c[j], wc[j], s);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        return s;
+    };
+    if (coarse) {
+        T s = dense_dot(crow, cv);
+        if (lane == 0) out[M + warp] = s;
+        return;
+    }
+    uint32_t q = warp - n;
+    if (q >= M) return;
+    uint32_t jb = g_ia[q], je = g_ia[q + 1];
+    T p[LPG];
+#pragma unroll
+    for (int l = 0; l < LPG; l++) p[l] = 0;
+    for (uint32_t j = jb; j < je; j++) {
+        uint32_t col = g_ja[j];
+        T y = col < M ? w[col] : dense_dot(C + (size_t)(col - M) * n, nullptr);
+        T g = g_a[j];
+        int l = (int)((j - jb) & (LPG - 1));
+#pragma unroll
+        for (int m = 0; m < LPG; m++)
+            if (m == l) p[m] = fmadd(g, y, p[m]);
+    }
+#pragma unroll
+    for (int o = LPG / 2; o > 0; o >>= 1) {
+        T t[LPG];
+#pragma unroll
+        for (int l = 0; l < LPG; l++) t[l] = p[l] + p[l ^ o];
+#pragma unroll
+        for (int l = 0; l < LPG; l++) p[l] = t[l];
+    }
+    if (lane == 0) out[q] = p[0];
+}
+
 static int pick_lpr(uint32_t n, uint32_t nnz) {
     double avg = n ? (double)nnz / n : 1;
     return avg <= 1.5 ? 1 : avg <= 3 ? 2 : avg <= 6 ? 4 : avg <= 12 ? 8 : avg <= 24 ? 16 : 32;
@@ -1083,6 +1252,7 @@ struct Builder {
         if (L.direct) { direct(L, f, x); return; }
         if (!explicit_solves) { ms_waves(l, f, x); return; }
         if (mid_call(l, f, x)) return;
+        if (ms_merged(l, f, x)) return;
         LevelWork<T>& w = W[l];
         uint32_t N = L.N, M = L.M;
         bool next = l + 1 < H.nlevels && L.n;
@@ -1108,6 +1278,106 @@ struct Builder {
     }
 
     bool explicit_solves = true;
+
+    // Merged sweep steps (k_merge_a / k_merge_b) at levels of at most
+    // MERGE_MAX_N rows. Opt-in (MLP_MERGE=1; MLP_MERGE_B=1 adds step B): on
+    // B200 at 26,907 rows they were slower than the separate kernels (solve
+    // 29.7 ms against 19.6 ms at 1.12 M cells), because a P1 row's thread
+    // recomputes its entries of r' one after another.
+    static constexpr uint32_t MERGE_MAX_N = 1u << 17;
+    static bool merge_enabled() {
+        const char* e = getenv("MLP_MERGE");
+        return e && e[0] == '1';
+    }
+    bool dense_next(const Level& L, uint32_t l) const {
+        return small && small->valid() && small->dense.p && small->first == l + 1 && small->N0 == L.n && L.n;
+    }
+    // rows of Af with the correction kernel's lane count, P1 rows one per thread
+    void step_a(const Level& L, int mode, const T* f, T* x, const T* r_in, T* r_out, const T* u_in, T* u_out,
+                T* w) {
+        uint32_t N = L.N, R = L.N - L.Md;
+        bool staged = L.Af.tile_max && L.Af.tile_max <= ST_MAX_NNZ && N >= 4 * ST_ROWS;
+        int lpu = mode == 0 ? (staged ? 1 : pick_lpr(N, L.Af.nnz)) : pick_lpr(N, L.Af.nnz);
+        int lpp = pick_lpr(R, L.P1.nnz);
+        uint32_t nbu = grid_for((size_t)N * lpu, 256), nbp = R ? grid_for(R, 256) : 0;
+        const uint32_t *aia = L.Af.ia.p, *aja = L.Af.ja.p, *pia = L.P1.ia.p, *pja = L.P1.ja.p;
+        const T *aa = vals<T>(L.Af), *pa = vals<T>(L.P1), *dv = dvals<T>(L);
+        auto go = [=](auto kern, cudaStream_t s) {
+            launch_k(kern, nbu + nbp, 256, 0, s, N, R, nbu, aia, aja, aa, pia, pja, pa, dv, f, x, r_in, r_out, u_in,
+                     u_out, w);
+        };
+#define MERGE_A_CASE(U, P)                                                                          \
+    if (lpu == U && lpp == P) {                                                                     \
+        if (mode == 0) op([=](cudaStream_t s) { go(k_merge_a<T, U, P, 0>, s); });                   \
+        else op([=](cudaStream_t s) { go(k_merge_a<T, U, P, 1>, s); });                             \
+        return;                                                                                     \
+    }
+        MERGE_A_CASE(1, 1) MERGE_A_CASE(1, 2) MERGE_A_CASE(1, 4) MERGE_A_CASE(1, 8)
+        MERGE_A_CASE(2, 1) MERGE_A_CASE(2, 2) MERGE_A_CASE(2, 4) MERGE_A_CASE(2, 8)
+        MERGE_A_CASE(4, 1) MERGE_A_CASE(4, 2) MERGE_A_CASE(4, 4) MERGE_A_CASE(4, 8)
+        MERGE_A_CASE(8, 1) MERGE_A_CASE(8, 2) MERGE_A_CASE(8, 4) MERGE_A_CASE(8, 8)
+#undef MERGE_A_CASE
+        MLP_THROW(ERR_INTERNAL, "merged step: unsupported lane counts");
+    }
+    bool merge_a_ok(const Level& L) const {
+        uint32_t N = L.N, R = L.N - L.Md;
+        bool staged = L.Af.tile_max && L.Af.tile_max <= ST_MAX_NNZ && N >= 4 * ST_ROWS;
+        int l0 = staged ? 1 : pick_lpr(N, L.Af.nnz), l1 = pick_lpr(N, L.Af.nnz), lp = pick_lpr(R, L.P1.nnz);
+        return l0 <= 8 && l1 <= 8 && lp <= 8;
+    }
+    void step_b(const Level& L, const T* w, T* out) {
+        uint32_t M = L.M, n = L.n;
+        int lpg = pick_lpr(M, L.G.nnz);
+        uint32_t blocks = grid_for((size_t)(M + n) * 32, 256);
+        const uint32_t *gia = L.G.ia.p, *gja = L.G.ja.p;
+        const T* ga = vals<T>(L.G);
+        const T* C = small->dense.p;
+        switch (lpg) {
+            case 1: op([=](cudaStream_t s) { launch_k(k_merge_b<T, 1>, blocks, 256, 0, s, M, n, gia, gja, ga, C, w, out); }); break;
+            case 2: op([=](cudaStream_t s) { launch_k(k_merge_b<T, 2>, blocks, 256, 0, s, M, n, gia, gja, ga, C, w, out); }); break;
+            case 4: op([=](cudaStream_t s) { launch_k(k_merge_b<T, 4>, blocks, 256, 0, s, M, n, gia, gja, ga, C, w, out); }); break;
+            default: op([=](cudaStream_t s) { launch_k(k_merge_b<T, 8>, blocks, 256, 0, s, M, n, gia, gja, ga, C, w, out); }); break;
+        }
+        bytes += (uint64_t)n * n * sizeof(T) + 2ull * n * sizeof(T);
+        if (M) bytes += (uint64_t)L.G.nnz * (4 + sizeof(T)) + 4ull * (M + 1) + sizeof(T) * (M + n + M);
+    }
+
+    // MultiSplitPrec::solve(l, f, x) with merged steps: sweep 1 = phase 1,
+    // step B (or the recursion and phase 2); sweep 2 = step A (residual),
+    // step B; sweeps 3.. = step A (correction of the previous sweep), step B;
+    // then the last correction x += u0.
+    bool ms_merged(uint32_t l, const T* f, T* x) {
+        Level& L = *H.lv[l];
+        if (!merge_enabled() || L.N > MERGE_MAX_N || L.niter < 2 || !merge_a_ok(L)) return false;
+        const char* eb = getenv("MLP_MERGE_B");
+        bool dn = eb && eb[0] == '1' && dense_next(L, l) && pick_lpr(L.M, L.G.nnz) <= 8;
+        bool next = l + 1 < H.nlevels && L.n;
+        LevelWork<T>& W_ = W[l];
+        if (!W_.r2.p) W_.r2.alloc(L.N);
+        if (!W_.u02.p) W_.u02.alloc(L.N);
+        uint32_t M = L.M;
+        T* w = W_.w.p;
+        auto stepB = [&](T* out) {
+            if (dn) { step_b(L, w, out); return; }
+            if (next) ms(l + 1, w + M, out + M);
+            phase2(L, w, out);
+        };
+        phase1(L, f, w, x);
+        stepB(x);
+        T *ra = W_.r.p, *rb = W_.r2.p, *ua = W_.u0.p, *ub = W_.u02.p;
+        step_a(L, 0, f, x, nullptr, ra, nullptr, ua, w);
+        bytes += spmv_bytes(L.Af) + (uint64_t)L.P1.nnz * (4 + sizeof(T)) + sizeof(T) * (uint64_t)L.N;
+        stepB(ua);
+        for (uint32_t it = 3; it <= L.niter; it++) {
+            step_a(L, 1, f, x, ra, rb, ua, ub, w);
+            bytes += spmv_bytes(L.Af) + (uint64_t)L.P1.nnz * (4 + sizeof(T)) + sizeof(T) * 4ull * L.N;
+            stepB(ub);
+            std::swap(ra, rb);
+            std::swap(ua, ub);
+        }
+        update(L, ua, x, nullptr, false);
+        return true;
+    }
 
     // The whole level-l call as one cluster launch (k_mid_level) when level
     // l + 1 is the tabulated dense sub-hierarchy and level l is small enough

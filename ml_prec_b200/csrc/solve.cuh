@@ -12,6 +12,7 @@ namespace mlp {
 template <class T>
 struct LevelWork {
     DBuf<T> r, w, u0;            // multi-split: residual, L-solve output, correction
+    DBuf<T> r2, u02;             // second residual / correction buffers of the merged sweeps
     DBuf<T> cu0, cu1, cx2, ctmp; // uh_cheb: Chebyshev vectors on the coarse slice
 };
 

@@ -22,15 +22,19 @@ def M():
     return M
 
 
-@pytest.fixture(params=["dense", "unfused", "small", "explicit", "waves"])
+@pytest.fixture(params=["dense", "merged", "fused", "small", "explicit", "waves"])
 def apply_path(request, monkeypatch):
     """Run each case through every apply path: the tabulated small-level
-    operator with the level above it fused into one cluster launch (default),
-    the same without the fused level kernel, the shared-memory small-level
-    kernel (tabulation off), the launch path with explicit triangular solves
-    (small kernel off), and the launch path with wavefront triangular solves."""
-    if request.param == "unfused":
-        monkeypatch.setenv("MLP_MID", "0")
+    operator with every sweep step a separate kernel (default), the same with
+    merged sweep steps at the small levels, the level above the tabulated
+    operator as one cluster launch, the shared-memory small-level kernel
+    (tabulation off), the launch path with explicit triangular solves (small
+    kernel off), and the launch path with wavefront triangular solves."""
+    if request.param == "merged":
+        monkeypatch.setenv("MLP_MERGE", "1")
+        monkeypatch.setenv("MLP_MERGE_B", "1")
+    if request.param == "fused":
+        monkeypatch.setenv("MLP_MID", "1")
     if request.param == "small":
         monkeypatch.setenv("MLP_DENSE_OP_MAX", "0")
     if request.param in ("explicit", "waves"):
@@ -170,6 +174,7 @@ def test_fused_level_kernel_matches_separate_launches(M, fp32, monkeypatch):
     A, b = M.CSRMatrix.spe(60, 220, 85, kx, ky, kz, c=1.0)
     f = np.random.default_rng(4).standard_normal(A.n)
     kw = dict(q=(0.8,), niter=(5,), max_levels=15, degree_max=2, fp32=fp32)
+    monkeypatch.setenv("MLP_MID", "1")
     P1 = M.MultiSplitPrec(A, **kw)
     z1 = P1.solve(f)
     st1 = M.SolverStats()
@@ -183,3 +188,29 @@ def test_fused_level_kernel_matches_separate_launches(M, fp32, monkeypatch):
     assert np.linalg.norm(z1 - z2) <= tz * np.linalg.norm(z2)
     assert abs(st1.niter - st2.niter) <= 1
     assert np.linalg.norm(x1 - x2) <= tx * np.linalg.norm(x2)
+
+
+@pytest.mark.parametrize("fp32", [False, True])
+def test_merged_sweep_steps_are_bit_identical(M, fp32, monkeypatch):
+    """60x220x85 layered field: at the small levels consecutive sweep steps run
+    as merged kernels that recompute the entries they need; they reproduce the
+    separate kernels' arithmetic, so the apply and the PCG iterates are
+    bit-identical."""
+    from ml_prec_b200 import fields
+    kx, ky, kz = fields.field("layered", 2)
+    A, b = M.CSRMatrix.spe(60, 220, 85, kx, ky, kz, c=1.0)
+    f = np.random.default_rng(5).standard_normal(A.n)
+    kw = dict(q=(0.8,), niter=(5,), max_levels=15, degree_max=2, fp32=fp32)
+    monkeypatch.setenv("MLP_MERGE", "1")
+    monkeypatch.setenv("MLP_MERGE_B", "1")
+    P1 = M.MultiSplitPrec(A, **kw)
+    z1 = P1.solve(f)
+    st1 = M.SolverStats()
+    x1 = M.PCGSolver(A, b, P1, stats=st1, eps=1e-8)
+    monkeypatch.setenv("MLP_MERGE", "0")
+    P2 = M.MultiSplitPrec(A, **kw)
+    z2 = P2.solve(f)
+    st2 = M.SolverStats()
+    x2 = M.PCGSolver(A, b, P2, stats=st2, eps=1e-8)
+    assert np.array_equal(z1, z2)
+    assert st1.niter == st2.niter and np.array_equal(x1, x2)
