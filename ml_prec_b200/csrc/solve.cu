@@ -79,38 +79,93 @@ __device__ __forceinline__ T staged_row(uint32_t j, uint32_t je, const uint32_t*
     return acc;
 }
 
+// Pipelined staged tiles. The dynamic shared memory holds two tile buffers
+// (column indices and values, cap entries each) and three row-start buffers;
+// while a tile's rows are summed, the next tile's column indices and values
+// and the row starts of the one after are already on their way (cp.async, 16
+// bytes per copy, from the 16-byte boundaries at or below the tile's first
+// entries). The matrix copies of the first tile are issued before
+// griddepcontrol.wait (the matrix is constant); x is only read after it.
+// Rows are summed by staged_row, so the result equals the unpipelined order.
+template <class T>
+__host__ __device__ constexpr uint32_t pipe_cap(uint32_t tile_max) { return (tile_max + 8 + 3) & ~3u; }
+constexpr uint32_t PIPE_IAS = ST_ROWS + 8;
+template <class T>
+__host__ __device__ constexpr size_t pipe_smem_bytes(uint32_t tile_max) {
+    return 2ull * pipe_cap<T>(tile_max) * (sizeof(T) + 4) + 3ull * PIPE_IAS * 4;
+}
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+    uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all_groups() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+template <class T, class Epi>
+__device__ __forceinline__ void spmv_pipe(uint32_t n, const uint32_t* __restrict__ ia, const uint32_t* __restrict__ ja,
+                                          const T* __restrict__ a, const T* __restrict__ x, uint32_t cap, Epi epi) {
+    extern __shared__ __align__(16) unsigned char pipe_smem[];
+    constexpr uint32_t VA = 16 / sizeof(T);
+    T* s_a = reinterpret_cast<T*>(pipe_smem);                   // 2 x cap
+    uint32_t* s_ja = reinterpret_cast<uint32_t*>(s_a + 2 * cap);  // 2 x cap
+    uint32_t* s_ia = s_ja + 2 * cap;                             // 3 x PIPE_IAS
+    const uint32_t ntiles = (n + ST_ROWS - 1) / ST_ROWS;
+    const uint32_t G = gridDim.x;
+    auto issue_ia = [&](uint32_t t, int b) {
+        uint32_t r0 = t * ST_ROWS, nr = min(ST_ROWS, n - r0);
+        uint32_t nv = (nr + 1 + 3) / 4;  // r0 is a multiple of 4: 16-byte aligned
+        for (uint32_t v = threadIdx.x; v < nv; v += blockDim.x) cp_async16(s_ia + b * PIPE_IAS + 4 * v, ia + r0 + 4 * v);
+    };
+    auto issue_tile = [&](uint32_t t, int bi, int b) {
+        uint32_t nr = min(ST_ROWS, n - t * ST_ROWS);
+        const uint32_t* sia = s_ia + bi * PIPE_IAS;
+        uint32_t e0 = sia[0], e1 = sia[nr];
+        uint32_t bj = e0 & ~3u, nvj = (e1 - bj + 3) / 4;
+        uint32_t ba = e0 & ~(VA - 1), nva = (e1 - ba + VA - 1) / VA;
+        for (uint32_t v = threadIdx.x; v < nvj; v += blockDim.x) cp_async16(s_ja + b * cap + 4 * v, ja + bj + 4 * v);
+        for (uint32_t v = threadIdx.x; v < nva; v += blockDim.x) cp_async16(s_a + b * cap + VA * v, a + ba + VA * v);
+    };
+    const uint32_t t0 = blockIdx.x;
+    if (t0 < ntiles) {
+        issue_ia(t0, 0);
+        cp_async_commit();
+        cp_async_wait_all_groups();
+        __syncthreads();
+        issue_tile(t0, 0, 0);
+        if (t0 + G < ntiles) issue_ia(t0 + G, 1);
+        cp_async_commit();
+    }
+    pdl_wait();
+    pdl_trigger();
+    uint32_t i = 0;
+    for (uint32_t t = t0; t < ntiles; t += G, i++) {
+        cp_async_wait_all_groups();
+        __syncthreads();
+        uint32_t tn = t + G;
+        if (tn < ntiles) {
+            issue_tile(tn, (i + 1) % 3, (i + 1) & 1);
+            if (tn + G < ntiles) issue_ia(tn + G, (i + 2) % 3);
+            cp_async_commit();
+        }
+        uint32_t r0 = t * ST_ROWS, nr = min(ST_ROWS, n - r0);
+        const uint32_t* sia = s_ia + (i % 3) * PIPE_IAS;
+        uint32_t e0 = sia[0];
+        uint32_t bj = e0 & ~3u, ba = e0 & ~(VA - 1);
+        if (threadIdx.x < nr) {
+            T acc = staged_row<T>(sia[threadIdx.x], sia[threadIdx.x + 1], s_ja + (i & 1) * cap, bj,
+                                  s_a + (i & 1) * cap, ba, [&](uint32_t c) { return x[c]; });
+            epi(r0 + threadIdx.x, acc);
+        }
+    }
+}
+
 template <class T, int MODE>  // MODE 0: y = A x, 1: y = f - A x
 __global__ void __launch_bounds__(ST_ROWS) k_spmv_staged(uint32_t n, const uint32_t* __restrict__ ia,
                                                          const uint32_t* __restrict__ ja, const T* __restrict__ a,
                                                          const T* __restrict__ x, T* __restrict__ y,
-                                                         const T* __restrict__ f) {
-    pdl_wait();
-    pdl_trigger();
-    __shared__ uint32_t s_ia[ST_ROWS + 1];
-    __shared__ __align__(16) uint32_t s_ja[ST_MAX_NNZ + 8];
-    __shared__ __align__(16) T s_a[ST_MAX_NNZ + 8];
-    constexpr uint32_t VA = 16 / sizeof(T);
-    uint32_t ntiles = (n + ST_ROWS - 1) / ST_ROWS;
-    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        uint32_t r0 = t * ST_ROWS, nr = min(ST_ROWS, n - r0);
-        for (uint32_t i = threadIdx.x; i <= nr; i += blockDim.x) s_ia[i] = ia[r0 + i];
-        __syncthreads();
-        uint32_t e0 = s_ia[0], e1 = s_ia[nr];
-        uint32_t bj = e0 & ~3u, nvj = (e1 - bj + 3) / 4;
-        uint32_t ba = e0 & ~(VA - 1), nva = (e1 - ba + VA - 1) / VA;
-        const uint4* gj = reinterpret_cast<const uint4*>(ja + bj);
-        const uint4* ga = reinterpret_cast<const uint4*>(a + ba);
-        for (uint32_t v = threadIdx.x; v < nvj; v += blockDim.x) reinterpret_cast<uint4*>(s_ja)[v] = gj[v];
-        for (uint32_t v = threadIdx.x; v < nva; v += blockDim.x) reinterpret_cast<uint4*>(s_a)[v] = ga[v];
-        __syncthreads();
-        if (threadIdx.x < nr) {
-            T acc = staged_row<T>(s_ia[threadIdx.x], s_ia[threadIdx.x + 1], s_ja, bj, s_a, ba,
-                                  [&](uint32_t c) { return x[c]; });
-            uint32_t row = r0 + threadIdx.x;
-            y[row] = MODE ? f[row] - acc : acc;
-        }
-        __syncthreads();
-    }
+                                                         const T* __restrict__ f, uint32_t cap) {
+    spmv_pipe<T>(n, ia, ja, a, x, cap, [&](uint32_t row, T acc) { y[row] = MODE ? f[row] - acc : acc; });
 }
 
 __global__ void k_tile_max(uint32_t n, const uint32_t* __restrict__ ia, uint32_t* __restrict__ out) {
@@ -121,6 +176,8 @@ __global__ void k_tile_max(uint32_t n, const uint32_t* __restrict__ ia, uint32_t
     atomicMax(out, ia[r1] - ia[r0]);
 }
 
+static void pipe_prepare_all(uint32_t tile_max);
+
 void csr_tile_stats(DCSR& m, cudaStream_t s) {
     if (!m.nrow) { m.tile_max = 0; return; }
     Tmp<uint32_t> d(1);
@@ -130,6 +187,8 @@ void csr_tile_stats(DCSR& m, cudaStream_t s) {
     CK_LAUNCH();
     CK(cudaMemcpyAsync(&m.tile_max, d.p, 4, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    // the staged kernels' launch shapes are worked out here, outside any stream capture
+    if (m.tile_max && m.tile_max <= ST_MAX_NNZ) pipe_prepare_all(m.tile_max);
 }
 
 static unsigned staged_grid(uint32_t n) {
@@ -137,13 +196,44 @@ static unsigned staged_grid(uint32_t n) {
     return (unsigned)std::max<uint32_t>(1, std::min<uint32_t>(nt, (uint32_t)num_sms() * 5));
 }
 
+// Grid of a pipelined staged kernel: the CTAs that fit on the device at once
+// with this shared memory (at most five per SM, and at most one per tile).
+template <class K>
+static unsigned pipe_grid(K kern, uint32_t n, size_t smem) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, size_t>, int> occ;
+    int per_sm = 0;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto key = std::make_pair((const void*)kern, smem);
+        auto it = occ.find(key);
+        if (it == occ.end()) {
+            cudaFuncAttributes fa;
+            CK(cudaFuncGetAttributes(&fa, kern));
+            CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(small_smem_limit() - fa.sharedSizeBytes)));
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, ST_ROWS, smem));
+            occ[key] = per_sm;
+        } else {
+            per_sm = it->second;
+        }
+    }
+    uint32_t nt = (n + ST_ROWS - 1) / ST_ROWS;
+    uint32_t g = (uint32_t)num_sms() * (uint32_t)std::max(1, std::min(per_sm, 5));
+    return (unsigned)std::max<uint32_t>(1, std::min<uint32_t>(nt, g));
+}
+
 template <class T>
 static void launch_spmv(uint32_t n, uint32_t nnz, const uint32_t* ia, const uint32_t* ja, const T* a, const T* x,
                         T* y, const T* f, cudaStream_t s, uint32_t tile_max = 0) {
     if (!n) return;
     if (tile_max && tile_max <= ST_MAX_NNZ && n >= 4 * ST_ROWS) {
-        if (f) launch_k(k_spmv_staged<T, 1>, staged_grid(n), ST_ROWS, 0, s, n, ia, ja, a, x, y, f);
-        else launch_k(k_spmv_staged<T, 0>, staged_grid(n), ST_ROWS, 0, s, n, ia, ja, a, x, y, f);
+        uint32_t cap = pipe_cap<T>(tile_max);
+        size_t smem = pipe_smem_bytes<T>(tile_max);
+        if (f) launch_k(k_spmv_staged<T, 1>, pipe_grid(k_spmv_staged<T, 1>, n, smem), ST_ROWS, smem, s, n, ia, ja, a, x,
+                        y, f, cap);
+        else launch_k(k_spmv_staged<T, 0>, pipe_grid(k_spmv_staged<T, 0>, n, smem), ST_ROWS, smem, s, n, ia, ja, a, x,
+                      y, f, cap);
         return;
     }
     double avg = (double)nnz / n;
@@ -1746,33 +1836,12 @@ __global__ void __launch_bounds__(ST_ROWS) k_pcg_spmv_dot_staged(uint32_t n, con
                                                                  const double* __restrict__ a,
                                                                  const double* __restrict__ p,
                                                                  double* __restrict__ Ap, double* partials,
-                                                                 PcgDev* d) {
-    __shared__ uint32_t s_ia[ST_ROWS + 1];
-    __shared__ __align__(16) uint32_t s_ja[ST_MAX_NNZ + 8];
-    __shared__ __align__(16) double s_a[ST_MAX_NNZ + 8];
+                                                                 PcgDev* d, uint32_t cap) {
     double part = 0;
-    uint32_t ntiles = (n + ST_ROWS - 1) / ST_ROWS;
-    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        uint32_t r0 = t * ST_ROWS, nr = min(ST_ROWS, n - r0);
-        for (uint32_t i = threadIdx.x; i <= nr; i += blockDim.x) s_ia[i] = ia[r0 + i];
-        __syncthreads();
-        uint32_t e0 = s_ia[0], e1 = s_ia[nr];
-        uint32_t bj = e0 & ~3u, nvj = (e1 - bj + 3) / 4;
-        uint32_t ba = e0 & ~1u, nva = (e1 - ba + 1) / 2;
-        const uint4* gj = reinterpret_cast<const uint4*>(ja + bj);
-        const uint4* ga = reinterpret_cast<const uint4*>(a + ba);
-        for (uint32_t v = threadIdx.x; v < nvj; v += blockDim.x) reinterpret_cast<uint4*>(s_ja)[v] = gj[v];
-        for (uint32_t v = threadIdx.x; v < nva; v += blockDim.x) reinterpret_cast<uint4*>(s_a)[v] = ga[v];
-        __syncthreads();
-        if (threadIdx.x < nr) {
-            double acc = staged_row<double>(s_ia[threadIdx.x], s_ia[threadIdx.x + 1], s_ja, bj, s_a, ba,
-                                            [&](uint32_t c) { return p[c]; });
-            uint32_t row = r0 + threadIdx.x;
-            Ap[row] = acc;
-            part += acc * p[row];
-        }
-        __syncthreads();
-    }
+    spmv_pipe<double>(n, ia, ja, a, p, cap, [&](uint32_t row, double acc) {
+        Ap[row] = acc;
+        part += acc * p[row];
+    });
     part = block_sum(part);
     double tot;
     if (finish_reduce(part, partials, &d->ticket[0], &tot) && threadIdx.x == 0) {
@@ -1780,6 +1849,25 @@ __global__ void __launch_bounds__(ST_ROWS) k_pcg_spmv_dot_staged(uint32_t n, con
         if (!(tot > 0)) d->status |= (tot != tot) ? 2 : 1;
         d->alpha = d->rz0 / tot;
     }
+}
+
+static void pipe_prepare_all(uint32_t tile_max) {
+    size_t s64 = pipe_smem_bytes<double>(tile_max), s32 = pipe_smem_bytes<float>(tile_max);
+    pipe_grid(k_spmv_staged<double, 0>, 0, s64);
+    pipe_grid(k_spmv_staged<double, 1>, 0, s64);
+    pipe_grid(k_spmv_staged<float, 0>, 0, s32);
+    pipe_grid(k_spmv_staged<float, 1>, 0, s32);
+    pipe_grid(k_pcg_spmv_dot_staged, 0, s64);
+}
+
+// Launch of k_pcg_spmv_dot_staged; its grid never exceeds staged_grid(n), the
+// size the reduction scratch of every caller is made for.
+static void launch_pcg_spmv_dot_staged(uint32_t n, const DCSR& Af, const double* p, double* Ap, double* partials,
+                                       PcgDev* d, cudaStream_t s) {
+    uint32_t cap = pipe_cap<double>(Af.tile_max);
+    size_t smem = pipe_smem_bytes<double>(Af.tile_max);
+    unsigned g = std::min(pipe_grid(k_pcg_spmv_dot_staged, n, smem), staged_grid(n));
+    k_pcg_spmv_dot_staged<<<g, ST_ROWS, smem, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p, Ap, partials, d, cap);
 }
 
 // x += alpha p; r -= alpha Ap; rr = (r, r)
@@ -1953,8 +2041,7 @@ static void record_iteration(Prec& P, const DCSR& Af, uint32_t n, bool flexible,
     double avg = (double)Af.nnz / n;
     int lpr = avg <= 3 ? 2 : avg <= 6 ? 4 : avg <= 12 ? 8 : avg <= 24 ? 16 : 32;
     if (staged) {
-        k_pcg_spmv_dot_staged<<<staged_grid(n), ST_ROWS, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, W.p.p, W.Ap.p,
-                                                                 W.partials.p, d);
+        launch_pcg_spmv_dot_staged(n, Af, W.p.p, W.Ap.p, W.partials.p, d, s);
     } else switch (lpr) {
         case 2: k_pcg_spmv_dot<2><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, W.p.p, W.Ap.p, W.partials.p, d); break;
         case 4: k_pcg_spmv_dot<4><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, W.p.p, W.Ap.p, W.partials.p, d); break;
@@ -2264,7 +2351,7 @@ int pcg_solve_hostloop(const DCSR& A, const double* b, Prec& P, double* x, doubl
     while (norm / init > eps) {
         if (maxit && it >= maxit) { rc = ERR_MAXIT; msg = "iteration cap reached"; break; }
         if (staged) {
-            k_pcg_spmv_dot_staged<<<Gs, ST_ROWS, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p.p, Ap.p, partials.p, d);
+            launch_pcg_spmv_dot_staged(n, Af, p.p, Ap.p, partials.p, d, s);
         } else switch (lpr) {
             case 2: k_pcg_spmv_dot<2><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p.p, Ap.p, partials.p, d); break;
             case 4: k_pcg_spmv_dot<4><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p.p, Ap.p, partials.p, d); break;
@@ -2430,7 +2517,7 @@ int pcg_solve_noalloc(const DCSR& A, const double* b, Prec& P, double* x, double
     while (norm / init > eps) {
         if (maxit && it >= maxit) { rc = ERR_MAXIT; msg = "iteration cap reached"; break; }
         if (staged) {
-            k_pcg_spmv_dot_staged<<<Gs, ST_ROWS, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p, Ap, partials, d);
+            launch_pcg_spmv_dot_staged(n, Af, p, Ap, partials, d, s);
         } else switch (lpr) {
             case 2: k_pcg_spmv_dot<2><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p, Ap, partials, d); break;
             case 4: k_pcg_spmv_dot<4><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p, Ap, partials, d); break;
