@@ -91,6 +91,7 @@ typedef struct {
     double q, alpha, beta, lmin, lmax;
     uint32_t L_nnz, U_nnz;
     uint32_t nwave_l, nwave_u; /* wavefronts of the level-scheduled L / U solves  */
+    uint32_t P1_nnz, G_nnz;    /* explicit triangular factors of the sweeps       */
 } mlp_level_info;
 
 const char* mlp_last_error(void);

@@ -57,6 +57,7 @@ class LevelInfo(C.Structure):
         ("lmax", C.c_double),
         ("L_nnz", C.c_uint32), ("U_nnz", C.c_uint32),
         ("nwave_l", C.c_uint32), ("nwave_u", C.c_uint32),
+        ("P1_nnz", C.c_uint32), ("G_nnz", C.c_uint32),
     ]
 
 

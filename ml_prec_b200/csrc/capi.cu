@@ -285,6 +285,8 @@ int mlp_prec_level_info(const mlp_prec* P, uint32_t level, mlp_level_info* info)
     info->L_nnz = L.L.nnz; info->U_nnz = L.U.nnz;
     info->nwave_l = L.lw_off.empty() ? 0 : (uint32_t)L.lw_off.size() - 1;
     info->nwave_u = L.uw_off.empty() ? 0 : (uint32_t)L.uw_off.size() - 1;
+    info->P1_nnz = L.P1.nnz;
+    info->G_nnz = L.G.nnz;
     API_END
 }
 

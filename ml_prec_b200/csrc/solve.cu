@@ -80,19 +80,22 @@ __device__ __forceinline__ T staged_row(uint32_t j, uint32_t je, const uint32_t*
 }
 
 // Pipelined staged tiles. The dynamic shared memory holds two tile buffers
-// (column indices and values, cap entries each) and three row-start buffers;
-// while a tile's rows are summed, the next tile's column indices and values
-// and the row starts of the one after are already on their way (cp.async, 16
-// bytes per copy, from the 16-byte boundaries at or below the tile's first
-// entries). The matrix copies of the first tile are issued before
-// griddepcontrol.wait (the matrix is constant); x is only read after it.
-// Rows are summed by staged_row, so the result equals the unpipelined order.
-template <class T>
-__host__ __device__ constexpr uint32_t pipe_cap(uint32_t tile_max) { return (tile_max + 8 + 3) & ~3u; }
+// and three row-start buffers; while a tile's rows are summed, the next
+// tile's column indices (and, with SA, its values) and the row starts of the
+// one after are already on their way (cp.async, 16 bytes per copy, from the
+// 16-byte boundaries at or below the tile's first entries). Without SA the
+// values are read from global memory in the summing loop (each row's values
+// are contiguous; the tile's lines are reused through L1), which halves the
+// shared memory of a CTA so twice as many warps fit on an SM. The matrix
+// copies of the first tile are issued before griddepcontrol.wait (the matrix
+// is constant); x is only read after it. Rows are summed in column order
+// (staged_row), so the result equals the unpipelined order.
 constexpr uint32_t PIPE_IAS = ST_ROWS + 8;
 template <class T>
+__host__ __device__ constexpr uint32_t pipe_cap(uint32_t tile_max) { return (tile_max + 8 + 3) & ~3u; }
+template <class T, bool SA>
 __host__ __device__ constexpr size_t pipe_smem_bytes(uint32_t tile_max) {
-    return 2ull * pipe_cap<T>(tile_max) * (sizeof(T) + 4) + 3ull * PIPE_IAS * 4;
+    return 2ull * pipe_cap<T>(tile_max) * ((SA ? sizeof(T) : 0) + 4) + 3ull * PIPE_IAS * 4;
 }
 
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
@@ -102,14 +105,14 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all_groups() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-template <class T, class Epi>
+template <class T, bool SA, class Epi>
 __device__ __forceinline__ void spmv_pipe(uint32_t n, const uint32_t* __restrict__ ia, const uint32_t* __restrict__ ja,
                                           const T* __restrict__ a, const T* __restrict__ x, uint32_t cap, Epi epi) {
     extern __shared__ __align__(16) unsigned char pipe_smem[];
     constexpr uint32_t VA = 16 / sizeof(T);
-    T* s_a = reinterpret_cast<T*>(pipe_smem);                   // 2 x cap
-    uint32_t* s_ja = reinterpret_cast<uint32_t*>(s_a + 2 * cap);  // 2 x cap
-    uint32_t* s_ia = s_ja + 2 * cap;                             // 3 x PIPE_IAS
+    T* s_a = reinterpret_cast<T*>(pipe_smem);                                // 2 x cap (SA only)
+    uint32_t* s_ja = reinterpret_cast<uint32_t*>(s_a + (SA ? 2 * cap : 0));  // 2 x cap
+    uint32_t* s_ia = s_ja + 2 * cap;                                         // 3 x PIPE_IAS
     const uint32_t ntiles = (n + ST_ROWS - 1) / ST_ROWS;
     const uint32_t G = gridDim.x;
     auto issue_ia = [&](uint32_t t, int b) {
@@ -122,9 +125,11 @@ __device__ __forceinline__ void spmv_pipe(uint32_t n, const uint32_t* __restrict
         const uint32_t* sia = s_ia + bi * PIPE_IAS;
         uint32_t e0 = sia[0], e1 = sia[nr];
         uint32_t bj = e0 & ~3u, nvj = (e1 - bj + 3) / 4;
-        uint32_t ba = e0 & ~(VA - 1), nva = (e1 - ba + VA - 1) / VA;
         for (uint32_t v = threadIdx.x; v < nvj; v += blockDim.x) cp_async16(s_ja + b * cap + 4 * v, ja + bj + 4 * v);
-        for (uint32_t v = threadIdx.x; v < nva; v += blockDim.x) cp_async16(s_a + b * cap + VA * v, a + ba + VA * v);
+        if (SA) {
+            uint32_t ba = e0 & ~(VA - 1), nva = (e1 - ba + VA - 1) / VA;
+            for (uint32_t v = threadIdx.x; v < nva; v += blockDim.x) cp_async16(s_a + b * cap + VA * v, a + ba + VA * v);
+        }
     };
     const uint32_t t0 = blockIdx.x;
     if (t0 < ntiles) {
@@ -153,19 +158,32 @@ __device__ __forceinline__ void spmv_pipe(uint32_t n, const uint32_t* __restrict
         uint32_t e0 = sia[0];
         uint32_t bj = e0 & ~3u, ba = e0 & ~(VA - 1);
         if (threadIdx.x < nr) {
-            T acc = staged_row<T>(sia[threadIdx.x], sia[threadIdx.x + 1], s_ja + (i & 1) * cap, bj,
-                                  s_a + (i & 1) * cap, ba, [&](uint32_t c) { return x[c]; });
+            T acc = SA ? staged_row<T>(sia[threadIdx.x], sia[threadIdx.x + 1], s_ja + (i & 1) * cap, bj,
+                                       s_a + (i & 1) * cap, ba, [&](uint32_t c) { return x[c]; })
+                       : staged_row<T>(sia[threadIdx.x], sia[threadIdx.x + 1], s_ja + (i & 1) * cap, bj, a, 0,
+                                       [&](uint32_t c) { return x[c]; });
             epi(r0 + threadIdx.x, acc);
         }
     }
 }
 
-template <class T, int MODE>  // MODE 0: y = A x, 1: y = f - A x
+template <class T, int MODE, bool SA>  // MODE 0: y = A x, 1: y = f - A x
 __global__ void __launch_bounds__(ST_ROWS) k_spmv_staged(uint32_t n, const uint32_t* __restrict__ ia,
                                                          const uint32_t* __restrict__ ja, const T* __restrict__ a,
                                                          const T* __restrict__ x, T* __restrict__ y,
                                                          const T* __restrict__ f, uint32_t cap) {
-    spmv_pipe<T>(n, ia, ja, a, x, cap, [&](uint32_t row, T acc) { y[row] = MODE ? f[row] - acc : acc; });
+    spmv_pipe<T, SA>(n, ia, ja, a, x, cap, [&](uint32_t row, T acc) { y[row] = MODE ? f[row] - acc : acc; });
+}
+
+// Whether the staged kernels copy the values into shared memory too
+// (MLP_PIPE_A=1) or read them from global memory (default).
+static bool pipe_stage_values() {
+    static int on = -1;
+    if (on < 0) {
+        const char* e = getenv("MLP_PIPE_A");
+        on = (e && e[0] == '1') ? 1 : 0;
+    }
+    return on == 1;
 }
 
 __global__ void k_tile_max(uint32_t n, const uint32_t* __restrict__ ia, uint32_t* __restrict__ out) {
@@ -197,7 +215,7 @@ static unsigned staged_grid(uint32_t n) {
 }
 
 // Grid of a pipelined staged kernel: the CTAs that fit on the device at once
-// with this shared memory (at most five per SM, and at most one per tile).
+// with this shared memory (at most eight per SM, and at most one per tile).
 template <class K>
 static unsigned pipe_grid(K kern, uint32_t n, size_t smem) {
     static std::mutex mu;
@@ -219,7 +237,7 @@ static unsigned pipe_grid(K kern, uint32_t n, size_t smem) {
         }
     }
     uint32_t nt = (n + ST_ROWS - 1) / ST_ROWS;
-    uint32_t g = (uint32_t)num_sms() * (uint32_t)std::max(1, std::min(per_sm, 5));
+    uint32_t g = (uint32_t)num_sms() * (uint32_t)std::max(1, std::min(per_sm, 8));
     return (unsigned)std::max<uint32_t>(1, std::min<uint32_t>(nt, g));
 }
 
@@ -229,11 +247,19 @@ static void launch_spmv(uint32_t n, uint32_t nnz, const uint32_t* ia, const uint
     if (!n) return;
     if (tile_max && tile_max <= ST_MAX_NNZ && n >= 4 * ST_ROWS) {
         uint32_t cap = pipe_cap<T>(tile_max);
-        size_t smem = pipe_smem_bytes<T>(tile_max);
-        if (f) launch_k(k_spmv_staged<T, 1>, pipe_grid(k_spmv_staged<T, 1>, n, smem), ST_ROWS, smem, s, n, ia, ja, a, x,
-                        y, f, cap);
-        else launch_k(k_spmv_staged<T, 0>, pipe_grid(k_spmv_staged<T, 0>, n, smem), ST_ROWS, smem, s, n, ia, ja, a, x,
-                      y, f, cap);
+        if (pipe_stage_values()) {
+            size_t smem = pipe_smem_bytes<T, true>(tile_max);
+            if (f) launch_k(k_spmv_staged<T, 1, true>, pipe_grid(k_spmv_staged<T, 1, true>, n, smem), ST_ROWS, smem, s,
+                            n, ia, ja, a, x, y, f, cap);
+            else launch_k(k_spmv_staged<T, 0, true>, pipe_grid(k_spmv_staged<T, 0, true>, n, smem), ST_ROWS, smem, s,
+                          n, ia, ja, a, x, y, f, cap);
+        } else {
+            size_t smem = pipe_smem_bytes<T, false>(tile_max);
+            if (f) launch_k(k_spmv_staged<T, 1, false>, pipe_grid(k_spmv_staged<T, 1, false>, n, smem), ST_ROWS, smem,
+                            s, n, ia, ja, a, x, y, f, cap);
+            else launch_k(k_spmv_staged<T, 0, false>, pipe_grid(k_spmv_staged<T, 0, false>, n, smem), ST_ROWS, smem,
+                          s, n, ia, ja, a, x, y, f, cap);
+        }
         return;
     }
     double avg = (double)nnz / n;
@@ -1831,6 +1857,7 @@ __global__ void __launch_bounds__(RB) k_pcg_spmv_dot(uint32_t n, const uint32_t*
 }
 
 // Staged form of k_pcg_spmv_dot (same tiles as k_spmv_staged).
+template <bool SA>
 __global__ void __launch_bounds__(ST_ROWS) k_pcg_spmv_dot_staged(uint32_t n, const uint32_t* __restrict__ ia,
                                                                  const uint32_t* __restrict__ ja,
                                                                  const double* __restrict__ a,
@@ -1838,7 +1865,7 @@ __global__ void __launch_bounds__(ST_ROWS) k_pcg_spmv_dot_staged(uint32_t n, con
                                                                  double* __restrict__ Ap, double* partials,
                                                                  PcgDev* d, uint32_t cap) {
     double part = 0;
-    spmv_pipe<double>(n, ia, ja, a, p, cap, [&](uint32_t row, double acc) {
+    spmv_pipe<double, SA>(n, ia, ja, a, p, cap, [&](uint32_t row, double acc) {
         Ap[row] = acc;
         part += acc * p[row];
     });
@@ -1852,12 +1879,18 @@ __global__ void __launch_bounds__(ST_ROWS) k_pcg_spmv_dot_staged(uint32_t n, con
 }
 
 static void pipe_prepare_all(uint32_t tile_max) {
-    size_t s64 = pipe_smem_bytes<double>(tile_max), s32 = pipe_smem_bytes<float>(tile_max);
-    pipe_grid(k_spmv_staged<double, 0>, 0, s64);
-    pipe_grid(k_spmv_staged<double, 1>, 0, s64);
-    pipe_grid(k_spmv_staged<float, 0>, 0, s32);
-    pipe_grid(k_spmv_staged<float, 1>, 0, s32);
-    pipe_grid(k_pcg_spmv_dot_staged, 0, s64);
+    size_t s64 = pipe_smem_bytes<double, true>(tile_max), s32 = pipe_smem_bytes<float, true>(tile_max);
+    size_t u64 = pipe_smem_bytes<double, false>(tile_max), u32 = pipe_smem_bytes<float, false>(tile_max);
+    pipe_grid(k_spmv_staged<double, 0, true>, 0, s64);
+    pipe_grid(k_spmv_staged<double, 1, true>, 0, s64);
+    pipe_grid(k_spmv_staged<float, 0, true>, 0, s32);
+    pipe_grid(k_spmv_staged<float, 1, true>, 0, s32);
+    pipe_grid(k_pcg_spmv_dot_staged<true>, 0, s64);
+    pipe_grid(k_spmv_staged<double, 0, false>, 0, u64);
+    pipe_grid(k_spmv_staged<double, 1, false>, 0, u64);
+    pipe_grid(k_spmv_staged<float, 0, false>, 0, u32);
+    pipe_grid(k_spmv_staged<float, 1, false>, 0, u32);
+    pipe_grid(k_pcg_spmv_dot_staged<false>, 0, u64);
 }
 
 // Launch of k_pcg_spmv_dot_staged; its grid never exceeds staged_grid(n), the
@@ -1865,9 +1898,15 @@ static void pipe_prepare_all(uint32_t tile_max) {
 static void launch_pcg_spmv_dot_staged(uint32_t n, const DCSR& Af, const double* p, double* Ap, double* partials,
                                        PcgDev* d, cudaStream_t s) {
     uint32_t cap = pipe_cap<double>(Af.tile_max);
-    size_t smem = pipe_smem_bytes<double>(Af.tile_max);
-    unsigned g = std::min(pipe_grid(k_pcg_spmv_dot_staged, n, smem), staged_grid(n));
-    k_pcg_spmv_dot_staged<<<g, ST_ROWS, smem, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p, Ap, partials, d, cap);
+    if (pipe_stage_values()) {
+        size_t smem = pipe_smem_bytes<double, true>(Af.tile_max);
+        unsigned g = std::min(pipe_grid(k_pcg_spmv_dot_staged<true>, n, smem), staged_grid(n));
+        k_pcg_spmv_dot_staged<true><<<g, ST_ROWS, smem, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p, Ap, partials, d, cap);
+    } else {
+        size_t smem = pipe_smem_bytes<double, false>(Af.tile_max);
+        unsigned g = std::min(pipe_grid(k_pcg_spmv_dot_staged<false>, n, smem), staged_grid(n));
+        k_pcg_spmv_dot_staged<false><<<g, ST_ROWS, smem, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p, Ap, partials, d, cap);
+    }
 }
 
 // x += alpha p; r -= alpha Ap; rr = (r, r)
