@@ -68,6 +68,9 @@ typedef struct {
     uint32_t nncheb;         /* uh_cheb Chebyshev degree per level                    */
     const uint32_t* ncheb;
     int32_t fp32;            /* 1: store and apply the hierarchy in FP32              */
+    int32_t autotune;        /* 1: time the row kernels' launch shapes (lanes per row,
+                                block size) on each level at build and keep the
+                                fastest (cached per level shape); 0: fixed heuristic */
 } mlp_prec_cfg;
 
 /* Solver statistics, the fields of SolverStats (solvers.h:15-28) plus the

@@ -38,6 +38,7 @@ class PrecCfg(C.Structure):
         ("nsigma", C.c_uint32), ("sigma", f64p),
         ("nncheb", C.c_uint32), ("ncheb", u32p),
         ("fp32", C.c_int32),
+        ("autotune", C.c_int32),
     ]
 
 

@@ -262,14 +262,14 @@ class PrecBase:
 
 
 def _make(A: CSRMatrix, kind, fp32=False, q=(0.8,), niter=(5,), coarse_n=0, max_levels=15, degree_max=2,
-          order="simple_1", use_tails=True, sigma=(3.0,), ncheb=(2,)):
+          order="simple_1", use_tails=True, sigma=(3.0,), ncheb=(2,), autotune=False):
     qa = np.asarray(q, np.float64)
     na = np.asarray(niter, np.uint32)
     sa = np.asarray(sigma, np.float64)
     ca = np.asarray(ncheb, np.uint32)
     cfg = PrecCfg(kind, len(qa), ptr(qa, f64p), len(na), ptr(na, u32p), coarse_n, max_levels, degree_max,
                   ORDERS[order] if isinstance(order, str) else order, int(use_tails),
-                  len(sa), ptr(sa, f64p), len(ca), ptr(ca, u32p), int(fp32))
+                  len(sa), ptr(sa, f64p), len(ca), ptr(ca, u32p), int(fp32), int(autotune))
     h = C.c_void_p()
     check(lib().mlp_prec_create(A.h, C.byref(cfg), C.byref(h)))
     return h

@@ -183,6 +183,7 @@ int mlp_prec_create(const mlp_matrix* A, const mlp_prec_cfg* c, mlp_prec** out) 
     if (!A || !c || !out) MLP_THROW(ERR_ARG, "null pointer");
     BuildCfg cfg;
     cfg.kind = c->kind;
+    cfg.autotune = c->autotune;
     if (c->kind != MLP_PREC_MSPLIT && c->kind != MLP_PREC_CHEB) MLP_THROW(ERR_CONFIG, "unknown preconditioner kind");
     if (c->kind == MLP_PREC_MSPLIT) {
         if (!c->nq || !c->q) MLP_THROW(ERR_CONFIG, "q list is empty");

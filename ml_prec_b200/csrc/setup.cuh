@@ -21,6 +21,7 @@ struct BuildCfg {
     std::vector<double> sigma{3.0};      // uh_cheb beta per level
     std::vector<uint32_t> ncheb{2};      // uh_cheb Chebyshev degree per level
     uint32_t dense_max = 8192;           // largest coarsest level solved directly
+    int autotune = 0;                    // time the row kernels' launch shapes at build
 };
 
 // One level of the hierarchy. Two indexings are kept:

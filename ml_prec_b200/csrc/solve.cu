@@ -555,7 +555,7 @@ struct RowPre {
 // [R, N). The first nb1 blocks take the P1 rows with LPR lanes per row, the
 // rest one diagonal row per thread.
 template <class T, int LPR>
-__global__ void __launch_bounds__(256) k_phase1(uint32_t R, uint32_t N, uint32_t nb1, const uint32_t* __restrict__ ia,
+__global__ void __launch_bounds__(512) k_phase1(uint32_t R, uint32_t N, uint32_t nb1, const uint32_t* __restrict__ ia,
                                                 const uint32_t* __restrict__ ja, const T* __restrict__ a,
                                                 const T* __restrict__ dval, const T* __restrict__ src,
                                                 T* __restrict__ w, T* __restrict__ out) {
@@ -585,7 +585,7 @@ __global__ void __launch_bounds__(256) k_phase1(uint32_t R, uint32_t N, uint32_t
 // y_j = w_j for eliminated columns (j < M) and out_j (the coarse solution the
 // recursion wrote) for coarse columns.
 template <class T, int LPR>
-__global__ void __launch_bounds__(256) k_phase2(uint32_t M, const uint32_t* __restrict__ ia,
+__global__ void __launch_bounds__(512) k_phase2(uint32_t M, const uint32_t* __restrict__ ia,
                                                 const uint32_t* __restrict__ ja, const T* __restrict__ a,
                                                 const T* __restrict__ w, T* out) {
     uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -605,7 +605,7 @@ __global__ void __launch_bounds__(256) k_phase2(uint32_t M, const uint32_t* __re
 // Correction step of a level sweep: x += u0 and, when more sweeps follow,
 // r -= A u0 (the residual f - A x updated in place of recomputing it).
 template <class T, int LPR>
-__global__ void __launch_bounds__(256) k_update(uint32_t n, const uint32_t* __restrict__ ia,
+__global__ void __launch_bounds__(512) k_update(uint32_t n, const uint32_t* __restrict__ ia,
                                                 const uint32_t* __restrict__ ja, const T* __restrict__ a,
                                                 const T* __restrict__ u0, T* __restrict__ x, T* __restrict__ r,
                                                 int do_r) {
@@ -1193,6 +1193,74 @@ static int pick_lpr(uint32_t n, uint32_t nnz) {
     }
 
 // ---------------------------------------------------------------------------
+// Launch-shape autotuner. With BuildCfg::autotune the plan builder times, for
+// every row kernel of a level (phase 1, phase 2, correction), each candidate
+// (lanes per row 1..16 up to twice the average row length, blocks of 128, 256
+// or 512 threads) on the level's own data, three launches per candidate after
+// one warm-up, CUDA events on the build stream, and keeps the fastest. The
+// choice is cached per (kernel, value type, rows, nonzeros), so an ensemble of
+// equal-shaped members, or a rebuild, tunes once. Without it the shape is the
+// fixed heuristic (pick_lpr lanes, 256 threads). The lane count changes the
+// order in which a row's products are added, so tuned and untuned plans agree
+// to rounding.
+// ---------------------------------------------------------------------------
+struct LaunchShape {
+    int lpr = 1;
+    unsigned block = 256;
+};
+
+namespace {
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, uint32_t, uint32_t>, LaunchShape> g_tune;
+}  // namespace
+
+template <class Launch>
+static LaunchShape tune_shape(int kind, int tsize, uint32_t rows, uint32_t nnz, cudaStream_t s, Launch launch) {
+    auto key = std::make_tuple(kind, tsize, rows, nnz);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune.find(key);
+        if (it != g_tune.end()) return it->second;
+    }
+    double avg = rows ? (double)nnz / rows : 1;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    LaunchShape best;
+    float best_ms = 1e30f;
+    for (int lpr : {1, 2, 4, 8, 16}) {
+        if (lpr > 1 && lpr > 2 * std::ceil(avg)) break;
+        for (unsigned block : {128u, 256u, 512u}) {
+            LaunchShape c{lpr, block};
+            launch(c, s);
+            CK(cudaEventRecord(e0, s));
+            for (int r = 0; r < 3; r++) launch(c, s);
+            CK(cudaEventRecord(e1, s));
+            CK(cudaEventSynchronize(e1));
+            CK(cudaGetLastError());
+            float ms = 0;
+            CK(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < best_ms) { best_ms = ms; best = c; }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[key] = best;
+    return best;
+}
+
+#define LPR_SWITCH_B(lpr, KERNEL, ...)                                    \
+    switch (lpr) {                                                        \
+        case 1: launch_k(KERNEL<T, 1>, __VA_ARGS__); break;               \
+        case 2: launch_k(KERNEL<T, 2>, __VA_ARGS__); break;               \
+        case 4: launch_k(KERNEL<T, 4>, __VA_ARGS__); break;               \
+        case 8: launch_k(KERNEL<T, 8>, __VA_ARGS__); break;               \
+        case 16: launch_k(KERNEL<T, 16>, __VA_ARGS__); break;             \
+        default: launch_k(KERNEL<T, 32>, __VA_ARGS__); break;             \
+    }
+
+// ---------------------------------------------------------------------------
 // Plan builder: replays the reference's recursion once on the host and records
 // the launches.
 // ---------------------------------------------------------------------------
@@ -1307,43 +1375,55 @@ struct Builder {
     }
     // One application of the level's split operator on src: phase 1 (L solve
     // and diagonal block), the recursion on the coarse slice, phase 2 (U solve).
+    bool autotune = false;
+    cudaStream_t tune_stream() const { return stream; }
+
     void phase1(const Level& L, const T* src, T* w, T* out) {
         uint32_t R = L.N - L.Md, N = L.N;
-        int lpr = pick_lpr(R, L.P1.nnz);
-        uint32_t nb1 = R ? grid_for((size_t)R * lpr, 256) : 0;
-        uint32_t nb2 = N > R ? grid_for(N - R, 256) : 0;
-        if (!nb1 && !nb2) return;
+        if (!R && N <= R) return;
         const uint32_t* ia = L.P1.ia.p;
         const uint32_t* ja = L.P1.ja.p;
         const T* a = vals<T>(L.P1);
         const T* dv = dvals<T>(L);
-        op([=](cudaStream_t s) {
-            LPR_SWITCH(lpr, k_phase1, nb1 + nb2, 256, 0, s, R, N, nb1, ia, ja, a, dv, src, w, out);
-        });
+        auto launch = [=](LaunchShape c, cudaStream_t s) {
+            uint32_t nb1 = R ? grid_for((size_t)R * c.lpr, c.block) : 0;
+            uint32_t nb2 = N > R ? grid_for(N - R, c.block) : 0;
+            LPR_SWITCH_B(c.lpr, k_phase1, nb1 + nb2, c.block, 0, s, R, N, nb1, ia, ja, a, dv, src, w, out);
+        };
+        LaunchShape c{pick_lpr(R, L.P1.nnz), 256};
+        if (autotune) c = tune_shape(1, sizeof(T), R, L.P1.nnz, tune_stream(), launch);
+        op([=](cudaStream_t s) { launch(c, s); });
         bytes += (uint64_t)L.P1.nnz * (4 + sizeof(T)) + 4ull * (R + 1) + sizeof(T) * (2ull * N + L.Md) ;
     }
     void phase2(const Level& L, const T* w, T* out) {
         uint32_t M = L.M;
         if (!M) return;
-        int lpr = pick_lpr(M, L.G.nnz);
         const uint32_t* ia = L.G.ia.p;
         const uint32_t* ja = L.G.ja.p;
         const T* a = vals<T>(L.G);
-        op([=](cudaStream_t s) {
-            LPR_SWITCH(lpr, k_phase2, grid_for((size_t)M * lpr, 256), 256, 0, s, M, ia, ja, a, w, out);
-        });
+        auto launch = [=](LaunchShape c, cudaStream_t s) {
+            LPR_SWITCH_B(c.lpr, k_phase2, grid_for((size_t)M * c.lpr, c.block), c.block, 0, s, M, ia, ja, a, w, out);
+        };
+        LaunchShape c{pick_lpr(M, L.G.nnz), 256};
+        if (autotune) c = tune_shape(2, sizeof(T), M, L.G.nnz, tune_stream(), launch);
+        op([=](cudaStream_t s) { launch(c, s); });
         bytes += (uint64_t)L.G.nnz * (4 + sizeof(T)) + 4ull * (M + 1) + sizeof(T) * (M + L.n + M);
     }
     void update(const Level& L, const T* u0, T* x, T* r, bool do_r) {
         uint32_t N = L.N;
-        int lpr = do_r ? pick_lpr(N, L.Af.nnz) : 1;
         const uint32_t* ia = L.Af.ia.p;
         const uint32_t* ja = L.Af.ja.p;
         const T* a = vals<T>(L.Af);
         int dr = do_r ? 1 : 0;
-        op([=](cudaStream_t s) {
-            LPR_SWITCH(lpr, k_update, grid_for((size_t)N * lpr, 256), 256, 0, s, N, ia, ja, a, u0, x, r, dr);
-        });
+        auto launch = [=](LaunchShape c, cudaStream_t s) {
+            LPR_SWITCH_B(c.lpr, k_update, grid_for((size_t)N * c.lpr, c.block), c.block, 0, s, N, ia, ja, a, u0, x, r,
+                         dr);
+        };
+        LaunchShape c{do_r ? pick_lpr(N, L.Af.nnz) : 1, 256};
+        // the tuning runs x += u0 on scratch: every buffer of the plan is
+        // rewritten before it is read in an apply
+        if (autotune && do_r) c = tune_shape(3, sizeof(T), N, L.Af.nnz, tune_stream(), launch);
+        op([=](cudaStream_t s) { launch(c, s); });
         bytes += sizeof(T) * 3ull * N + (do_r ? spmv_bytes(L.Af) : 0);
     }
 
@@ -1717,6 +1797,7 @@ std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, c
         Builder<double> B{H, P->w64, P->plan, P->sp64.get()};
         B.explicit_solves = explicit_solves;
         B.stream = s;
+        B.autotune = cfg.autotune != 0;
         if (H.kind == PREC_MSPLIT) B.ms(0, P->fin, P->fout);
         else B.ch(0, P->fin, P->fout);
         P->bytes_per_apply = B.bytes;
@@ -1737,6 +1818,7 @@ std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, c
         Builder<float> B{H, P->w32, P->plan, P->sp32.get()};
         B.explicit_solves = explicit_solves;
         B.stream = s;
+        B.autotune = cfg.autotune != 0;
         const double* fin = P->fin;
         float* f32 = P->f32.p;
         B.op([=](cudaStream_t st) { launch_k(k_to_f32, grid_for(N0, 256), 256, 0, st, N0, fin, f32); });

@@ -6,7 +6,9 @@ nz in [10, 85] (seeded) and its own i.i.d. log-normal field (the
 small-mesh model), its own matrix and FP32-stored multi-split hierarchy; the forward
 solves (right-hand side from the Dirichlet faces) and the adjoint solves
 (misfit gradient at 25 observation cells) of all realizations each run as one
-graph launch (mlp_ensemble_solve). Sharding the ensemble over several GPUs
+graph launch (mlp_ensemble_solve). The members' row kernels take their launch
+shapes from the build-time autotuner (mlp_prec_cfg.autotune). Sharding the
+ensemble over several GPUs
 assigns whole realizations to ranks (no data exchange during the solves).
 """
 from __future__ import annotations
@@ -45,7 +47,7 @@ def shard(dims, rank, world):
 class Ensemble:
     """Matrices, hierarchies and the two ensemble graphs (forward, adjoint)."""
 
-    def __init__(self, dims, field_seed0=100, fp32=True, prec_kw=None, nobs=25, obs_seed=9):
+    def __init__(self, dims, field_seed0=100, fp32=True, prec_kw=None, nobs=25, obs_seed=9, autotune=True):
         import torch
         self.dims = list(dims)
         self.fp32 = fp32
@@ -55,7 +57,7 @@ class Ensemble:
         for i, (nx, ny, nz) in enumerate(self.dims):
             kx, ky, kz = fields.field("iid", field_seed0 + i)
             A, b = api.CSRMatrix.spe(nx, ny, nz, kx, ky, kz, c=1.0, dirichlet=True)
-            P = api.MultiSplitPrec(A, fp32=fp32, **kw)
+            P = api.MultiSplitPrec(A, fp32=fp32, autotune=autotune, **kw)
             self.A.append(A)
             self.P.append(P)
             self.b.append(torch.from_numpy(b).cuda())

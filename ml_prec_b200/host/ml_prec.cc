@@ -531,6 +531,7 @@ MultiSplitPrec::MultiSplitPrec(const SkylineMatrix& A, const Config& cfg) {
     c.order = order_s == "none" ? MLP_ORDER_NONE : order_s == "original" ? MLP_ORDER_ORIGINAL
               : order_s == "block" ? MLP_ORDER_BLOCK : MLP_ORDER_SIMPLE_1;
     c.fp32 = cfg.fp32;
+    c.autotune = cfg.autotune;
     create(A, c);
 }
 
@@ -550,6 +551,7 @@ Prec::Prec(const SkylineMatrix& A, const Config& cfg) {
     c.use_tails = cfg.use_tails;
     c.max_levels = 30;
     c.fp32 = cfg.fp32;
+    c.autotune = cfg.autotune;
     create(A, c);
 }
 
@@ -625,11 +627,12 @@ static void usage() {
                  "     --eps E                       PCG relative residual (default 1e-6)\n"
                  "     --fp32                        FP32-stored hierarchy, flexible FP64 PCG\n"
                  "     --dirichlet                   p = 1 / p = 0 on the x faces (right-hand side from them)\n"
-                 "     --perm FILE                   permeability file (default spe_perm.dat; .bin = raw doubles)\n";
+                 "     --perm FILE                   permeability file (default spe_perm.dat; .bin = raw doubles)\n"
+                 "     --autotune                    time the row kernels' launch shapes at build\n";
 }
 
 int set_params(int argc, char* argv[], Config& cfg) {
-    enum { OPT_EPS = 1000, OPT_FP32, OPT_DIRICHLET, OPT_PERM };
+    enum { OPT_EPS = 1000, OPT_FP32, OPT_DIRICHLET, OPT_PERM, OPT_AUTOTUNE };
     static struct option long_options[] = {
         {"ntests", required_argument, nullptr, 'a'},        {"niters", required_argument, nullptr, 'b'},
         {"c", required_argument, nullptr, 'c'},             {"prec-config-file", required_argument, nullptr, 'C'},
@@ -642,7 +645,8 @@ int set_params(int argc, char* argv[], Config& cfg) {
         {"nx", required_argument, nullptr, 'x'},            {"ny", required_argument, nullptr, 'y'},
         {"nz", required_argument, nullptr, 'z'},            {"eps", required_argument, nullptr, OPT_EPS},
         {"fp32", no_argument, nullptr, OPT_FP32},           {"dirichlet", no_argument, nullptr, OPT_DIRICHLET},
-        {"perm", required_argument, nullptr, OPT_PERM},     {nullptr, 0, nullptr, 0}};
+        {"perm", required_argument, nullptr, OPT_PERM},     {"autotune", no_argument, nullptr, OPT_AUTOTUNE},
+        {nullptr, 0, nullptr, 0}};
     optind = 1;
     while (true) {
         int idx = 0;
@@ -688,6 +692,7 @@ int set_params(int argc, char* argv[], Config& cfg) {
             case OPT_FP32: cfg.fp32 = true; break;
             case OPT_DIRICHLET: cfg.dirichlet = true; break;
             case OPT_PERM: cfg.perm_file = arg; break;
+            case OPT_AUTOTUNE: cfg.autotune = true; break;
             default: return 1;
         }
     }

@@ -192,6 +192,7 @@ struct Config {
     std::string vector;
     /* additions of this implementation */
     bool fp32 = false;          // FP32-stored hierarchy inside flexible FP64 PCG
+    bool autotune = false;      // time the row kernels' launch shapes at build
     bool dirichlet = false;     // x-face Dirichlet terms of the benchmark problem
     double eps = 1e-6;          // main.cc:129 fixes 1e-6; here it is an option
     std::string perm_file = "spe_perm.dat";

@@ -214,3 +214,33 @@ def test_merged_sweep_steps_are_bit_identical(M, fp32, monkeypatch):
     x2 = M.PCGSolver(A, b, P2, stats=st2, eps=1e-8)
     assert np.array_equal(z1, z2)
     assert st1.niter == st2.niter and np.array_equal(x1, x2)
+
+
+@pytest.mark.parametrize("name", ["ms_iid_12x22x6", "ms_layered_16x22x8_c01"])
+def test_autotuned_launch_shapes_match_reference(M, name):
+    """Plans whose row kernels take their launch shapes from the build-time
+    autotuner (lanes per row, block size) give the reference's PCG result:
+    iterations within 1, solution within 1e-10 relative."""
+    g = load_golden(name)
+    A = gpu_matrix(M, g)
+    kw = dict(q=(0.8,), niter=tuple(int(t) for t in str(g["options"].get("level_niter", "5")).split()),
+              max_levels=g["options"].get("max_levels", 15), degree_max=g["options"].get("degree_max", 2))
+    P = M.MultiSplitPrec(A, autotune=True, **kw)
+    st = M.SolverStats()
+    x = M.PCGSolver(A, g["b"], P, stats=st, eps=1e-8)
+    assert abs(st.niter - int(g["niter"])) <= 1
+    assert np.linalg.norm(x - g["x"]) <= 1e-10 * np.linalg.norm(g["x"])
+
+
+def test_autotuned_full_size_pcg(M):
+    """60x220x85: autotuned plan against the fixed-heuristic plan, same
+    tolerance and iterations within 1."""
+    from ml_prec_b200 import fields
+    kx, ky, kz = fields.field("layered", 2)
+    A, b = M.CSRMatrix.spe(60, 220, 85, kx, ky, kz, c=1.0)
+    kw = dict(q=(0.8,), niter=(5,), max_levels=15, degree_max=2)
+    st1, st2 = M.SolverStats(), M.SolverStats()
+    x1 = M.PCGSolver(A, b, M.MultiSplitPrec(A, autotune=True, **kw), stats=st1, eps=1e-8)
+    x2 = M.PCGSolver(A, b, M.MultiSplitPrec(A, **kw), stats=st2, eps=1e-8)
+    assert abs(st1.niter - st2.niter) <= 1 and st1.final_rel <= 1e-8
+    assert np.linalg.norm(x1 - x2) <= 1e-9 * np.linalg.norm(x2)
