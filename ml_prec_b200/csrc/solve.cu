@@ -1094,20 +1094,65 @@ __global__ void __launch_bounds__(256) k_merge_a(uint32_t N, uint32_t R, uint32_
             if (row >= R) u_out[row] = d * rn;
         }
     } else {
-        uint32_t q = (blockIdx.x - nbu) * blockDim.x + threadIdx.x;
+        // One warp per P1 row: lane e recomputes the entry r'_k of the row's
+        // entries e, e + 32, ... (all lanes at once), then the products are
+        // added in entry order with k_phase1's lane split. The row's first 32
+        // entries and their Af row bounds are loaded before the wait.
+        uint32_t q = ((blockIdx.x - nbu) * blockDim.x + threadIdx.x) >> 5;
+        int lane = threadIdx.x & 31;
+        bool act = q < R;
         uint32_t jb = 0, je = 0;
-        if (q < R) {
+        if (act) {
             jb = p1_ia[q];
             je = p1_ia[q + 1];
         }
+        uint32_t k0 = 0, kb0 = 0, ke0 = 0;
+        T a0 = 0;
+        if (jb + lane < je) {
+            k0 = p1_ja[jb + lane];
+            a0 = p1_a[jb + lane];
+            kb0 = af_ia[k0];
+            ke0 = af_ia[k0 + 1];
+        }
         pdl_wait();
         pdl_trigger();
-        if (q >= R) return;
-        T s = lane_split_sum<T, LPP>(jb, je, p1_ja, p1_a, [&](uint32_t k) {
-            T t = lane_split_sum<T, LPU>(af_ia[k], af_ia[k + 1], af_ja, af_a, [&](uint32_t c) { return v[c]; });
-            return MODE == 0 ? f[k] - t : r_in[k] - t;
-        });
-        w[q] = s;
+        if (!act) return;  // the whole warp
+        T p[LPP];
+#pragma unroll
+        for (int l = 0; l < LPP; l++) p[l] = 0;
+        for (uint32_t base = jb; base < je; base += 32) {
+            uint32_t j = base + lane;
+            T av = 0, rv = 0;
+            if (j < je) {
+                uint32_t k = k0, kb = kb0, ke = ke0;
+                av = a0;
+                if (base != jb) {
+                    k = p1_ja[j];
+                    av = p1_a[j];
+                    kb = af_ia[k];
+                    ke = af_ia[k + 1];
+                }
+                T t = lane_split_sum<T, LPU>(kb, ke, af_ja, af_a, [&](uint32_t c) { return v[c]; });
+                rv = (MODE == 0 ? f[k] : r_in[k]) - t;
+            }
+            uint32_t cnt = min(32u, je - base);
+            for (uint32_t e = 0; e < cnt; e++) {
+                T ae = __shfl_sync(0xffffffffu, av, e), re = __shfl_sync(0xffffffffu, rv, e);
+                int l = (int)((base - jb + e) & (LPP - 1));
+#pragma unroll
+                for (int m = 0; m < LPP; m++)
+                    if (m == l) p[m] = fmadd(ae, re, p[m]);
+            }
+        }
+#pragma unroll
+        for (int o = LPP / 2; o > 0; o >>= 1) {
+            T t2[LPP];
+#pragma unroll
+            for (int l = 0; l < LPP; l++) t2[l] = p[l] + p[l ^ o];
+#pragma unroll
+            for (int l = 0; l < LPP; l++) p[l] = t2[l];
+        }
+        if (lane == 0) w[q] = p[0];
     }
 }
 
@@ -1476,14 +1521,17 @@ struct Builder {
     bool explicit_solves = true;
 
     // Merged sweep steps (k_merge_a / k_merge_b) at levels of at most
-    // MERGE_MAX_N rows. Opt-in (MLP_MERGE=1; MLP_MERGE_B=1 adds step B): on
-    // B200 at 26,907 rows they were slower than the separate kernels (solve
-    // 29.7 ms against 19.6 ms at 1.12 M cells), because a P1 row's thread
-    // recomputes its entries of r' one after another.
+    // MERGE_MAX_N rows without the autotuner (their arithmetic reproduces the
+    // fixed launch shapes). Step A is on by default (MLP_MERGE=0 turns it
+    // off): with a warp per P1 row recomputing its entries of r' in parallel
+    // it takes the 1.12 M-cell solve from 18.56 to 18.13 ms on B200 (one thread
+    // per row doing it serially had made it 29.7 ms). Step B is opt-in
+    // (MLP_MERGE_B=1): it recomputes the coarse entries from the dense operator,
+    // about 18 MB of L2 reads per launch at 26,907 rows, and measured slower.
     static constexpr uint32_t MERGE_MAX_N = 1u << 17;
     static bool merge_enabled() {
         const char* e = getenv("MLP_MERGE");
-        return e && e[0] == '1';
+        return !(e && e[0] == '0');
     }
     bool dense_next(const Level& L, uint32_t l) const {
         return small && small->valid() && small->dense.p && small->first == l + 1 && small->N0 == L.n && L.n;
@@ -1495,7 +1543,7 @@ struct Builder {
         bool staged = L.Af.tile_max && L.Af.tile_max <= ST_MAX_NNZ && N >= 4 * ST_ROWS;
         int lpu = mode == 0 ? (staged ? 1 : pick_lpr(N, L.Af.nnz)) : pick_lpr(N, L.Af.nnz);
         int lpp = pick_lpr(R, L.P1.nnz);
-        uint32_t nbu = grid_for((size_t)N * lpu, 256), nbp = R ? grid_for(R, 256) : 0;
+        uint32_t nbu = grid_for((size_t)N * lpu, 256), nbp = R ? grid_for((size_t)R * 32, 256) : 0;
         const uint32_t *aia = L.Af.ia.p, *aja = L.Af.ja.p, *pia = L.P1.ia.p, *pja = L.P1.ja.p;
         const T *aa = vals<T>(L.Af), *pa = vals<T>(L.P1), *dv = dvals<T>(L);
         auto go = [=](auto kern, cudaStream_t s) {
@@ -1544,7 +1592,7 @@ struct Builder {
     // then the last correction x += u0.
     bool ms_merged(uint32_t l, const T* f, T* x) {
         Level& L = *H.lv[l];
-        if (!merge_enabled() || L.N > MERGE_MAX_N || L.niter < 2 || !merge_a_ok(L)) return false;
+        if (!merge_enabled() || autotune || L.N > MERGE_MAX_N || L.niter < 2 || !merge_a_ok(L)) return false;
         const char* eb = getenv("MLP_MERGE_B");
         bool dn = eb && eb[0] == '1' && dense_next(L, l) && pick_lpr(L.M, L.G.nnz) <= 8;
         bool next = l + 1 < H.nlevels && L.n;

@@ -22,16 +22,18 @@ def M():
     return M
 
 
-@pytest.fixture(params=["dense", "merged", "fused", "small", "explicit", "waves"])
+@pytest.fixture(params=["dense", "separate", "merged_b", "fused", "small", "explicit", "waves"])
 def apply_path(request, monkeypatch):
     """Run each case through every apply path: the tabulated small-level
-    operator with every sweep step a separate kernel (default), the same with
-    merged sweep steps at the small levels, the level above the tabulated
-    operator as one cluster launch, the shared-memory small-level kernel
-    (tabulation off), the launch path with explicit triangular solves (small
-    kernel off), and the launch path with wavefront triangular solves."""
-    if request.param == "merged":
-        monkeypatch.setenv("MLP_MERGE", "1")
+    operator with the correction and phase-1 steps of the small levels merged
+    (default), the same with every sweep step a separate kernel, with the coarse
+    product and phase 2 merged too, the level above the tabulated operator as
+    one cluster launch, the shared-memory small-level kernel (tabulation off),
+    the launch path with explicit triangular solves (small kernel off), and the
+    launch path with wavefront triangular solves."""
+    if request.param == "separate":
+        monkeypatch.setenv("MLP_MERGE", "0")
+    if request.param == "merged_b":
         monkeypatch.setenv("MLP_MERGE_B", "1")
     if request.param == "fused":
         monkeypatch.setenv("MLP_MID", "1")
