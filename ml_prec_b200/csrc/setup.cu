@@ -1203,7 +1203,11 @@ static void build_frames(Hierarchy& H, cudaStream_t s) {
         trace("frame operators");
         csr_tile_stats(li.Af, s);
         if (H.kind == PREC_CHEB && l > 0) csr_tile_stats(li.As, s);
-        if (!li.direct) build_explicit(li, s);
+        if (!li.direct) {
+            build_explicit(li, s);
+            csr_tile_stats(li.P1, s);
+            csr_tile_stats(li.G, s);
+        }
         trace("explicit solves");
     }
 }

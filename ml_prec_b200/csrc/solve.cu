@@ -105,9 +105,10 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all_groups() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-template <class T, bool SA, class Epi>
-__device__ __forceinline__ void spmv_pipe(uint32_t n, const uint32_t* __restrict__ ia, const uint32_t* __restrict__ ja,
-                                          const T* __restrict__ a, const T* __restrict__ x, uint32_t cap, Epi epi) {
+template <class T, bool SA, class Val, class Epi>
+__device__ __forceinline__ void spmv_pipe_v(uint32_t n, const uint32_t* __restrict__ ia,
+                                            const uint32_t* __restrict__ ja, const T* __restrict__ a, Val val,
+                                            uint32_t cap, Epi epi) {
     extern __shared__ __align__(16) unsigned char pipe_smem[];
     constexpr uint32_t VA = 16 / sizeof(T);
     T* s_a = reinterpret_cast<T*>(pipe_smem);                                // 2 x cap (SA only)
@@ -159,12 +160,49 @@ __device__ __forceinline__ void spmv_pipe(uint32_t n, const uint32_t* __restrict
         uint32_t bj = e0 & ~3u, ba = e0 & ~(VA - 1);
         if (threadIdx.x < nr) {
             T acc = SA ? staged_row<T>(sia[threadIdx.x], sia[threadIdx.x + 1], s_ja + (i & 1) * cap, bj,
-                                       s_a + (i & 1) * cap, ba, [&](uint32_t c) { return x[c]; })
-                       : staged_row<T>(sia[threadIdx.x], sia[threadIdx.x + 1], s_ja + (i & 1) * cap, bj, a, 0,
-                                       [&](uint32_t c) { return x[c]; });
+                                       s_a + (i & 1) * cap, ba, val)
+                       : staged_row<T>(sia[threadIdx.x], sia[threadIdx.x + 1], s_ja + (i & 1) * cap, bj, a, 0, val);
             epi(r0 + threadIdx.x, acc);
         }
     }
+}
+
+template <class T, bool SA, class Epi>
+__device__ __forceinline__ void spmv_pipe(uint32_t n, const uint32_t* __restrict__ ia, const uint32_t* __restrict__ ja,
+                                          const T* __restrict__ a, const T* __restrict__ x, uint32_t cap, Epi epi) {
+    spmv_pipe_v<T, SA>(n, ia, ja, a, [&](uint32_t c) { return x[c]; }, cap, epi);
+}
+
+// The sweep steps of a large level on the same tile pipeline (rows summed
+// serially in column order): phase 1 (w = P1 src on rows < R, then the
+// diagonal rows out = dval src), phase 2 (out_q = sum G_qj (j < M ? w_j :
+// out_j)) and the correction (x += u0; r -= A u0).
+template <class T>
+__global__ void __launch_bounds__(ST_ROWS) k_phase1_staged(uint32_t R, uint32_t N, const uint32_t* __restrict__ ia,
+                                                           const uint32_t* __restrict__ ja, const T* __restrict__ a,
+                                                           const T* __restrict__ dval, const T* __restrict__ src,
+                                                           T* __restrict__ w, T* __restrict__ out, uint32_t cap) {
+    spmv_pipe_v<T, false>(R, ia, ja, a, [&](uint32_t c) { return src[c]; }, cap,
+                          [&](uint32_t row, T acc) { w[row] = acc; });
+    for (uint32_t q = R + blockIdx.x * blockDim.x + threadIdx.x; q < N; q += gridDim.x * blockDim.x)
+        out[q] = dval[q - R] * src[q];
+}
+template <class T>
+__global__ void __launch_bounds__(ST_ROWS) k_phase2_staged(uint32_t M, const uint32_t* __restrict__ ia,
+                                                           const uint32_t* __restrict__ ja, const T* __restrict__ a,
+                                                           const T* __restrict__ w, T* out, uint32_t cap) {
+    spmv_pipe_v<T, false>(M, ia, ja, a, [&](uint32_t c) { return c < M ? w[c] : out[c]; }, cap,
+                          [&](uint32_t row, T acc) { out[row] = acc; });
+}
+template <class T>
+__global__ void __launch_bounds__(ST_ROWS) k_update_staged(uint32_t N, const uint32_t* __restrict__ ia,
+                                                           const uint32_t* __restrict__ ja, const T* __restrict__ a,
+                                                           const T* __restrict__ u0, T* __restrict__ x,
+                                                           T* __restrict__ r, uint32_t cap) {
+    spmv_pipe_v<T, false>(N, ia, ja, a, [&](uint32_t c) { return u0[c]; }, cap, [&](uint32_t row, T acc) {
+        x[row] += u0[row];
+        r[row] -= acc;
+    });
 }
 
 template <class T, int MODE, bool SA>  // MODE 0: y = A x, 1: y = f - A x
@@ -1241,7 +1279,8 @@ static int pick_lpr(uint32_t n, uint32_t nnz) {
 // Launch-shape autotuner. With BuildCfg::autotune the plan builder times, for
 // every row kernel of a level (phase 1, phase 2, correction), each candidate
 // (lanes per row 1..16 up to twice the average row length, blocks of 128, 256
-// or 512 threads) on the level's own data, three launches per candidate after
+// or 512 threads, and at levels above MERGE_MAX_N rows the pipelined tile
+// kernel, lpr = 0) on the level's own data, three launches per candidate after
 // one warm-up, CUDA events on the build stream, and keeps the fastest. The
 // choice is cached per (kernel, value type, rows, nonzeros), so an ensemble of
 // equal-shaped members, or a rebuild, tunes once. Without it the shape is the
@@ -1260,7 +1299,8 @@ std::map<std::tuple<int, int, uint32_t, uint32_t>, LaunchShape> g_tune;
 }  // namespace
 
 template <class Launch>
-static LaunchShape tune_shape(int kind, int tsize, uint32_t rows, uint32_t nnz, cudaStream_t s, Launch launch) {
+static LaunchShape tune_shape(int kind, int tsize, uint32_t rows, uint32_t nnz, cudaStream_t s, Launch launch,
+                              bool staged_candidate = false) {
     auto key = std::make_tuple(kind, tsize, rows, nnz);
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -1273,9 +1313,11 @@ static LaunchShape tune_shape(int kind, int tsize, uint32_t rows, uint32_t nnz, 
     CK(cudaEventCreate(&e1));
     LaunchShape best;
     float best_ms = 1e30f;
-    for (int lpr : {1, 2, 4, 8, 16}) {
+    for (int lpr : {0, 1, 2, 4, 8, 16}) {
+        if (lpr == 0 && !staged_candidate) continue;
         if (lpr > 1 && lpr > 2 * std::ceil(avg)) break;
         for (unsigned block : {128u, 256u, 512u}) {
+            if (lpr == 0 && block != ST_ROWS) continue;  // the pipelined tile kernel has one shape
             LaunchShape c{lpr, block};
             launch(c, s);
             CK(cudaEventRecord(e0, s));
@@ -1423,6 +1465,14 @@ struct Builder {
     bool autotune = false;
     cudaStream_t tune_stream() const { return stream; }
 
+    // The pipelined tile kernels are a tuner candidate for the sweep steps of
+    // levels above MERGE_MAX_N rows (measured slower than the lane-split row
+    // kernels at the 1.12 M-cell levels 0 and 1 with the fixed shapes: solve
+    // 20.2 ms against 18.1 ms, the P1 and G rows being 1.6-2.6 entries long).
+    static bool staged_ok(const Level& L, const DCSR& m, uint32_t rows) {
+        return L.N > MERGE_MAX_N && rows >= 4 * ST_ROWS && m.tile_max && m.tile_max <= ST_MAX_NNZ;
+    }
+
     void phase1(const Level& L, const T* src, T* w, T* out) {
         uint32_t R = L.N - L.Md, N = L.N;
         if (!R && N <= R) return;
@@ -1430,13 +1480,21 @@ struct Builder {
         const uint32_t* ja = L.P1.ja.p;
         const T* a = vals<T>(L.P1);
         const T* dv = dvals<T>(L);
+        bool st = staged_ok(L, L.P1, R);
+        uint32_t cap = st ? pipe_cap<T>(L.P1.tile_max) : 0;
+        size_t smem = st ? pipe_smem_bytes<T, false>(L.P1.tile_max) : 0;
         auto launch = [=](LaunchShape c, cudaStream_t s) {
+            if (c.lpr == 0) {
+                launch_k(k_phase1_staged<T>, pipe_grid(k_phase1_staged<T>, R, smem), ST_ROWS, smem, s, R, N, ia, ja,
+                         a, dv, src, w, out, cap);
+                return;
+            }
             uint32_t nb1 = R ? grid_for((size_t)R * c.lpr, c.block) : 0;
             uint32_t nb2 = N > R ? grid_for(N - R, c.block) : 0;
             LPR_SWITCH_B(c.lpr, k_phase1, nb1 + nb2, c.block, 0, s, R, N, nb1, ia, ja, a, dv, src, w, out);
         };
         LaunchShape c{pick_lpr(R, L.P1.nnz), 256};
-        if (autotune) c = tune_shape(1, sizeof(T), R, L.P1.nnz, tune_stream(), launch);
+        if (autotune) c = tune_shape(1, sizeof(T), R, L.P1.nnz, tune_stream(), launch, st);
         op([=](cudaStream_t s) { launch(c, s); });
         bytes += (uint64_t)L.P1.nnz * (4 + sizeof(T)) + 4ull * (R + 1) + sizeof(T) * (2ull * N + L.Md) ;
     }
@@ -1446,11 +1504,19 @@ struct Builder {
         const uint32_t* ia = L.G.ia.p;
         const uint32_t* ja = L.G.ja.p;
         const T* a = vals<T>(L.G);
+        bool st = staged_ok(L, L.G, M);
+        uint32_t cap = st ? pipe_cap<T>(L.G.tile_max) : 0;
+        size_t smem = st ? pipe_smem_bytes<T, false>(L.G.tile_max) : 0;
         auto launch = [=](LaunchShape c, cudaStream_t s) {
+            if (c.lpr == 0) {
+                launch_k(k_phase2_staged<T>, pipe_grid(k_phase2_staged<T>, M, smem), ST_ROWS, smem, s, M, ia, ja, a, w,
+                         out, cap);
+                return;
+            }
             LPR_SWITCH_B(c.lpr, k_phase2, grid_for((size_t)M * c.lpr, c.block), c.block, 0, s, M, ia, ja, a, w, out);
         };
         LaunchShape c{pick_lpr(M, L.G.nnz), 256};
-        if (autotune) c = tune_shape(2, sizeof(T), M, L.G.nnz, tune_stream(), launch);
+        if (autotune) c = tune_shape(2, sizeof(T), M, L.G.nnz, tune_stream(), launch, st);
         op([=](cudaStream_t s) { launch(c, s); });
         bytes += (uint64_t)L.G.nnz * (4 + sizeof(T)) + 4ull * (M + 1) + sizeof(T) * (M + L.n + M);
     }
@@ -1460,14 +1526,22 @@ struct Builder {
         const uint32_t* ja = L.Af.ja.p;
         const T* a = vals<T>(L.Af);
         int dr = do_r ? 1 : 0;
+        bool st = do_r && staged_ok(L, L.Af, N);
+        uint32_t cap = st ? pipe_cap<T>(L.Af.tile_max) : 0;
+        size_t smem = st ? pipe_smem_bytes<T, false>(L.Af.tile_max) : 0;
         auto launch = [=](LaunchShape c, cudaStream_t s) {
+            if (c.lpr == 0) {
+                launch_k(k_update_staged<T>, pipe_grid(k_update_staged<T>, N, smem), ST_ROWS, smem, s, N, ia, ja, a, u0,
+                         x, r, cap);
+                return;
+            }
             LPR_SWITCH_B(c.lpr, k_update, grid_for((size_t)N * c.lpr, c.block), c.block, 0, s, N, ia, ja, a, u0, x, r,
                          dr);
         };
         LaunchShape c{do_r ? pick_lpr(N, L.Af.nnz) : 1, 256};
         // the tuning runs x += u0 on scratch: every buffer of the plan is
         // rewritten before it is read in an apply
-        if (autotune && do_r) c = tune_shape(3, sizeof(T), N, L.Af.nnz, tune_stream(), launch);
+        if (autotune && do_r) c = tune_shape(3, sizeof(T), N, L.Af.nnz, tune_stream(), launch, st);
         op([=](cudaStream_t s) { launch(c, s); });
         bytes += sizeof(T) * 3ull * N + (do_r ? spmv_bytes(L.Af) : 0);
     }
@@ -2021,6 +2095,12 @@ static void pipe_prepare_all(uint32_t tile_max) {
     pipe_grid(k_spmv_staged<float, 0, false>, 0, u32);
     pipe_grid(k_spmv_staged<float, 1, false>, 0, u32);
     pipe_grid(k_pcg_spmv_dot_staged<false>, 0, u64);
+    pipe_grid(k_phase1_staged<double>, 0, u64);
+    pipe_grid(k_phase2_staged<double>, 0, u64);
+    pipe_grid(k_update_staged<double>, 0, u64);
+    pipe_grid(k_phase1_staged<float>, 0, u32);
+    pipe_grid(k_phase2_staged<float>, 0, u32);
+    pipe_grid(k_update_staged<float>, 0, u32);
 }
 
 // Launch of k_pcg_spmv_dot_staged; its grid never exceeds staged_grid(n), the
