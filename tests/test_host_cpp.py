@@ -107,3 +107,21 @@ def test_driver_runs_config_file(tmp_path):
     assert abs(it - it_o) <= 1
     log = open(tmp_path / "res" / "trace.log").read()
     assert "Number of iterations" in log and "Level 0:" in log
+
+
+@pytest.mark.gpu
+def test_driver_runs_uh_cheb(tmp_path):
+    """The driver's -p uh_cheb path (Prec(A, cfg) from the command line: sigma
+    3, Chebyshev degree 4) reaches the oracle's iteration count within 1."""
+    from oracle import oracle as O
+    _build()
+    (nx, ny, nz), (kx, ky, kz), perm, _ = _case(tmp_path, 20, 22, 8)
+    r = subprocess.run([DRIVER, "-p", "uh_cheb", "-s", "3", "-b", "4", "-x", str(nx), "-y", str(ny), "-z", str(nz),
+                        "--perm", perm, "--dirichlet", "--eps", "1e-8"],
+                       capture_output=True, text=True, timeout=300, cwd=str(tmp_path))
+    assert r.returncode == 0, r.stdout + r.stderr
+    it = int(re.search(r"Number of iterations : (\d+)", r.stdout).group(1))
+    A, b = O.assemble(nx, ny, nz, kx, ky, kz, c=1.0, dirichlet=True)
+    P = O.Prec(A, "cheb", sigma=(3.0,), ncheb=(4,), use_tails=True)
+    _, it_o, _, rc = O.pcg(A, b, P, eps=1e-8)
+    assert rc == 0 and abs(it - it_o) <= 1
