@@ -182,6 +182,10 @@ void pool_release(void* p) {
     P.pending[it->second.dev].push_back(p);
 }
 
+// Cached free bytes kept per device; above this the largest cached blocks are
+// given back with cudaFree (the caller has just synchronised the device).
+static constexpr size_t POOL_KEEP_BYTES = (size_t)16 << 30;
+
 void pool_recycle(int dev) {
     Pool& P = pool();
     std::lock_guard<std::mutex> lk(P.mu);
@@ -193,6 +197,15 @@ void pool_recycle(int dev) {
         P.live.erase(it);
     }
     pend.clear();
+    auto& fl = P.free_[dev];
+    size_t cached = 0;
+    for (auto& kv : fl) cached += kv.first;
+    while (cached > POOL_KEEP_BYTES && !fl.empty()) {
+        auto last = std::prev(fl.end());
+        cached -= last->first;
+        cudaFree(last->second);
+        fl.erase(last);
+    }
 }
 
 void pool_sync_recycle() {
