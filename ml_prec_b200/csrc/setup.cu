@@ -1019,11 +1019,15 @@ static void counting_sort(const std::vector<int>& lev, uint32_t nrows, std::vect
 
 
 // Explicit forms of the level's triangular solves (P1 and G, setup.cuh).
-static void build_explicit(Level& li, cudaStream_t s) {
+// Slot capacities start from the ones the previously built (coarser) level
+// needed (p1_cap, g_cap; updated on return): rows get longer towards the fine
+// levels, so this saves the attempts that would overflow. The rows computed do
+// not depend on the capacity.
+static void build_explicit(Level& li, cudaStream_t s, uint32_t& p1_cap, uint32_t& g_cap) {
     uint32_t M = li.M, R = li.N - li.Md;
     Tmp<int> flags(1);
     // P1
-    for (uint32_t cap = 16;; cap *= 2) {
+    for (uint32_t cap = std::max<uint32_t>(16, p1_cap);; cap *= 2) {
         if (cap > 65536) MLP_THROW(ERR_LIMIT, "explicit L solve row exceeds 65536 entries");
         Tmp<uint32_t> scol((size_t)R * cap + 1), slen(R + 1);
         Tmp<double> sval((size_t)R * cap + 1);
@@ -1045,12 +1049,13 @@ static void build_explicit(Level& li, cudaStream_t s) {
         if (R) k_slots_emit<<<grid_for(R, 128), 128, 0, s>>>(R, cap, scol.p, sval.p, li.P1.ia.p, li.P1.ja.p, li.P1.a.p);
         CK_LAUNCH();
         CK(cudaStreamSynchronize(s));
+        p1_cap = cap;
         break;
     }
     // G
     li.G.nrow = M; li.G.ncol = R; li.G.nnz = 0;
     if (!M) { li.G.ia.alloc(1); li.G.ia.zero(s); li.G.ja.alloc(1); li.G.a.alloc(1); return; }
-    for (uint32_t cap = 16;; cap *= 2) {
+    for (uint32_t cap = std::max<uint32_t>(16, g_cap);; cap *= 2) {
         if (cap > 65536) MLP_THROW(ERR_LIMIT, "explicit U solve row exceeds 65536 entries");
         Tmp<uint32_t> scol((size_t)M * cap + 1), slen(M + 1);
         Tmp<double> sval((size_t)M * cap + 1);
@@ -1070,12 +1075,14 @@ static void build_explicit(Level& li, cudaStream_t s) {
         k_slots_emit<<<grid_for(M, 128), 128, 0, s>>>(M, cap, scol.p, sval.p, li.G.ia.p, li.G.ja.p, li.G.a.p);
         CK_LAUNCH();
         CK(cudaStreamSynchronize(s));
+        g_cap = cap;
         break;
     }
 }
 
 // Builds the frame-order operators of every level, bottom-up.
 static void build_frames(Hierarchy& H, cudaStream_t s) {
+    uint32_t p1_cap = 16, g_cap = 16;
     for (int l = (int)H.nlevels - 1; l >= 0; l--) {
         Level& li = *H.lv[l];
         uint32_t N = li.N;
@@ -1204,7 +1211,7 @@ static void build_frames(Hierarchy& H, cudaStream_t s) {
         csr_tile_stats(li.Af, s);
         if (H.kind == PREC_CHEB && l > 0) csr_tile_stats(li.As, s);
         if (!li.direct) {
-            build_explicit(li, s);
+            build_explicit(li, s, p1_cap, g_cap);
             csr_tile_stats(li.P1, s);
             csr_tile_stats(li.G, s);
         }
