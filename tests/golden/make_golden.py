@@ -9,7 +9,7 @@ solve, and dumps the hierarchy. This script stores the inputs and those outputs
 as compressed .npz files. It needs the reference sources (REF below) and is run
 only when the fixtures are regenerated; the tests read the .npz files.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]   # all cases by default
 """
 from __future__ import annotations
 
@@ -37,6 +37,7 @@ CASES = {
     "ms_deg1_12x22x6": ("iid", 5, 12, 22, 6, 1.0, "msplit", {"degree_max": 1, "level_niter": "3 4"}),
     "ms_tiny_1x1x1": ("iid", 1, 1, 1, 1, 1.0, "msplit", {}),
     "ms_line_1x1x7": ("iid", 1, 1, 1, 7, 1.0, "msplit", {}),
+    "ms_none_12x22x6": ("iid", 1, 12, 22, 6, 1.0, "msplit", {"elim_order": "none", "max_levels": 3}),
     "ch_layered_16x22x8": ("layered", 2, 16, 22, 8, 1.0, "cheb", {"sigmas": [3.0], "niters": [4]}),
     "ch_iid_12x22x6": ("iid", 4, 12, 22, 6, 1.0, "cheb", {"sigmas": [3.0, 2.5], "niters": [2, 3]}),
 }
@@ -46,7 +47,10 @@ def main():
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={REF}"], check=True)
     with tempfile.TemporaryDirectory() as td:
         perms = {}
+        wanted = sys.argv[1:] or list(CASES)
         for name, (model, seed, nx, ny, nz, c, prec, opt) in CASES.items():
+            if name not in wanted:
+                continue
             key = (model, seed)
             if key not in perms:
                 kx, ky, kz = fields.field(model, seed)
@@ -63,6 +67,7 @@ def main():
                 cfg = os.path.join(od, "msplit.cfg")
                 with open(cfg, "w") as fh:
                     fh.write(O.msplit_cfg_text(level_niter=opt.get("level_niter", "5"),
+                                               elim_order=opt.get("elim_order", "simple_1"),
                                                degree_max=opt.get("degree_max", 2),
                                                max_levels=opt.get("max_levels", 15)))
                 kw["cfg"] = cfg

@@ -23,7 +23,8 @@ def prec_kwargs(g):
     o = g["options"]
     if g["prec"] == "msplit":
         return dict(kind="msplit", q=(0.8,), niter=tuple(int(t) for t in str(o.get("level_niter", "5")).split()),
-                    max_levels=o.get("max_levels", 15), degree_max=o.get("degree_max", 2), order="simple_1")
+                    max_levels=o.get("max_levels", 15), degree_max=o.get("degree_max", 2),
+                    order=o.get("elim_order", "simple_1"))
     return dict(kind="cheb", sigma=tuple(o["sigmas"]), ncheb=tuple(o["niters"]), use_tails=True)
 
 
