@@ -408,12 +408,15 @@ def main():
     if ws > 1:
         import torch
         import torch.distributed as dist
-        t = torch.tensor([t_step, ens["fwd_ms"] if ens else 0.0, ens["adj_ms"] if ens else 0.0],
-                         dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e = res.get("e2e")
+        t = torch.tensor([t_step, ens["fwd_ms"] if ens else 0.0, ens["adj_ms"] if ens else 0.0,
+                          e2e["value"] if e2e else 0.0], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)  # every timing is the slowest rank's
         t_step = float(t[0])
         if ens:
             ens["fwd_ms"], ens["adj_ms"] = float(t[1]), float(t[2])
+        if e2e:
+            e2e["value"] = float(t[3])
         dist.barrier()
         dist.destroy_process_group()
     if rank != 0:
