@@ -16,11 +16,16 @@ Rank 0 prints one JSON line. `value`: device-timed seconds per step of the
 FP64 path, max over ranks (every rank solves its own replica; no data-path
 collective; "weak" scaling). `e2e`: the same step through the C ABI with host
 buffers (matrix and right-hand side uploaded, solution downloaded), host-timed.
-`forms`: the FP32-stored hierarchy inside flexible FP64 PCG (time and accuracy
-against a tight FP64 solve), the adjoint gradient (time against one forward
-solve), and the 64-realization ensemble solved in one graph launch per rank
-(sharded over ranks). `roofline`: the level-0 staged CSR SpMV. `cpu_baseline`:
-the reference itself (oracle/_ref, single-threaded) on the same problem.
+`forms`: the FP64 step with launch shapes from the build-time autotuner, the
+FP32-stored hierarchy inside flexible FP64 PCG (time with fixed and tuned
+shapes, accuracy against a tight FP64 solve), the adjoint gradient (time
+against one forward solve), and the 64-realization ensemble solved in one
+graph launch per rank (sharded over ranks). `roofline`: the level-0 CSR SpMV
+(pipelined tile kernel), 50 graph-recorded launches over two alternating
+matrix copies, with the DRAM traffic of an ncu capture. `cpu_baseline`: the
+reference itself (oracle/_ref, single-threaded) on the same problem.
+`--no-forms` and `--no-cpu-baseline` leave out those extra measurements (the
+profiling runs use them); the timed steps are the same.
 """
 from __future__ import annotations
 
