@@ -192,18 +192,24 @@ int mlp_ensemble_solve(mlp_ensemble* E, const double* const* b_dev, double* cons
 int mlp_ensemble_destroy(mlp_ensemble* E);
 
 /* PCG that allocates no device memory. It has no counterpart in the
- * reference: it serves callers that cannot call cudaMalloc while they run
- * (code recording into a stream capture, hosts whose device memory belongs to
- * their own allocator). It computes exactly what mlp_pcg_device computes, but
- * the solver's vectors and reduction scratch live in one file-scope device
- * array of the library, sized for at most 131072 unknowns (about 5 MB, held by
- * every GPU that loads the library until the process exits); larger systems
- * are rejected with MLP_ERR_LIMIT. The matrix and the preconditioner must have
- * been created beforehand (those calls allocate). The first call on a device
- * looks up the array's device address; make that first call before any stream
- * capture. All calls share the one array: calls that overlap on the GPU (other
- * threads, other streams) race and must be serialised by the caller. t_solve_ms
- * is host wall time. */
+ * reference. It serves host applications that cannot let a library call
+ * cudaMalloc while they solve: their device memory is owned by their own
+ * allocator (a framework's caching allocator that has reserved the device, or
+ * a process held to a fixed device-memory budget), so an allocation from
+ * inside this library would fail or break the host's accounting. It computes
+ * exactly what mlp_pcg_device computes, but the solver's vectors, reduction
+ * scratch and start vector live in one file-scope device array of the
+ * library, sized for at most 131072 unknowns (about 6 MB, held by every GPU
+ * that loads the library until the process exits); larger systems are
+ * rejected with MLP_ERR_LIMIT. The matrix and the preconditioner must have
+ * been created beforehand (those calls allocate). Every call looks up the
+ * array's address on the current device; the first call on a device (unless
+ * an earlier call into the library on that device did it) loads the library's
+ * device code there, which is what places the array, so make that first call
+ * before any stream capture. All calls share the one array, which keeps the
+ * last call's contents: calls that overlap on the GPU (other threads, other
+ * streams) race and must be serialised by the caller. The call waits on the
+ * host for the device after every iteration. t_solve_ms is host wall time. */
 int mlp_pcg_device_noalloc(const mlp_matrix* A, const double* b_dev, mlp_prec* P, double* x_dev, double eps,
                            uint32_t maxit, int32_t flexible, mlp_stats* stats, void* stream);
 

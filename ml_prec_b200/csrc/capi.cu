@@ -1,5 +1,6 @@
 // extern "C" entry points (include/mlp_b200.h). Each one converts exceptions
 // into a status code plus a per-thread message.
+#include <cmath>
 #include <cstring>
 
 #include "../../include/mlp_b200.h"
@@ -81,8 +82,10 @@ int mlp_matrix_create(uint32_t n, const uint32_t* ia, const uint32_t* ja, const 
         if (ia[i + 1] <= ia[i]) MLP_THROW(ERR_ARG, "every row needs at least its diagonal (row " + std::to_string(i) + ")");
         if (ja[ia[i]] != i) MLP_THROW(ERR_ARG, "diagonal must come first in row " + std::to_string(i));
     }
-    for (uint32_t k = 0; k < nnz; k++)
+    for (uint32_t k = 0; k < nnz; k++) {
         if (ja[k] >= n) MLP_THROW(ERR_ARG, "column index out of range");
+        if (!std::isfinite(a[k])) MLP_THROW(ERR_NOT_FINITE, "non-finite matrix value at entry " + std::to_string(k));
+    }
     auto* M = new mlp_matrix();
     try {
         M->s = new_stream();
@@ -196,7 +199,11 @@ int mlp_prec_create(const mlp_matrix* A, const mlp_prec_cfg* c, mlp_prec** out) 
         cfg.max_levels = c->max_levels;
         cfg.degree_max = c->degree_max;
         cfg.order = c->order;
+        // the tail group of elim_order = original (the reference reads its flag
+        // uninitialised, multi_split_prec.h:17; here it is Config::use_tails)
+        cfg.use_tails = c->use_tails;
         if (cfg.max_levels == 0) MLP_THROW(ERR_CONFIG, "max_levels must be positive");
+        if (cfg.order < MLP_ORDER_NONE || cfg.order > MLP_ORDER_SIMPLE_1) MLP_THROW(ERR_CONFIG, "unknown elim_order");
     } else {
         if (!c->nsigma || !c->sigma) MLP_THROW(ERR_CONFIG, "sigma list is empty");
         if (!c->nncheb || !c->ncheb) MLP_THROW(ERR_CONFIG, "niters list is empty");
@@ -249,7 +256,7 @@ int mlp_prec_apply(mlp_prec* P, const double* f, double* x, void* stream) {
     if (!P || !f || !x) MLP_THROW(ERR_ARG, "null pointer");
     cudaStream_t s = stream ? (cudaStream_t)stream : P->s;
     apply_natural(P, f, x, s);
-    if (!stream) CK(cudaStreamSynchronize(s));
+    if (!stream) check_persist(*P->P, s);
     API_END
 }
 
@@ -262,7 +269,7 @@ int mlp_prec_apply_host(mlp_prec* P, const double* f, double* x) {
     CK(cudaMemcpyAsync(P->tmp_in.p, f, (size_t)n * 8, cudaMemcpyHostToDevice, P->s));
     apply_natural(P, P->tmp_in.p, P->tmp_out.p, P->s);
     CK(cudaMemcpyAsync(x, P->tmp_out.p, (size_t)n * 8, cudaMemcpyDeviceToHost, P->s));
-    CK(cudaStreamSynchronize(P->s));
+    check_persist(*P->P, P->s);
     API_END
 }
 

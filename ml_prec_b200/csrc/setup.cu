@@ -303,6 +303,67 @@ __global__ void k_bucket_none(uint32_t N, const int* __restrict__ nout, const in
     bucket[i] = (nin[i] == 0 && nout[i] == 0) ? 1 : 0;
 }
 
+// Buckets of order_original after its tail group (multi_split_mark.cc:120-151):
+// 0: group 2 (in <= 2 or out <= 2, index order), 1: still linked (index
+// order), 2: no links (reversed); marked tail nodes are skipped.
+__global__ void k_bucket_original(uint32_t N, const int* __restrict__ nout, const int* __restrict__ nin,
+                                  const uint8_t* __restrict__ marked, uint8_t* __restrict__ bucket) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    uint8_t b;
+    if (marked[i]) b = 255;
+    else if (nin[i] <= 2 || nout[i] <= 2) b = 0;
+    else b = (nin[i] == 0 && nout[i] == 0) ? 2 : 1;
+    bucket[i] = b;
+}
+
+// order_block (multi_split_mark.cc:193-252) on the 60x220x85 mesh: the inner
+// nodes of the 5x5x5 blocks (i, j, k not on a block face) that keep a link,
+// block after block (K, J, I) and inside a block in (k, j, i) order. Thread p
+// takes the p-th inner position of that order and flags whether it is taken;
+// a scan of the flags gives each taken node its place in map.
+constexpr uint32_t BLK_NX = 60, BLK_NY = 220, BLK_NZ = 85, BLK_B = 5;
+constexpr uint32_t BLK_IN = BLK_B - 2;  // inner nodes per block side
+constexpr uint32_t BLK_NI = BLK_NX / BLK_B, BLK_NJ = BLK_NY / BLK_B, BLK_NK = BLK_NZ / BLK_B;
+constexpr uint32_t BLK_POS = BLK_NI * BLK_NJ * BLK_NK * BLK_IN * BLK_IN * BLK_IN;
+static_assert(BLK_NX % BLK_B == 0 && BLK_NY % BLK_B == 0 && BLK_NZ % BLK_B == 0, "whole blocks");
+
+__device__ __forceinline__ uint32_t block_pos_node(uint32_t p) {
+    uint32_t t = p % BLK_IN;  // i - I - 1
+    uint32_t q = p / BLK_IN;
+    uint32_t u = q % BLK_IN;  // j - J - 1
+    q /= BLK_IN;
+    uint32_t v = q % BLK_IN;  // k - K - 1
+    q /= BLK_IN;
+    uint32_t I = q % BLK_NI;
+    q /= BLK_NI;
+    uint32_t J = q % BLK_NJ;
+    uint32_t K = q / BLK_NJ;
+    uint32_t i = I * BLK_B + 1 + t, j = J * BLK_B + 1 + u, k = K * BLK_B + 1 + v;
+    return (k * BLK_NY + j) * BLK_NX + i;
+}
+__global__ void k_block_flags(const int* __restrict__ nout, const int* __restrict__ nin, uint32_t* __restrict__ flag) {
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= BLK_POS) return;
+    uint32_t id = block_pos_node(p);
+    flag[p] = (nin[id] || nout[id]) ? 1u : 0u;
+}
+__global__ void k_block_place(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ pos,
+                              uint32_t* __restrict__ map, uint8_t* __restrict__ marked) {
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= BLK_POS || !flag[p]) return;
+    uint32_t id = block_pos_node(p);
+    map[pos[p]] = id;
+    marked[id] = 1;
+}
+// The remaining nodes of order_block: 0 linked (index order), 1 no links (reversed).
+__global__ void k_bucket_rest(uint32_t N, const int* __restrict__ nout, const int* __restrict__ nin,
+                              const uint8_t* __restrict__ marked, uint8_t* __restrict__ bucket) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    bucket[i] = marked[i] ? 255 : ((nin[i] == 0 && nout[i] == 0) ? 1 : 0);
+}
+
 // Remaining nodes after the uh_cheb tail group (cheb_mark.cc:177-189):
 // 0 = still linked (coarse, index order), 1 = no links (diagonal, reversed),
 // marked nodes are skipped.
@@ -859,6 +920,66 @@ static void sparse_lu_level(Level& li, Level& ln, const uint8_t* keep, const dou
     }
 }
 
+// The tail group of order_original (multi_split_mark.cc:41-113). Starting at
+// every node (index order) that keeps one outgoing and at most one incoming
+// link, the walk eliminates the node when its only links join it to the node
+// its outgoing link points to, removes those links and moves on to that node;
+// a node left with no links at the end of a walk is eliminated too. Each walk
+// changes the link counts that the next start test and the next walk read, so
+// the group is one ordered pass: it runs on the host (one pass over the level's
+// links, a few milliseconds at 1.12 M nodes, where one GPU thread would spend
+// an L2 round trip per step), on the link flags and counts of the marking
+// kernel, and returns the eliminated nodes in order. nin / nout are updated in
+// place as the reference updates them.
+static std::vector<uint32_t> original_tails(uint32_t N, const std::vector<uint32_t>& ia,
+                                            const std::vector<uint32_t>& ja, std::vector<uint8_t> keep,
+                                            std::vector<int>& nin, std::vector<int>& nout,
+                                            std::vector<uint8_t>& marked) {
+    std::vector<uint32_t> order;
+    auto find_col = [&](uint32_t row, uint32_t col) -> int64_t {
+        // column col among row's off-diagonal entries (sorted after the diagonal)
+        uint32_t lo = ia[row] + 1, hi = ia[row + 1];
+        while (lo < hi) {
+            uint32_t mid = (lo + hi) / 2;
+            if (ja[mid] < col) lo = mid + 1;
+            else hi = mid;
+        }
+        return (lo < ia[row + 1] && ja[lo] == col) ? (int64_t)lo : -1;
+    };
+    for (uint32_t i = 0; i < N; i++) {
+        if (!(nout[i] == 1 && nin[i] <= 1)) continue;
+        uint32_t i0 = i;
+        for (;;) {
+            if (nout[i0] != 1) break;
+            uint32_t j_ = ia[i0] + 1;
+            while (j_ < ia[i0 + 1] && !keep[j_]) j_++;
+            if (j_ == ia[i0 + 1])
+                MLP_THROW(ERR_INTERNAL, "Row " + std::to_string(i0) + ": remaining link was not found");
+            uint32_t i1 = ja[j_];
+            int64_t back = find_col(i1, i0);
+            bool aji = back >= 0 && keep[back];
+            if (!(nin[i0] == 0 || (nin[i0] == 1 && aji))) break;
+            order.push_back(i0);
+            marked[i0] = 1;
+            keep[j_] = 0;
+            if (aji) {
+                keep[back] = 0;
+                nin[i0]--;
+                nout[i1]--;
+            }
+            nout[i0] = -1;
+            nin[i1]--;
+            i0 = i1;
+        }
+        if (nout[i0] == 0 && nin[i0] == 0) {
+            order.push_back(i0);
+            marked[i0] = 1;
+            nout[i0] = -1;
+        }
+    }
+    return order;
+}
+
 static void build_level_msplit(Hierarchy& H, const BuildCfg& cfg, uint32_t level, Scratch& S, cudaStream_t s) {
     Level& li = *H.lv[level];
     const DCSR& A = li.A;
@@ -897,8 +1018,50 @@ static void build_level_msplit(Hierarchy& H, const BuildCfg& cfg, uint32_t level
         std::vector<uint32_t> cnt = stable_partition(N, S.bucket.p, 2, 2u, li.map.p, 0, s);
         li.M = 0;
         li.Md = cnt[1];
+    } else if (cfg.order == ORDER_ORIGINAL) {
+        // order_original (multi_split_mark.cc:27-154): tails (host pass), then
+        // group 2 and the remaining nodes on the device
+        S.marked.alloc(N);
+        uint32_t ntail = 0;
+        if (cfg.use_tails) {
+            std::vector<uint32_t> ia = A.ia.download(s, (size_t)N + 1), ja = A.ja.download(s, A.nnz);
+            std::vector<uint8_t> keep = S.keep.download(s, A.nnz);
+            std::vector<int> nin = S.nin.download(s, N), nout = S.nout.download(s, N);
+            std::vector<uint8_t> marked(N, 0);
+            std::vector<uint32_t> tails = original_tails(N, ia, ja, std::move(keep), nin, nout, marked);
+            ntail = (uint32_t)tails.size();
+            if (ntail) CK(cudaMemcpyAsync(li.map.p, tails.data(), (size_t)ntail * 4, cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(S.marked.p, marked.data(), N, cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(S.nin.p, nin.data(), (size_t)N * 4, cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(S.nout.p, nout.data(), (size_t)N * 4, cudaMemcpyHostToDevice, s));
+            CK(cudaStreamSynchronize(s));  // the host vectors go out of scope
+        } else {
+            S.marked.zero(s);
+        }
+        k_bucket_original<<<grid_for(N, 256), 256, 0, s>>>(N, S.nout.p, S.nin.p, S.marked.p, S.bucket.p);
+        CK_LAUNCH();
+        std::vector<uint32_t> cnt = stable_partition(N, S.bucket.p, 3, 4u, li.map.p, ntail, s);
+        li.M = ntail + cnt[0];
+        li.Md = cnt[2];
+    } else if (cfg.order == ORDER_BLOCK) {
+        // order_block (multi_split_mark.cc:193-252): only the 60x220x85 mesh
+        if (N != BLK_NX * BLK_NY * BLK_NZ)
+            MLP_THROW(ERR_CONFIG, "Wrong mesh size: " + std::to_string(N) + " (expected 1122000)");
+        S.marked.alloc(N);
+        S.marked.zero(s);
+        Tmp<uint32_t> flag(BLK_POS), pos((size_t)BLK_POS + 1);
+        k_block_flags<<<grid_for(BLK_POS, 256), 256, 0, s>>>(S.nout.p, S.nin.p, flag.p);
+        CK_LAUNCH();
+        uint32_t nb = exclusive_scan_u32(flag.p, pos.p, BLK_POS, s);
+        k_block_place<<<grid_for(BLK_POS, 256), 256, 0, s>>>(flag.p, pos.p, li.map.p, S.marked.p);
+        CK_LAUNCH();
+        k_bucket_rest<<<grid_for(N, 256), 256, 0, s>>>(N, S.nout.p, S.nin.p, S.marked.p, S.bucket.p);
+        CK_LAUNCH();
+        std::vector<uint32_t> cnt = stable_partition(N, S.bucket.p, 2, 2u, li.map.p, nb, s);
+        li.M = nb;
+        li.Md = cnt[1];
     } else {
-        MLP_THROW(ERR_CONFIG, "elim_order must be simple_1 or none");
+        MLP_THROW(ERR_CONFIG, "unknown elim_order");
     }
     S.rmap.alloc(N);
     k_rmap<<<grid_for(N, 256), 256, 0, s>>>(N, li.map.p, S.rmap.p);

@@ -12,8 +12,7 @@
 #include <map>
 #include <mutex>
 
-#include <cooperative_groups.h>
-
+#include "persist.cuh"
 #include "small.cuh"
 #include "solve.cuh"
 
@@ -213,17 +212,6 @@ __global__ void __launch_bounds__(ST_ROWS) k_spmv_staged(uint32_t n, const uint3
     spmv_pipe<T, SA>(n, ia, ja, a, x, cap, [&](uint32_t row, T acc) { y[row] = MODE ? f[row] - acc : acc; });
 }
 
-// Whether the staged kernels copy the values into shared memory too
-// (MLP_PIPE_A=1) or read them from global memory (default).
-static bool pipe_stage_values() {
-    static int on = -1;
-    if (on < 0) {
-        const char* e = getenv("MLP_PIPE_A");
-        on = (e && e[0] == '1') ? 1 : 0;
-    }
-    return on == 1;
-}
-
 __global__ void k_tile_max(uint32_t n, const uint32_t* __restrict__ ia, uint32_t* __restrict__ out) {
     uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t r0 = t * ST_ROWS;
@@ -285,19 +273,11 @@ static void launch_spmv(uint32_t n, uint32_t nnz, const uint32_t* ia, const uint
     if (!n) return;
     if (tile_max && tile_max <= ST_MAX_NNZ && n >= 4 * ST_ROWS) {
         uint32_t cap = pipe_cap<T>(tile_max);
-        if (pipe_stage_values()) {
-            size_t smem = pipe_smem_bytes<T, true>(tile_max);
-            if (f) launch_k(k_spmv_staged<T, 1, true>, pipe_grid(k_spmv_staged<T, 1, true>, n, smem), ST_ROWS, smem, s,
-                            n, ia, ja, a, x, y, f, cap);
-            else launch_k(k_spmv_staged<T, 0, true>, pipe_grid(k_spmv_staged<T, 0, true>, n, smem), ST_ROWS, smem, s,
-                          n, ia, ja, a, x, y, f, cap);
-        } else {
-            size_t smem = pipe_smem_bytes<T, false>(tile_max);
-            if (f) launch_k(k_spmv_staged<T, 1, false>, pipe_grid(k_spmv_staged<T, 1, false>, n, smem), ST_ROWS, smem,
-                            s, n, ia, ja, a, x, y, f, cap);
-            else launch_k(k_spmv_staged<T, 0, false>, pipe_grid(k_spmv_staged<T, 0, false>, n, smem), ST_ROWS, smem,
-                          s, n, ia, ja, a, x, y, f, cap);
-        }
+        size_t smem = pipe_smem_bytes<T, false>(tile_max);
+        if (f) launch_k(k_spmv_staged<T, 1, false>, pipe_grid(k_spmv_staged<T, 1, false>, n, smem), ST_ROWS, smem, s, n,
+                        ia, ja, a, x, y, f, cap);
+        else launch_k(k_spmv_staged<T, 0, false>, pipe_grid(k_spmv_staged<T, 0, false>, n, smem), ST_ROWS, smem, s, n,
+                      ia, ja, a, x, y, f, cap);
         return;
     }
     double avg = (double)nnz / n;
@@ -451,7 +431,7 @@ __global__ void k_cheb2(uint32_t n, T* __restrict__ x2, const T* __restrict__ u1
     pdl_wait();
     pdl_trigger();
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) x2[i] = x2[i] * malpha + c * u1[i];
+    if (i < n) x2[i] = fmadd(x2[i], malpha, c * u1[i]);
 }
 // Chebyshev step k >= 3 (cheb_solve.cc:98-99): x2 = u1 - alpha*x2 + beta*(u1-u0)
 template <class T>
@@ -460,7 +440,10 @@ __global__ void k_chebk(uint32_t n, T* __restrict__ x2, const T* __restrict__ u1
     pdl_wait();
     pdl_trigger();
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) x2[i] = u1[i] - alpha * x2[i] + beta * (u1[i] - u0[i]);
+    if (i < n) {
+        T a1 = u1[i];
+        x2[i] = fmadd(beta, a1 - u0[i], fmadd(-alpha, x2[i], a1));
+    }
 }
 
 // Dense coarsest level: x = C^{-1} f, one warp per row.
@@ -664,394 +647,6 @@ __global__ void __launch_bounds__(512) k_update(uint32_t n, const uint32_t* __re
     }
 }
 
-// ---- fused level solve (one cluster) ------------------------------------------
-// A whole MultiSplitPrec::solve(l, f, x) call of a mid-size level whose coarse
-// sub-hierarchy is tabulated as one dense operator: all niter sweeps (phase 1,
-// the dense coarse product, phase 2, the residual / correction step) in ONE
-// launch of one 16-CTA thread-block cluster, with a cluster barrier between
-// the steps instead of a kernel boundary.
-//
-// * The level's vectors (f, x, w, r, u0) live in the cluster's distributed
-//   shared memory: CTA o owns entries [o*chv, (o+1)*chv) of each, and any CTA
-//   reads or writes them through the owner's shared-memory window (DSMEM), so
-//   no step waits on a global-memory round trip. f is loaded at the start, x
-//   written back at the end.
-// * CTA c takes the same balanced slice of rows in every step (P1 rows,
-//   diagonal rows, dense-operator rows, G rows, level-matrix rows) and copies
-//   those matrix rows into its own shared memory once, with cp.async; the
-//   dense operator's rows are read from L2.
-// Rows are summed serially in column order (the separate kernels may split a
-// row over several lanes, so the two paths agree to rounding, not bit for bit).
-template <class T>
-struct MidArgs {
-    uint32_t N, M, R, n, niter;
-    uint32_t trace;  // MLP_MID_TRACE=1: CTA 0 prints the time of every step (diagnostics)
-    const uint32_t *p1_ia, *p1_ja, *g_ia, *g_ja, *af_ia, *af_ja;
-    const T *p1_a, *g_a, *af_a, *dval, *C;
-    const T* f;
-    T* x;
-};
-
-__device__ __forceinline__ uint64_t gtimer() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ void cluster_barrier() {
-    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
-
-template <class T>
-__device__ __forceinline__ T ldcg(const T* p) { return __ldcg(p); }
-
-// Rows [c * ceil(rows / cs), ...) of CTA c.
-__host__ __device__ __forceinline__ void mid_slice(uint32_t rows, uint32_t cs, uint32_t c, uint32_t& r0,
-                                                    uint32_t& r1) {
-    uint32_t ch = (rows + cs - 1) / cs;
-    r0 = min(rows, c * ch);
-    r1 = min(rows, r0 + ch);
-}
-
-// Entries per CTA of each distributed vector (a multiple of 4, so every
-// owner's slice starts on a 16-byte boundary).
-__host__ __device__ __forceinline__ uint32_t mid_chunk(uint32_t N, uint32_t cs) {
-    return ((N + cs - 1) / cs + 3) & ~3u;
-}
-
-// Rows of CTA c in the three row steps: P1 (k = 0) and G (k = 1) rows in equal
-// slices; level-matrix rows (k = 2) by vector ownership, so that the
-// correction step updates x and r in the CTA's own shared memory.
-__host__ __device__ __forceinline__ void mid_rows(int k, uint32_t R, uint32_t M, uint32_t N, uint32_t cs, uint32_t c,
-                                                   uint32_t& r0, uint32_t& r1) {
-    if (k == 0) { mid_slice(R, cs, c, r0, r1); return; }
-    if (k == 1) { mid_slice(M, cs, c, r0, r1); return; }
-    uint32_t ch = mid_chunk(N, cs);
-    r0 = min(N, c * ch);
-    r1 = min(N, r0 + ch);
-}
-
-// Shared-memory layout of one CTA: the five vector slices (chv entries each:
-// f, x, w, r, u0), the staged coarse slice of w, then the matrix rows. Every
-// matrix array is copied from the 16-byte boundary at or below its first
-// element, so each region holds a few leading elements before the slice and
-// is indexed with that offset.
-struct MidLayout {
-    uint32_t r0[3], nr[3], e0[3], nnz[3];  // P1, G, level matrix
-    uint32_t c0, nc, d0, nd;                 // dense rows, diagonal rows
-    uint32_t chv;
-    size_t off_v, off_w, off_a[3], off_d;   // in units of T
-    size_t off_ia[3], off_ja[3];            // in units of uint32_t
-    size_t bytes;
-};
-
-template <class T>
-__host__ __device__ inline void mid_layout(MidLayout& L, uint32_t cs, uint32_t c, uint32_t R, uint32_t M, uint32_t N,
-                                           uint32_t n, const uint32_t* e_start, const uint32_t* e_end) {
-    constexpr size_t VT = 16 / sizeof(T);
-    auto pad_t = [](size_t cnt) { return (cnt + 2 * VT + VT - 1) / VT * VT; };
-    auto pad_u = [](size_t cnt) { return (cnt + 8 + 3) / 4 * 4; };
-    for (int k = 0; k < 3; k++) {
-        uint32_t a, b;
-        mid_rows(k, R, M, N, cs, c, a, b);
-        L.r0[k] = a;
-        L.nr[k] = b - a;
-        L.e0[k] = e_start[k];
-        L.nnz[k] = e_end[k] - e_start[k];
-    }
-    uint32_t a, b;
-    mid_slice(n, cs, c, a, b);
-    L.c0 = a; L.nc = b - a;
-    L.chv = mid_chunk(N, cs);
-    // diagonal rows [R, N): the ones this CTA owns
-    a = max(R, min(N, c * L.chv));
-    b = max(a, min(N, (c + 1) * L.chv));
-    L.d0 = a - R; L.nd = b - a;
-    size_t o = 0;
-    L.off_v = o; o += 5 * (size_t)L.chv;  // chv is a multiple of 4: each slice 16-byte aligned
-    L.off_w = o; o += pad_t(n);
-    for (int k = 0; k < 3; k++) { L.off_a[k] = o; o += pad_t(L.nnz[k]); }
-    L.off_d = o; o += pad_t(L.nd);
-    size_t u = o * sizeof(T) / 4;
-    for (int k = 0; k < 3; k++) {
-        L.off_ia[k] = u; u += pad_u(L.nr[k] + 1);
-        L.off_ja[k] = u; u += pad_u(L.nnz[k]);
-    }
-    L.bytes = u * 4;
-}
-
-// Starts the copy of src[i0, i1) into the 16-byte aligned region dst with
-// cp.async, from the 16-byte boundary at or below src + i0; returns the index
-// shift (element i lands at dst[i - shift]). The last vector may read up to 15
-// bytes past src + i1 (device buffers carry 16 bytes of slack). Completion:
-// cp_async_wait_all() then a barrier.
-template <class E>
-__device__ __forceinline__ size_t copy_async(E* dst, const E* src, size_t i0, size_t i1) {
-    constexpr size_t V = 16 / sizeof(E);
-    size_t b = i0 & ~(V - 1);
-    if (i1 <= i0) return b;
-    size_t nv = (i1 - b + V - 1) / V;
-    const char* s = reinterpret_cast<const char*>(src + b);
-    uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
-    for (size_t v = threadIdx.x; v < nv; v += blockDim.x)
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d + (uint32_t)(v * 16)), "l"(s + v * 16)
-                     : "memory");
-    return b;
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
-// Distributed vector: entry i lives in CTA i / chv at local index i % chv of
-// the same region; owner() divides with a precomputed reciprocal (exact for
-// i < 2^17 and chv < 2^14).
-template <class T>
-struct DVec {
-    T* local;       // this CTA's slice (same offset in every CTA)
-    uint32_t chv, inv, rank;
-    __device__ __forceinline__ T* at(uint32_t i) const {
-        uint32_t o = __umulhi(i, inv);
-        T* p = local + (i - o * chv);
-        if (o == rank) return p;  // own slice: plain shared-memory access
-        return cooperative_groups::this_cluster().map_shared_rank(p, o);
-    }
-    __device__ __forceinline__ T ld(uint32_t i) const { return *at(i); }
-    __device__ __forceinline__ void st(uint32_t i, T v) const { *at(i) = v; }
-};
-
-// One thread per row; a thread takes MID_U rows at once and first issues the
-// vector gathers of the first MID_K entries of each, so up to MID_U * MID_K
-// gathers are in flight together; the products are then added in row order
-// (the order of a serial loop over the row).
-constexpr int MID_U = 2, MID_K = 4, MID_CV = 16;
-
-template <class T, class Val, class Store>
-__device__ __forceinline__ void smem_rows(uint32_t nrows, const uint32_t* ia, const uint32_t* ja, size_t bj,
-                                          const T* a, size_t ba, Val val, Store store) {
-    for (uint32_t base = 0; base < nrows; base += blockDim.x * MID_U) {
-        T av[MID_U][MID_K], xv[MID_U][MID_K];
-        uint32_t jb[MID_U], je[MID_U];
-#pragma unroll
-        for (int u = 0; u < MID_U; u++) {
-            uint32_t row = base + u * blockDim.x + threadIdx.x;
-            jb[u] = je[u] = 0;
-            if (row < nrows) {
-                jb[u] = ia[row];
-                je[u] = ia[row + 1];
-            }
-#pragma unroll
-            for (int k = 0; k < MID_K; k++) {
-                uint32_t j = jb[u] + k;
-                av[u][k] = 0;
-                xv[u][k] = 0;
-                if (j < je[u]) {
-                    av[u][k] = a[j - ba];
-                    xv[u][k] = val(ja[j - bj]);
-                }
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < MID_U; u++) {
-            uint32_t row = base + u * blockDim.x + threadIdx.x;
-            if (row >= nrows) continue;
-            T s = 0;
-#pragma unroll
-            for (int k = 0; k < MID_K; k++)
-                if (jb[u] + k < je[u]) s += av[u][k] * xv[u][k];
-            for (uint32_t j = jb[u] + MID_K; j < je[u]; j++) s += a[j - ba] * val(ja[j - bj]);
-            store(row, s);
-        }
-    }
-}
-
-template <class T>
-__global__ void __launch_bounds__(1024) k_mid_level(MidArgs<T> A) {
-    extern __shared__ __align__(16) unsigned char mid_smem[];
-    const uint32_t c = blockIdx.x, cs = gridDim.x;
-    const uint32_t N = A.N, M = A.M, R = A.R, n = A.n;
-    const bool tr = A.trace && c == 0 && threadIdx.x == 0;
-    uint64_t ts[28];
-    int nts = 0;
-    if (tr) ts[nts++] = gtimer();
-    const uint32_t* gia[3] = {A.p1_ia, A.g_ia, A.af_ia};
-    const uint32_t* gja[3] = {A.p1_ja, A.g_ja, A.af_ja};
-    const T* ga[3] = {A.p1_a, A.g_a, A.af_a};
-    uint32_t es[3], ee[3];
-    for (int k = 0; k < 3; k++) {
-        uint32_t a, b;
-        mid_rows(k, R, M, N, cs, c, a, b);
-        es[k] = gia[k][a];
-        ee[k] = gia[k][b];
-    }
-    MidLayout L;
-    mid_layout<T>(L, cs, c, R, M, N, n, es, ee);
-    T* sv = reinterpret_cast<T*>(mid_smem);
-    uint32_t* su = reinterpret_cast<uint32_t*>(mid_smem);
-    const uint32_t chv = L.chv;
-    const uint32_t inv = (uint32_t)((0x100000000ull + chv - 1) / chv);
-    DVec<T> vf{sv + L.off_v, chv, inv, c}, vx{sv + L.off_v + chv, chv, inv, c},
-        vw{sv + L.off_v + 2 * chv, chv, inv, c}, vr{sv + L.off_v + 3 * chv, chv, inv, c},
-        vu{sv + L.off_v + 4 * chv, chv, inv, c};
-    // copy this CTA's matrix rows and its slice of f into shared memory
-    const uint32_t* ia_s[3];
-    const uint32_t* ja_s[3];
-    const T* a_s[3];
-    size_t bj[3], ba[3];
-    for (int k = 0; k < 3; k++) {
-        ba[k] = copy_async(sv + L.off_a[k], ga[k], L.e0[k], L.e0[k] + L.nnz[k]);
-        bj[k] = copy_async(su + L.off_ja[k], gja[k], L.e0[k], L.e0[k] + L.nnz[k]);
-        size_t bi = copy_async(su + L.off_ia[k], gia[k], L.r0[k], L.r0[k] + L.nr[k] + 1);
-        ia_s[k] = su + L.off_ia[k] + (L.r0[k] - bi);  // ia_s[k][row] = ia[r0 + row]
-        ja_s[k] = su + L.off_ja[k];
-        a_s[k] = sv + L.off_a[k];
-    }
-    size_t bd = copy_async(sv + L.off_d, A.dval, L.d0, L.d0 + L.nd);
-    const uint32_t v0 = min(N, c * chv), v1 = min(N, v0 + chv);
-    // f (a slice of the caller's vector, not necessarily 16-byte aligned): plain loads
-#pragma unroll 2
-    for (uint32_t i = v0 + threadIdx.x; i < v1; i += blockDim.x) vf.local[i - v0] = ldcg(A.f + i);
-    cp_async_wait_all();
-    __syncthreads();
-    cluster_barrier();  // every slice of f is in place before anyone reads it
-    if (tr) ts[nts++] = gtimer();
-    const T* dv = sv + L.off_d + (L.d0 - bd);  // dv[i] = dval[d0 + i]
-    T* wc = sv + L.off_w;
-    const uint32_t p0 = L.r0[0], g0 = L.r0[1], f0 = L.r0[2];
-    for (uint32_t it = 1; it <= A.niter; it++) {
-        const DVec<T>& src = it == 1 ? vf : vr;
-        const DVec<T>& out = it == 1 ? vx : vu;
-        // phase 1: w = P1 src (rows < R); out = dval * src (rows >= R)
-        smem_rows<T>(L.nr[0], ia_s[0], ja_s[0], bj[0], a_s[0], ba[0], [&](uint32_t col) { return src.ld(col); },
-                     [&](uint32_t row, T v) { vw.st(p0 + row, v); });
-#pragma unroll 4
-        for (uint32_t i = threadIdx.x; i < L.nd; i += blockDim.x) {
-            uint32_t q = R + L.d0 + i;
-            out.st(q, dv[i] * src.ld(q));
-        }
-        cluster_barrier();
-        if (tr && nts < 27) ts[nts++] = gtimer();
-        // coarse slice: out[M + i] = sum_j C_ij w[M + j], one warp per row;
-        // w's coarse slice is staged in shared memory first
-        for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) wc[j] = vw.ld(M + j);
-        __syncthreads();
-        {
-            const uint32_t warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-            const int lane = threadIdx.x & 31;
-            for (uint32_t i = warp; i < L.nc; i += nwarp) {
-                const T* crow = A.C + (size_t)(L.c0 + i) * n;
-                T s = 0;
-                T cv[MID_CV];  // the lane's first MID_CV entries of the row, all loads in flight at once
-#pragma unroll
-                for (int k = 0; k < MID_CV; k++) {
-                    uint32_t j = lane + 32 * k;
-                    cv[k] = j < n ? __ldg(crow + j) : T(0);
-                }
-#pragma unroll
-                for (int k = 0; k < MID_CV; k++) {
-                    uint32_t j = lane + 32 * k;
-                    if (j < n) s += cv[k] * wc[j];
-                }
-                for (uint32_t j = lane + 32 * MID_CV; j < n; j += 32) s += __ldg(crow + j) * wc[j];
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-                if (lane == 0) out.st(M + L.c0 + i, s);
-            }
-        }
-        cluster_barrier();
-        if (tr && nts < 27) ts[nts++] = gtimer();
-        // phase 2: out_q = sum_j G_qj (j < M ? w_j : out_j), q < M
-        smem_rows<T>(L.nr[1], ia_s[1], ja_s[1], bj[1], a_s[1], ba[1],
-                     [&](uint32_t col) { return col < M ? vw.ld(col) : out.ld(col); },
-                     [&](uint32_t row, T v) { out.st(g0 + row, v); });
-        if (A.niter < 2) break;
-        cluster_barrier();
-        if (tr && nts < 27) ts[nts++] = gtimer();
-        if (it == 1) {
-            // r = f - A x
-            smem_rows<T>(L.nr[2], ia_s[2], ja_s[2], bj[2], a_s[2], ba[2], [&](uint32_t col) { return vx.ld(col); },
-                         [&](uint32_t row, T v) { vr.st(f0 + row, vf.ld(f0 + row) - v); });
-        } else if (it < A.niter) {
-            // x += u0; r -= A u0
-            smem_rows<T>(L.nr[2], ia_s[2], ja_s[2], bj[2], a_s[2], ba[2], [&](uint32_t col) { return vu.ld(col); },
-                         [&](uint32_t row, T v) {
-                             uint32_t q = f0 + row;
-                             vx.st(q, vx.ld(q) + vu.ld(q));
-                             vr.st(q, vr.ld(q) - v);
-                         });
-        } else {
-#pragma unroll 4
-            for (uint32_t i = threadIdx.x; i < L.nr[2]; i += blockDim.x) {
-                uint32_t q = f0 + i;
-                vx.st(q, vx.ld(q) + vu.ld(q));
-            }
-        }
-        if (it < A.niter) {
-            cluster_barrier();
-            if (tr && nts < 27) ts[nts++] = gtimer();
-        }
-    }
-    cluster_barrier();  // every update of x is done before the owners write it out
-    for (uint32_t i = v0 + threadIdx.x; i < v1; i += blockDim.x) A.x[i] = vx.local[i - v0];
-    if (tr) {
-        ts[nts++] = gtimer();
-        printf("[k_mid_level] N=%u steps=%d total %.2f us: copy-in %.2f", N, nts, (ts[nts - 1] - ts[0]) * 1e-3,
-               (ts[1] - ts[0]) * 1e-3);
-        for (int k = 2; k < nts; k++) printf(" %.2f", (ts[k] - ts[k - 1]) * 1e-3);
-        printf("\n");
-    }
-}
-
-// Whether the fused level kernel can run as a 16-CTA cluster with this much
-// shared memory. The path is opt-in (MLP_MID=1): measured on B200 at 26,907
-// rows, one fused call (20 dependent steps) took 84 us against 55 us for the
-// same steps as separate graph-launched kernels with programmatic dependent
-// launch, because each step still waits on scattered gathers that one
-// cluster serves more slowly than the whole GPU.
-template <class T>
-static bool mid_cluster_ok(int cs, size_t smem) {
-    const char* e = getenv("MLP_MID");
-    if (!(e && e[0] == '1')) return false;
-    static int attr_set = 0;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_mid_level<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-        cudaFuncSetAttribute(k_mid_level<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)small_smem_limit());
-        cudaGetLastError();
-        attr_set = 1;
-    }
-    if (smem > small_smem_limit()) return false;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(cs);
-    cfg.blockDim = dim3(1024);
-    cfg.dynamicSmemBytes = smem;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = cs;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    int nc = 0;
-    bool ok = cudaOccupancyMaxActiveClusters(&nc, k_mid_level<T>, &cfg) == cudaSuccess && nc > 0;
-    cudaGetLastError();
-    return ok;
-}
-
-template <class T>
-static void launch_mid(const MidArgs<T>& a, int cs, size_t smem, cudaStream_t s) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(cs);
-    cfg.blockDim = dim3(1024);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = cs;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, k_mid_level<T>, a);
-}
-
 // ---- merged sweep steps --------------------------------------------------------
 // At a small level every kernel boundary costs more than the kernel's work, so
 // consecutive steps of the sweep are merged where the data allows, and each
@@ -1194,75 +789,16 @@ __global__ void __launch_bounds__(256) k_merge_a(uint32_t N, uint32_t R, uint32_
     }
 }
 
-// Step B with the coarse slice tabulated (C, n x n): warps [0, n) compute
-// u0_C = C w_C as k_dense_gemv does; warps [n, n + M) compute the E rows
-// u0_q = sum_j G_qj y_j (LPG-lane split), y_j = w_j (j < M) or the coarse
-// entry recomputed by the whole warp exactly as k_dense_gemv computes it.
-template <class T, int LPG>
-__global__ void __launch_bounds__(256) k_merge_b(uint32_t M, uint32_t n, const uint32_t* __restrict__ g_ia,
-                                                 const uint32_t* __restrict__ g_ja, const T* __restrict__ g_a,
-                                                 const T* __restrict__ C, const T* __restrict__ w, T* __restrict__ out) {
-    constexpr int CV = 16;
-    uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
-    const T* wc = w + M;
-    // the dense row of a coarse warp is constant: loaded before the wait
-    bool coarse = warp < n;
-    const T* crow = C + (size_t)(coarse ? warp : 0) * n;
-    T cv[CV];
-#pragma unroll
-    for (int k = 0; k < CV; k++) {
-        uint32_t j = lane + 32 * k;
-        cv[k] = (coarse && j < n) ? crow[j] : T(0);
-    }
-    pdl_wait();
-    pdl_trigger();
-    auto dense_dot = [&](const T* c, const T* pre) {
-        T s = 0;
-#pragma unroll
-        for (int k = 0; k < CV; k++) {
-            uint32_t j = lane + 32 * k;
-            if (j < n) s = fmadd(pre ? pre[k] : c[j], wc[j], s);
-        }
-        for (uint32_t j = lane + 32 * CV; j < n; j += 32) s = fmadd(c[j], wc[j], s);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        return s;
-    };
-    if (coarse) {
-        T s = dense_dot(crow, cv);
-        if (lane == 0) out[M + warp] = s;
-        return;
-    }
-    uint32_t q = warp - n;
-    if (q >= M) return;
-    uint32_t jb = g_ia[q], je = g_ia[q + 1];
-    T p[LPG];
-#pragma unroll
-    for (int l = 0; l < LPG; l++) p[l] = 0;
-    for (uint32_t j = jb; j < je; j++) {
-        uint32_t col = g_ja[j];
-        T y = col < M ? w[col] : dense_dot(C + (size_t)(col - M) * n, nullptr);
-        T g = g_a[j];
-        int l = (int)((j - jb) & (LPG - 1));
-#pragma unroll
-        for (int m = 0; m < LPG; m++)
-            if (m == l) p[m] = fmadd(g, y, p[m]);
-    }
-#pragma unroll
-    for (int o = LPG / 2; o > 0; o >>= 1) {
-        T t[LPG];
-#pragma unroll
-        for (int l = 0; l < LPG; l++) t[l] = p[l] + p[l ^ o];
-#pragma unroll
-        for (int l = 0; l < LPG; l++) p[l] = t[l];
-    }
-    if (lane == 0) out[q] = p[0];
-}
-
 static int pick_lpr(uint32_t n, uint32_t nnz) {
     double avg = n ? (double)nnz / n : 1;
     return avg <= 1.5 ? 1 : avg <= 3 ? 2 : avg <= 6 ? 4 : avg <= 12 ? 8 : avg <= 24 ? 16 : 32;
+}
+
+// Lanes per row of the SpMV launch_spmv picks (the staged tile kernel sums a
+// row serially, as one lane does).
+static uint32_t spmv_lpr(uint32_t n, uint32_t nnz, uint32_t tile_max) {
+    if (tile_max && tile_max <= ST_MAX_NNZ && n >= 4 * ST_ROWS) return 1;
+    return (uint32_t)pick_lpr(n, nnz);
 }
 
 #define LPR_SWITCH(lpr, KERNEL, ...)                                      \
@@ -1380,18 +916,82 @@ struct Builder {
     const SmallPlan<T>* small = nullptr;
     uint64_t bytes = 0;
 
+    // ---- persistent recording -------------------------------------------
+    // While ps is set, the step functions append descriptors for k_persist
+    // instead of recording launches; persist_region() wraps a whole level
+    // call (and everything below it) into one launch.
+    std::vector<PStep<T>>* ps = nullptr;
+    std::vector<DBuf<uint8_t>>* pdesc = nullptr;  // owner of the descriptor arrays
+    PBar* pbar = nullptr;
+    bool persist = false;                         // persistent regions allowed
+    uint32_t persist_max_n = 0;                   // largest level that starts a region
+    uint32_t persist_regions = 0, persist_steps = 0;
+
+    static PStep<T> pstep(uint32_t op, uint32_t lpr, uint32_t n0, uint32_t n1, const uint32_t* ia,
+                          const uint32_t* ja, const T* a, const T* dval, const void* v0, const void* v1,
+                          const void* v2 = nullptr, double s0 = 0, double s1 = 0, uint32_t mode = 0) {
+        PStep<T> st;
+        memset(&st, 0, sizeof st);
+        st.op = op;
+        st.lpr = lpr < 1 ? 1 : lpr;  // the tile kernels (lpr 0) sum a row serially, as one lane does
+        st.mode = mode;
+        st.n0 = n0;
+        st.n1 = n1;
+        st.ia = ia;
+        st.ja = ja;
+        st.a = a;
+        st.dval = dval;
+        st.v[0] = const_cast<void*>(v0);
+        st.v[1] = const_cast<void*>(v1);
+        st.v[2] = const_cast<void*>(v2);
+        st.s0 = s0;
+        st.s1 = s1;
+        return st;
+    }
+
+    // Whether the call of level l (and every level below it) can run as one
+    // persistent launch: every step there has a descriptor form (the
+    // shared-memory small-level kernel has none).
+    bool persist_ok(uint32_t l) const {
+        if (!persist || ps || autotune || !explicit_solves) return false;
+        if (H.lv[l]->N > persist_max_n) return false;
+        if (small && small->valid() && !small->dense.p && small->first >= l) return false;
+        return true;
+    }
+
+    template <class Body>
+    void persist_region(Body body) {
+        std::vector<PStep<T>> v;
+        ps = &v;
+        body();
+        ps = nullptr;
+        if (v.empty()) return;
+        pdesc->emplace_back();
+        DBuf<uint8_t>& d = pdesc->back();
+        d.alloc(v.size() * sizeof(PStep<T>));
+        CK(cudaMemcpy(d.p, v.data(), v.size() * sizeof(PStep<T>), cudaMemcpyHostToDevice));
+        const PStep<T>* dp = reinterpret_cast<const PStep<T>*>(d.p);
+        uint32_t n = (uint32_t)v.size();
+        PBar* bar = pbar;
+        op([=](cudaStream_t s) { launch_persist<T>(dp, n, bar, s); });
+        persist_regions++;
+        persist_steps += n;
+    }
+
     bool small_call(uint32_t l, const T* f, T* x) {
         if (!small || !small->valid() || l != small->first) return false;
         const SmallPlan<T>* sp = small;
         if (sp->dense.p) {
             uint32_t n = sp->N0;
             const T* C = sp->dense.p;
-            op([=](cudaStream_t s) {
+            if (ps) ps->push_back(pstep(PS_DENSE, 32, n, 0, nullptr, nullptr, C, nullptr, f, x));
+            else op([=](cudaStream_t s) {
                 launch_k(k_dense_gemv<T>, grid_for((size_t)n * 32, 256), 256, 0, s, n, C, f, x);
             });
             bytes += (uint64_t)n * n * sizeof(T) + 2ull * n * sizeof(T);
             return true;
         }
+        if (ps) MLP_THROW(ERR_INTERNAL, "small-level kernel inside a persistent region");
         op([=](cudaStream_t s) { launch_small<T>(*sp, f, x, s); });
         bytes += sp->h.bytes_static + 2ull * sizeof(T) * sp->N0;
         return true;
@@ -1457,12 +1057,14 @@ struct Builder {
     void direct(const Level& L, const T* f, T* x) {
         uint32_t n = L.N;
         const T* C = cinv<T>(L);
-        op([=](cudaStream_t s) { launch_k(k_dense_gemv<T>, grid_for((size_t)n * 32, 256), 256, 0, s, n, C, f, x); });
+        if (ps) ps->push_back(pstep(PS_DENSE, 32, n, 0, nullptr, nullptr, C, nullptr, f, x));
+        else op([=](cudaStream_t s) { launch_k(k_dense_gemv<T>, grid_for((size_t)n * 32, 256), 256, 0, s, n, C, f, x); });
         bytes += (uint64_t)n * n * sizeof(T) + 2ull * n * sizeof(T);
     }
     // One application of the level's split operator on src: phase 1 (L solve
     // and diagonal block), the recursion on the coarse slice, phase 2 (U solve).
     bool autotune = false;
+    cudaStream_t stream = nullptr;  // stream of the build (tuning launches)
     cudaStream_t tune_stream() const { return stream; }
 
     // The pipelined tile kernels are a tuner candidate for the sweep steps of
@@ -1495,7 +1097,8 @@ struct Builder {
         };
         LaunchShape c{pick_lpr(R, L.P1.nnz), 256};
         if (autotune) c = tune_shape(1, sizeof(T), R, L.P1.nnz, tune_stream(), launch, st);
-        op([=](cudaStream_t s) { launch(c, s); });
+        if (ps) ps->push_back(pstep(PS_PHASE1, (uint32_t)c.lpr, R, N, ia, ja, a, dv, src, w, out));
+        else op([=](cudaStream_t s) { launch(c, s); });
         bytes += (uint64_t)L.P1.nnz * (4 + sizeof(T)) + 4ull * (R + 1) + sizeof(T) * (2ull * N + L.Md) ;
     }
     void phase2(const Level& L, const T* w, T* out) {
@@ -1517,7 +1120,8 @@ struct Builder {
         };
         LaunchShape c{pick_lpr(M, L.G.nnz), 256};
         if (autotune) c = tune_shape(2, sizeof(T), M, L.G.nnz, tune_stream(), launch, st);
-        op([=](cudaStream_t s) { launch(c, s); });
+        if (ps) ps->push_back(pstep(PS_PHASE2, (uint32_t)c.lpr, M, 0, ia, ja, a, nullptr, w, out));
+        else op([=](cudaStream_t s) { launch(c, s); });
         bytes += (uint64_t)L.G.nnz * (4 + sizeof(T)) + 4ull * (M + 1) + sizeof(T) * (M + L.n + M);
     }
     void update(const Level& L, const T* u0, T* x, T* r, bool do_r) {
@@ -1542,7 +1146,8 @@ struct Builder {
         // the tuning runs x += u0 on scratch: every buffer of the plan is
         // rewritten before it is read in an apply
         if (autotune && do_r) c = tune_shape(3, sizeof(T), N, L.Af.nnz, tune_stream(), launch, st);
-        op([=](cudaStream_t s) { launch(c, s); });
+        if (ps) ps->push_back(pstep(PS_UPDATE, (uint32_t)c.lpr, N, 0, ia, ja, a, nullptr, u0, x, r, 0, 0, dr));
+        else op([=](cudaStream_t s) { launch(c, s); });
         bytes += sizeof(T) * 3ull * N + (do_r ? spmv_bytes(L.Af) : 0);
     }
 
@@ -1562,12 +1167,15 @@ struct Builder {
     // triangular solves in explicit form: each sweep is phase 1, the recursion
     // and phase 2; the correction sweeps update the residual in place.
     void ms(uint32_t l, const T* f, T* x) {
+        if (persist_ok(l)) {
+            persist_region([&] { ms(l, f, x); });
+            return;
+        }
         if (small_call(l, f, x)) return;
         Level& L = *H.lv[l];
         if (L.direct) { direct(L, f, x); return; }
         if (!explicit_solves) { ms_waves(l, f, x); return; }
-        if (mid_call(l, f, x)) return;
-        if (ms_merged(l, f, x)) return;
+        if (!ps && ms_merged(l, f, x)) return;
         LevelWork<T>& w = W[l];
         uint32_t N = L.N, M = L.M;
         bool next = l + 1 < H.nlevels && L.n;
@@ -1581,7 +1189,8 @@ struct Builder {
             const T* a = vals<T>(L.Af);
             uint32_t nnz = L.Af.nnz, tm = L.Af.tile_max;
             T* r = w.r.p;
-            op([=](cudaStream_t s) { launch_spmv<T>(N, nnz, ia, ja, a, x, r, f, s, tm); });
+            if (ps) ps->push_back(pstep(PS_RESID, spmv_lpr(N, nnz, tm), N, 0, ia, ja, a, nullptr, x, r, f));
+            else op([=](cudaStream_t s) { launch_spmv<T>(N, nnz, ia, ja, a, x, r, f, s, tm); });
             bytes += spmv_bytes(L.Af);
         }
         for (uint32_t it = 2; it <= L.niter; it++) {
@@ -1594,21 +1203,16 @@ struct Builder {
 
     bool explicit_solves = true;
 
-    // Merged sweep steps (k_merge_a / k_merge_b) at levels of at most
-    // MERGE_MAX_N rows without the autotuner (their arithmetic reproduces the
-    // fixed launch shapes). Step A is on by default (MLP_MERGE=0 turns it
-    // off): with a warp per P1 row recomputing its entries of r' in parallel
-    // it takes the 1.12 M-cell solve from 18.56 to 18.13 ms on B200 (one thread
-    // per row doing it serially had made it 29.7 ms). Step B is opt-in
-    // (MLP_MERGE_B=1): it recomputes the coarse entries from the dense operator,
-    // about 18 MB of L2 reads per launch at 26,907 rows, and measured slower.
+    // Merged sweep steps (k_merge_a) at levels of at most MERGE_MAX_N rows
+    // without the autotuner (their arithmetic reproduces the fixed launch
+    // shapes). On by default (MLP_MERGE=0 turns it off): with a warp per P1 row
+    // recomputing its entries of r' in parallel it takes the 1.12 M-cell solve
+    // from 18.56 to 18.13 ms on B200 (one thread per row doing it serially had
+    // made it 29.7 ms).
     static constexpr uint32_t MERGE_MAX_N = 1u << 17;
     static bool merge_enabled() {
         const char* e = getenv("MLP_MERGE");
         return !(e && e[0] == '0');
-    }
-    bool dense_next(const Level& L, uint32_t l) const {
-        return small && small->valid() && small->dense.p && small->first == l + 1 && small->N0 == L.n && L.n;
     }
     // rows of Af with the correction kernel's lane count, P1 rows one per thread
     void step_a(const Level& L, int mode, const T* f, T* x, const T* r_in, T* r_out, const T* u_in, T* u_out,
@@ -1643,23 +1247,6 @@ struct Builder {
         int l0 = staged ? 1 : pick_lpr(N, L.Af.nnz), l1 = pick_lpr(N, L.Af.nnz), lp = pick_lpr(R, L.P1.nnz);
         return l0 <= 8 && l1 <= 8 && lp <= 8;
     }
-    void step_b(const Level& L, const T* w, T* out) {
-        uint32_t M = L.M, n = L.n;
-        int lpg = pick_lpr(M, L.G.nnz);
-        uint32_t blocks = grid_for((size_t)(M + n) * 32, 256);
-        const uint32_t *gia = L.G.ia.p, *gja = L.G.ja.p;
-        const T* ga = vals<T>(L.G);
-        const T* C = small->dense.p;
-        switch (lpg) {
-            case 1: op([=](cudaStream_t s) { launch_k(k_merge_b<T, 1>, blocks, 256, 0, s, M, n, gia, gja, ga, C, w, out); }); break;
-            case 2: op([=](cudaStream_t s) { launch_k(k_merge_b<T, 2>, blocks, 256, 0, s, M, n, gia, gja, ga, C, w, out); }); break;
-            case 4: op([=](cudaStream_t s) { launch_k(k_merge_b<T, 4>, blocks, 256, 0, s, M, n, gia, gja, ga, C, w, out); }); break;
-            default: op([=](cudaStream_t s) { launch_k(k_merge_b<T, 8>, blocks, 256, 0, s, M, n, gia, gja, ga, C, w, out); }); break;
-        }
-        bytes += (uint64_t)n * n * sizeof(T) + 2ull * n * sizeof(T);
-        if (M) bytes += (uint64_t)L.G.nnz * (4 + sizeof(T)) + 4ull * (M + 1) + sizeof(T) * (M + n + M);
-    }
-
     // MultiSplitPrec::solve(l, f, x) with merged steps: sweep 1 = phase 1,
     // step B (or the recursion and phase 2); sweep 2 = step A (residual),
     // step B; sweeps 3.. = step A (correction of the previous sweep), step B;
@@ -1667,8 +1254,6 @@ struct Builder {
     bool ms_merged(uint32_t l, const T* f, T* x) {
         Level& L = *H.lv[l];
         if (!merge_enabled() || autotune || L.N > MERGE_MAX_N || L.niter < 2 || !merge_a_ok(L)) return false;
-        const char* eb = getenv("MLP_MERGE_B");
-        bool dn = eb && eb[0] == '1' && dense_next(L, l) && pick_lpr(L.M, L.G.nnz) <= 8;
         bool next = l + 1 < H.nlevels && L.n;
         LevelWork<T>& W_ = W[l];
         if (!W_.r2.p) W_.r2.alloc(L.N);
@@ -1676,7 +1261,6 @@ struct Builder {
         uint32_t M = L.M;
         T* w = W_.w.p;
         auto stepB = [&](T* out) {
-            if (dn) { step_b(L, w, out); return; }
             if (next) ms(l + 1, w + M, out + M);
             phase2(L, w, out);
         };
@@ -1694,66 +1278,6 @@ struct Builder {
             std::swap(ua, ub);
         }
         update(L, ua, x, nullptr, false);
-        return true;
-    }
-
-    // The whole level-l call as one cluster launch (k_mid_level) when level
-    // l + 1 is the tabulated dense sub-hierarchy and level l is small enough
-    // for one cluster to sweep it.
-    static constexpr uint32_t MID_MAX_N = 1u << 17;
-    std::map<uint32_t, size_t> mid_smem;   // level -> shared memory of its fused kernel
-    cudaStream_t stream = nullptr;         // stream of the build (level data downloads)
-
-    // Shared memory of the largest CTA slice (row starts at the slice bounds).
-    size_t mid_smem_bytes(const Level& L, const MidArgs<T>& a, int cs) {
-        std::vector<uint32_t> ia1 = L.P1.ia.download(stream, (size_t)a.R + 1);
-        std::vector<uint32_t> ia2 = L.G.ia.download(stream, (size_t)a.M + 1);
-        std::vector<uint32_t> ia3 = L.Af.ia.download(stream, (size_t)a.N + 1);
-        const std::vector<uint32_t>* ias[3] = {&ia1, &ia2, &ia3};
-        size_t smem = 0;
-        for (int c = 0; c < cs; c++) {
-            uint32_t es[3], ee[3];
-            for (int k = 0; k < 3; k++) {
-                uint32_t r0, r1;
-                mid_rows(k, a.R, a.M, a.N, cs, c, r0, r1);
-                es[k] = (*ias[k])[r0];
-                ee[k] = (*ias[k])[r1];
-            }
-            MidLayout ml;
-            mid_layout<T>(ml, cs, c, a.R, a.M, a.N, a.n, es, ee);
-            smem = std::max(smem, ml.bytes);
-        }
-        return (smem + 15) & ~(size_t)15;
-    }
-
-    bool mid_call(uint32_t l, const T* f, T* x) {
-        Level& L = *H.lv[l];
-        if (!small || !small->valid() || !small->dense.p || small->first != l + 1) return false;
-        if (L.N > MID_MAX_N || !L.n || L.niter < 1 || small->N0 != L.n) return false;
-        const int cs = 16;
-        MidArgs<T> a{};
-        a.N = L.N; a.M = L.M; a.R = L.N - L.Md; a.n = small->N0; a.niter = L.niter;
-        a.p1_ia = L.P1.ia.p; a.p1_ja = L.P1.ja.p; a.p1_a = vals<T>(L.P1);
-        a.g_ia = L.G.ia.p; a.g_ja = L.G.ja.p; a.g_a = vals<T>(L.G);
-        a.af_ia = L.Af.ia.p; a.af_ja = L.Af.ja.p; a.af_a = vals<T>(L.Af);
-        a.dval = dvals<T>(L);
-        a.C = small->dense.p;
-        a.f = f; a.x = x;
-        const char* tre = getenv("MLP_MID_TRACE");
-        a.trace = (tre && tre[0] == '1') ? 1 : 0;
-        auto hit = mid_smem.find(l);
-        size_t smem = hit != mid_smem.end() ? hit->second : mid_smem_bytes(L, a, cs);
-        mid_smem[l] = smem;
-        if (!smem || !mid_cluster_ok<T>(cs, smem)) return false;
-        op([=](cudaStream_t s) { launch_mid<T>(a, cs, smem, s); });
-        // bytes: the same as the separate steps
-        uint32_t R = a.R, N = L.N, M = L.M, n = a.n;
-        for (uint32_t it = 1; it <= L.niter; it++) {
-            bytes += (uint64_t)L.P1.nnz * (4 + sizeof(T)) + 4ull * (R + 1) + sizeof(T) * (2ull * N + L.Md);
-            bytes += (uint64_t)n * n * sizeof(T) + 2ull * n * sizeof(T);
-            if (M) bytes += (uint64_t)L.G.nnz * (4 + sizeof(T)) + 4ull * (M + 1) + sizeof(T) * (M + n + M);
-            if (L.niter >= 2) bytes += it == 1 ? spmv_bytes(L.Af) : sizeof(T) * 3ull * N + (it < L.niter ? spmv_bytes(L.Af) : 0);
-        }
         return true;
     }
 
@@ -1789,6 +1313,10 @@ struct Builder {
 
     // Prec::solve(level, f, x) (cheb_solve.cc:13-123)
     void ch(uint32_t l, const T* f, T* x) {
+        if (persist_ok(l)) {
+            persist_region([&] { ch(l, f, x); });
+            return;
+        }
         if (small_call(l, f, x)) return;
         Level& L = *H.lv[l];
         LevelWork<T>& w = W[l];
@@ -1815,37 +1343,45 @@ struct Builder {
             auto scale = [&](T* v, double al) {
                 if (is_equal1(al)) return;
                 T a = (T)al;
-                op([=](cudaStream_t s) { launch_k(k_scale<T>, grid_for(n, 256), 256, 0, s, n, v, a); });
+                if (ps) ps->push_back(pstep(PS_SCALE, 1, n, 0, nullptr, nullptr, nullptr, nullptr, v, nullptr, nullptr, (double)a));
+                else op([=](cudaStream_t s) { launch_k(k_scale<T>, grid_for(n, 256), 256, 0, s, n, v, a); });
+            };
+            auto resid = [&](const T* u, T* y) {
+                if (ps) ps->push_back(pstep(PS_RESID, spmv_lpr(n, snnz, stm), n, 0, sia, sja, sa, nullptr, u, y, F));
+                else op([=](cudaStream_t s) { launch_spmv<T>(n, snnz, sia, sja, sa, u, y, F, s, stm); });
             };
             if (nch > 1) { ch(l + 1, F, u1); scale(u1, alpha); }
             else { ch(l + 1, F, x2); scale(x2, alpha); }
             if (nch > 1) {
                 alpha = 4 / (lmax - lmin) * cheb_poly(eta, 1) / cheb_poly(eta, 2);
                 beta = cheb_poly(eta, 0) / cheb_poly(eta, 2);
-                op([=](cudaStream_t s) { launch_spmv<T>(n, snnz, sia, sja, sa, u1, tmp, F, s, stm); });
+                resid(u1, tmp);
                 // tmp = F - A u1 above; the reference forms A u1 - F: negate via the scalars
                 ch(l + 1, tmp, x2);
                 // x2 := -alpha * solve(A u1 - F) + (1+beta) u1 = alpha * solve(F - A u1) + (1+beta) u1
                 double c = is_equal1(1 + beta) ? 1.0 : 1 + beta;
                 T ma = (T)alpha, cc = (T)c;
-                op([=](cudaStream_t s) { launch_k(k_cheb2<T>, grid_for(n, 256), 256, 0, s, n, x2, (const T*)u1, ma, cc); });
+                if (ps) ps->push_back(pstep(PS_CHEB2, 1, n, 0, nullptr, nullptr, nullptr, nullptr, x2, u1, nullptr, (double)ma, (double)cc));
+                else op([=](cudaStream_t s) { launch_k(k_cheb2<T>, grid_for(n, 256), 256, 0, s, n, x2, (const T*)u1, ma, cc); });
                 bytes += spmv_bytes(Ln.As) + 3ull * sizeof(T) * n;
             }
             for (uint32_t i = 3; i <= nch; i++) {
                 T* t = u0; u0 = u1; u1 = x2; x2 = t;  // cheb_solve.cc:87-89
                 alpha = 4 / (lmax - lmin) * cheb_poly(eta, i - 1) / cheb_poly(eta, i);
                 beta = cheb_poly(eta, i - 2) / cheb_poly(eta, i);
-                op([=](cudaStream_t s) { launch_spmv<T>(n, snnz, sia, sja, sa, u1, tmp, F, s, stm); });
+                resid(u1, tmp);
                 ch(l + 1, tmp, x2);
                 // x2 = u1 - alpha*solve(A u1 - F) + beta*(u1-u0) = u1 + alpha*solve(F - A u1) + ...
                 T ma = (T)(-alpha), bb = (T)beta;
                 T* u0c = u0; T* u1c = u1; T* x2c = x2;
-                op([=](cudaStream_t s) { launch_k(k_chebk<T>, grid_for(n, 256), 256, 0, s, n, x2c, (const T*)u1c, (const T*)u0c, ma, bb); });
+                if (ps) ps->push_back(pstep(PS_CHEBK, 1, n, 0, nullptr, nullptr, nullptr, nullptr, x2c, u1c, u0c, (double)ma, (double)bb));
+                else op([=](cudaStream_t s) { launch_k(k_chebk<T>, grid_for(n, 256), 256, 0, s, n, x2c, (const T*)u1c, (const T*)u0c, ma, bb); });
                 bytes += spmv_bytes(Ln.As) + 4ull * sizeof(T) * n;
             }
             T* xo = x + M;
             T* fin = x2;
-            op([=](cudaStream_t s) { launch_k(k_copy<T>, grid_for(n, 256), 256, 0, s, n, (const T*)fin, xo); });
+            if (ps) ps->push_back(pstep(PS_COPY, 1, n, 0, nullptr, nullptr, nullptr, nullptr, fin, xo));
+            else op([=](cudaStream_t s) { launch_k(k_copy<T>, grid_for(n, 256), 256, 0, s, n, (const T*)fin, xo); });
         }
         if (explicit_solves) phase2(L, w.w.p, x);
         else usolve(L, w.w.p, x);
@@ -1897,6 +1433,39 @@ static uint32_t small_budget() {
     return 200 * 1024;
 }
 
+// Persistent regions (k_persist) are on unless MLP_PERSIST=0; a region starts
+// at the first level of at most MLP_PERSIST_MAX_N rows (default 524,288, so
+// that a 1.12 M-cell level 0 keeps its bandwidth-bound separate kernels).
+static bool persist_enabled() {
+    const char* e = getenv("MLP_PERSIST");
+    return !(e && e[0] == '0');
+}
+static uint32_t persist_max_n() {
+    const char* e = getenv("MLP_PERSIST_MAX_N");
+    if (e && *e) return (uint32_t)strtoul(e, nullptr, 10);
+    return 1u << 19;
+}
+
+template <class T>
+static void builder_persist(Builder<T>& B, Prec& P) {
+    B.persist = persist_enabled();
+    B.persist_max_n = persist_max_n();
+    B.pdesc = &P.pdesc;
+    B.pbar = P.pbar.p;
+}
+
+void check_persist(Prec& P, cudaStream_t s) {
+    if (!P.persist_regions) return;
+    PBar h;
+    CK(cudaMemcpyAsync(&h, P.pbar.p, sizeof h, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (h.err) {
+        CK(cudaMemsetAsync(P.pbar.p, 0, sizeof(PBar), s));
+        CK(cudaStreamSynchronize(s));
+        MLP_THROW(ERR_INTERNAL, "a grid barrier of the persistent apply gave up waiting");
+    }
+}
+
 std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, cudaStream_t s) {
     ArenaScope arena;
     auto P = std::unique_ptr<Prec>(new Prec());
@@ -1910,6 +1479,8 @@ std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, c
     P->fout_buf.alloc(N0);
     P->fin = P->fin_buf.p;
     P->fout = P->fout_buf.p;
+    P->pbar.alloc(1);
+    P->pbar.zero(s);
     const char* ex = getenv("MLP_EXPLICIT");
     bool explicit_solves = !(ex && ex[0] == '0');
     if (!fp32) {
@@ -1920,9 +1491,12 @@ std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, c
         B.explicit_solves = explicit_solves;
         B.stream = s;
         B.autotune = cfg.autotune != 0;
+        builder_persist(B, *P);
         if (H.kind == PREC_MSPLIT) B.ms(0, P->fin, P->fout);
         else B.ch(0, P->fin, P->fout);
         P->bytes_per_apply = B.bytes;
+        P->persist_regions = B.persist_regions;
+        P->persist_steps = B.persist_steps;
     } else {
         for (uint32_t l = 0; l < H.nlevels; l++) {
             Level& L = *H.lv[l];
@@ -1941,15 +1515,24 @@ std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, c
         B.explicit_solves = explicit_solves;
         B.stream = s;
         B.autotune = cfg.autotune != 0;
+        builder_persist(B, *P);
         const double* fin = P->fin;
         float* f32 = P->f32.p;
-        B.op([=](cudaStream_t st) { launch_k(k_to_f32, grid_for(N0, 256), 256, 0, st, N0, fin, f32); });
-        if (H.kind == PREC_MSPLIT) B.ms(0, P->f32.p, P->z32.p);
-        else B.ch(0, P->f32.p, P->z32.p);
         float* z32 = P->z32.p;
         double* fout = P->fout;
-        B.op([=](cudaStream_t st) { launch_k(k_to_f64, grid_for(N0, 256), 256, 0, st, N0, (const float*)z32, fout); });
+        auto top = [&] {
+            if (B.ps) B.ps->push_back(Builder<float>::pstep(PS_TOF32, 1, N0, 0, nullptr, nullptr, nullptr, nullptr, fin, f32));
+            else B.op([=](cudaStream_t st) { launch_k(k_to_f32, grid_for(N0, 256), 256, 0, st, N0, fin, f32); });
+            if (H.kind == PREC_MSPLIT) B.ms(0, f32, z32);
+            else B.ch(0, f32, z32);
+            if (B.ps) B.ps->push_back(Builder<float>::pstep(PS_TOF64, 1, N0, 0, nullptr, nullptr, nullptr, nullptr, z32, fout));
+            else B.op([=](cudaStream_t st) { launch_k(k_to_f64, grid_for(N0, 256), 256, 0, st, N0, (const float*)z32, fout); });
+        };
+        if (B.persist_ok(0)) B.persist_region(top);
+        else top();
         P->bytes_per_apply = B.bytes + 12ull * N0 * 2;
+        P->persist_regions = B.persist_regions;
+        P->persist_steps = B.persist_steps;
     }
     CK(cudaStreamSynchronize(s));
     trace("plan + small levels");
@@ -2083,13 +1666,7 @@ __global__ void __launch_bounds__(ST_ROWS) k_pcg_spmv_dot_staged(uint32_t n, con
 }
 
 static void pipe_prepare_all(uint32_t tile_max) {
-    size_t s64 = pipe_smem_bytes<double, true>(tile_max), s32 = pipe_smem_bytes<float, true>(tile_max);
     size_t u64 = pipe_smem_bytes<double, false>(tile_max), u32 = pipe_smem_bytes<float, false>(tile_max);
-    pipe_grid(k_spmv_staged<double, 0, true>, 0, s64);
-    pipe_grid(k_spmv_staged<double, 1, true>, 0, s64);
-    pipe_grid(k_spmv_staged<float, 0, true>, 0, s32);
-    pipe_grid(k_spmv_staged<float, 1, true>, 0, s32);
-    pipe_grid(k_pcg_spmv_dot_staged<true>, 0, s64);
     pipe_grid(k_spmv_staged<double, 0, false>, 0, u64);
     pipe_grid(k_spmv_staged<double, 1, false>, 0, u64);
     pipe_grid(k_spmv_staged<float, 0, false>, 0, u32);
@@ -2108,15 +1685,9 @@ static void pipe_prepare_all(uint32_t tile_max) {
 static void launch_pcg_spmv_dot_staged(uint32_t n, const DCSR& Af, const double* p, double* Ap, double* partials,
                                        PcgDev* d, cudaStream_t s) {
     uint32_t cap = pipe_cap<double>(Af.tile_max);
-    if (pipe_stage_values()) {
-        size_t smem = pipe_smem_bytes<double, true>(Af.tile_max);
-        unsigned g = std::min(pipe_grid(k_pcg_spmv_dot_staged<true>, n, smem), staged_grid(n));
-        k_pcg_spmv_dot_staged<true><<<g, ST_ROWS, smem, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p, Ap, partials, d, cap);
-    } else {
-        size_t smem = pipe_smem_bytes<double, false>(Af.tile_max);
-        unsigned g = std::min(pipe_grid(k_pcg_spmv_dot_staged<false>, n, smem), staged_grid(n));
-        k_pcg_spmv_dot_staged<false><<<g, ST_ROWS, smem, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p, Ap, partials, d, cap);
-    }
+    size_t smem = pipe_smem_bytes<double, false>(Af.tile_max);
+    unsigned g = std::min(pipe_grid(k_pcg_spmv_dot_staged<false>, n, smem), staged_grid(n));
+    k_pcg_spmv_dot_staged<false><<<g, ST_ROWS, smem, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p, Ap, partials, d, cap);
 }
 
 // x += alpha p; r -= alpha Ap; rr = (r, r)
@@ -2255,8 +1826,8 @@ __global__ void k_pcg_start(PcgDev* d, const PcgParams* prm, cudaGraphConditiona
     d->eps = eps;
     d->it = 0;
     d->maxit = prm->maxit;
-    d->status = 0;
-    if (!(init / init > eps)) cudaGraphSetConditional(h, 0u);
+    d->status = isfinite(init) ? 0 : 2;
+    if (!(init / init > eps) || d->status) cudaGraphSetConditional(h, 0u);
 }
 
 PcgWork::~PcgWork() {
@@ -2454,6 +2025,7 @@ int pcg_solve(const DCSR& A, const double* b, Prec& P, double* x, double eps, ui
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     count_launches(start_launches(P, flexible) + (uint64_t)h.it * iteration_launches(P, flexible));
+    check_persist(P, s);
     int rc;
     std::string msg;
     read_stats(h, st, rc, msg);
@@ -2518,6 +2090,7 @@ int ensemble_solve(Ensemble& E, const std::vector<const double*>& b, const std::
         CK(cudaMemcpyAsync(&hs[i], P.pcg.d.p, sizeof(PcgDev), cudaMemcpyDeviceToHost, s));
     }
     CK(cudaStreamSynchronize(s));
+    for (Prec* P : E.members) check_persist(*P, s);
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
@@ -2594,10 +2167,11 @@ int pcg_solve_hostloop(const DCSR& A, const double* b, Prec& P, double* x, doubl
     int lpr = avg <= 3 ? 2 : avg <= 6 ? 4 : avg <= 12 ? 8 : avg <= 24 ? 16 : 32;
     int rc = OK;
     std::string msg;
+    if (!std::isfinite(init)) { rc = ERR_NOT_FINITE; msg = "non-finite initial residual norm"; }
     bool staged = Af.tile_max && Af.tile_max <= ST_MAX_NNZ && n >= 4 * ST_ROWS;
     unsigned Gs = staged_grid(n);
     if (staged && 2 * (size_t)Gs > partials.n) partials.alloc(2 * (size_t)Gs);
-    while (norm / init > eps) {
+    while (rc == OK && norm / init > eps) {
         if (maxit && it >= maxit) { rc = ERR_MAXIT; msg = "iteration cap reached"; break; }
         if (staged) {
             launch_pcg_spmv_dot_staged(n, Af, p.p, Ap.p, partials.p, d, s);
@@ -2634,6 +2208,7 @@ int pcg_solve_hostloop(const DCSR& A, const double* b, Prec& P, double* x, doubl
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFreeHost(hpin);
+    check_persist(P, s);
     st.niter = it;
     st.final_norm = norm;
     st.final_rel = norm / init;
@@ -2651,38 +2226,58 @@ namespace mlp {
 // ---------------------------------------------------------------------------
 // PCG without device allocation.
 //
-// Callers that cannot allocate device memory while they run (code executing
-// inside a stream capture, or hosts that own the whole device pool through a
-// custom allocator) use this variant of pcg_solve. The solver's own vectors and
-// reduction scratch live in the file-scope array below instead of buffers from
-// cudaMalloc; the matrix and the preconditioner handle were built beforehand.
-// The array holds up to NOALLOC_MAX_N unknowns; every GPU that loads the
-// library holds it (about 5 MB) until the process exits.
+// Some host applications cannot let a library call cudaMalloc while they
+// solve: their device memory is owned by their own allocator (a framework's
+// caching allocator that has reserved the device, or a process held to a fixed
+// device-memory budget), so an allocation from inside this library would fail
+// or break the host's accounting. They use this variant of pcg_solve. The
+// solver's own vectors, its reduction scratch and the start vector live in the
+// file-scope array below instead of buffers from cudaMalloc; the matrix and
+// the preconditioner handle were built beforehand (those calls allocate). The
+// array holds up to NOALLOC_MAX_N unknowns; every GPU that loads the library
+// holds it (about 6 MB) until the process exits.
 // ---------------------------------------------------------------------------
 static constexpr uint32_t NOALLOC_MAX_N = 131072;
 static constexpr uint32_t NOALLOC_GRID = 1024;  // largest reduction grid used
 static constexpr size_t NOALLOC_HDR = 16;       // doubles reserved for PcgDev
-static constexpr size_t NOALLOC_DOUBLES = NOALLOC_HDR + 2 * (size_t)NOALLOC_GRID + 5 * (size_t)NOALLOC_MAX_N;
+static constexpr size_t NOALLOC_DOUBLES = NOALLOC_HDR + 2 * (size_t)NOALLOC_GRID + 6 * (size_t)NOALLOC_MAX_N;
 static_assert(sizeof(PcgDev) <= NOALLOC_HDR * sizeof(double), "PcgDev must fit the header");
 
 static __device__ __align__(256) double g_pcg_scratch[NOALLOC_DOUBLES];
 
-// Device address of g_pcg_scratch for the current device. The name is only a
-// host-side stand-in for the array, so the address is taken once per device
-// with cudaGetSymbolAddress while that device is current, and cached.
+// Device address of g_pcg_scratch on the current device. In host code the
+// array's name is only a stand-in, so every call looks the address up with
+// cudaGetSymbolAddress while the caller's device is current (the lookup
+// allocates nothing once the library's device code is loaded on the device);
+// a context recreated after cudaDeviceReset therefore gets the array's new
+// address rather than a stale one.
 static double* noalloc_scratch() {
-    static std::mutex mu;
-    static std::map<int, double*> addr;
-    int dev = 0;
-    CK(cudaGetDevice(&dev));
-    std::lock_guard<std::mutex> lk(mu);
-    auto it = addr.find(dev);
-    if (it != addr.end()) return it->second;
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_pcg_scratch);
     if (e != cudaSuccess) MLP_THROW(ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    addr[dev] = (double*)p;
     return (double*)p;
+}
+
+// generate_x0 (solvers.cc:9-21) for NOALLOC_MAX_N unknowns, made once on the
+// host: srandom(3) with a fixed sequence, so the start vector of a system of n
+// unknowns is the first n entries.
+static const std::vector<double>& noalloc_x0_host() {
+    static std::once_flag once;
+    static std::vector<double> h;
+    std::call_once(once, [] {
+        h.resize(NOALLOC_MAX_N);
+        struct random_data rd;
+        memset(&rd, 0, sizeof rd);
+        char state[128];
+        initstate_r(3, state, sizeof state, &rd);
+        srandom_r(3, &rd);
+        for (uint32_t i = 0; i < NOALLOC_MAX_N; i++) {
+            int32_t v;
+            random_r(&rd, &v);
+            h[i] = 20. * (v - 0.5 * RAND_MAX) / RAND_MAX + 100;
+        }
+    });
+    return h;
 }
 
 uint32_t pcg_noalloc_max_n() { return NOALLOC_MAX_N; }
@@ -2709,33 +2304,16 @@ int pcg_solve_noalloc(const DCSR& A, const double* b, Prec& P, double* x, double
     double* p = bf + NOALLOC_MAX_N;
     double* Ap = p + NOALLOC_MAX_N;
     double* rprev = Ap + NOALLOC_MAX_N;
+    double* x0 = rprev + NOALLOC_MAX_N;
     double* r = P.fin_buf.p;
     double* z = P.fout_buf.p;
     // the array keeps the previous call's contents: the reduction tickets and
     // status flags must start at zero
     CK(cudaMemsetAsync(d, 0, sizeof(PcgDev), s));
-    // x0 of generate_x0 (solvers.cc:9-21), staged through a host stack buffer
-    // into p (natural order), then permuted into the frame like b
-    {
-        struct random_data rd;
-        memset(&rd, 0, sizeof rd);
-        char state[128];
-        initstate_r(3, state, sizeof state, &rd);
-        srandom_r(3, &rd);
-        double chunk[2048];
-        for (uint32_t i0 = 0; i0 < n; i0 += 2048) {
-            uint32_t m = std::min<uint32_t>(2048, n - i0);
-            for (uint32_t i = 0; i < m; i++) {
-                int32_t v;
-                random_r(&rd, &v);
-                chunk[i] = 20. * (v - 0.5 * RAND_MAX) / RAND_MAX + 100;
-            }
-            CK(cudaMemcpyAsync(p + i0, chunk, (size_t)m * 8, cudaMemcpyHostToDevice, s));
-            CK(cudaStreamSynchronize(s));
-        }
-    }
+    // x0 of generate_x0 in natural order, then permuted into the frame like b
+    CK(cudaMemcpyAsync(x0, noalloc_x0_host().data(), (size_t)n * 8, cudaMemcpyHostToDevice, s));
     gather(n, L0.phi.p, b, bf, s);
-    gather(n, L0.phi.p, p, xf, s);
+    gather(n, L0.phi.p, x0, xf, s);
     launch_spmv<double>(n, Af.nnz, Af.ia.p, Af.ja.p, Af.a.p, xf, r, bf, s, Af.tile_max);
     CK_LAUNCH();
     auto fetch = [&]() -> PcgDev {
@@ -2760,10 +2338,11 @@ int pcg_solve_noalloc(const DCSR& A, const double* b, Prec& P, double* x, double
     int lpr = avg <= 3 ? 2 : avg <= 6 ? 4 : avg <= 12 ? 8 : avg <= 24 ? 16 : 32;
     int rc = OK;
     std::string msg;
+    if (!std::isfinite(init)) { rc = ERR_NOT_FINITE; msg = "non-finite initial residual norm"; }
     bool staged = Af.tile_max && Af.tile_max <= ST_MAX_NNZ && n >= 4 * ST_ROWS;
     unsigned Gs = staged_grid(n);
     if (staged && Gs > 2 * NOALLOC_GRID) MLP_THROW(ERR_LIMIT, "reduction grid exceeds the static scratch");
-    while (norm / init > eps) {
+    while (rc == OK && norm / init > eps) {
         if (maxit && it >= maxit) { rc = ERR_MAXIT; msg = "iteration cap reached"; break; }
         if (staged) {
             launch_pcg_spmv_dot_staged(n, Af, p, Ap, partials, d, s);
@@ -2794,6 +2373,7 @@ int pcg_solve_noalloc(const DCSR& A, const double* b, Prec& P, double* x, double
     }
     scatter(n, L0.phi.p, xf, x, s);
     CK(cudaStreamSynchronize(s));
+    check_persist(P, s);
     st.niter = it;
     st.final_norm = norm;
     st.final_rel = norm / init;

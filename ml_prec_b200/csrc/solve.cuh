@@ -3,6 +3,7 @@
 
 #include <functional>
 
+#include "persist.cuh"
 #include "setup.cuh"
 
 namespace mlp {
@@ -61,6 +62,10 @@ struct Prec {
     cudaGraphExec_t graph = nullptr;
     cudaStream_t stream = nullptr;
     uint64_t bytes_per_apply = 0;  // algorithmic bytes of one apply
+    // persistent regions of the plan: step descriptors and the grid barrier
+    std::vector<DBuf<uint8_t>> pdesc;
+    DBuf<PBar> pbar;
+    uint32_t persist_regions = 0, persist_steps = 0;
     PcgWork pcg;
     Prec();
     ~Prec();
@@ -68,6 +73,9 @@ struct Prec {
 
 std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, cudaStream_t s);
 void prec_apply_frame(Prec& P, cudaStream_t s);  // fout = B fin
+// Throws ERR_INTERNAL (and clears the flag) when a grid barrier of a
+// persistent region gave up waiting since the last check; synchronises s.
+void check_persist(Prec& P, cudaStream_t s);
 
 // Records the largest nnz of a 256-row tile (decides the staged SpMV).
 void csr_tile_stats(DCSR& m, cudaStream_t s);

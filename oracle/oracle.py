@@ -248,7 +248,7 @@ def ref_available():
 
 def run_ref(outdir, *, perm=None, csr=None, rhs=None, nx=60, ny=220, nz=85, c=1.0, prec="msplit",
             cfg=None, eps=1e-8, dump=False, no_solve=False, sigmas=None, niters=None, apply=None,
-            reps=1, dirichlet=True, timeout=None):
+            reps=1, dirichlet=True, timeout=None, ms_use_tails=None):
     """Runs oracle/_ref/ref_driver; returns the parsed result.json."""
     args = [REF_DRIVER, "--out", outdir, "--nx", str(nx), "--ny", str(ny), "--nz", str(nz),
             "--c", repr(float(c)), "--prec", prec, "--eps", repr(float(eps)), "--reps", str(reps)]
@@ -272,6 +272,8 @@ def run_ref(outdir, *, perm=None, csr=None, rhs=None, nx=60, ny=220, nz=85, c=1.
         args += ["--niters", ",".join(str(int(s)) for s in niters)]
     if apply is not None:
         args += ["--apply", apply]
+    if ms_use_tails is not None:
+        args += ["--ms-use-tails", str(int(ms_use_tails))]
     os.makedirs(outdir, exist_ok=True)
     subprocess.run(args, check=True, stdout=subprocess.DEVNULL, timeout=timeout)
     with open(os.path.join(outdir, "result.json")) as f:

@@ -32,6 +32,7 @@
 #include <iterator>
 #include <map>
 #include <memory>
+#include <new>
 #include <set>
 #include <sstream>
 #include <stack>
@@ -103,6 +104,7 @@ struct Args {
     std::vector<uint> niters;
     std::string apply_in;  // optional: one preconditioner apply on this vector
     int reps = 1;
+    int ms_use_tails = -1;  // >= 0: value of MultiSplitPrec::use_tails (see below)
 };
 
 static std::vector<double> parse_list_d(const char* s) {
@@ -139,6 +141,7 @@ int main(int argc, char** argv) {
         else if (k == "--niters") { std::vector<double> d = parse_list_d(val()); for (double x : d) a.niters.push_back((uint)x); }
         else if (k == "--apply") a.apply_in = val();
         else if (k == "--reps") a.reps = atoi(val());
+        else if (k == "--ms-use-tails") a.ms_use_tails = atoi(val());
         else { fprintf(stderr, "unknown arg %s\n", k.c_str()); return 2; }
     }
 
@@ -229,7 +232,17 @@ int main(int argc, char** argv) {
         if (a.prec == "msplit") {
             cfg.prec = MULTI_SPLIT_PREC;
             cfg.prec_conf_file = a.cfgfile;
-            B = new MultiSplitPrec(A, cfg);
+            if (a.ms_use_tails >= 0) {
+                // MultiSplitPrec never sets its use_tails member (multi_split_prec.h:17)
+                // before order_original reads it (multi_split_mark.cc:42). To pin the
+                // value for a parity case, the object is constructed in storage whose
+                // bytes all hold the wanted value (0 or 1).
+                void* mem = ::operator new(sizeof(MultiSplitPrec));
+                memset(mem, a.ms_use_tails ? 1 : 0, sizeof(MultiSplitPrec));
+                B = new (mem) MultiSplitPrec(A, cfg);
+            } else {
+                B = new MultiSplitPrec(A, cfg);
+            }
         } else if (a.prec == "cheb") {
             cfg.prec = UH_CHEB_PREC;
             B = new Prec(A, cfg);

@@ -38,16 +38,58 @@ CASES = {
     "ms_tiny_1x1x1": ("iid", 1, 1, 1, 1, 1.0, "msplit", {}),
     "ms_line_1x1x7": ("iid", 1, 1, 1, 7, 1.0, "msplit", {}),
     "ms_none_12x22x6": ("iid", 1, 12, 22, 6, 1.0, "msplit", {"elim_order": "none", "max_levels": 3}),
+    "ms_original_16x22x8": ("layered", 2, 16, 22, 8, 1.0, "msplit", {"elim_order": "original", "use_tails": 1}),
+    "ms_original_notails_20x22x10": ("iid", 6, 20, 22, 10, 1.0, "msplit",
+                                     {"elim_order": "original", "use_tails": 0}),
     "ch_layered_16x22x8": ("layered", 2, 16, 22, 8, 1.0, "cheb", {"sigmas": [3.0], "niters": [4]}),
     "ch_iid_12x22x6": ("iid", 4, 12, 22, 6, 1.0, "cheb", {"sigmas": [3.0, 2.5], "niters": [2, 3]}),
 }
+
+# Configurations the reference rejects while it builds the hierarchy: the
+# message of its exception is stored (name.json) and the library must fail
+# with the same message. elim_order = block accepts only the 60x220x85 mesh,
+# so it fails on any other mesh at level 0 and on every mesh at level 1
+# (multi_split_mark.cc:201-203); the size in the level-1 message is what
+# level 0 left over, which pins the level-0 block ordering's M + Md.
+ERRORS = {
+    "err_block_60x220x85": ("layered", 2, 60, 220, 85, 1.0, {"elim_order": "block"}),
+    "err_block_16x22x8": ("layered", 2, 16, 22, 8, 1.0, {"elim_order": "block"}),
+}
+
+
+def run_errors(td, wanted):
+    import re
+    for name, (model, seed, nx, ny, nz, c, opt) in ERRORS.items():
+        if name not in wanted:
+            continue
+        kx, ky, kz = fields.field(model, seed)
+        od = os.path.join(td, name)
+        os.makedirs(od)
+        fn = os.path.join(od, "perm.bin")
+        fields.write_perm_bin(fn, kx, ky, kz)
+        cfg = os.path.join(od, "msplit.cfg")
+        with open(cfg, "w") as fh:
+            fh.write(O.msplit_cfg_text(elim_order=opt["elim_order"]))
+        r = subprocess.run([O.REF_DRIVER, "--out", od, "--perm", fn, "--nx", str(nx), "--ny", str(ny), "--nz",
+                            str(nz), "--c", repr(float(c)), "--prec", "msplit", "--cfg", cfg, "--no-solve"],
+                           capture_output=True, text=True)
+        assert r.returncode != 0, f"{name}: the reference accepted the configuration"
+        m = re.search(r"EXCEPTION \(([^)]*)\): (.*)", r.stderr)
+        assert m, r.stderr[-2000:]
+        where = m.group(1).replace(os.path.join(REF, ""), "")
+        rec = dict(model=model, seed=seed, nx=nx, ny=ny, nz=nz, c=c, options=opt, where=where,
+                   message=m.group(2).strip())
+        with open(os.path.join(OUT, f"{name}.json"), "w") as fh:
+            json.dump(rec, fh, indent=1)
+        print(name, rec["message"], flush=True)
 
 
 def main():
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={REF}"], check=True)
     with tempfile.TemporaryDirectory() as td:
         perms = {}
-        wanted = sys.argv[1:] or list(CASES)
+        wanted = sys.argv[1:] or list(CASES) + list(ERRORS)
+        run_errors(td, wanted)
         for name, (model, seed, nx, ny, nz, c, prec, opt) in CASES.items():
             if name not in wanted:
                 continue
@@ -71,6 +113,10 @@ def main():
                                                degree_max=opt.get("degree_max", 2),
                                                max_levels=opt.get("max_levels", 15)))
                 kw["cfg"] = cfg
+                if "use_tails" in opt:
+                    # MultiSplitPrec reads use_tails without setting it (multi_split_prec.h:17);
+                    # the driver pins it for the case
+                    kw["ms_use_tails"] = opt["use_tails"]
             else:
                 kw["sigmas"] = opt["sigmas"]
                 kw["niters"] = opt["niters"]

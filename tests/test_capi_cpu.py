@@ -67,6 +67,12 @@ def test_argument_errors_need_no_device():
     ja = np.array([0, 0, 0, 0], np.uint32)
     rc = lib.mlp_matrix_create(2, ia.ctypes.data_as(u32), ja.ctypes.data_as(u32), a.ctypes.data_as(f64), C.byref(h))
     assert rc == 1 and b"row 1" in lib.mlp_last_error()
+    # a NaN matrix value is refused before anything reaches a device (MLP_ERR_NOT_FINITE)
+    ia = np.array([0, 2, 4], np.uint32)
+    ja = np.array([0, 1, 1, 0], np.uint32)
+    a = np.array([2.0, -1.0, np.nan, -1.0])
+    rc = lib.mlp_matrix_create(2, ia.ctypes.data_as(u32), ja.ctypes.data_as(u32), a.ctypes.data_as(f64), C.byref(h))
+    assert rc == 5 and b"non-finite matrix value at entry 2" in lib.mlp_last_error()
     # null handles
     assert lib.mlp_prec_create(None, None, None) == 1
     assert lib.mlp_pcg(None, None, None, None, 1e-8, 0, 0, None) == 1

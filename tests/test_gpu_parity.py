@@ -22,21 +22,22 @@ def M():
     return M
 
 
-@pytest.fixture(params=["dense", "separate", "merged_b", "fused", "small", "explicit", "waves"])
+@pytest.fixture(params=["persistent", "persist_split", "dense", "separate", "small", "explicit", "waves"])
 def apply_path(request, monkeypatch):
-    """Run each case through every apply path: the tabulated small-level
-    operator with the correction and phase-1 steps of the small levels merged
-    (default), the same with every sweep step a separate kernel, with the coarse
-    product and phase 2 merged too, the level above the tabulated operator as
-    one cluster launch, the shared-memory small-level kernel (tabulation off),
-    the launch path with explicit triangular solves (small kernel off), and the
-    launch path with wavefront triangular solves."""
+    """Run each case through every apply path: the whole apply as one
+    persistent launch (default at these sizes), the finest level as separate
+    launches around a persistent launch of the levels below it, the tabulated
+    small-level operator with separate launches and the correction and
+    phase-1 steps of the small levels merged, the same with every sweep step a
+    separate kernel, the shared-memory small-level kernel (tabulation off),
+    the launch path with explicit triangular solves (small kernel off), and
+    the launch path with wavefront triangular solves."""
+    if request.param == "persist_split":
+        monkeypatch.setenv("MLP_PERSIST_MAX_N", "1200")
+    if request.param in ("dense", "separate", "small", "explicit", "waves"):
+        monkeypatch.setenv("MLP_PERSIST", "0")
     if request.param == "separate":
         monkeypatch.setenv("MLP_MERGE", "0")
-    if request.param == "merged_b":
-        monkeypatch.setenv("MLP_MERGE_B", "1")
-    if request.param == "fused":
-        monkeypatch.setenv("MLP_MID", "1")
     if request.param == "small":
         monkeypatch.setenv("MLP_DENSE_OP_MAX", "0")
     if request.param in ("explicit", "waves"):
@@ -134,7 +135,7 @@ def test_full_size_hierarchy_and_pcg_against_oracle(M):
     x = M.PCGSolver(A, b, P, stats=st, eps=1e-8)
     xo, it, rel, rc = O.pcg(Ao, bo, Po, 1e-8)
     assert rc == 0 and abs(st.niter - it) <= 1
-    assert np.linalg.norm(x - xo) <= 1e-9 * np.linalg.norm(xo)
+    assert np.linalg.norm(x - xo) <= 1e-10 * np.linalg.norm(xo)
 
 
 @pytest.mark.parametrize("fp32", [False, True])
@@ -165,57 +166,32 @@ def test_iteration_cap_ends_the_device_loop(M):
 
 
 @pytest.mark.parametrize("fp32", [False, True])
-def test_fused_level_kernel_matches_separate_launches(M, fp32, monkeypatch):
-    """60x220x85 layered field: the level above the tabulated sub-hierarchy
-    (26,907 rows) runs as one cluster launch. Its rows are summed serially, the
-    separate kernels may split a row over lanes, so the two agree to rounding:
-    the apply within 1e-13 (FP64) / 1e-5 (FP32) relative, the PCG iterations
-    within 1 and the solutions within 1e-10 (FP64) / 1e-6 (FP32)."""
-    from ml_prec_b200 import fields
-    kx, ky, kz = fields.field("layered", 2)
-    A, b = M.CSRMatrix.spe(60, 220, 85, kx, ky, kz, c=1.0)
-    f = np.random.default_rng(4).standard_normal(A.n)
-    kw = dict(q=(0.8,), niter=(5,), max_levels=15, degree_max=2, fp32=fp32)
-    monkeypatch.setenv("MLP_MID", "1")
-    P1 = M.MultiSplitPrec(A, **kw)
-    z1 = P1.solve(f)
-    st1 = M.SolverStats()
-    x1 = M.PCGSolver(A, b, P1, stats=st1, eps=1e-8)
-    monkeypatch.setenv("MLP_MID", "0")
-    P2 = M.MultiSplitPrec(A, **kw)
-    z2 = P2.solve(f)
-    st2 = M.SolverStats()
-    x2 = M.PCGSolver(A, b, P2, stats=st2, eps=1e-8)
-    tz, tx = (1e-5, 1e-6) if fp32 else (1e-13, 1e-10)
-    assert np.linalg.norm(z1 - z2) <= tz * np.linalg.norm(z2)
-    assert abs(st1.niter - st2.niter) <= 1
-    assert np.linalg.norm(x1 - x2) <= tx * np.linalg.norm(x2)
-
-
-@pytest.mark.parametrize("fp32", [False, True])
-def test_merged_sweep_steps_are_bit_identical(M, fp32, monkeypatch):
-    """60x220x85 layered field: at the small levels consecutive sweep steps run
-    as merged kernels that recompute the entries they need; they reproduce the
-    separate kernels' arithmetic, so the apply and the PCG iterates are
-    bit-identical."""
+def test_apply_forms_are_bit_identical(M, fp32, monkeypatch):
+    """60x220x85 layered field: the levels below the finest one run as one
+    persistent launch (default); as separate launches with the correction and
+    phase-1 steps of the small levels merged; and as separate launches with
+    every sweep step its own kernel. All three repeat the same arithmetic (same
+    products, lane split and butterfly order), so the apply and the PCG
+    iterates are bit-identical."""
     from ml_prec_b200 import fields
     kx, ky, kz = fields.field("layered", 2)
     A, b = M.CSRMatrix.spe(60, 220, 85, kx, ky, kz, c=1.0)
     f = np.random.default_rng(5).standard_normal(A.n)
     kw = dict(q=(0.8,), niter=(5,), max_levels=15, degree_max=2, fp32=fp32)
-    monkeypatch.setenv("MLP_MERGE", "1")
-    monkeypatch.setenv("MLP_MERGE_B", "1")
-    P1 = M.MultiSplitPrec(A, **kw)
-    z1 = P1.solve(f)
-    st1 = M.SolverStats()
-    x1 = M.PCGSolver(A, b, P1, stats=st1, eps=1e-8)
-    monkeypatch.setenv("MLP_MERGE", "0")
-    P2 = M.MultiSplitPrec(A, **kw)
-    z2 = P2.solve(f)
-    st2 = M.SolverStats()
-    x2 = M.PCGSolver(A, b, P2, stats=st2, eps=1e-8)
-    assert np.array_equal(z1, z2)
-    assert st1.niter == st2.niter and np.array_equal(x1, x2)
+    out = []
+    for env in ({}, {"MLP_PERSIST": "0"}, {"MLP_PERSIST": "0", "MLP_MERGE": "0"}):
+        for k in ("MLP_PERSIST", "MLP_MERGE"):
+            monkeypatch.delenv(k, raising=False)
+        for k, v in env.items():
+            monkeypatch.setenv(k, v)
+        P = M.MultiSplitPrec(A, **kw)
+        z = P.solve(f)
+        st = M.SolverStats()
+        x = M.PCGSolver(A, b, P, stats=st, eps=1e-8)
+        out.append((z, st.niter, x))
+    for z, it, x in out[1:]:
+        assert np.array_equal(z, out[0][0])
+        assert it == out[0][1] and np.array_equal(x, out[0][2])
 
 
 @pytest.mark.parametrize("name", ["ms_iid_12x22x6", "ms_layered_16x22x8_c01"])

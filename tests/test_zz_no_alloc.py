@@ -1,12 +1,13 @@
 """The allocation-free PCG entry point, mlp_pcg_device_noalloc.
 
-It exists for callers that cannot allocate device memory while they solve (for
-example code recording into a stream capture, or a host whose device memory is
-owned by its own allocator); its vectors live in a static device array of the
+It exists for host applications that cannot let the library call cudaMalloc
+while they solve, because their device memory is owned by their own allocator
+or held to a fixed budget; its vectors live in a static device array of the
 library instead. It must return what mlp_pcg_device returns, call after call
-(the shared array keeps the previous call's contents), and refuse systems
-larger than the array. This file is collected last so that a run stopping at
-the first failure has already run every other test.
+(the shared array keeps the previous call's contents), allocate no device
+memory while it runs, and refuse systems larger than the array. This file is
+collected last so that a run stopping at the first failure has already run
+every other test.
 """
 import ctypes as C
 
@@ -40,10 +41,16 @@ def test_noalloc_matches_allocating_pcg_twice(fp32):
     dev = torch.device("cuda", 0)
     b_dev = torch.from_numpy(b).to(dev)
     x_ref, it_ref = _solve(M, "mlp_pcg_device", A, P, b_dev, torch.empty_like(b_dev), fp32)
-    for _ in range(2):  # two calls in a row share the static scratch
-        x, it = _solve(M, "mlp_pcg_device_noalloc", A, P, b_dev, torch.empty_like(b_dev), fp32)
+    outs = [torch.empty_like(b_dev) for _ in range(2)]
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info(0)[0]
+    for out in outs:  # two calls in a row share the static scratch
+        x, it = _solve(M, "mlp_pcg_device_noalloc", A, P, b_dev, out, fp32)
         assert it == it_ref
         assert np.linalg.norm(x - x_ref) <= TOL * np.linalg.norm(x_ref)
+    torch.cuda.synchronize()
+    # the device's free memory is unchanged: nothing was allocated on it
+    assert torch.cuda.mem_get_info(0)[0] == free_before
 
 
 def test_noalloc_rejects_systems_beyond_its_array():
