@@ -62,7 +62,8 @@ typedef struct {
     uint32_t max_levels;     /* multi-split max_levels                                */
     uint32_t degree_max;     /* multi-split simple_1 elimination bound                */
     int32_t order;           /* MLP_ORDER_*                                           */
-    int32_t use_tails;       /* uh_cheb tail elimination (Config::use_tails)          */
+    int32_t use_tails;       /* tail elimination (Config::use_tails): uh_cheb, and the
+                                tail group of multi-split elim_order = original      */
     uint32_t nsigma;         /* uh_cheb sigma (= beta) per level                      */
     const double* sigma;
     uint32_t nncheb;         /* uh_cheb Chebyshev degree per level                    */
@@ -71,6 +72,15 @@ typedef struct {
     int32_t autotune;        /* 1: time the row kernels' launch shapes (lanes per row,
                                 block size) on each level at build and keep the
                                 fastest (cached per level shape); 0: fixed heuristic */
+    uint32_t neps;           /* multi-split inner_iter = dynamic (msplit.cfg level_eps,
+                                multi_split_constr.cc:198-203, 256-264): per-level eps,
+                                entry 0 ignored, last value repeats; each level call
+                                sweeps until ||f - A x|| / ||f|| < eps
+                                (multi_split_solve.cc:119-134), at most 1,000 sweeps
+                                per level call and 100,000 per apply (the reference
+                                has no cap; reaching one returns MLP_ERR_MAXIT).
+                                neps = 0: the fixed niter.                           */
+    const double* level_eps;
 } mlp_prec_cfg;
 
 /* Solver statistics, the fields of SolverStats (solvers.h:15-28) plus the
@@ -95,6 +105,7 @@ typedef struct {
     uint32_t L_nnz, U_nnz;
     uint32_t nwave_l, nwave_u; /* wavefronts of the level-scheduled L / U solves  */
     uint32_t P1_nnz, G_nnz;    /* explicit triangular factors of the sweeps       */
+    double eps;                /* dynamic inner iterations: the level's eps (0 = fixed niter) */
 } mlp_level_info;
 
 const char* mlp_last_error(void);
@@ -144,6 +155,15 @@ int mlp_prec_level_export(const mlp_prec* P, uint32_t level, uint32_t* map, uint
                           uint32_t* A_ja, double* A_a, double* dval);
 /* Algorithmic HBM bytes of one apply (the roofline numerator). */
 int mlp_prec_bytes_per_apply(const mlp_prec* P, uint64_t* bytes);
+/* Profiling aid without a reference counterpart: replays the apply (on the
+ * vector of the last apply, in frame order) reps times launch by launch with
+ * CUDA events between the launches and reports, per launch, its mean device
+ * time (ms), its algorithmic bytes and its name ("phase1 L1", "persistent L1":
+ * the step and the level whose call recorded it; names are written with
+ * stride name_len). *nops receives the number of launches; at most cap
+ * entries are written. */
+int mlp_prec_profile(mlp_prec* P, uint32_t reps, uint32_t cap, uint32_t* nops, double* ms, uint64_t* bytes,
+                     char* names, uint32_t name_len);
 
 /* ---- solver ----------------------------------------------------------------
  * PCGSolver(A, b, B, x, stats, eps, NORM_L2) (solvers.h:31-32, pcg.cc:8-102):
@@ -164,6 +184,18 @@ int mlp_pcg_device(const mlp_matrix* A, const double* b_dev, mlp_prec* P, double
  * whose right-hand side is small next to A x0. */
 int mlp_pcg_device_x0(const mlp_matrix* A, const double* b_dev, mlp_prec* P, double* x_dev, double eps,
                       uint32_t maxit, int32_t flexible, int32_t x0_mode, mlp_stats* stats, void* stream);
+
+/* ChebSolver(A, lmin, lmax, b, B, x, eps, NORM_L2) (solvers.h:42-43,
+ * modules/solvers/cheb.cc:9-100): the Chebyshev iteration with preconditioner
+ * P, for spectral bounds lmin < lmax of the preconditioned operator (uh_cheb
+ * level 0: mlp_level_info lmin / lmax, what project/main.cc:143-148 passes).
+ * x0 from generate_x0; stops when ||r|| / ||r0|| <= eps (1e-14 absolute
+ * floor); stats->niter counts the steps as the reference reports them. maxit
+ * as for mlp_pcg. */
+int mlp_cheb_solve(const mlp_matrix* A, const double* b_host, mlp_prec* P, double* x_host, double lmin,
+                   double lmax, double eps, uint32_t maxit, mlp_stats* stats);
+int mlp_cheb_solve_device(const mlp_matrix* A, const double* b_dev, mlp_prec* P, double* x_dev, double lmin,
+                          double lmax, double eps, uint32_t maxit, mlp_stats* stats, void* stream);
 
 /* Differentiation form (no reference counterpart: the reference has no
  * gradients). For a matrix made by mlp_matrix_create_spe, writes

@@ -4,6 +4,6 @@ multilevel preconditioners of ml_prec, behind the reference's host interface.
 The compute path is the CUDA library ml_prec_b200/lib/libmlp_b200.so (C ABI in
 include/mlp_b200.h); this package is its Python binding.
 """
-from .api import (Config, ConfigError, ConfigFile, CSRMatrix, MultiSplitPrec, PCGSolver, Prec,  # noqa: F401
-                  PrecBase, SolverStats, generate_x0, msplit_params)
+from .api import (ChebSolver, Config, ConfigError, ConfigFile, CSRMatrix, MultiSplitPrec, PCGSolver,  # noqa: F401
+                  Prec, PrecBase, SolverStats, generate_x0, msplit_params)
 from ._capi import MlpError, LIB_PATH  # noqa: F401

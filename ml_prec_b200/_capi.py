@@ -22,9 +22,9 @@ EXPORTS = [
     "mlp_matrix_create", "mlp_matrix_create_spe", "mlp_matrix_destroy", "mlp_matrix_size",
     "mlp_matrix_download", "mlp_spmv", "mlp_spmv_host",
     "mlp_prec_create", "mlp_prec_destroy", "mlp_prec_apply", "mlp_prec_apply_host", "mlp_prec_nlevels",
-    "mlp_prec_level_info", "mlp_prec_level_export", "mlp_prec_bytes_per_apply",
+    "mlp_prec_level_info", "mlp_prec_level_export", "mlp_prec_bytes_per_apply", "mlp_prec_profile",
     "mlp_pcg", "mlp_pcg_device", "mlp_pcg_device_x0", "mlp_matrix_grad_logk", "mlp_pcg_device_noalloc",
-    "mlp_launch_count", "mlp_generate_x0", "mlp_ensemble_create", "mlp_ensemble_solve", "mlp_ensemble_destroy",
+    "mlp_launch_count", "mlp_generate_x0", "mlp_cheb_solve", "mlp_cheb_solve_device", "mlp_ensemble_create", "mlp_ensemble_solve", "mlp_ensemble_destroy",
 ]
 
 
@@ -39,6 +39,7 @@ class PrecCfg(C.Structure):
         ("nncheb", C.c_uint32), ("ncheb", u32p),
         ("fp32", C.c_int32),
         ("autotune", C.c_int32),
+        ("neps", C.c_uint32), ("level_eps", f64p),
     ]
 
 
@@ -59,6 +60,7 @@ class LevelInfo(C.Structure):
         ("L_nnz", C.c_uint32), ("U_nnz", C.c_uint32),
         ("nwave_l", C.c_uint32), ("nwave_u", C.c_uint32),
         ("P1_nnz", C.c_uint32), ("G_nnz", C.c_uint32),
+        ("eps", C.c_double),
     ]
 
 
@@ -97,9 +99,15 @@ def lib():
         L.mlp_prec_level_export.argtypes = [vp, C.c_uint32, u32p, u32p, u32p, f64p, u32p, u32p, f64p,
                                              u32p, u32p, f64p, f64p]
         L.mlp_prec_bytes_per_apply.argtypes = [vp, C.POINTER(C.c_uint64)]
+        L.mlp_prec_profile.argtypes = [vp, C.c_uint32, C.c_uint32, u32p, f64p, C.POINTER(C.c_uint64), C.c_char_p,
+                                       C.c_uint32]
         L.mlp_pcg.argtypes = [vp, f64p, vp, f64p, C.c_double, C.c_uint32, C.c_int32, C.POINTER(Stats)]
         L.mlp_pcg_device.argtypes = [vp, vp, vp, vp, C.c_double, C.c_uint32, C.c_int32, C.POINTER(Stats), vp]
         L.mlp_generate_x0.argtypes = [f64p, C.c_uint32]
+        L.mlp_cheb_solve.argtypes = [vp, f64p, vp, f64p, C.c_double, C.c_double, C.c_double, C.c_uint32,
+                                     C.POINTER(Stats)]
+        L.mlp_cheb_solve_device.argtypes = [vp, vp, vp, vp, C.c_double, C.c_double, C.c_double, C.c_uint32,
+                                            C.POINTER(Stats), vp]
         L.mlp_pcg_device_noalloc.argtypes = [vp, vp, vp, vp, C.c_double, C.c_uint32, C.c_int32,
                                              C.POINTER(Stats), vp]
         L.mlp_launch_count.argtypes = [C.POINTER(C.c_uint64)]

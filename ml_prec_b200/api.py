@@ -99,8 +99,9 @@ def msplit_params(cfg: Config) -> dict:
 
     A config file overrides the command-line values (:179-180). Cases the
     reference leaves undefined are errors here: a missing config file (the
-    reference continues with an empty q list, :230-232 then :256) and the
-    dynamic inner iterations (unbounded loop, not supported)."""
+    reference continues with an empty q list, :230-232 then :256). Dynamic
+    inner iterations (inner_iter = dynamic, level_eps) are capped on the device
+    (the reference loops without a cap)."""
     if cfg.prec_conf_file:
         try:
             f = ConfigFile(cfg.prec_conf_file)
@@ -113,10 +114,12 @@ def msplit_params(cfg: Config) -> dict:
         stop = f.read("elim_stop", "degree")
         coarse_n = f.read("coarse_n", 0)
         nlevels = f.read("max_levels", 15)
+        level_eps = None
         if inner == "fixed":
             niters = [int(float(t)) for t in f.read("level_niter", "5").split()]
         elif inner == "dynamic":
-            raise ConfigError("inner_iter = dynamic is not supported")
+            niters = [5]
+            level_eps = [float(t) for t in f.read("level_eps", "1e-2").split()]
         else:
             raise ConfigError(f"Unknown inner_iter type: {inner}")
         if lu not in ("exact", "ilut"):
@@ -130,6 +133,7 @@ def msplit_params(cfg: Config) -> dict:
         else:
             raise ConfigError(f"Unknown elim_stop type: {stop}")
     else:
+        level_eps = None
         qs = list(cfg.sigmas)
         niters = list(cfg.niters)
         order = "original" if cfg.use_tails else "none"
@@ -141,7 +145,7 @@ def msplit_params(cfg: Config) -> dict:
     if not qs:
         raise ConfigError("empty q list")
     return dict(q=qs, niter=niters, order=order, coarse_n=coarse_n, max_levels=nlevels,
-                degree_max=degree_max)
+                degree_max=degree_max, level_eps=level_eps, use_tails=cfg.use_tails)
 
 
 class CSRMatrix:
@@ -249,6 +253,21 @@ class PrecBase:
         d["dval"] = dv[:Md]
         return d
 
+    def profile(self, reps=3):
+        """Per launch of the apply: (name, mean ms, algorithmic bytes), timed
+        launch by launch with CUDA events (mlp_prec_profile); run an apply
+        first, the replay uses its input."""
+        n = C.c_uint32()
+        check(lib().mlp_prec_profile(self.h, reps, 0, C.byref(n), None, None, None, 0))
+        cap = n.value
+        ms = np.zeros(max(cap, 1))
+        by = (C.c_uint64 * max(cap, 1))()
+        names = C.create_string_buffer(64 * max(cap, 1))
+        check(lib().mlp_prec_profile(self.h, reps, cap, C.byref(n), ptr(ms, f64p), by, names, 64))
+        raw = names.raw
+        return [(raw[64 * k:64 * (k + 1)].split(b"\0", 1)[0].decode(), float(ms[k]), int(by[k]))
+                for k in range(cap)]
+
     @property
     def bytes_per_apply(self):
         b = C.c_uint64()
@@ -262,14 +281,16 @@ class PrecBase:
 
 
 def _make(A: CSRMatrix, kind, fp32=False, q=(0.8,), niter=(5,), coarse_n=0, max_levels=15, degree_max=2,
-          order="simple_1", use_tails=True, sigma=(3.0,), ncheb=(2,), autotune=False):
+          order="simple_1", use_tails=True, sigma=(3.0,), ncheb=(2,), autotune=False, level_eps=None):
     qa = np.asarray(q, np.float64)
     na = np.asarray(niter, np.uint32)
     sa = np.asarray(sigma, np.float64)
     ca = np.asarray(ncheb, np.uint32)
+    ea = np.asarray(level_eps if level_eps is not None else [], np.float64)
     cfg = PrecCfg(kind, len(qa), ptr(qa, f64p), len(na), ptr(na, u32p), coarse_n, max_levels, degree_max,
                   ORDERS[order] if isinstance(order, str) else order, int(use_tails),
-                  len(sa), ptr(sa, f64p), len(ca), ptr(ca, u32p), int(fp32), int(autotune))
+                  len(sa), ptr(sa, f64p), len(ca), ptr(ca, u32p), int(fp32), int(autotune),
+                  len(ea), ptr(ea, f64p) if len(ea) else None)
     h = C.c_void_p()
     check(lib().mlp_prec_create(A.h, C.byref(cfg), C.byref(h)))
     return h
@@ -308,6 +329,14 @@ class Prec(PrecBase):
         self.fp32 = fp32
         self.h = _make(A, 1, fp32=fp32, **kw)
 
+    def lmin(self):
+        """Lower spectral bound of level 0 (Prec::lmin, cheb_prec.h:121)."""
+        return self.level_info(0)["lmin"]
+
+    def lmax(self):
+        """Upper spectral bound of level 0 (Prec::lmax, cheb_prec.h:122)."""
+        return self.level_info(0)["lmax"]
+
 
 @dataclasses.dataclass
 class SolverStats:
@@ -331,6 +360,26 @@ def PCGSolver(A: CSRMatrix, b, B: PrecBase, x=None, stats: Optional[SolverStats]
         flexible = bool(getattr(B, "fp32", False))
     st = Stats()
     check(lib().mlp_pcg(A.h, ptr(b, f64p), B.h, ptr(out, f64p), eps, maxit, int(flexible), C.byref(st)))
+    if stats is not None:
+        stats.niter = st.niter
+        stats.napply = st.napply
+        stats.init_norm = st.init_norm
+        stats.final_norm = st.final_norm
+        stats.final_rel = st.final_rel
+        stats.t_sol = st.t_solve_ms / 1e3
+        stats.t_const = st.t_setup_ms / 1e3
+    return out
+
+
+def ChebSolver(A: CSRMatrix, lmin: float, lmax: float, b, B: PrecBase, x=None,
+               stats: Optional[SolverStats] = None, eps: float = 1e-10, maxit: int = 0):
+    """ChebSolver(A, lmin, lmax, b, B, x, eps) (solvers.h:42-43, cheb.cc:9-100)
+    with host vectors; lmin, lmax bound the spectrum of B A (uh_cheb's level-0
+    bounds, Prec.lmin / Prec.lmax)."""
+    b = np.ascontiguousarray(b, np.float64)
+    out = np.empty_like(b) if x is None else x
+    st = Stats()
+    check(lib().mlp_cheb_solve(A.h, ptr(b, f64p), B.h, ptr(out, f64p), lmin, lmax, eps, maxit, C.byref(st)))
     if stats is not None:
         stats.niter = st.niter
         stats.napply = st.napply

@@ -193,6 +193,10 @@ int mlp_prec_create(const mlp_matrix* A, const mlp_prec_cfg* c, mlp_prec** out) 
         if (!c->nniter || !c->niter) MLP_THROW(ERR_CONFIG, "level_niter list is empty");
         cfg.q.assign(c->q, c->q + c->nq);
         cfg.niter.assign(c->niter, c->niter + c->nniter);
+        if (c->neps) {
+            if (!c->level_eps) MLP_THROW(ERR_CONFIG, "level_eps list is null");
+            cfg.eps.assign(c->level_eps, c->level_eps + c->neps);
+        }
         for (double q : cfg.q)
             if (!(q >= 0 && q < 1)) MLP_THROW(ERR_CONFIG, "q must lie in [0, 1)");
         cfg.coarse_n = c->coarse_n;
@@ -273,6 +277,23 @@ int mlp_prec_apply_host(mlp_prec* P, const double* f, double* x) {
     API_END
 }
 
+int mlp_prec_profile(mlp_prec* P, uint32_t reps, uint32_t cap, uint32_t* nops, double* ms, uint64_t* bytes,
+                     char* names, uint32_t name_len) {
+    API_BEGIN
+    if (!P || !nops) MLP_THROW(ERR_ARG, "null pointer");
+    std::vector<OpProfile> pr = profile_apply(*P->P, reps, P->s);
+    *nops = (uint32_t)pr.size();
+    for (uint32_t k = 0; k < pr.size() && k < cap; k++) {
+        if (ms) ms[k] = pr[k].ms;
+        if (bytes) bytes[k] = pr[k].bytes;
+        if (names && name_len) {
+            strncpy(names + (size_t)k * name_len, pr[k].name.c_str(), name_len - 1);
+            names[(size_t)k * name_len + name_len - 1] = 0;
+        }
+    }
+    API_END
+}
+
 int mlp_prec_nlevels(const mlp_prec* P, uint32_t* nl) {
     API_BEGIN
     if (!P || !nl) MLP_THROW(ERR_ARG, "null pointer");
@@ -289,6 +310,7 @@ int mlp_prec_level_info(const mlp_prec* P, uint32_t level, mlp_level_info* info)
     memset(info, 0, sizeof *info);
     info->N = L.N; info->nnz = L.nnz; info->M = L.M; info->Md = L.Md; info->n = L.n;
     info->niter = L.niter; info->ncheb = L.ncheb; info->direct = L.direct;
+    info->eps = L.eps;
     info->q = L.q; info->alpha = L.alpha; info->beta = L.beta; info->lmin = L.lmin; info->lmax = L.lmax;
     info->L_nnz = L.L.nnz; info->U_nnz = L.U.nnz;
     info->nwave_l = L.lw_off.empty() ? 0 : (uint32_t)L.lw_off.size() - 1;
@@ -401,6 +423,46 @@ int mlp_pcg_device_noalloc(const mlp_matrix* A, const double* b_dev, mlp_prec* P
         stats->t_solve_ms = st.t_total_ms;
         stats->t_setup_ms = P->setup_ms;
     }
+    return rc;
+    API_END
+}
+
+static void fill_stats(mlp_stats* stats, const PcgStats& st, double setup_ms) {
+    if (!stats) return;
+    stats->niter = st.niter;
+    stats->napply = st.napply;
+    stats->init_norm = st.init_norm;
+    stats->final_norm = st.final_norm;
+    stats->final_rel = st.final_rel;
+    stats->t_solve_ms = st.t_total_ms;
+    stats->t_setup_ms = setup_ms;
+}
+
+int mlp_cheb_solve_device(const mlp_matrix* A, const double* b_dev, mlp_prec* P, double* x_dev, double lmin,
+                          double lmax, double eps, uint32_t maxit, mlp_stats* stats, void* stream) {
+    API_BEGIN
+    if (!A || !b_dev || !P || !x_dev) MLP_THROW(ERR_ARG, "null pointer");
+    cudaStream_t s = stream ? (cudaStream_t)stream : P->s;
+    PcgStats st;
+    int rc = cheb_solve(A->A, b_dev, *P->P, x_dev, lmin, lmax, eps, maxit, st, s);
+    fill_stats(stats, st, P->setup_ms);
+    return rc;
+    API_END
+}
+
+int mlp_cheb_solve(const mlp_matrix* A, const double* b_host, mlp_prec* P, double* x_host, double lmin,
+                   double lmax, double eps, uint32_t maxit, mlp_stats* stats) {
+    API_BEGIN
+    if (!A || !b_host || !P || !x_host) MLP_THROW(ERR_ARG, "null pointer");
+    uint32_t n = A->A.nrow;
+    P->tmp_in.alloc(n);
+    P->tmp_out.alloc(n);
+    CK(cudaMemcpyAsync(P->tmp_in.p, b_host, (size_t)n * 8, cudaMemcpyHostToDevice, P->s));
+    PcgStats st;
+    int rc = cheb_solve(A->A, P->tmp_in.p, *P->P, P->tmp_out.p, lmin, lmax, eps, maxit, st, P->s);
+    CK(cudaMemcpyAsync(x_host, P->tmp_out.p, (size_t)n * 8, cudaMemcpyDeviceToHost, P->s));
+    CK(cudaStreamSynchronize(P->s));
+    fill_stats(stats, st, P->setup_ms);
     return rc;
     API_END
 }

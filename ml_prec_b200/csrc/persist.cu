@@ -164,6 +164,21 @@ __device__ __forceinline__ void step_rows(const PStep<T>& st) {
     }
 }
 
+// k_dense_gemv: a warp per row, lane l adds columns l, l + 32, ... in order
+// (in the operator's type CT), then the butterfly.
+template <class T, class CT>
+__device__ __forceinline__ void dense_rows(uint32_t n, const CT* __restrict__ C, const T* f, T* x) {
+    WarpIdx w;
+    for (uint32_t row = w.g; row < n; row += w.W) {
+        const CT* c = C + (size_t)row * n;
+        CT s = 0;
+        for (uint32_t j = w.lane; j < n; j += 32) s = fmadd_p(__ldg(c + j), (CT)f[j], s);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (w.lane == 0) x[row] = (T)s;
+    }
+}
+
 template <class T>
 __device__ void run_step(const PStep<T>& st) {
     switch (st.op) {
@@ -197,18 +212,10 @@ __device__ void run_step(const PStep<T>& st) {
             break;
         case PS_DENSE: {
             const uint32_t n = st.n0;
-            const T* C = st.a;
             const T* f = static_cast<const T*>(st.v[0]);
             T* x = static_cast<T*>(st.v[1]);
-            WarpIdx w;
-            for (uint32_t row = w.g; row < n; row += w.W) {
-                const T* c = C + (size_t)row * n;
-                T s = 0;
-                for (uint32_t j = w.lane; j < n; j += 32) s = fmadd_p(__ldg(c + j), f[j], s);
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-                if (w.lane == 0) x[row] = s;
-            }
+            if (st.mode == 1) dense_rows<T, double>(n, static_cast<const double*>(st.v[2]), f, x);
+            else dense_rows<T, T>(n, st.a, f, x);
             break;
         }
         case PS_SCALE: {
@@ -258,21 +265,115 @@ __device__ void run_step(const PStep<T>& st) {
     }
 }
 
+// Sum of v over the CTA (valid in thread 0), fixed order: warp butterflies,
+// then warp 0 adds the warp sums.
+__device__ __forceinline__ double cta_sum(double v) {
+    __shared__ double sh[PK_THREADS / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = 0;
+    if (threadIdx.x < 32) {
+        t = threadIdx.x < (PK_THREADS / 32) ? sh[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    }
+    __syncthreads();
+    return t;
+}
+
 template <class T>
 __global__ void __launch_bounds__(PK_THREADS, 2) k_persist(const PStep<T>* __restrict__ steps, uint32_t nsteps,
                                                             PBar* bar) {
     constexpr uint32_t NW = sizeof(PStep<T>) / 4;
     __shared__ __align__(16) uint32_t sbuf[2][NW];
+    __shared__ uint32_t spc[2];
+    __shared__ double s_init[PK_MAXLOOP];
+    __shared__ uint32_t s_cnt[PK_MAXLOOP];
+    __shared__ uint32_t s_next, s_total;
     const uint32_t* gsrc = reinterpret_cast<const uint32_t*>(steps);
-    if (threadIdx.x < NW) sbuf[0][threadIdx.x] = __ldg(gsrc + threadIdx.x);
+    auto fetch = [&](uint32_t pc, int b) {
+        if (threadIdx.x < NW) sbuf[b][threadIdx.x] = __ldg(gsrc + (size_t)pc * NW + threadIdx.x);
+        if (threadIdx.x == 0) spc[b] = pc;
+    };
+    fetch(0, 0);
+    if (threadIdx.x == 0) {
+        spc[1] = 0xffffffffu;
+        s_total = 0;
+    }
     __syncthreads();
     unsigned target = 0;
-    for (uint32_t i = 0; i < nsteps; i++) {
-        // the next descriptor is fetched while this step runs
-        if (i + 1 < nsteps && threadIdx.x < NW) sbuf[(i + 1) & 1][threadIdx.x] = __ldg(gsrc + (size_t)(i + 1) * NW + threadIdx.x);
-        run_step<T>(*reinterpret_cast<const PStep<T>*>(sbuf[i & 1]));
-        if (i + 1 < nsteps && !pk_barrier(bar, target)) break;
+    uint32_t pc = 0;
+    int cur = 0;
+    bool ok = true;
+    while (pc < nsteps) {
+        if (spc[cur] != pc) {  // after a jump: the step was not prefetched
+            __syncthreads();
+            fetch(pc, cur);
+            __syncthreads();
+        }
+        const PStep<T>& st = *reinterpret_cast<const PStep<T>*>(sbuf[cur]);
+        // the next descriptor in program order is fetched while this step runs
+        if (pc + 1 < nsteps) fetch(pc + 1, cur ^ 1);
+        uint32_t next = pc + 1;
+        bool sync_grid = true;
+        if (st.op == PS_NORM2) {
+            const T* v = static_cast<const T*>(st.v[0]);
+            double part = 0;
+            for_each(0, st.n0, [&](uint32_t i) {
+                double t = (double)v[i];
+                part += t * t;
+            });
+            part = cta_sum(part);
+            if (threadIdx.x == 0) bar->red[blockIdx.x] = part;
+        } else if (st.op == PS_LOOPTEST || st.op == PS_JUMP) {
+            // a decision every CTA takes alike: thread 0 computes it from data
+            // all CTAs see the same, and the CTA reads it back from shared memory
+            if (threadIdx.x < 32) {
+                uint32_t slot = st.mode & 255u;
+                uint32_t nx = pc + 1;
+                if (st.op == PS_LOOPTEST) {
+                    double t = 0;
+                    for (uint32_t b = threadIdx.x; b < gridDim.x; b += 32) t += ((volatile double*)bar->red)[b];
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+                    double nrm = sqrt(t);
+                    if (threadIdx.x == 0) {
+                        if (st.mode & 256u) {
+                            s_init[slot] = nrm;
+                            s_cnt[slot] = 0;
+                        } else if (nrm / s_init[slot] < st.s0) {
+                            nx = st.target;
+                        }
+                    }
+                } else if (threadIdx.x == 0) {
+                    if (++s_cnt[slot] >= PK_LOOP_CAP || ++s_total >= PK_TOTAL_CAP) {
+                        atomicCAS(&bar->err, 0, 2);
+                        nx = nsteps;  // stop
+                    } else {
+                        nx = st.target;
+                    }
+                }
+                if (threadIdx.x == 0) s_next = nx;
+            }
+            __syncthreads();
+            next = s_next;
+            sync_grid = false;  // nothing was written to global memory
+        } else {
+            run_step<T>(st);
+        }
+        if (next < nsteps) {
+            if (sync_grid) {
+                if (!pk_barrier(bar, target)) { ok = false; break; }
+            } else {
+                __syncthreads();
+            }
+        }
+        pc = next;
+        cur ^= 1;
     }
+    (void)ok;
     // Every CTA has left its last barrier wait once exitc reaches the grid
     // size, so the last one to leave resets the counters for the next launch.
     __syncthreads();
@@ -296,6 +397,8 @@ unsigned persist_grid() {
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persist<T>, PK_THREADS, 0));
         if (per_sm < 1) MLP_THROW(ERR_INTERNAL, "persistent apply kernel does not fit on an SM");
         g = (unsigned)num_sms() * (unsigned)std::min(per_sm, 2);
+        if (g > sizeof(PBar::red) / sizeof(double))
+            MLP_THROW(ERR_INTERNAL, "persistent apply grid exceeds its reduction buffer");
     }
     return g;
 }

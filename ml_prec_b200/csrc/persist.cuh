@@ -28,15 +28,27 @@ enum PsOp : uint32_t {
     PS_COPY = 8,    // k_copy: dst = src
     PS_TOF32 = 9,   // k_to_f32: float dst = double src
     PS_TOF64 = 10,  // k_to_f64: double dst = float src
+    // control flow of the dynamic inner iterations (multi_split_solve.cc:119-134)
+    PS_NORM2 = 11,     // per-CTA partial sums of v_i^2 into the reduction buffer
+    PS_LOOPTEST = 12,  // ||v|| from the partials; mode bit 8 set: record it as the
+                       // loop's initial norm; else jump to target when ||v|| / init < s0
+    PS_JUMP = 13,      // back to target; counts the loop's sweeps against its cap
 };
+
+// Loops (nested dynamic level calls) one program may hold; the sweeps of one
+// level call, and of all level calls of one launch, before the apply gives up
+// (the reference has no cap; nested loops multiply, so the total is capped too).
+static constexpr uint32_t PK_MAXLOOP = 16;
+static constexpr uint32_t PK_LOOP_CAP = 1000;
+static constexpr uint32_t PK_TOTAL_CAP = 100000;
 
 // One step. Fields not used by an op are zero.
 template <class T>
 struct alignas(16) PStep {
     uint32_t op;
     uint32_t lpr;    // lanes per row of the replaced kernel (1 = a serial row sum)
-    uint32_t mode;   // PS_UPDATE: 1 = also r -= Af u0
-    uint32_t pad;
+    uint32_t mode;   // PS_UPDATE: 1 = also r -= Af u0; loop ops: loop slot (+ 256 = record init)
+    uint32_t target; // PS_LOOPTEST / PS_JUMP: step index to go to
     uint32_t n0, n1; // sizes (rows; second bound)
     uint32_t pad2[2];
     const uint32_t* ia;
@@ -49,14 +61,16 @@ struct alignas(16) PStep {
 
 // Grid barrier state of one persistent plan (device memory, zeroed once).
 // count: arrivals (grows by the grid size per barrier, reset by the last CTA
-// to leave the kernel); exitc: CTAs that left; err: set when a barrier wait
-// ran out of its iteration limit (the kernel then stops early and the host
-// reports the error).
+// to leave the kernel); exitc: CTAs that left; err: 1 when a barrier wait ran
+// out of its iteration limit, 2 when a dynamic level iteration reached
+// PK_LOOP_CAP sweeps (the kernel then stops early and the host reports it).
+// red: one partial sum per CTA for the norms of the dynamic iterations.
 struct PBar {
     unsigned count;
     unsigned exitc;
     int err;
     unsigned pad;
+    double red[2048];
 };
 
 // Threads per CTA of k_persist.

@@ -1080,7 +1080,10 @@ static void build_level_msplit(Hierarchy& H, const BuildCfg& cfg, uint32_t level
     }
     if (lc.n) {
         ln.q = level + 1 < cfg.q.size() ? cfg.q[level + 1] : cfg.q.back();
-        ln.niter = level + 1 < cfg.niter.size() ? cfg.niter[level + 1] : cfg.niter.back();
+        // multi_split_constr.cc:256-264: a fixed count, or with dynamic inner
+        // iterations an eps (niter keeps the Level() default 0 then)
+        if (!cfg.eps.empty()) ln.eps = level + 1 < cfg.eps.size() ? cfg.eps[level + 1] : cfg.eps.back();
+        else ln.niter = level + 1 < cfg.niter.size() ? cfg.niter[level + 1] : cfg.niter.back();
         build_level_msplit(H, cfg, level + 1, S, s);
     } else {
         H.lv.pop_back();
@@ -1425,7 +1428,7 @@ std::unique_ptr<Hierarchy> build_hierarchy(const DCSR& A0, const BuildCfg& cfg, 
         l0.niter = 1;
         build_level_msplit(*H, cfg, 0, S, s);
         Level& last = *H->lv[H->nlevels - 1];
-        if (last.M == 0) { last.niter = 0; last.q = 0; }
+        if (last.M == 0) { last.niter = 0; last.eps = 0; last.q = 0; }
     } else {
         // cheb_constr.cc:292-365
         if (cfg.sigma.empty() || cfg.ncheb.empty()) MLP_THROW(ERR_CONFIG, "sigmas and niters must be non-empty");

@@ -15,6 +15,8 @@ struct BuildCfg {
     int kind = PREC_MSPLIT;
     std::vector<double> q{0.8};          // multi-split q per level (last repeats)
     std::vector<uint32_t> niter{5};      // inner iterations per level (entry 0 ignored)
+    std::vector<double> eps;             // inner_iter = dynamic: level_eps per level (entry 0
+                                         // ignored); empty = the fixed niter
     uint32_t coarse_n = 0, max_levels = 15, degree_max = 2;
     int order = ORDER_SIMPLE_1;
     int use_tails = 1;
@@ -37,6 +39,7 @@ struct Level {
     // parameters
     double q = 0;
     uint32_t niter = 0;
+    double eps = 0;  // dynamic inner iterations: sweep until ||f - A x|| / ||f|| < eps
     double alpha = 1, beta = 1, lmin = 0, lmax = 0;
     uint32_t ncheb = 0;
     // sizes

@@ -446,33 +446,36 @@ __global__ void k_chebk(uint32_t n, T* __restrict__ x2, const T* __restrict__ u1
     }
 }
 
-// Dense coarsest level: x = C^{-1} f, one warp per row.
-template <class T>
-__global__ void k_dense_gemv(uint32_t n, const T* __restrict__ C, const T* __restrict__ f, T* __restrict__ x) {
+// Dense coarsest level: x = C^{-1} f, one warp per row. The operator's type
+// CT may be wider than the vectors' T: the FP32 hierarchy keeps its coarsest
+// solve (the dense inverse, or the tabulated small-level operator standing in
+// for it) in FP64 and accumulates in FP64.
+template <class T, class CT = T>
+__global__ void k_dense_gemv(uint32_t n, const CT* __restrict__ C, const T* __restrict__ f, T* __restrict__ x) {
     // the operator is constant: its row is loaded before the wait (see RowPre)
     constexpr int CV = 16;
     uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
-    const T* c = C + (size_t)(row < n ? row : 0) * n;
-    T cv[CV];
+    const CT* c = C + (size_t)(row < n ? row : 0) * n;
+    CT cv[CV];
 #pragma unroll
     for (int k = 0; k < CV; k++) {
         uint32_t j = lane + 32 * k;
-        cv[k] = (row < n && j < n) ? c[j] : T(0);
+        cv[k] = (row < n && j < n) ? c[j] : CT(0);
     }
     pdl_wait();
     pdl_trigger();
     if (row >= n) return;
-    T s = 0;
+    CT s = 0;
 #pragma unroll
     for (int k = 0; k < CV; k++) {
         uint32_t j = lane + 32 * k;
-        if (j < n) s = fmadd(cv[k], f[j], s);
+        if (j < n) s = fmadd(cv[k], (CT)f[j], s);
     }
-    for (uint32_t j = lane + 32 * CV; j < n; j += 32) s = fmadd(c[j], f[j], s);
+    for (uint32_t j = lane + 32 * CV; j < n; j += 32) s = fmadd(c[j], (CT)f[j], s);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) x[row] = s;
+    if (lane == 0) x[row] = (T)s;
 }
 
 __global__ void k_to_f32(uint32_t n, const double* __restrict__ a, float* __restrict__ b) {
@@ -954,18 +957,27 @@ struct Builder {
     // shared-memory small-level kernel has none).
     bool persist_ok(uint32_t l) const {
         if (!persist || ps || autotune || !explicit_solves) return false;
-        if (H.lv[l]->N > persist_max_n) return false;
+        if (H.lv[l]->N > persist_max_n && !dynamic()) return false;
         if (small && small->valid() && !small->dense.p && small->first >= l) return false;
         return true;
+    }
+
+    bool dynamic() const {
+        for (uint32_t l = 0; l < H.nlevels; l++)
+            if (H.lv[l]->eps != 0) return true;
+        return false;
     }
 
     template <class Body>
     void persist_region(Body body) {
         std::vector<PStep<T>> v;
+        uint64_t b0 = bytes;
         ps = &v;
         body();
         ps = nullptr;
         if (v.empty()) return;
+        uint64_t region = bytes - b0;
+        bytes = b0;  // the region's bytes belong to its one launch
         pdesc->emplace_back();
         DBuf<uint8_t>& d = pdesc->back();
         d.alloc(v.size() * sizeof(PStep<T>));
@@ -973,12 +985,35 @@ struct Builder {
         const PStep<T>* dp = reinterpret_cast<const PStep<T>*>(d.p);
         uint32_t n = (uint32_t)v.size();
         PBar* bar = pbar;
-        op([=](cudaStream_t s) { launch_persist<T>(dp, n, bar, s); });
+        op([=](cudaStream_t s) { launch_persist<T>(dp, n, bar, s); }, "persistent");
+        bytes += region;
         persist_regions++;
         persist_steps += n;
     }
 
+    // FP32 hierarchy: the tabulated operator of the small levels in FP64
+    const SmallPlan<double>* small64 = nullptr;
+
+    // x = C f with an FP64 operator (vectors of type T, FP64 sums)
+    void dense64(uint32_t n, const double* C, const T* f, T* x) {
+        if (ps) {
+            PStep<T> st = pstep(PS_DENSE, 32, n, 0, nullptr, nullptr, nullptr, nullptr, f, x);
+            st.mode = 1;  // the operator is FP64
+            st.v[2] = const_cast<double*>(C);
+            ps->push_back(st);
+        } else {
+            op([=](cudaStream_t s) {
+                launch_k(k_dense_gemv<T, double>, grid_for((size_t)n * 32, 256), 256, 0, s, n, C, f, x);
+            }, "dense");
+        }
+        bytes += (uint64_t)n * n * 8 + 2ull * n * sizeof(T);
+    }
+
     bool small_call(uint32_t l, const T* f, T* x) {
+        if (small64 && small64->valid() && small64->dense.p && l == small64->first) {
+            dense64(small64->N0, small64->dense.p, f, x);
+            return true;
+        }
         if (!small || !small->valid() || l != small->first) return false;
         const SmallPlan<T>* sp = small;
         if (sp->dense.p) {
@@ -987,18 +1022,29 @@ struct Builder {
             if (ps) ps->push_back(pstep(PS_DENSE, 32, n, 0, nullptr, nullptr, C, nullptr, f, x));
             else op([=](cudaStream_t s) {
                 launch_k(k_dense_gemv<T>, grid_for((size_t)n * 32, 256), 256, 0, s, n, C, f, x);
-            });
+            }, "dense");
             bytes += (uint64_t)n * n * sizeof(T) + 2ull * n * sizeof(T);
             return true;
         }
         if (ps) MLP_THROW(ERR_INTERNAL, "small-level kernel inside a persistent region");
-        op([=](cudaStream_t s) { launch_small<T>(*sp, f, x, s); });
+        op([=](cudaStream_t s) { launch_small<T>(*sp, f, x, s); }, "small");
         bytes += sp->h.bytes_static + 2ull * sizeof(T) * sp->N0;
         return true;
     }
 
-    void op(std::function<void(cudaStream_t)> f) {
+    // Level whose call is being recorded (names the ops for profiling).
+    uint32_t cur_level = 0;
+    struct LevelScope {
+        uint32_t& r;
+        uint32_t saved;
+        LevelScope(uint32_t& r_, uint32_t l) : r(r_), saved(r_) { r = l; }
+        ~LevelScope() { r = saved; }
+    };
+
+    void op(std::function<void(cudaStream_t)> f, const char* name = "op") {
         plan.ops.push_back(std::move(f));
+        plan.names.push_back(std::string(name) + " L" + std::to_string(cur_level));
+        plan.bytes_start.push_back(bytes);
         plan.launches++;
     }
 
@@ -1011,14 +1057,14 @@ struct Builder {
         for (size_t d = 0; d < dt; d++) {
             uint32_t r0 = L.lw_off[d], r1 = L.lw_off[d + 1];
             if (r1 <= r0) continue;
-            op([=](cudaStream_t s) { launch_k(k_lwave<T>, grid_for(r1 - r0, 128), 128, 0, s, r0, r1, ia, ja, a, src, w); });
+            op([=](cudaStream_t s) { launch_k(k_lwave<T>, grid_for(r1 - r0, 128), 128, 0, s, r0, r1, ia, ja, a, src, w); }, "lwave");
         }
         if (dt < nw) {
             const uint32_t* off = L.lw_off_d.p;
             uint32_t d0 = (uint32_t)dt, d1 = (uint32_t)nw;
             op([=](cudaStream_t s) {
                 launch_k(k_lwave_tail<T>, 1, TAIL_THREADS, 0, s, d0, d1, off, ia, ja, a, src, w);
-            });
+            }, "lwave_tail");
         }
     }
     void coarse_diag(const Level& L, const T* src, T* w, T* out) {
@@ -1030,7 +1076,7 @@ struct Builder {
         const T* dv = dvals<T>(L);
         op([=](cudaStream_t s) {
             launch_k(k_lcoarse_diag<T>, grid_for(N - M, 128), 128, 0, s, M, R, N, ia, ja, a, src, w, dv, out);
-        });
+        }, "lcoarse_diag");
     }
     void usolve(const Level& L, const T* w, T* out) {
         const uint32_t* ia = L.Uf.ia.p;
@@ -1044,21 +1090,25 @@ struct Builder {
             if (o1 <= o0) continue;
             op([=](cudaStream_t s) {
                 launch_k(k_uwave<T>, grid_for(o1 - o0, 128), 128, 0, s, o1 - o0, rows + o0, ia, ja, a, w, out);
-            });
+            }, "uwave");
         }
         if (dt < nw) {
             const uint32_t* off = L.uw_off_d.p;
             uint32_t d0 = (uint32_t)dt, d1 = (uint32_t)nw;
             op([=](cudaStream_t s) {
                 launch_k(k_uwave_tail<T>, 1, TAIL_THREADS, 0, s, d0, d1, off, rows, ia, ja, a, w, out);
-            });
+            }, "uwave_tail");
         }
     }
     void direct(const Level& L, const T* f, T* x) {
         uint32_t n = L.N;
+        if (!std::is_same<T, double>::value) {
+            dense64(n, L.cinv.p, f, x);  // the coarsest solve stays FP64
+            return;
+        }
         const T* C = cinv<T>(L);
         if (ps) ps->push_back(pstep(PS_DENSE, 32, n, 0, nullptr, nullptr, C, nullptr, f, x));
-        else op([=](cudaStream_t s) { launch_k(k_dense_gemv<T>, grid_for((size_t)n * 32, 256), 256, 0, s, n, C, f, x); });
+        else op([=](cudaStream_t s) { launch_k(k_dense_gemv<T>, grid_for((size_t)n * 32, 256), 256, 0, s, n, C, f, x); }, "dense");
         bytes += (uint64_t)n * n * sizeof(T) + 2ull * n * sizeof(T);
     }
     // One application of the level's split operator on src: phase 1 (L solve
@@ -1098,7 +1148,7 @@ struct Builder {
         LaunchShape c{pick_lpr(R, L.P1.nnz), 256};
         if (autotune) c = tune_shape(1, sizeof(T), R, L.P1.nnz, tune_stream(), launch, st);
         if (ps) ps->push_back(pstep(PS_PHASE1, (uint32_t)c.lpr, R, N, ia, ja, a, dv, src, w, out));
-        else op([=](cudaStream_t s) { launch(c, s); });
+        else op([=](cudaStream_t s) { launch(c, s); }, "phase1");
         bytes += (uint64_t)L.P1.nnz * (4 + sizeof(T)) + 4ull * (R + 1) + sizeof(T) * (2ull * N + L.Md) ;
     }
     void phase2(const Level& L, const T* w, T* out) {
@@ -1121,7 +1171,7 @@ struct Builder {
         LaunchShape c{pick_lpr(M, L.G.nnz), 256};
         if (autotune) c = tune_shape(2, sizeof(T), M, L.G.nnz, tune_stream(), launch, st);
         if (ps) ps->push_back(pstep(PS_PHASE2, (uint32_t)c.lpr, M, 0, ia, ja, a, nullptr, w, out));
-        else op([=](cudaStream_t s) { launch(c, s); });
+        else op([=](cudaStream_t s) { launch(c, s); }, "phase2");
         bytes += (uint64_t)L.G.nnz * (4 + sizeof(T)) + 4ull * (M + 1) + sizeof(T) * (M + L.n + M);
     }
     void update(const Level& L, const T* u0, T* x, T* r, bool do_r) {
@@ -1147,7 +1197,7 @@ struct Builder {
         // rewritten before it is read in an apply
         if (autotune && do_r) c = tune_shape(3, sizeof(T), N, L.Af.nnz, tune_stream(), launch, st);
         if (ps) ps->push_back(pstep(PS_UPDATE, (uint32_t)c.lpr, N, 0, ia, ja, a, nullptr, u0, x, r, 0, 0, dr));
-        else op([=](cudaStream_t s) { launch(c, s); });
+        else op([=](cudaStream_t s) { launch(c, s); }, "update");
         bytes += sizeof(T) * 3ull * N + (do_r ? spmv_bytes(L.Af) : 0);
     }
 
@@ -1167,6 +1217,7 @@ struct Builder {
     // triangular solves in explicit form: each sweep is phase 1, the recursion
     // and phase 2; the correction sweeps update the residual in place.
     void ms(uint32_t l, const T* f, T* x) {
+        LevelScope scope(cur_level, l);
         if (persist_ok(l)) {
             persist_region([&] { ms(l, f, x); });
             return;
@@ -1176,6 +1227,7 @@ struct Builder {
         if (L.direct) { direct(L, f, x); return; }
         if (!explicit_solves) { ms_waves(l, f, x); return; }
         if (!ps && ms_merged(l, f, x)) return;
+        if (L.eps != 0) { ms_dynamic(l, f, x); return; }
         LevelWork<T>& w = W[l];
         uint32_t N = L.N, M = L.M;
         bool next = l + 1 < H.nlevels && L.n;
@@ -1190,7 +1242,7 @@ struct Builder {
             uint32_t nnz = L.Af.nnz, tm = L.Af.tile_max;
             T* r = w.r.p;
             if (ps) ps->push_back(pstep(PS_RESID, spmv_lpr(N, nnz, tm), N, 0, ia, ja, a, nullptr, x, r, f));
-            else op([=](cudaStream_t s) { launch_spmv<T>(N, nnz, ia, ja, a, x, r, f, s, tm); });
+            else op([=](cudaStream_t s) { launch_spmv<T>(N, nnz, ia, ja, a, x, r, f, s, tm); }, "residual");
             bytes += spmv_bytes(L.Af);
         }
         for (uint32_t it = 2; it <= L.niter; it++) {
@@ -1202,6 +1254,50 @@ struct Builder {
     }
 
     bool explicit_solves = true;
+
+    // MultiSplitPrec::solve(l, f, x) with dynamic inner iterations
+    // (multi_split_solve.cc:95-157 with li.eps != 0): after the first sweep,
+    // r = f - A x; stop when ||r|| / ||f|| < eps, else sweep on r and add the
+    // correction. The loop runs inside the persistent launch (a test step that
+    // every CTA evaluates alike, and a jump back), so the number of sweeps is
+    // decided on the device.
+    void ms_dynamic(uint32_t l, const T* f, T* x) {
+        if (!ps) MLP_THROW(ERR_CONFIG, "inner_iter = dynamic needs the persistent apply (MLP_PERSIST=0 is set)");
+        if (l >= PK_MAXLOOP) MLP_THROW(ERR_LIMIT, "dynamic inner iterations on more than 16 levels");
+        Level& L = *H.lv[l];
+        LevelWork<T>& w = W[l];
+        uint32_t N = L.N, M = L.M;
+        bool next = l + 1 < H.nlevels && L.n;
+        const uint32_t* ia = L.Af.ia.p;
+        const uint32_t* ja = L.Af.ja.p;
+        const T* a = vals<T>(L.Af);
+        T *r = w.r.p, *u0 = w.u0.p;
+        auto push = [&](uint32_t op, uint32_t mode, const void* v0, double s0 = 0) {
+            PStep<T> st = pstep(op, 1, N, 0, nullptr, nullptr, nullptr, nullptr, v0, nullptr);
+            st.mode = mode;
+            st.s0 = s0;
+            ps->push_back(st);
+            return ps->size() - 1;
+        };
+        push(PS_NORM2, l, f);
+        push(PS_LOOPTEST, l | 256u, nullptr);  // init_norm = ||f||
+        phase1(L, f, w.w.p, x);
+        if (next) ms(l + 1, w.w.p + M, x + M);
+        phase2(L, w.w.p, x);
+        uint32_t top = (uint32_t)ps->size();
+        ps->push_back(pstep(PS_RESID, spmv_lpr(N, L.Af.nnz, L.Af.tile_max), N, 0, ia, ja, a, nullptr, x, r, f));
+        push(PS_NORM2, l, r);
+        size_t test = push(PS_LOOPTEST, l, nullptr, L.eps);
+        phase1(L, r, w.w.p, u0);
+        if (next) ms(l + 1, w.w.p + M, u0 + M);
+        phase2(L, w.w.p, u0);
+        ps->push_back(pstep(PS_UPDATE, 1, N, 0, nullptr, nullptr, nullptr, nullptr, u0, x, nullptr, 0, 0, 0));
+        size_t jmp = push(PS_JUMP, l, nullptr);
+        (*ps)[jmp].target = top;
+        (*ps)[test].target = (uint32_t)ps->size();
+        // one extra sweep in the byte count (the number of sweeps is data dependent)
+        bytes += spmv_bytes(L.Af) + 3ull * sizeof(T) * N;
+    }
 
     // Merged sweep steps (k_merge_a) at levels of at most MERGE_MAX_N rows
     // without the autotuner (their arithmetic reproduces the fixed launch
@@ -1230,8 +1326,8 @@ struct Builder {
         };
 #define MERGE_A_CASE(U, P)                                                                          \
     if (lpu == U && lpp == P) {                                                                     \
-        if (mode == 0) op([=](cudaStream_t s) { go(k_merge_a<T, U, P, 0>, s); });                   \
-        else op([=](cudaStream_t s) { go(k_merge_a<T, U, P, 1>, s); });                             \
+        if (mode == 0) op([=](cudaStream_t s) { go(k_merge_a<T, U, P, 0>, s); }, "merge_a");                   \
+        else op([=](cudaStream_t s) { go(k_merge_a<T, U, P, 1>, s); }, "merge_a");                             \
         return;                                                                                     \
     }
         MERGE_A_CASE(1, 1) MERGE_A_CASE(1, 2) MERGE_A_CASE(1, 4) MERGE_A_CASE(1, 8)
@@ -1283,6 +1379,7 @@ struct Builder {
 
     // Wavefront form of ms (the L and U solves one wavefront at a time).
     void ms_waves(uint32_t l, const T* f, T* x) {
+        LevelScope scope(cur_level, l);
         Level& L = *H.lv[l];
         LevelWork<T>& w = W[l];
         uint32_t N = L.N, M = L.M;
@@ -1300,19 +1397,20 @@ struct Builder {
             const T* a = vals<T>(L.Af);
             uint32_t nnz = L.Af.nnz;
             T* r = w.r.p;
-            op([=](cudaStream_t s) { launch_spmv<T>(N, nnz, ia, ja, a, x, r, f, s); });
+            op([=](cudaStream_t s) { launch_spmv<T>(N, nnz, ia, ja, a, x, r, f, s); }, "residual");
             lsolve(L, r, w.w.p);
             coarse_diag(L, r, w.w.p, w.u0.p);
             if (has_next && L.n) ms(l + 1, w.w.p + M, w.u0.p + M);
             usolve(L, w.w.p, w.u0.p);
             T* u0 = w.u0.p;
-            op([=](cudaStream_t s) { launch_k(k_axpy1<T>, grid_for(N, 256), 256, 0, s, N, x, (const T*)u0); });
+            op([=](cudaStream_t s) { launch_k(k_axpy1<T>, grid_for(N, 256), 256, 0, s, N, x, (const T*)u0); }, "axpy");
             bytes += sweep_bytes(L) + spmv_bytes(L.Af) + 3ull * sizeof(T) * N;
         }
     }
 
     // Prec::solve(level, f, x) (cheb_solve.cc:13-123)
     void ch(uint32_t l, const T* f, T* x) {
+        LevelScope scope(cur_level, l);
         if (persist_ok(l)) {
             persist_region([&] { ch(l, f, x); });
             return;
@@ -1344,11 +1442,11 @@ struct Builder {
                 if (is_equal1(al)) return;
                 T a = (T)al;
                 if (ps) ps->push_back(pstep(PS_SCALE, 1, n, 0, nullptr, nullptr, nullptr, nullptr, v, nullptr, nullptr, (double)a));
-                else op([=](cudaStream_t s) { launch_k(k_scale<T>, grid_for(n, 256), 256, 0, s, n, v, a); });
+                else op([=](cudaStream_t s) { launch_k(k_scale<T>, grid_for(n, 256), 256, 0, s, n, v, a); }, "scale");
             };
             auto resid = [&](const T* u, T* y) {
                 if (ps) ps->push_back(pstep(PS_RESID, spmv_lpr(n, snnz, stm), n, 0, sia, sja, sa, nullptr, u, y, F));
-                else op([=](cudaStream_t s) { launch_spmv<T>(n, snnz, sia, sja, sa, u, y, F, s, stm); });
+                else op([=](cudaStream_t s) { launch_spmv<T>(n, snnz, sia, sja, sa, u, y, F, s, stm); }, "residual");
             };
             if (nch > 1) { ch(l + 1, F, u1); scale(u1, alpha); }
             else { ch(l + 1, F, x2); scale(x2, alpha); }
@@ -1362,7 +1460,7 @@ struct Builder {
                 double c = is_equal1(1 + beta) ? 1.0 : 1 + beta;
                 T ma = (T)alpha, cc = (T)c;
                 if (ps) ps->push_back(pstep(PS_CHEB2, 1, n, 0, nullptr, nullptr, nullptr, nullptr, x2, u1, nullptr, (double)ma, (double)cc));
-                else op([=](cudaStream_t s) { launch_k(k_cheb2<T>, grid_for(n, 256), 256, 0, s, n, x2, (const T*)u1, ma, cc); });
+                else op([=](cudaStream_t s) { launch_k(k_cheb2<T>, grid_for(n, 256), 256, 0, s, n, x2, (const T*)u1, ma, cc); }, "cheb2");
                 bytes += spmv_bytes(Ln.As) + 3ull * sizeof(T) * n;
             }
             for (uint32_t i = 3; i <= nch; i++) {
@@ -1375,13 +1473,13 @@ struct Builder {
                 T ma = (T)(-alpha), bb = (T)beta;
                 T* u0c = u0; T* u1c = u1; T* x2c = x2;
                 if (ps) ps->push_back(pstep(PS_CHEBK, 1, n, 0, nullptr, nullptr, nullptr, nullptr, x2c, u1c, u0c, (double)ma, (double)bb));
-                else op([=](cudaStream_t s) { launch_k(k_chebk<T>, grid_for(n, 256), 256, 0, s, n, x2c, (const T*)u1c, (const T*)u0c, ma, bb); });
+                else op([=](cudaStream_t s) { launch_k(k_chebk<T>, grid_for(n, 256), 256, 0, s, n, x2c, (const T*)u1c, (const T*)u0c, ma, bb); }, "chebk");
                 bytes += spmv_bytes(Ln.As) + 4ull * sizeof(T) * n;
             }
             T* xo = x + M;
             T* fin = x2;
             if (ps) ps->push_back(pstep(PS_COPY, 1, n, 0, nullptr, nullptr, nullptr, nullptr, fin, xo));
-            else op([=](cudaStream_t s) { launch_k(k_copy<T>, grid_for(n, 256), 256, 0, s, n, (const T*)fin, xo); });
+            else op([=](cudaStream_t s) { launch_k(k_copy<T>, grid_for(n, 256), 256, 0, s, n, (const T*)fin, xo); }, "copy");
         }
         if (explicit_solves) phase2(L, w.w.p, x);
         else usolve(L, w.w.p, x);
@@ -1402,7 +1500,7 @@ static void alloc_work(Hierarchy& H, std::vector<LevelWork<T>>& W) {
         if (L.direct) continue;
         W[l].w.alloc(L.N - L.Md + 1);
         if (H.kind == PREC_MSPLIT) {
-            if (L.niter >= 2) { W[l].r.alloc(L.N); W[l].u0.alloc(L.N); }
+            if (L.niter >= 2 || L.eps != 0) { W[l].r.alloc(L.N); W[l].u0.alloc(L.N); }
         } else if (l + 1 < H.nlevels) {
             uint32_t n = H.lv[l + 1]->N;
             W[l].cu0.alloc(n); W[l].cu1.alloc(n); W[l].cx2.alloc(n); W[l].ctmp.alloc(n);
@@ -1456,12 +1554,16 @@ static void builder_persist(Builder<T>& B, Prec& P) {
 
 void check_persist(Prec& P, cudaStream_t s) {
     if (!P.persist_regions) return;
-    PBar h;
-    CK(cudaMemcpyAsync(&h, P.pbar.p, sizeof h, cudaMemcpyDeviceToHost, s));
+    unsigned h[4];  // count, exitc, err, pad
+    CK(cudaMemcpyAsync(h, P.pbar.p, sizeof h, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    if (h.err) {
-        CK(cudaMemsetAsync(P.pbar.p, 0, sizeof(PBar), s));
+    int err = (int)h[2];
+    if (err) {
+        CK(cudaMemsetAsync(P.pbar.p, 0, sizeof h, s));
         CK(cudaStreamSynchronize(s));
+        if (err == 2)
+            MLP_THROW(ERR_MAXIT, "a dynamic level iteration reached its cap (" + std::to_string(PK_LOOP_CAP) +
+                                     " sweeps per level call, " + std::to_string(PK_TOTAL_CAP) + " per apply)");
         MLP_THROW(ERR_INTERNAL, "a grid barrier of the persistent apply gave up waiting");
     }
 }
@@ -1483,10 +1585,15 @@ std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, c
     P->pbar.zero(s);
     const char* ex = getenv("MLP_EXPLICIT");
     bool explicit_solves = !(ex && ex[0] == '0');
+    // With dynamic inner iterations a level call is no fixed linear operator,
+    // so the sub-hierarchy is neither tabulated nor packed for the one-CTA
+    // kernel; the whole apply runs persistent.
+    bool dyn = false;
+    for (uint32_t l = 0; l < H.nlevels; l++) dyn = dyn || H.lv[l]->eps != 0;
     if (!fp32) {
         alloc_work<double>(H, P->w64);
         P->sp64.reset(new SmallPlan<double>());
-        if (small_budget()) build_small<double>(H, *P->sp64, small_budget(), s);
+        if (small_budget() && !dyn) build_small<double>(H, *P->sp64, small_budget(), s);
         Builder<double> B{H, P->w64, P->plan, P->sp64.get()};
         B.explicit_solves = explicit_solves;
         B.stream = s;
@@ -1495,6 +1602,7 @@ std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, c
         if (H.kind == PREC_MSPLIT) B.ms(0, P->fin, P->fout);
         else B.ch(0, P->fin, P->fout);
         P->bytes_per_apply = B.bytes;
+        P->plan.bytes_total = B.bytes;
         P->persist_regions = B.persist_regions;
         P->persist_steps = B.persist_steps;
     } else {
@@ -1504,14 +1612,28 @@ std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, c
             if (!L.direct) { make_f32(L.P1, s); make_f32(L.G, s); }
             if (H.kind == PREC_CHEB && l > 0) make_f32(L.As, s);
             make_f32(L.dval, L.dval32, L.Md, s);
+            // the FP32 copy of a dense inverse serves only the one-CTA small-level
+            // kernel (sub-hierarchies too large to tabulate); the plan applies the
+            // FP64 inverse
             if (L.direct) make_f32(L.cinv, L.cinv32, (size_t)L.N * L.N, s);
         }
         alloc_work<float>(H, P->w32);
+        // The small levels: their tabulated operator stands in for the
+        // coarsest solve and is kept in FP64 (tabulated from the FP64 levels);
+        // when they are not tabulated, the one-CTA kernel runs them in FP32.
+        P->sp64.reset(new SmallPlan<double>());
         P->sp32.reset(new SmallPlan<float>());
-        if (small_budget()) build_small<float>(H, *P->sp32, small_budget(), s);
+        if (small_budget() && !dyn) {
+            build_small<double>(H, *P->sp64, small_budget(), s);
+            if (!P->sp64->dense.p) {
+                P->sp64.reset(new SmallPlan<double>());
+                build_small<float>(H, *P->sp32, small_budget(), s);
+            }
+        }
         P->f32.alloc(N0);
         P->z32.alloc(N0);
         Builder<float> B{H, P->w32, P->plan, P->sp32.get()};
+        B.small64 = P->sp64.get();
         B.explicit_solves = explicit_solves;
         B.stream = s;
         B.autotune = cfg.autotune != 0;
@@ -1522,15 +1644,16 @@ std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, c
         double* fout = P->fout;
         auto top = [&] {
             if (B.ps) B.ps->push_back(Builder<float>::pstep(PS_TOF32, 1, N0, 0, nullptr, nullptr, nullptr, nullptr, fin, f32));
-            else B.op([=](cudaStream_t st) { launch_k(k_to_f32, grid_for(N0, 256), 256, 0, st, N0, fin, f32); });
+            else B.op([=](cudaStream_t st) { launch_k(k_to_f32, grid_for(N0, 256), 256, 0, st, N0, fin, f32); }, "to_f32");
             if (H.kind == PREC_MSPLIT) B.ms(0, f32, z32);
             else B.ch(0, f32, z32);
             if (B.ps) B.ps->push_back(Builder<float>::pstep(PS_TOF64, 1, N0, 0, nullptr, nullptr, nullptr, nullptr, z32, fout));
-            else B.op([=](cudaStream_t st) { launch_k(k_to_f64, grid_for(N0, 256), 256, 0, st, N0, (const float*)z32, fout); });
+            else B.op([=](cudaStream_t st) { launch_k(k_to_f64, grid_for(N0, 256), 256, 0, st, N0, (const float*)z32, fout); }, "to_f64");
         };
         if (B.persist_ok(0)) B.persist_region(top);
         else top();
         P->bytes_per_apply = B.bytes + 12ull * N0 * 2;
+        P->plan.bytes_total = B.bytes;
         P->persist_regions = B.persist_regions;
         P->persist_steps = B.persist_steps;
     }
@@ -1549,6 +1672,39 @@ std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, c
     trace("graph");
     trace_flush();
     return P;
+}
+
+std::vector<OpProfile> profile_apply(Prec& P, uint32_t reps, cudaStream_t s) {
+    const Plan& pl = P.plan;
+    size_t n = pl.ops.size();
+    std::vector<OpProfile> out(n);
+    if (!n) return out;
+    std::vector<cudaEvent_t> ev(n + 1);
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    if (reps < 1) reps = 1;
+    for (uint32_t r = 0; r < reps; r++) {
+        for (size_t k = 0; k < n; k++) {
+            CK(cudaEventRecord(ev[k], s));
+            pl.ops[k](s);
+        }
+        CK(cudaEventRecord(ev[n], s));
+        CK(cudaEventSynchronize(ev[n]));
+        CK(cudaGetLastError());
+        for (size_t k = 0; k < n; k++) {
+            float ms = 0;
+            CK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+            out[k].ms += ms / reps;
+        }
+    }
+    count_launches((uint64_t)reps * pl.launches);
+    for (auto& e : ev) cudaEventDestroy(e);
+    for (size_t k = 0; k < n; k++) {
+        out[k].name = pl.names[k];
+        uint64_t end = k + 1 < n ? pl.bytes_start[k + 1] : pl.bytes_total;
+        out[k].bytes = end - pl.bytes_start[k];
+    }
+    check_persist(P, s);
+    return out;
 }
 
 void prec_apply_frame(Prec& P, cudaStream_t s) {
@@ -2031,6 +2187,188 @@ int pcg_solve(const DCSR& A, const double* b, Prec& P, double* x, double eps, ui
     read_stats(h, st, rc, msg);
     st.t_total_ms = ms;
     if (rc != OK) set_last_error(msg);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// ChebSolver (modules/solvers/cheb.cc:9-100): the Chebyshev iteration as the
+// outer solver, for a preconditioner with known spectral bounds (uh_cheb's
+// level-0 lmin / lmax). Like PCG it runs as one graph: start, the first step,
+// a conditional WHILE loop of steps, scatter. The recurrence coefficients
+// cheb(eta, k) (misc.cc:232-242) are tabulated on the host for every step the
+// cap allows, so they are the reference's values; the two state vectors of
+// the three-term recurrence alternate roles by the parity of the step count
+// (the new iterate overwrites the oldest one element by element), and the
+// current iterate is also written to one fixed vector for the residual.
+// Element arithmetic keeps the reference's separate multiplies and adds.
+// ---------------------------------------------------------------------------
+struct ChebDev {
+    double rr, init, eps;
+    unsigned ticket;
+    int status;      // 2: not finite
+    uint32_t niter;  // the reference's niter (1 at the start, 2 after step 1)
+    uint32_t maxit;
+};
+
+__global__ void k_cheb_start(ChebDev* d, double eps, uint32_t maxit) {
+    double init = sqrt(d->rr);
+    if (init * eps < 1e-14) eps = 1e-14 / init;  // check_and_replace_eps, solvers.cc:49-58
+    d->init = init;
+    d->eps = eps;
+    d->niter = 1;
+    d->maxit = maxit;
+    d->status = isfinite(init) ? 0 : 2;
+}
+
+// Step 1 (cheb.cc:38-46): u1 = x; x = alpha B r + u1 (dscal, then daxpy).
+__global__ void k_cheb_first(uint32_t n, double alpha, int scale, const double* __restrict__ z,
+                             double* __restrict__ u1, double* __restrict__ x, double* __restrict__ xcur) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double x0 = x[i];
+    u1[i] = x0;
+    double v = scale ? __dmul_rn(alpha, z[i]) : z[i];
+    v = __dadd_rn(v, x0);
+    x[i] = v;
+    xcur[i] = v;
+}
+
+// Steps 2+ (cheb.cc:58-72): x = u1 + alpha B r + beta (u1 - u0) with
+// alpha = 4/(lmax-lmin) T(k-1)/T(k), beta = T(k-2)/T(k), k = niter. The new
+// iterate goes to U[k % 2] (the oldest state vector, read first), the newest
+// is U[(k + 1) % 2].
+__global__ void k_cheb_step(uint32_t n, const ChebDev* __restrict__ d, const double* __restrict__ T, double c4,
+                            const double* __restrict__ z, double* U0, double* U1, double* __restrict__ xcur) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t k = d->niter;
+    double alpha = c4 * T[k - 1] / T[k];
+    double beta = T[k - 2] / T[k];
+    double* unew = (k & 1) ? U1 : U0;
+    const double* u1 = (k & 1) ? U0 : U1;
+    double a1 = u1[i], a0 = unew[i];
+    double v = __dadd_rn(__dadd_rn(a1, __dmul_rn(alpha, z[i])), __dmul_rn(beta, __dsub_rn(a1, a0)));
+    unew[i] = v;
+    xcur[i] = v;
+}
+
+// norm of the new residual, niter++ (cheb.cc:74-78), and the loop condition.
+__global__ void k_cheb_check(ChebDev* d, cudaGraphConditionalHandle h) {
+    double norm = sqrt(d->rr);
+    if (!isfinite(norm)) d->status |= 2;
+    d->niter++;
+    bool go = norm / d->init > d->eps && d->status == 0 && (d->niter - 1) < d->maxit;
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+int cheb_solve(const DCSR& A, const double* b, Prec& P, double* x, double lmin, double lmax, double eps,
+               uint32_t maxit, PcgStats& st, cudaStream_t s) {
+    if (maxit == 0) maxit = PCG_DEFAULT_MAXIT;
+    const Level& L0 = *P.H->lv[0];
+    const DCSR& Af = L0.Af;
+    uint32_t n = A.nrow;
+    if (n != L0.N) MLP_THROW(ERR_ARG, "matrix and preconditioner sizes differ");
+    if (!n) MLP_THROW(ERR_ARG, "empty system");
+    if (!(lmax > lmin) || !(lmin > 0)) MLP_THROW(ERR_ARG, "ChebSolver needs 0 < lmin < lmax");
+    double eta = (lmax + lmin) / (lmax - lmin);
+    // cheb(eta, k) for k = 0 .. maxit + 2, the reference's own formula (host libm)
+    std::vector<double> Th(maxit + 3);
+    for (uint32_t k = 0; k < Th.size(); k++) Th[k] = cheb_poly(eta, k);
+    DBuf<double> T(Th.size()), xf(n), bf(n), U0(n), U1(n), xcur(n), bnat(n), xnat(n);
+    unsigned G = (unsigned)std::max(1, std::min<int>((int)grid_for(n, RB), num_sms() * 4));
+    DBuf<double> partials(G);
+    DBuf<ChebDev> d(1);
+    T.upload(Th.data(), Th.size(), s);
+    d.zero(s);
+    CK(cudaMemcpyAsync(bnat.p, b, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
+    double* r = P.fin_buf.p;
+    double* z = P.fout_buf.p;
+    const double* x0 = x0_device(n, s);
+    double alpha1 = 2 / (lmax + lmin);
+    int scale1 = std::fabs(alpha1 - 1.0) <= 2.220446049250313e-16 ? 0 : 1;  // dscal skips alpha = 1
+    double c4 = 4 / (lmax - lmin);
+    ChebDev* dd = d.p;
+    cudaGraph_t g;
+    CK(cudaGraphCreate(&g, 0));
+    cudaGraphExec_t ex = nullptr;
+    try {
+        cudaGraphConditionalHandle h;
+        CK(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+        CK(cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        gather(n, L0.phi.p, bnat.p, bf.p, s);
+        gather(n, L0.phi.p, x0, U1.p, s);  // x = generate_x0
+        launch_spmv<double>(n, Af.nnz, Af.ia.p, Af.ja.p, Af.a.p, U1.p, r, bf.p, s, Af.tile_max);
+        k_dot_simple<<<G, RB, 0, s>>>(n, r, r, partials.p, &dd->ticket, &dd->rr);
+        k_cheb_start<<<1, 1, 0, s>>>(dd, eps, maxit);
+        P.plan.run(s);  // z = B r
+        k_cheb_first<<<grid_for(n, 256), 256, 0, s>>>(n, alpha1, scale1, z, U0.p, U1.p, xcur.p);
+        launch_spmv<double>(n, Af.nnz, Af.ia.p, Af.ja.p, Af.a.p, xcur.p, r, bf.p, s, Af.tile_max);
+        k_dot_simple<<<G, RB, 0, s>>>(n, r, r, partials.p, &dd->ticket, &dd->rr);
+        k_cheb_check<<<1, 1, 0, s>>>(dd, h);
+        cudaError_t le = cudaGetLastError();
+        cudaStreamCaptureStatus cs;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        CK(cudaStreamGetCaptureInfo(s, &cs, nullptr, nullptr, &deps, &ndeps));
+        std::vector<cudaGraphNode_t> dv(deps, deps + ndeps);
+        cudaGraph_t got;
+        CK(cudaStreamEndCapture(s, &got));
+        if (le != cudaSuccess) MLP_THROW(ERR_CUDA, cudaGetErrorString(le));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t cnode;
+        CK(cudaGraphAddNode(&cnode, g, dv.data(), dv.size(), &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        CK(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        P.plan.run(s);  // z = B r
+        k_cheb_step<<<grid_for(n, 256), 256, 0, s>>>(n, dd, T.p, c4, z, U0.p, U1.p, xcur.p);
+        launch_spmv<double>(n, Af.nnz, Af.ia.p, Af.ja.p, Af.a.p, xcur.p, r, bf.p, s, Af.tile_max);
+        k_dot_simple<<<G, RB, 0, s>>>(n, r, r, partials.p, &dd->ticket, &dd->rr);
+        k_cheb_check<<<1, 1, 0, s>>>(dd, h);
+        le = cudaGetLastError();
+        CK(cudaStreamEndCapture(s, &got));
+        if (le != cudaSuccess) MLP_THROW(ERR_CUDA, cudaGetErrorString(le));
+        CK(cudaStreamBeginCaptureToGraph(s, g, &cnode, nullptr, 1, cudaStreamCaptureModeThreadLocal));
+        scatter(n, L0.phi.p, xcur.p, xnat.p, s);
+        le = cudaGetLastError();
+        CK(cudaStreamEndCapture(s, &got));
+        if (le != cudaSuccess) MLP_THROW(ERR_CUDA, cudaGetErrorString(le));
+    } catch (...) {
+        cudaGraphDestroy(g);
+        throw;
+    }
+    ex = instantiate(g);
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, s));
+    cudaError_t lerr = cudaGraphLaunch(ex, s);
+    CK(cudaEventRecord(e1, s));
+    ChebDev hd;
+    CK(cudaMemcpyAsync(&hd, d.p, sizeof hd, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(x, xnat.p, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    cudaGraphExecDestroy(ex);
+    if (lerr != cudaSuccess) MLP_THROW(ERR_CUDA, std::string("graph launch: ") + cudaGetErrorString(lerr));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    check_persist(P, s);
+    uint32_t steps = hd.niter >= 2 ? hd.niter - 1 : 0;  // cheb.cc:84 niter--
+    count_launches(8 + P.plan.launches + (uint64_t)(steps ? steps - 1 : 0) * (4 + P.plan.launches));
+    st.niter = steps;
+    st.napply = steps;
+    st.init_norm = hd.init;
+    st.final_norm = std::sqrt(hd.rr);
+    st.final_rel = st.final_norm / hd.init;
+    st.t_total_ms = ms;
+    int rc = OK;
+    if (hd.status & 2) { rc = ERR_NOT_FINITE; set_last_error("non-finite residual norm in ChebSolver"); }
+    else if (steps >= maxit && st.final_rel > hd.eps) { rc = ERR_MAXIT; set_last_error("iteration cap reached"); }
     return rc;
 }
 

@@ -21,9 +21,22 @@ struct LevelWork {
 // applies the preconditioner z = B r, both vectors in level-0 frame order.
 struct Plan {
     std::vector<std::function<void(cudaStream_t)>> ops;
+    std::vector<std::string> names;      // per op: step and level ("phase1 L1", "persistent L1")
+    std::vector<uint64_t> bytes_start;   // per op: algorithmic bytes of the apply before it
+    uint64_t bytes_total = 0;
     size_t launches = 0;
     void run(cudaStream_t s) const;
 };
+
+// One timed replay of the apply, launch by launch (events between launches):
+// per op its name, mean device time and algorithmic bytes.
+struct OpProfile {
+    std::string name;
+    double ms = 0;
+    uint64_t bytes = 0;
+};
+struct Prec;
+std::vector<OpProfile> profile_apply(Prec& P, uint32_t reps, cudaStream_t s);
 
 template <class T>
 struct SmallPlan;
@@ -98,6 +111,11 @@ struct PcgStats {
 // preconditioner is applied in reduced precision).
 int pcg_solve(const DCSR& A, const double* b, Prec& P, double* x, double eps, uint32_t maxit, bool flexible,
               PcgStats& st, cudaStream_t s);
+
+// ChebSolver (cheb.cc:9-100) with x0 of generate_x0, b and x device vectors in
+// natural order, spectral bounds lmin < lmax of the preconditioned operator.
+int cheb_solve(const DCSR& A, const double* b, Prec& P, double* x, double lmin, double lmax, double eps,
+               uint32_t maxit, PcgStats& st, cudaStream_t s);
 
 // pcg_solve with every solver vector and reduction scratch in a static device
 // array instead of allocations (at most pcg_noalloc_max_n() unknowns).

@@ -58,10 +58,18 @@ void load(Vector& v, const std::string& filename, DumpType type) {
         for (uint i = 0; i < n; i++) is >> v[i];
         if (!is) THROW_EXCEPTION("Short vector file \"" << filename << "\"");
     } else if (type == BINARY) {
-        std::ifstream is(filename.c_str(), std::ios::binary);
+        std::ifstream is(filename.c_str(), std::ios::binary | std::ios::ate);
         if (!is.good()) THROW_EXCEPTION("Problem reading file \"" << filename << "\"");
+        const uint64_t bytes = (uint64_t)is.tellg();
+        is.seekg(0);
         uint n = 0;
         is.read(reinterpret_cast<char*>(&n), sizeof(uint));
+        if (n && bytes == sizeof(uint) + (uint64_t)n * sizeof(uint))
+            // the reference's BINARY vector dump writes n * sizeof(uint) bytes of the
+            // n doubles (vector.cc:42-46): half of the values are not in the file
+            THROW_EXCEPTION("Vector file \"" << filename << "\" holds " << n << " values in " << n * sizeof(uint)
+                            << " bytes (the reference's BINARY vector dump, vector.cc:42-46, drops half of "
+                               "them); write it as ASCII");
         v.assign(n, 0.0);
         is.read(reinterpret_cast<char*>(v.data()), (std::streamsize)n * sizeof(double));
         if (!is) THROW_EXCEPTION("Short vector file \"" << filename << "\"");
@@ -185,9 +193,13 @@ void CSRMatrix::load(const std::string& filename, DumpType type) {
     } else if (type == MATRIX_MARKET) {
         std::ifstream is(filename.c_str());
         if (!is.good()) THROW_EXCEPTION("Problem reading file \"" << filename << "\"");
+        // banner, then any '%' comment lines, then "rows cols nonzeros". The
+        // reference skips exactly one line after the banner (csrmatrix.cc:221-224),
+        // so it cannot read its own dumps (csrmatrix.cc:345-351 writes no comment
+        // line); reading past the comment lines accepts both.
         std::string line;
         std::getline(is, line);  // banner
-        std::getline(is, line);  // one comment line
+        while (is.peek() == '%') std::getline(is, line);
         uint nz = 0;
         is >> nrow >> ncol >> nz;
         // rows as ordered maps: a repeated (i, j) keeps its last value
@@ -472,6 +484,7 @@ static std::vector<T> number_list(const std::string& s) {
 MultiSplitPrec::MultiSplitPrec(const SkylineMatrix& A, const Config& cfg) {
     std::vector<double> qs;
     std::vector<uint32_t> niters;
+    std::vector<double> epss;  // inner_iter = dynamic
     std::string order_s;
     uint32_t coarse_n, nlevels, degree_max = 3;
     if (!cfg.prec_conf_file.empty()) {
@@ -492,7 +505,7 @@ MultiSplitPrec::MultiSplitPrec(const SkylineMatrix& A, const Config& cfg) {
         if (inner == "fixed")
             niters = number_list<uint32_t>(f->read<std::string>("level_niter", "5"));
         else if (inner == "dynamic")
-            THROW_EXCEPTION("inner_iter = dynamic is not implemented");
+            epss = number_list<double>(f->read<std::string>("level_eps", "1e-2"));
         else
             THROW_EXCEPTION("Unknown inner_iter type: " << inner);
         if (lu == "ilut")
@@ -530,6 +543,9 @@ MultiSplitPrec::MultiSplitPrec(const SkylineMatrix& A, const Config& cfg) {
     c.degree_max = degree_max;
     c.order = order_s == "none" ? MLP_ORDER_NONE : order_s == "original" ? MLP_ORDER_ORIGINAL
               : order_s == "block" ? MLP_ORDER_BLOCK : MLP_ORDER_SIMPLE_1;
+    c.use_tails = cfg.use_tails;  // the tail group of elim_order = original
+    c.neps = epss.size();
+    c.level_eps = epss.empty() ? nullptr : epss.data();
     c.fp32 = cfg.fp32;
     c.autotune = cfg.autotune;
     create(A, c);

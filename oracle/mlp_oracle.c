@@ -550,13 +550,18 @@ or_prec* or_prec_build(const or_csr* A, const or_prec_cfg* cfg, char* err, int e
         P->levels = (or_level*)calloc(P->nlevels + 1, sizeof(or_level));
         for (uint32_t l = 0; l < P->nlevels; l++) {
             P->levels[l].q = l >= cfg->nq ? cfg->q[cfg->nq - 1] : cfg->q[l];
+            /* multi_split_constr.cc:256-264: level 0 always one iteration; the
+             * others a fixed count or, with dynamic inner iterations, an eps
+             * (niter keeps the Level() default 0 then) */
             if (l == 0) P->levels[l].niter = 1;
+            else if (cfg->neps) P->levels[l].eps = l >= cfg->neps ? cfg->level_eps[cfg->neps - 1] : cfg->level_eps[l];
             else P->levels[l].niter = l >= cfg->nnit ? cfg->niter[cfg->nnit - 1] : cfg->niter[l];
         }
         csr_copy(&P->levels[0].A, A);
         rc = ms_construct(P, cfg, 0, err, errlen);
         if (rc == 0 && P->levels[P->nlevels - 1].M == 0) {
             P->levels[P->nlevels - 1].niter = 0;
+            P->levels[P->nlevels - 1].eps = 0;
             P->levels[P->nlevels - 1].q = 0;
         }
     } else {
@@ -644,9 +649,19 @@ static void solve_diag(const or_level* li, const double* f, double* x) {
     }
 }
 
-/* MultiSplitPrec::solve(level, f, x) (multi_split_solve.cc:59-157), fixed inner
- * iterations. */
-static void ms_solve(const or_prec* P, uint32_t level, const double* f, double* x) {
+static double or_dnrm2(const double* x, uint32_t n) {
+    double s = 0; /* blas.cc:52-54: sqrt(ddot(x, x)), a sequential sum */
+    for (uint32_t i = 0; i < n; i++) s += x[i] * x[i];
+    return sqrt(s);
+}
+
+/* Sweeps of one dynamic level call before the oracle gives up (the reference
+ * has no cap and would loop for ever). */
+#define OR_LEVEL_SWEEP_CAP 100000u
+
+/* MultiSplitPrec::solve(level, f, x) (multi_split_solve.cc:59-157): fixed inner
+ * iterations, or with li->eps != 0 sweeps until ||f - A x|| / ||f|| < eps. */
+static void ms_solve(or_prec* P, uint32_t level, const double* f, double* x) {
     const or_level* li = &P->levels[level];
     uint32_t N = li->N, M = li->M;
     uint32_t n = level < P->nlevels - 1 ? P->levels[level + 1].N : 0;
@@ -657,6 +672,7 @@ static void ms_solve(const or_prec* P, uint32_t level, const double* f, double* 
     double* wk = level_work(P, level);
     double *r = wk, *w = wk + N, *u0 = wk + 2 * (size_t)N, *x2 = wk + 3 * (size_t)N, *F = wk + 4 * (size_t)N;
     memcpy(r, f, 8 * (size_t)N);
+    double init_norm = li->eps != 0 ? or_dnrm2(r, N) : 0;
     solve_L(li, r, w);
     if (level < P->nlevels - 1) {
         memcpy(F, w + M, 8 * (size_t)n);
@@ -665,9 +681,13 @@ static void ms_solve(const or_prec* P, uint32_t level, const double* f, double* 
     }
     solve_U(li, w, x);
     solve_diag(li, r, x);
-    for (uint32_t it = 2; it <= li->niter; it++) {
+    for (uint32_t it = 2; li->eps != 0 || it <= li->niter; it++) {
         or_spmv(&li->A, x, r);
         for (uint32_t i = 0; i < N; i++) r[i] = f[i] - r[i];
+        if (li->eps != 0) {
+            if (or_dnrm2(r, N) / init_norm < li->eps) break;
+            if (it > OR_LEVEL_SWEEP_CAP) { P->apply_err = 1; break; }
+        }
         solve_L(li, r, w);
         if (level < P->nlevels - 1) {
             memcpy(F, w + M, 8 * (size_t)n);
@@ -740,8 +760,58 @@ static void ch_solve(const or_prec* P, uint32_t level, const double* f, double* 
 }
 
 void or_prec_apply(const or_prec* P, const double* f, double* x) {
-    if (P->kind == OR_PREC_MSPLIT) ms_solve(P, 0, f, x);
+    if (P->kind == OR_PREC_MSPLIT) ms_solve((or_prec*)P, 0, f, x);  /* apply_err is the only write */
     else ch_solve(P, 0, f, x);
+}
+
+/* ---- ChebSolver (cheb.cc:9-100) -------------------------------------------- */
+int or_cheb_solve(const or_csr* A, const double* b, const or_prec* P, double lmin, double lmax, double* x_out,
+                  double eps, uint32_t* niter_out, double* final_rel, uint32_t maxit) {
+    uint32_t n = A->nrow;
+    double* r = (double*)malloc(8 * (size_t)n);
+    double* buf[3];
+    for (int k = 0; k < 3; k++) buf[k] = (double*)malloc(8 * (size_t)n);
+    double *x = buf[0], *u1 = buf[1], *u0 = buf[2];
+    double eta = (lmax + lmin) / (lmax - lmin);
+    or_generate_x0(x, n);
+    or_spmv(A, x, r);
+    for (uint32_t i = 0; i < n; i++) r[i] = b[i] - r[i];
+    double norm = sqrt(ddot(r, r, n)), init_norm = norm;
+    uint32_t niter = 1;
+    if (init_norm * eps < 1e-14) eps = 1e-14 / init_norm; /* solvers.cc:49-58 */
+    /* step 1: u1 = x; x = alpha B r + u1 */
+    double alpha = 2 / (lmax + lmin), beta;
+    memcpy(u1, x, 8 * (size_t)n);
+    or_prec_apply(P, r, x);
+    dscal(alpha, x, n);
+    daxpy(1, u1, x, n);
+    or_spmv(A, x, r);
+    for (uint32_t i = 0; i < n; i++) r[i] = b[i] - r[i];
+    norm = sqrt(ddot(r, r, n));
+    niter++;
+    if (maxit == 0) maxit = 100000; /* the checker must always return */
+    int rc = 0;
+    while (norm / init_norm > eps) {
+        if (niter - 1 >= maxit) { rc = -3; break; }
+        double* t = u0; u0 = x; x = t; /* u0.swap(x) */
+        t = u1; u1 = u0; u0 = t;       /* u1.swap(u0) */
+        alpha = 4 / (lmax - lmin) * or_cheb(eta, niter - 1) / or_cheb(eta, niter);
+        beta = or_cheb(eta, niter - 2) / or_cheb(eta, niter);
+        or_prec_apply(P, r, x);
+        for (uint32_t k = 0; k < n; k++) x[k] = u1[k] + alpha * x[k] + beta * (u1[k] - u0[k]);
+        or_spmv(A, x, r);
+        for (uint32_t i = 0; i < n; i++) r[i] = b[i] - r[i];
+        norm = sqrt(ddot(r, r, n));
+        niter++;
+    }
+    niter--; /* cheb.cc:84 */
+    memcpy(x_out, x, 8 * (size_t)n);
+    *niter_out = niter;
+    *final_rel = norm / init_norm;
+    free(r);
+    for (int k = 0; k < 3; k++) free(buf[k]);
+    if (rc == 0 && P->apply_err) rc = -4;
+    return rc;
 }
 
 /* ---- PCG (pcg.cc:8-102) ---------------------------------------------------- */
@@ -787,6 +857,7 @@ int or_pcg_ex(const or_csr* A, const double* b, const or_prec* P, double* x, dou
         it++;
     }
     if (rc == 0 && it == 0) rc = -2;
+    if (rc == 0 && P->apply_err) rc = -4; /* a dynamic level iteration hit its cap */
     *niter_out = it;
     *final_rel = norm / init_norm;
     free(r); free(z); free(p); free(Ap);

@@ -57,11 +57,15 @@ typedef struct {
     /* uh_cheb (cheb_constr.cc:292-365) */
     uint32_t nsig;  const double* sigma;  /* beta per level */
     uint32_t nch;   const uint32_t* ncheb;/* Chebyshev degree per level */
+    /* multi-split inner_iter = dynamic (multi_split_constr.cc:198-203): level_eps
+     * per level, index 0 ignored, last one repeats; neps = 0 keeps fixed niter */
+    uint32_t neps;  const double* level_eps;
 } or_prec_cfg;
 
 typedef struct {
     uint32_t N, nnz, M, Md, niter;
     double q;
+    double eps;        /* dynamic inner iterations: stop when ||r|| / ||f|| < eps */
     or_csr A;          /* level matrix (level 0: copy of the input) */
     or_csr L, U;       /* factors (multi_split_prec.h:31-33) */
     uint32_t* map;     /* permuted -> original */
@@ -81,6 +85,7 @@ typedef struct {
     or_level* levels;
     double* work;       /* scratch for apply */
     char err[256];
+    int apply_err;      /* set when a dynamic level iteration hit its cap */
 } or_prec;
 
 or_prec* or_prec_build(const or_csr* A, const or_prec_cfg* cfg, char* err, int errlen);
@@ -101,6 +106,11 @@ int or_pcg(const or_csr* A, const double* b, const or_prec* P, double* x, double
 /* or_pcg with a choice of start: x0_mode 0 = generate_x0, 1 = zero. */
 int or_pcg_ex(const or_csr* A, const double* b, const or_prec* P, double* x, double eps,
               uint32_t* niter, double* final_rel, uint32_t maxit, int x0_mode);
+
+/* ChebSolver (cheb.cc:9-100) with the preconditioner's spectral bounds;
+ * *niter as the reference reports it. Returns 0, or -3 at the cap. */
+int or_cheb_solve(const or_csr* A, const double* b, const or_prec* P, double lmin, double lmax, double* x,
+                  double eps, uint32_t* niter, double* final_rel, uint32_t maxit);
 
 /* Differentiation form (no reference counterpart): dJ/d(ln K) per cell for
  * the SPE matrix with Dirichlet x-faces, given p (A p = b) and lambda

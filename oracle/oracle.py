@@ -36,13 +36,14 @@ class PrecCfg(C.Structure):
         ("order", C.c_int), ("use_tails", C.c_int),
         ("nsig", C.c_uint32), ("sigma", f64p),
         ("nch", C.c_uint32), ("ncheb", u32p),
+        ("neps", C.c_uint32), ("level_eps", f64p),
     ]
 
 
 class Level(C.Structure):
     _fields_ = [
         ("N", C.c_uint32), ("nnz", C.c_uint32), ("M", C.c_uint32), ("Md", C.c_uint32),
-        ("niter", C.c_uint32), ("q", C.c_double),
+        ("niter", C.c_uint32), ("q", C.c_double), ("eps", C.c_double),
         ("A", CSR), ("L", CSR), ("U", CSR),
         ("map", u32p), ("rmap", u32p), ("dval", f64p),
         ("alpha", C.c_double), ("beta", C.c_double), ("lmin", C.c_double), ("lmax", C.c_double),
@@ -78,6 +79,8 @@ def lib():
         L.or_pcg_ex.argtypes = [C.POINTER(CSR), f64p, C.c_void_p, f64p, C.c_double,
                                 C.POINTER(C.c_uint32), C.POINTER(C.c_double), C.c_uint32, C.c_int]
         L.or_grad_logk.argtypes = [C.c_uint32] * 3 + [f64p] * 3 + [C.c_int, f64p, f64p, f64p]
+        L.or_cheb_solve.argtypes = [C.POINTER(CSR), f64p, C.c_void_p, C.c_double, C.c_double, f64p, C.c_double,
+                                    C.POINTER(C.c_uint32), C.POINTER(C.c_double), C.c_uint32]
         L.or_cheb.argtypes = [C.c_double, C.c_uint32]
         L.or_cheb.restype = C.c_double
         _lib = L
@@ -156,14 +159,17 @@ class Prec:
     """Oracle preconditioner (multi-split or uh_cheb)."""
 
     def __init__(self, A: Matrix, kind="msplit", q=(0.8,), niter=(5,), coarse_n=0, max_levels=15,
-                 degree_max=2, order="simple_1", use_tails=True, sigma=(3.0,), ncheb=(2,)):
+                 degree_max=2, order="simple_1", use_tails=True, sigma=(3.0,), ncheb=(2,), level_eps=None):
+        """level_eps: per-level eps of msplit.cfg inner_iter = dynamic (index 0
+        ignored, the last repeats); None keeps the fixed niter."""
         self._keep = []
         qa = np.asarray(q, np.float64); na = np.asarray(niter, np.uint32)
         sa = np.asarray(sigma, np.float64); ca = np.asarray(ncheb, np.uint32)
-        self._keep += [qa, na, sa, ca, A]
+        ea = np.asarray(level_eps if level_eps is not None else [], np.float64)
+        self._keep += [qa, na, sa, ca, ea, A]
         cfg = PrecCfg(0 if kind == "msplit" else 1, len(qa), _p(qa, f64p), len(na), _p(na, u32p),
                       coarse_n, max_levels, degree_max, ORDERS[order], int(use_tails),
-                      len(sa), _p(sa, f64p), len(ca), _p(ca, u32p))
+                      len(sa), _p(sa, f64p), len(ca), _p(ca, u32p), len(ea), _p(ea, f64p) if len(ea) else None)
         err = C.create_string_buffer(256)
         self.h = lib().or_prec_build(A.c, C.byref(cfg), err, 256)
         if not self.h:
@@ -182,7 +188,7 @@ class Prec:
 
     def level(self, l):
         lv = lib().or_prec_level(self.h, l).contents
-        d = dict(N=lv.N, nnz=lv.nnz, M=lv.M, Md=lv.Md, niter=lv.niter, q=lv.q,
+        d = dict(N=lv.N, nnz=lv.nnz, M=lv.M, Md=lv.Md, niter=lv.niter, q=lv.q, eps=lv.eps,
                  alpha=lv.alpha, beta=lv.beta, lmin=lv.lmin, lmax=lv.lmax, ncheb=lv.ncheb)
         d["A"] = _csr_to_numpy(lv.A)
         if l < self.nlevels and lv.map:
@@ -207,6 +213,16 @@ def pcg(A: Matrix, b, P: Prec, eps=1e-8, maxit=0, x0_zero=False):
     rel = C.c_double(0)
     rc = lib().or_pcg_ex(A.c, _p(b, f64p), P.h, _p(x, f64p), eps, C.byref(it), C.byref(rel), maxit,
                          1 if x0_zero else 0)
+    return x, it.value, rel.value, rc
+
+
+def cheb_solve(A: Matrix, b, P: Prec, lmin, lmax, eps=1e-8, maxit=0):
+    """ChebSolver restated; returns (x, niter, final_rel, rc). rc -3: cap reached."""
+    b = np.ascontiguousarray(b, np.float64)
+    x = np.zeros(A.n)
+    it = C.c_uint32(0)
+    rel = C.c_double(0)
+    rc = lib().or_cheb_solve(A.c, _p(b, f64p), P.h, lmin, lmax, _p(x, f64p), eps, C.byref(it), C.byref(rel), maxit)
     return x, it.value, rel.value, rc
 
 
@@ -248,7 +264,7 @@ def ref_available():
 
 def run_ref(outdir, *, perm=None, csr=None, rhs=None, nx=60, ny=220, nz=85, c=1.0, prec="msplit",
             cfg=None, eps=1e-8, dump=False, no_solve=False, sigmas=None, niters=None, apply=None,
-            reps=1, dirichlet=True, timeout=None, ms_use_tails=None):
+            reps=1, dirichlet=True, timeout=None, ms_use_tails=None, solver=None, dump_formats=False):
     """Runs oracle/_ref/ref_driver; returns the parsed result.json."""
     args = [REF_DRIVER, "--out", outdir, "--nx", str(nx), "--ny", str(ny), "--nz", str(nz),
             "--c", repr(float(c)), "--prec", prec, "--eps", repr(float(eps)), "--reps", str(reps)]
@@ -274,15 +290,29 @@ def run_ref(outdir, *, perm=None, csr=None, rhs=None, nx=60, ny=220, nz=85, c=1.
         args += ["--apply", apply]
     if ms_use_tails is not None:
         args += ["--ms-use-tails", str(int(ms_use_tails))]
+    if solver is not None:
+        args += ["--solver", solver]
+    if dump_formats:
+        args += ["--dump-formats"]
     os.makedirs(outdir, exist_ok=True)
-    subprocess.run(args, check=True, stdout=subprocess.DEVNULL, timeout=timeout)
+    with open(os.path.join(outdir, "log.txt"), "w") as log:
+        subprocess.run(args, check=True, stdout=log, timeout=timeout)
     with open(os.path.join(outdir, "result.json")) as f:
-        return json.load(f)
+        res = json.load(f)
+    if solver == "cheb":
+        # ChebSolver's last log line: "#<steps>: relative -> ..." (cheb.cc:86-93)
+        import re
+        steps = re.findall(r"#(\d+): relative", open(os.path.join(outdir, "log.txt")).read())
+        res["niter"] = int(steps[-1])
+    return res
 
 
 def msplit_cfg_text(q="0.8", level_niter="5", elim_order="simple_1", degree_max=2, coarse_n=0,
-                    max_levels=15):
-    """An msplit.cfg in the reference's key = value format (project/msplit.cfg)."""
-    return (f"q = {q}\ninner_iter = fixed\nlevel_niter = {level_niter}\nlu_method = exact\n"
+                    max_levels=15, level_eps=None):
+    """An msplit.cfg in the reference's key = value format (project/msplit.cfg);
+    level_eps (a string of per-level values) selects inner_iter = dynamic."""
+    inner = (f"inner_iter = dynamic\nlevel_eps = {level_eps}\n" if level_eps is not None
+             else f"inner_iter = fixed\nlevel_niter = {level_niter}\n")
+    return (f"q = {q}\n{inner}lu_method = exact\n"
             f"elim_order = {elim_order}\nelim_stop = degree\ndegree_max = {degree_max}\n"
             f"coarse_n = {coarse_n}\nmax_levels = {max_levels}\n")

@@ -99,12 +99,13 @@ struct Args {
     std::string perm, csr, rhs, out = ".", cfgfile, prec = "msplit";
     uint nx = 60, ny = 220, nz = 85;
     double c = 0.1, eps = 1e-8;
-    bool dirichlet = true, dump = false, no_solve = false;
+    bool dirichlet = true, dump = false, no_solve = false, dump_formats = false;
     std::vector<double> sigmas;
     std::vector<uint> niters;
     std::string apply_in;  // optional: one preconditioner apply on this vector
     int reps = 1;
     int ms_use_tails = -1;  // >= 0: value of MultiSplitPrec::use_tails (see below)
+    std::string solver = "pcg";  // "cheb": ChebSolver with uh_cheb's level-0 bounds (main.cc:141-149)
 };
 
 static std::vector<double> parse_list_d(const char* s) {
@@ -136,12 +137,14 @@ int main(int argc, char** argv) {
         else if (k == "--eps") a.eps = atof(val());
         else if (k == "--no-dirichlet") a.dirichlet = false;
         else if (k == "--dump") a.dump = true;
+        else if (k == "--dump-formats") a.dump_formats = true;
         else if (k == "--no-solve") a.no_solve = true;
         else if (k == "--sigmas") a.sigmas = parse_list_d(val());
         else if (k == "--niters") { std::vector<double> d = parse_list_d(val()); for (double x : d) a.niters.push_back((uint)x); }
         else if (k == "--apply") a.apply_in = val();
         else if (k == "--reps") a.reps = atoi(val());
         else if (k == "--ms-use-tails") a.ms_use_tails = atoi(val());
+        else if (k == "--solver") a.solver = val();
         else { fprintf(stderr, "unknown arg %s\n", k.c_str()); return 2; }
     }
 
@@ -200,6 +203,14 @@ int main(int argc, char** argv) {
     if (a.dump) {
         dump_csr("A0.csr", A);
         write_raw("b.f64", &b[0], 8 * (size_t)b.size());
+    }
+    if (a.dump_formats) {
+        // the reference's own writers (csrmatrix.cc:302-355, vector.cc:18-49)
+        dump("ref_A.dat", A, BINARY);
+        dump("ref_A.crs", A, ASCII);
+        dump("ref_A.mm", A, MATRIX_MARKET);
+        dump("ref_b.crs", b, ASCII);
+        dump("ref_b.dat", b, BINARY);
     }
 
     Config cfg;
@@ -314,7 +325,14 @@ int main(int argc, char** argv) {
         double best = 0;
         for (int r = 0; r < a.reps; r++) {
             double ts = now();
-            PCGSolver(A, b, *B, x, stats, a.eps, NORM_L2, true);
+            if (a.solver == "cheb") {
+                // ChebSolver reports its step count only in its log ("#n: relative -> ...")
+                Prec* Pc = dynamic_cast<Prec*>(B);
+                if (!Pc) { fprintf(stderr, "ChebSolver needs the uh_cheb preconditioner\n"); return 2; }
+                ChebSolver(A, Pc->lmin(), Pc->lmax(), b, *Pc, x, a.eps, NORM_L2, true);
+            } else {
+                PCGSolver(A, b, *B, x, stats, a.eps, NORM_L2, true);
+            }
             double te = now() - ts;
             solves.push_back(te);
             if (r == 0 || te < best) best = te;

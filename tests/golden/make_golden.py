@@ -41,8 +41,12 @@ CASES = {
     "ms_original_16x22x8": ("layered", 2, 16, 22, 8, 1.0, "msplit", {"elim_order": "original", "use_tails": 1}),
     "ms_original_notails_20x22x10": ("iid", 6, 20, 22, 10, 1.0, "msplit",
                                      {"elim_order": "original", "use_tails": 0}),
+    "ms_dynamic_16x22x8_c01": ("layered", 2, 16, 22, 8, 0.1, "msplit", {"level_eps": "0 1e-2"}),
+    "ms_dynamic_12x22x6": ("iid", 1, 12, 22, 6, 1.0, "msplit", {"level_eps": "0 1e-1 1e-3"}),
     "ch_layered_16x22x8": ("layered", 2, 16, 22, 8, 1.0, "cheb", {"sigmas": [3.0], "niters": [4]}),
     "ch_iid_12x22x6": ("iid", 4, 12, 22, 6, 1.0, "cheb", {"sigmas": [3.0, 2.5], "niters": [2, 3]}),
+    # the same preconditioner with ChebSolver as the outer iteration (x, niter are ChebSolver's)
+    "chs_layered_16x22x8": ("layered", 2, 16, 22, 8, 1.0, "cheb", {"sigmas": [3.0], "niters": [4], "solver": "cheb"}),
 }
 
 # Configurations the reference rejects while it builds the hierarchy: the
@@ -111,7 +115,8 @@ def main():
                     fh.write(O.msplit_cfg_text(level_niter=opt.get("level_niter", "5"),
                                                elim_order=opt.get("elim_order", "simple_1"),
                                                degree_max=opt.get("degree_max", 2),
-                                               max_levels=opt.get("max_levels", 15)))
+                                               max_levels=opt.get("max_levels", 15),
+                                               level_eps=opt.get("level_eps")))
                 kw["cfg"] = cfg
                 if "use_tails" in opt:
                     # MultiSplitPrec reads use_tails without setting it (multi_split_prec.h:17);
@@ -120,6 +125,8 @@ def main():
             else:
                 kw["sigmas"] = opt["sigmas"]
                 kw["niters"] = opt["niters"]
+                if "solver" in opt:
+                    kw["solver"] = opt["solver"]
             res = O.run_ref(od, perm=perms[key], nx=nx, ny=ny, nz=nz, c=c, prec=prec, eps=1e-8, dump=True,
                             apply=os.path.join(od, "f_in.f64"), **kw)
             _, _, ia, ja, a = O.read_csr(os.path.join(od, "A0.csr"))

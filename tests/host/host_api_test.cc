@@ -5,6 +5,11 @@
 //       host logic only, no GPU: ConfigFile parsing, command-line parsing,
 //       matrix and vector file formats, the skyline transform, configuration
 //       errors raised before any device call. Prints "ok" on success.
+//   host_api_test ref-files <dir>
+//       files written by the reference's own writers (csrmatrix.cc:302-355,
+//       vector.cc:18-49; oracle/ref/ref_driver --dump-formats) load into the
+//       same matrix and vector as the raw arrays beside them (A0.csr, b.f64);
+//       the reference's BINARY vector file is refused with a message. No GPU.
 //   host_api_test solve <nx> <ny> <nz> <perm.bin> <cfg> <eps> <fp32> <x.bin>
 //       SPEMesh + Dirichlet matrix, MultiSplitPrec(A, cfg) from the config
 //       file, PCGSolver; writes x (BINARY vector format) and prints
@@ -12,7 +17,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <fstream>
+#include <iterator>
 #include <memory>
 
 #include "ml_prec.h"
@@ -152,10 +159,10 @@ static int cpu(const std::string& dir) {
     CHECK(throws([&] { MultiSplitPrec P(S, cfg); }, "Unknown elim_order type: optimal"));
     {
         std::ofstream f(dir + "/dyn.cfg");
-        f << "inner_iter = dynamic\n";
+        f << "inner_iter = adaptive\n";
     }
     cfg.prec_conf_file = dir + "/dyn.cfg";
-    CHECK(throws([&] { MultiSplitPrec P(S, cfg); }, "dynamic"));
+    CHECK(throws([&] { MultiSplitPrec P(S, cfg); }, "Unknown inner_iter type: adaptive"));
     cfg.prec_conf_file.clear();
     cfg.sigmas.assign(1, 1.5);
     CHECK(throws([&] { MultiSplitPrec P(S, cfg); }, "All sigmas must be < 1"));
@@ -164,6 +171,53 @@ static int cpu(const std::string& dir) {
     CHECK(throws([&] { Prec P(S, cc); }, "All sigmas must be > 1"));
     std::vector<double> t = {3, 1, 2, 5, 4, 9};
     CHECK(avg_time(t) == (2 + 3 + 4) / 3.0);
+    std::printf("ok\n");
+    return 0;
+}
+
+static std::vector<char> read_all(const std::string& fn) {
+    std::ifstream is(fn.c_str(), std::ios::binary);
+    return std::vector<char>((std::istreambuf_iterator<char>(is)), std::istreambuf_iterator<char>());
+}
+
+static int ref_files(const std::string& dir) {
+    // raw arrays: A0.csr = uint nrow, ncol, ia[nrow+1], ja[nnz], a[nnz]; b.f64 = doubles
+    std::vector<char> raw = read_all(dir + "/A0.csr");
+    CHECK(raw.size() >= 8);
+    uint nrow, ncol;
+    std::memcpy(&nrow, raw.data(), 4);
+    std::memcpy(&ncol, raw.data() + 4, 4);
+    std::vector<uint> ia(nrow + 1);
+    std::memcpy(ia.data(), raw.data() + 8, 4 * (size_t)(nrow + 1));
+    uint nnz = ia[nrow];
+    std::vector<uint> ja(nnz);
+    std::vector<double> a(nnz);
+    std::memcpy(ja.data(), raw.data() + 8 + 4 * (size_t)(nrow + 1), 4 * (size_t)nnz);
+    std::memcpy(a.data(), raw.data() + 8 + 4 * (size_t)(nrow + 1) + 4 * (size_t)nnz, 8 * (size_t)nnz);
+    std::vector<char> rb = read_all(dir + "/b.f64");
+    std::vector<double> b(rb.size() / 8);
+    std::memcpy(b.data(), rb.data(), rb.size());
+    auto same = [&](const SkylineMatrix& S, double tol, double atol) {
+        CHECK(S.rows() == nrow && S.cols() == ncol && S.get_ia().size() == ia.size());
+        for (uint i = 0; i <= nrow; i++) CHECK(S.get_ia()[i] == ia[i]);
+        for (uint k = 0; k < nnz; k++) {
+            CHECK(S.get_ja()[k] == ja[k]);
+            CHECK(std::fabs(S.get_a()[k] - a[k]) <= tol * std::fabs(a[k]) + atol);
+        }
+    };
+    SkylineMatrix S1, S2, S3;
+    S1.load(dir + "/ref_A.dat", BINARY, false);
+    same(S1, 0.0, 0.0);  // BINARY: the same bits
+    S2.load(dir + "/ref_A.crs", ASCII, false);
+    same(S2, 1e-15, 0.0);  // 16 significant digits
+    S3.load(dir + "/ref_A.mm", MATRIX_MARKET, true);
+    same(S3, 1e-15, 5e-16);  // 15 decimals after the point (fixed notation)
+    Vector v;
+    load(v, dir + "/ref_b.crs", ASCII);
+    CHECK(v.size() == b.size());
+    for (size_t i = 0; i < b.size(); i++) CHECK(std::fabs(v[i] - b[i]) <= 1e-15 * std::fabs(b[i]));
+    Vector w;
+    CHECK(throws([&] { load(w, dir + "/ref_b.dat", BINARY); }, "vector.cc:42-46"));
     std::printf("ok\n");
     return 0;
 }
@@ -195,6 +249,7 @@ int main(int argc, char** argv) {
     try {
         if (argc >= 3 && std::string(argv[1]) == "cpu") return cpu(argv[2]);
         if (argc >= 2 && std::string(argv[1]) == "solve") return solve(argc, argv);
+        if (argc >= 3 && std::string(argv[1]) == "ref-files") return ref_files(argv[2]);
         std::fprintf(stderr, "usage: host_api_test cpu <dir> | solve ...\n");
         return 2;
     } catch (const Exception& e) {

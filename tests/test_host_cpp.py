@@ -41,6 +41,34 @@ def test_host_logic(tmp_path):
     assert r.stdout.strip() == "ok"
 
 
+def test_reference_written_files_load(tmp_path):
+    """The reference's own writers (csrmatrix.cc:302-355, vector.cc:18-49), run
+    by the compiled reference driver, produce BINARY / ASCII / MatrixMarket
+    matrix files and ASCII / BINARY vector files of a 16x22x8 problem; the C++
+    host interface loads the matrices and the ASCII vector back to the
+    reference's own raw arrays, reads the MatrixMarket file the reference itself
+    cannot (it skips the size line as a comment, csrmatrix.cc:221-224), and
+    refuses the reference's BINARY vector file, which holds only n * 4 of its
+    n * 8 value bytes (vector.cc:42-46), with a message."""
+    from ml_prec_b200 import fields
+    from oracle import oracle as O
+    if not O.ref_available():
+        pytest.skip("reference driver not built")
+    exe = _build()
+    kx, ky, kz = fields.field("iid", 1)
+    perm = str(tmp_path / "perm.bin")
+    fields.write_perm_bin(perm, kx, ky, kz)
+    cfg = str(tmp_path / "msplit.cfg")
+    with open(cfg, "w") as f:
+        f.write(O.msplit_cfg_text())
+    out = str(tmp_path / "ref")
+    O.run_ref(out, perm=perm, nx=16, ny=22, nz=8, c=1.0, cfg=cfg, no_solve=True, dump=True, dump_formats=True,
+              timeout=300)
+    r = subprocess.run([exe, "ref-files", out], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.strip() == "ok"
+
+
 def test_driver_help():
     _build()
     r = subprocess.run([DRIVER, "-h"], capture_output=True, text=True, timeout=60)

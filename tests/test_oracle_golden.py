@@ -46,7 +46,11 @@ def test_apply_and_pcg_bit_exact(name):
     P = oracle_prec(A, g)
     z = P.apply(g["f_in"])
     assert np.array_equal(z, g["apply_out"])
-    x, it, rel, rc = O.pcg(A, g["b"], P, 1e-8)
+    if g["options"].get("solver") == "cheb":
+        lv = P.level(0)
+        x, it, rel, rc = O.cheb_solve(A, g["b"], P, lv["lmin"], lv["lmax"], 1e-8)
+    else:
+        x, it, rel, rc = O.pcg(A, g["b"], P, 1e-8)
     assert rc == 0
     assert it == int(g["niter"])
     assert np.array_equal(x, g["x"])

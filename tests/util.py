@@ -24,7 +24,8 @@ def prec_kwargs(g):
     if g["prec"] == "msplit":
         return dict(kind="msplit", q=(0.8,), niter=tuple(int(t) for t in str(o.get("level_niter", "5")).split()),
                     max_levels=o.get("max_levels", 15), degree_max=o.get("degree_max", 2),
-                    order=o.get("elim_order", "simple_1"), use_tails=bool(o.get("use_tails", 1)))
+                    order=o.get("elim_order", "simple_1"), use_tails=bool(o.get("use_tails", 1)),
+                    level_eps=(tuple(float(t) for t in o["level_eps"].split()) if "level_eps" in o else None))
     return dict(kind="cheb", sigma=tuple(o["sigmas"]), ncheb=tuple(o["niters"]), use_tails=True)
 
 
