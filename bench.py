@@ -230,8 +230,22 @@ def run_ours(args, ws, rank, local):
         P32 = M.MultiSplitPrec(A, fp32=True, **MSPLIT)
         x32, _ = host_solve(P32, EPS, True)
         x32b, st10 = host_solve(P32, 1e-10, True)
-        del P32
         nrm = np.linalg.norm(x_true)
+        # the loosest tolerance at which the FP32-form solution is within 1e-8 of
+        # the tight FP64 solution, with the device time of both forms there
+        Pm = M.MultiSplitPrec(A, **MSPLIT)
+        matched = None
+        for e_m in (1e-8, 1e-9, 1e-10, 1e-11, 1e-12):
+            xm, stm = host_solve(P32, e_m, True)
+            if np.linalg.norm(xm - x_true) / nrm <= 1e-8:
+                t32m = min(solve(P32, True, e_m).t_solve_ms for _ in range(3))
+                s64m = [solve(Pm, False, e_m) for _ in range(3)]
+                t64m = min(t.t_solve_ms for t in s64m)
+                matched = dict(eps=e_m, x_err=float(np.linalg.norm(xm - x_true) / nrm), iters=stm.niter,
+                               solve_ms=t32m, fp64_iters=s64m[0].niter, fp64_solve_ms=t64m,
+                               solve_speedup_vs_fp64=t64m / t32m)
+                break
+        del P32, Pm
         out["fp32"] = dict(s_per_step=float(np.mean(t32)), iters=st32.niter, setup_ms=st32.t_setup_ms,
                            solve_ms=st32.t_solve_ms, bytes_per_apply=nb32,
                            solve_speedup_vs_fp64=st64.t_solve_ms / st32.t_solve_ms,
@@ -243,7 +257,8 @@ def run_ours(args, ws, rank, local):
                            x_err_fp64_1e8=float(np.linalg.norm(x64 - x_true) / nrm),
                            x_err_fp32_1e10=float(np.linalg.norm(x32b - x_true) / nrm),
                            iters_1e10=st10.niter, rel_res_1e10=st10.final_rel,
-                           x_diff_fp32_vs_fp64_1e8=float(np.linalg.norm(x32 - x64) / nrm))
+                           x_diff_fp32_vs_fp64_1e8=float(np.linalg.norm(x32 - x64) / nrm),
+                           within_1e8_of_fp64=matched)
 
         # ---- adjoint gradient on the same mesh ----
         rng = np.random.default_rng(2)
@@ -278,6 +293,50 @@ def run_ours(args, ws, rank, local):
         out["ensemble"] = dict(fwd_ms=float(np.median(fwd)), adj_ms=float(np.median(adj)),
                                looped_ms=float(np.median(loop)), members=len(mine),
                                cells=int(sum(np.prod(dims[i]) for i in mine)))
+
+    # ---- per-launch profile of one apply (the roofline's dominant kernel) ----
+    # One apply of the plan, launch by launch, with CUDA events between the
+    # launches (mlp_prec_profile): per launch group its time and algorithmic
+    # bytes. With a 126 MB L2 the levels below the finest one are largely
+    # L2-resident, so their GB/s can exceed the HBM peak.
+    Pp = M.MultiSplitPrec(A, **MSPLIT)
+    Pp.solve(np.random.default_rng(3).standard_normal(N))
+    prof = Pp.profile(5)
+    groups = {}
+    for nm, ms_, by in prof:
+        g = groups.setdefault(nm, [0, 0.0, 0])
+        g[0] += 1
+        g[1] += ms_
+        g[2] += by
+    out["apply_profile"] = sorted(([nm, c, ms_, by] for nm, (c, ms_, by) in groups.items()), key=lambda t: -t[2])
+    out["apply_profile_ms"] = float(sum(t[1] for t in prof))
+    del Pp
+
+    if not args.no_forms:
+        # ---- the harder c = 0.1 problem (6 levels on this field) ----
+        A01, b01 = M.CSRMatrix.spe(NX, NY, NZ, kx, ky, kz, c=0.1, dirichlet=True)
+        b01_d = torch.from_numpy(b01).to(dev)
+        x01_d = torch.empty_like(b01_d)
+        t01, st01, nl01 = [], None, 0
+        for k in range(3 + max(3, args.steps // 2)):
+            flush_l2(flush)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            P01 = M.MultiSplitPrec(A01, **MSPLIT)
+            st01 = Stats()
+            check(lib().mlp_pcg_device(A01.h, C.c_void_p(b01_d.data_ptr()), P01.h, C.c_void_p(x01_d.data_ptr()),
+                                       EPS, 0, 0, C.byref(st01), C.c_void_p(stream.cuda_stream)))
+            e1.record(stream)
+            e1.synchronize()
+            nl01 = P01.nlevels
+            if k >= 3:
+                t01.append(e0.elapsed_time(e1) / 1e3)
+            del P01
+        out["c01"] = dict(s_per_step=float(np.mean(t01)), iters=st01.niter, levels=nl01,
+                          setup_ms=st01.t_setup_ms, solve_ms=st01.t_solve_ms, steps=len(t01))
+        del A01
 
     # ---- roofline: level-0 SpMV (staged kernel), events on its stream ----
     # 50 launches back to back between two events, alternating between two
@@ -346,7 +405,24 @@ def run_ours(args, ws, rank, local):
     return out
 
 
-def reference_cpu(steps, warmup, timeout=1800):
+def cpu_info():
+    """Host CPU model and the cores the process may use."""
+    model = "unknown"
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except AttributeError:
+        cores = os.cpu_count() or 1
+    return model, cores
+
+
+def reference_cpu(steps, warmup, timeout=1800, c=C_REACT):
     """The reference's own CPU build (oracle/_ref/ref_driver) on the same problem."""
     from oracle import oracle as O
     from ml_prec_b200 import fields
@@ -359,13 +435,54 @@ def reference_cpu(steps, warmup, timeout=1800):
         cfg = os.path.join(td, "msplit.cfg")
         with open(cfg, "w") as f:
             f.write(O.msplit_cfg_text())
-        r = O.run_ref(os.path.join(td, "out"), perm=perm, nx=NX, ny=NY, nz=NZ, c=C_REACT, prec="msplit",
+        r = O.run_ref(os.path.join(td, "out"), perm=perm, nx=NX, ny=NY, nz=NZ, c=c, prec="msplit",
                       cfg=cfg, eps=EPS, reps=warmup + steps, timeout=timeout)
     su = r["t_setup_all"][warmup:]
     so = r["t_solve_all"][warmup:]
     per = [x + y for x, y in zip(su, so)]
     return dict(value=float(np.mean(per)), setup=float(np.mean(su)), solve=float(np.mean(so)),
                 niter=r["niter"], steps=len(per))
+
+
+def reference_ensemble(count, timeout=900):
+    """min(count, cores) concurrent single-threaded reference processes, one
+    ensemble realization each (the ensemble form's meshes and fields, matrices
+    written in the reference's BINARY CSR format and loaded by its own reader):
+    aggregate solves per second over the wall time of the batch."""
+    from oracle import oracle as O
+    from ml_prec_b200 import ensemble, fields
+    if not O.ref_available():
+        return None
+    model, cores = cpu_info()
+    k = min(count, cores)
+    dims = ensemble.realization_dims(64)[:k]
+    with tempfile.TemporaryDirectory() as td:
+        cfg = os.path.join(td, "msplit.cfg")
+        with open(cfg, "w") as f:
+            f.write(O.msplit_cfg_text())
+        jobs = []
+        for i, d in enumerate(dims):
+            kx, ky, kz = fields.field("iid", 1000 + i)
+            A, b = O.assemble(*d, kx, ky, kz, 1.0, True)
+            fa, fb = os.path.join(td, f"A{i}.csr"), os.path.join(td, f"b{i}.f64")
+            O.write_csr(fa, A.ia, A.ja, A.a)
+            b.tofile(fb)
+            od = os.path.join(td, f"o{i}")
+            os.makedirs(od)
+            jobs.append([O.REF_DRIVER, "--out", od, "--csr", fa, "--rhs", fb, "--prec", "msplit", "--cfg", cfg,
+                         "--eps", repr(EPS)])
+        t0 = time.perf_counter()
+        procs = [subprocess.Popen(j, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL) for j in jobs]
+        rcs = [p.wait(timeout=timeout) for p in procs]
+        wall = time.perf_counter() - t0
+        per = []
+        for i in range(k):
+            if rcs[i] == 0:
+                r = json.load(open(os.path.join(td, f"o{i}", "result.json")))
+                per.append(r["t_setup"] + r["t_solve"])
+    return dict(processes=k, cores=cores, cpu_model=model, wall_s=wall, solves_per_s=len(per) / wall,
+                mean_solve_s=float(np.mean(per)) if per else None, failed=k - len(per),
+                cells=int(sum(np.prod(d) for d in dims)))
 
 
 def main():
@@ -433,14 +550,28 @@ def main():
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
     achieved = res["spmv_bytes"] / (res["spmv_ms"] / 1e3) / 1e9
+    prof = res["apply_profile"]
+    top = prof[0]  # [name, launches, ms, bytes] of the launch group with the most time in one apply
+    apply_groups = [{"launch": nm, "launches": c, "ms": round(ms_, 4), "MB": round(by / 1e6, 3),
+                     "GBps": round(by / (ms_ / 1e3) / 1e9, 1) if ms_ > 0 else None,
+                     "frac": round(by / (ms_ / 1e3) / 1e9 / hbm, 3) if ms_ > 0 else None}
+                    for nm, c, ms_, by in prof[:10]]
     st64 = res["st64"]
     cpu = None
     if not args.no_cpu_baseline:
         r = reference_cpu(1, 0)
         if r:
+            model, cores = cpu_info()
             cpu = {"value": r["value"], "unit": UNIT, "cores": 1, "kind": "reference",
                    "sample": "one full setup+PCG solve of the same 60x220x85 problem (single-threaded reference)",
-                   "iters": r["niter"], "setup_s": r["setup"], "solve_s": r["solve"]}
+                   "iters": r["niter"], "setup_s": r["setup"], "solve_s": r["solve"],
+                   "host_cpu": model, "host_cores": cores}
+            if not args.no_forms:
+                r01 = reference_cpu(1, 0, c=0.1)
+                if r01:
+                    cpu["c01"] = {"value": r01["value"], "iters": r01["niter"], "setup_s": r01["setup"],
+                                  "solve_s": r01["solve"]}
+                cpu["ensemble_concurrent"] = reference_ensemble(64)
     line = {
         "metric": METRIC, "value": t_step, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t_step * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
@@ -453,6 +584,7 @@ def main():
         "iters": st64.niter, "setup_ms": st64.t_setup_ms, "solve_ms": st64.t_solve_ms,
         "forms": None if ens is None else {
             "autotuned_fp64": res.get("autotuned"),
+            "c01": res.get("c01"),
             "fp32_prec": res["fp32"],
             "adjoint": res["adjoint"],
             "ensemble": dict(ens, realizations=64, solves_per_s=64 / (ens["fwd_ms"] / 1e3),
@@ -461,15 +593,25 @@ def main():
         },
         "e2e": res.get("e2e"),
         "gpu_launches": res["nlaunch"],
-        "roofline": {"bound": "hbm", "kernel": "level-0 CSR SpMV y = A x (k_spmv_staged, pipelined tiles), 1.12M rows",
-                     "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+        "roofline": {"bound": "hbm", "kernel": f"{top[0]} (the apply's launch group with the most device time)",
+                     "achieved": top[3] / (top[2] / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
+                     "frac": top[3] / (top[2] / 1e3) / 1e9 / hbm,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s",
-                     "bytes_per_launch": res["spmv_bytes"], "ms_per_launch": res["spmv_ms"],
-                     "timing": "50 launches back to back in one CUDA graph, two matrix copies alternated "
-                               "(232 MB > L2), CUDA events around the replay",
-                     "traffic": SPMV_DRAM_TRAFFIC,
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch of the same kernel "
-                                       "on this matrix (profiles/spmv_level0_60x220x85.md)"},
+                     "bytes_per_launch": top[3] / top[1], "ms_per_launch": top[2] / top[1],
+                     "timing": "one apply replayed launch by launch (mlp_prec_profile, 5 replays), CUDA events "
+                               "between the launches on the apply's stream",
+                     "traffic": None,
+                     "traffic_source": "see profiles/ for the ncu DRAM traffic of this kernel",
+                     "apply_groups": apply_groups,
+                     "apply_ms_launch_by_launch": res["apply_profile_ms"],
+                     "spmv_level0": {"kernel": "level-0 CSR SpMV y = A x (k_spmv_staged, pipelined tiles)",
+                                     "achieved": achieved, "frac": achieved / hbm,
+                                     "bytes_per_launch": res["spmv_bytes"], "ms_per_launch": res["spmv_ms"],
+                                     "timing": "50 launches back to back in one CUDA graph, two matrix copies "
+                                               "alternated (232 MB > L2)",
+                                     "traffic": SPMV_DRAM_TRAFFIC,
+                                     "traffic_source": "taken from profiles/spmv_level0_60x220x85.md (an ncu capture "
+                                                       "of one launch on this matrix), not measured in this run"}},
         "prec_bytes_per_apply": res["nb64"],
         "cpu_baseline": cpu,
         "clocks": res["clocks"],

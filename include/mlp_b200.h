@@ -41,6 +41,11 @@ typedef struct mlp_prec mlp_prec;     /* device-resident preconditioner hierarch
 /* Preconditioner kinds. */
 #define MLP_PREC_MSPLIT 0 /* MultiSplitPrec, multi_split_prec.h:15-113 */
 #define MLP_PREC_CHEB 1   /* Prec ("uh_cheb"), cheb_prec.h:13-127     */
+#define MLP_PREC_SYM 2    /* SymPrec, sym_prec.h:13-27: the uh_cheb Prec of the symmetric
+                             part (a_ij = max(a_ij, a_ji) off the diagonal), applied as a
+                             PCG solve to 1e-14 from generate_x0 (sym_prec.cc:8-40); takes
+                             the uh_cheb fields of mlp_prec_cfg. The outer mlp_pcg on such a
+                             handle runs host-driven, one device solve per application. */
 
 /* Node orderings (msplit.cfg key elim_order, multi_split_constr.cc:246-249). */
 #define MLP_ORDER_NONE 0

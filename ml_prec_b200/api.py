@@ -338,6 +338,24 @@ class Prec(PrecBase):
         return self.level_info(0)["lmax"]
 
 
+class SymPrec(PrecBase):
+    """SymPrec(A, cfg) (sym_prec.h:13-27) built on the GPU: the uh_cheb Prec of
+    the symmetric part of A (a_ij = max(a_ij, a_ji) off the diagonal), applied
+    as a PCG solve to 1e-14 (sym_prec.cc:8-40)."""
+
+    def __init__(self, A: CSRMatrix, cfg: Optional[Config] = None, fp32: bool = False, **kw):
+        if cfg is not None:
+            if any(s <= 1 for s in cfg.sigmas):
+                raise ConfigError("All sigmas must be > 1")
+            kw.setdefault("sigma", tuple(cfg.sigmas))
+            kw.setdefault("ncheb", tuple(cfg.niters))
+            kw.setdefault("use_tails", cfg.use_tails)
+            fp32 = fp32 or cfg.fp32
+        self.A = A
+        self.fp32 = fp32
+        self.h = _make(A, 2, fp32=fp32, **kw)
+
+
 @dataclasses.dataclass
 class SolverStats:
     niter: int = 0

@@ -22,10 +22,15 @@ struct mlp_matrix {
 };
 
 struct mlp_prec {
-    std::unique_ptr<Prec> P;
+    std::unique_ptr<Prec> P;  // SymPrec: the uh_cheb hierarchy of the symmetric part
     cudaStream_t s = nullptr;
     double setup_ms = 0;
     DBuf<double> tmp_in, tmp_out;
+    // SymPrec (sym_prec.h:13-27): the symmetric part and the accuracy of the
+    // inner solve that applies the preconditioner
+    bool sym = false;
+    DCSR Asym;
+    double sym_eps = 1e-14;
     ~mlp_prec() {
         P.reset();
         if (s) cudaStreamDestroy(s);
@@ -187,7 +192,9 @@ int mlp_prec_create(const mlp_matrix* A, const mlp_prec_cfg* c, mlp_prec** out) 
     BuildCfg cfg;
     cfg.kind = c->kind;
     cfg.autotune = c->autotune;
-    if (c->kind != MLP_PREC_MSPLIT && c->kind != MLP_PREC_CHEB) MLP_THROW(ERR_CONFIG, "unknown preconditioner kind");
+    if (c->kind != MLP_PREC_MSPLIT && c->kind != MLP_PREC_CHEB && c->kind != MLP_PREC_SYM)
+        MLP_THROW(ERR_CONFIG, "unknown preconditioner kind");
+    if (c->kind == MLP_PREC_SYM) cfg.kind = PREC_CHEB;  // the uh_cheb Prec of the symmetric part
     if (c->kind == MLP_PREC_MSPLIT) {
         if (!c->nq || !c->q) MLP_THROW(ERR_CONFIG, "q list is empty");
         if (!c->nniter || !c->niter) MLP_THROW(ERR_CONFIG, "level_niter list is empty");
@@ -224,7 +231,13 @@ int mlp_prec_create(const mlp_matrix* A, const mlp_prec_cfg* c, mlp_prec** out) 
         CK(cudaEventCreate(&e0));
         CK(cudaEventCreate(&e1));
         CK(cudaEventRecord(e0, H->s));
-        H->P = make_prec(A->A, cfg, c->fp32 != 0, H->s);
+        if (c->kind == MLP_PREC_SYM) {
+            H->sym = true;
+            symmetrize(A->A, H->Asym, H->s);
+            H->P = make_prec(H->Asym, cfg, c->fp32 != 0, H->s);
+        } else {
+            H->P = make_prec(A->A, cfg, c->fp32 != 0, H->s);
+        }
         CK(cudaEventRecord(e1, H->s));
         CK(cudaEventSynchronize(e1));
         float ms = 0;
@@ -247,7 +260,16 @@ int mlp_prec_destroy(mlp_prec* P) {
     API_END
 }
 
+// SymPrec::solve (sym_prec.cc:8-17): PCGSolver(Asym, f, B, x, 1e-14) from
+// generate_x0; the reference throws when that solve fails, so does this.
+static void apply_sym(mlp_prec* P, const double* f, double* x, cudaStream_t s) {
+    PcgStats st;
+    int rc = pcg_solve(P->Asym, f, *P->P, x, P->sym_eps, 0, P->P->fp32, st, s);
+    if (rc != OK) MLP_THROW(rc, std::string("SymPrec inner solve: ") + last_error());
+}
+
 static void apply_natural(mlp_prec* P, const double* f, double* x, cudaStream_t s) {
+    if (P->sym) { apply_sym(P, f, x, s); return; }
     Prec& Q = *P->P;
     const Level& L0 = *Q.H->lv[0];
     gather(L0.N, L0.phi.p, f, Q.fin_buf.p, s);
@@ -359,11 +381,18 @@ int mlp_prec_bytes_per_apply(const mlp_prec* P, uint64_t* bytes) {
 static int pcg_common(const mlp_matrix* A, const double* b_dev, mlp_prec* P, double* x_dev, double eps,
                       uint32_t maxit, int32_t flexible, mlp_stats* stats, cudaStream_t s) {
     PcgStats st;
-    // MLP_PCG_HOSTLOOP=1 selects the host-driven loop (the tests check the
-    // device-resident solve against it)
-    const char* hl = getenv("MLP_PCG_HOSTLOOP");
-    int rc = (hl && hl[0] == '1') ? pcg_solve_hostloop(A->A, b_dev, *P->P, x_dev, eps, maxit, flexible != 0, st, s)
+    int rc;
+    if (P->sym) {
+        // the outer PCG on A itself; each application is a solve with Asym
+        rc = pcg_solve_cb(A->A, b_dev, [&](const double* r, double* z) { apply_sym(P, r, z, s); }, x_dev, eps, maxit,
+                          flexible != 0, st, s);
+    } else {
+        // MLP_PCG_HOSTLOOP=1 selects the host-driven loop (the tests check the
+        // device-resident solve against it)
+        const char* hl = getenv("MLP_PCG_HOSTLOOP");
+        rc = (hl && hl[0] == '1') ? pcg_solve_hostloop(A->A, b_dev, *P->P, x_dev, eps, maxit, flexible != 0, st, s)
                                   : pcg_solve(A->A, b_dev, *P->P, x_dev, eps, maxit, flexible != 0, st, s);
+    }
     if (stats) {
         stats->niter = st.niter;
         stats->napply = st.napply;
@@ -413,6 +442,7 @@ int mlp_pcg_device_noalloc(const mlp_matrix* A, const double* b_dev, mlp_prec* P
     if (!A || !b_dev || !P || !x_dev) MLP_THROW(ERR_ARG, "null pointer");
     cudaStream_t s = stream ? (cudaStream_t)stream : P->s;
     PcgStats st;
+    if (P->sym) MLP_THROW(ERR_ARG, "the allocation-free PCG does not take a SymPrec handle");
     int rc = pcg_solve_noalloc(A->A, b_dev, *P->P, x_dev, eps, maxit, flexible != 0, st, s);
     if (stats) {
         stats->niter = st.niter;
@@ -444,6 +474,7 @@ int mlp_cheb_solve_device(const mlp_matrix* A, const double* b_dev, mlp_prec* P,
     if (!A || !b_dev || !P || !x_dev) MLP_THROW(ERR_ARG, "null pointer");
     cudaStream_t s = stream ? (cudaStream_t)stream : P->s;
     PcgStats st;
+    if (P->sym) MLP_THROW(ERR_ARG, "ChebSolver needs the uh_cheb preconditioner (main.cc:141-149)");
     int rc = cheb_solve(A->A, b_dev, *P->P, x_dev, lmin, lmax, eps, maxit, st, s);
     fill_stats(stats, st, P->setup_ms);
     return rc;
@@ -458,6 +489,7 @@ int mlp_cheb_solve(const mlp_matrix* A, const double* b_host, mlp_prec* P, doubl
     P->tmp_in.alloc(n);
     P->tmp_out.alloc(n);
     CK(cudaMemcpyAsync(P->tmp_in.p, b_host, (size_t)n * 8, cudaMemcpyHostToDevice, P->s));
+    if (P->sym) MLP_THROW(ERR_ARG, "ChebSolver needs the uh_cheb preconditioner (main.cc:141-149)");
     PcgStats st;
     int rc = cheb_solve(A->A, P->tmp_in.p, *P->P, P->tmp_out.p, lmin, lmax, eps, maxit, st, P->s);
     CK(cudaMemcpyAsync(x_host, P->tmp_out.p, (size_t)n * 8, cudaMemcpyDeviceToHost, P->s));
@@ -473,6 +505,7 @@ int mlp_pcg_device_x0(const mlp_matrix* A, const double* b_dev, mlp_prec* P, dou
     if (!A || !b_dev || !P || !x_dev) MLP_THROW(ERR_ARG, "null pointer");
     if (x0_mode < 0 || x0_mode > 2) MLP_THROW(ERR_ARG, "x0_mode must be 0, 1 or 2");
     cudaStream_t s = stream ? (cudaStream_t)stream : P->s;
+    if (P->sym && x0_mode != 0) MLP_THROW(ERR_ARG, "a SymPrec solve starts from generate_x0 only");
     set_pcg_x0_mode(x0_mode);
     return pcg_common(A, b_dev, P, x_dev, eps, maxit, flexible, stats, s);
     API_END
@@ -512,6 +545,7 @@ int mlp_ensemble_create(uint32_t count, mlp_prec* const* P, int32_t flexible, in
     std::vector<Prec*> members;
     for (uint32_t i = 0; i < count; i++) {
         if (!P[i]) MLP_THROW(ERR_ARG, "null member handle");
+        if (P[i]->sym) MLP_THROW(ERR_ARG, "an ensemble member cannot be a SymPrec handle");
         for (uint32_t j = 0; j < i; j++)
             if (P[j] == P[i]) MLP_THROW(ERR_ARG, "a handle appears twice in the ensemble");
         members.push_back(P[i]->P.get());

@@ -2191,6 +2191,138 @@ int pcg_solve(const DCSR& A, const double* b, Prec& P, double* x, double eps, ui
 }
 
 // ---------------------------------------------------------------------------
+// SymPrec (modules/prec/sym/sym_prec.cc:8-40): the preconditioner is a PCG
+// solve (eps 1e-14) with the uh_cheb preconditioner of the matrix's symmetric
+// part. Its construction symmetrizes the matrix on the device; the solver
+// around it is the PCG loop below, driven from the host one iteration at a
+// time because each application is itself a whole device-resident solve.
+// ---------------------------------------------------------------------------
+// a_ij = max(a_ij, a_ji) off the diagonal, a missing a_ji counting as 0
+// (sym_prec.cc:28-33; the reference's in-place row loop gives the same
+// values, each pair's maximum, whatever the row order)
+__global__ void k_symmetrize(uint32_t n, const uint32_t* __restrict__ ia, const uint32_t* __restrict__ ja,
+                             const double* __restrict__ a, double* __restrict__ out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t rs = ia[i], re = ia[i + 1];
+    out[rs] = a[rs];
+    for (uint32_t j_ = rs + 1; j_ < re; j_++) {
+        uint32_t j = ja[j_];
+        uint32_t lo = ia[j] + 1, hi = ia[j + 1];
+        while (lo < hi) {
+            uint32_t mid = (lo + hi) / 2;
+            if (ja[mid] < i) lo = mid + 1;
+            else hi = mid;
+        }
+        double d = (lo < ia[j + 1] && ja[lo] == i) ? a[lo] : 0.0;
+        double v = a[j_];
+        out[j_] = d > v ? d : v;
+    }
+}
+
+void symmetrize(const DCSR& A, DCSR& S, cudaStream_t s) {
+    S.alloc(A.nrow, A.ncol, A.nnz);
+    CK(cudaMemcpyAsync(S.ia.p, A.ia.p, ((size_t)A.nrow + 1) * 4, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(S.ja.p, A.ja.p, (size_t)A.nnz * 4, cudaMemcpyDeviceToDevice, s));
+    if (A.nrow) {
+        k_symmetrize<<<grid_for(A.nrow, 256), 256, 0, s>>>(A.nrow, A.ia.p, A.ja.p, A.a.p, S.a.p);
+        CK_LAUNCH();
+    }
+    csr_tile_stats(S, s);
+}
+
+// PCGSolver (pcg.cc:8-102) on natural-order device vectors with the
+// preconditioner given as a call z = B r (each call may run whole device
+// solves); one host round trip per iteration, the same kernels as the
+// device-resident loop.
+int pcg_solve_cb(const DCSR& A, const double* b, const std::function<void(const double*, double*)>& apply,
+                 double* x, double eps, uint32_t maxit, bool flexible, PcgStats& st, cudaStream_t s) {
+    if (maxit == 0) maxit = PCG_DEFAULT_MAXIT;
+    uint32_t n = A.nrow;
+    if (!n) MLP_THROW(ERR_ARG, "empty system");
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, s));
+    DBuf<double> r(n), z(n), p(n), Ap(n), rprev(flexible ? n : 1);
+    unsigned G = (unsigned)std::max(1, std::min<int>((int)grid_for(n, RB), num_sms() * 4));
+    bool staged = A.tile_max && A.tile_max <= ST_MAX_NNZ && n >= 4 * ST_ROWS;
+    DBuf<double> partials(2 * (size_t)std::max<unsigned>(G, staged_grid(n)));
+    DBuf<PcgDev> dd(1);
+    dd.zero(s);
+    PcgDev* d = dd.p;
+    CK(cudaMemcpyAsync(x, x0_device(n, s), (size_t)n * 8, cudaMemcpyDeviceToDevice, s));  // generate_x0
+    launch_spmv<double>(n, A.nnz, A.ia.p, A.ja.p, A.a.p, x, r.p, b, s, A.tile_max);
+    CK_LAUNCH();
+    k_dot_simple<<<G, RB, 0, s>>>(n, r.p, r.p, partials.p, &d->ticket[1], &d->rr);
+    CK_LAUNCH();
+    auto fetch = [&]() -> PcgDev {
+        PcgDev h;
+        CK(cudaMemcpyAsync(&h, d, sizeof(PcgDev), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        return h;
+    };
+    apply(r.p, z.p);
+    CK(cudaMemcpyAsync(p.p, z.p, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
+    k_dot_simple<<<G, RB, 0, s>>>(n, r.p, z.p, partials.p, &d->ticket[2], &d->rz0);
+    CK_LAUNCH();
+    if (flexible) CK(cudaMemcpyAsync(rprev.p, r.p, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
+    PcgDev h = fetch();
+    double norm = std::sqrt(h.rr), init = norm;
+    st.init_norm = init;
+    int rc = OK;
+    std::string msg;
+    if (!std::isfinite(init)) { rc = ERR_NOT_FINITE; msg = "non-finite initial residual norm"; }
+    if (init * eps < 1e-14) eps = 1e-14 / init;  // check_and_replace_eps, solvers.cc:49-58
+    uint32_t it = 0, napply = 1;
+    int lpr = pick_lpr(n, A.nnz);
+    if (lpr < 2) lpr = 2;
+    while (rc == OK && norm / init > eps) {
+        if (maxit && it >= maxit) { rc = ERR_MAXIT; msg = "iteration cap reached"; break; }
+        if (staged) {
+            launch_pcg_spmv_dot_staged(n, A, p.p, Ap.p, partials.p, d, s);
+        } else switch (lpr) {
+            case 2: k_pcg_spmv_dot<2><<<G, RB, 0, s>>>(n, A.ia.p, A.ja.p, A.a.p, p.p, Ap.p, partials.p, d); break;
+            case 4: k_pcg_spmv_dot<4><<<G, RB, 0, s>>>(n, A.ia.p, A.ja.p, A.a.p, p.p, Ap.p, partials.p, d); break;
+            case 8: k_pcg_spmv_dot<8><<<G, RB, 0, s>>>(n, A.ia.p, A.ja.p, A.a.p, p.p, Ap.p, partials.p, d); break;
+            case 16: k_pcg_spmv_dot<16><<<G, RB, 0, s>>>(n, A.ia.p, A.ja.p, A.a.p, p.p, Ap.p, partials.p, d); break;
+            default: k_pcg_spmv_dot<32><<<G, RB, 0, s>>>(n, A.ia.p, A.ja.p, A.a.p, p.p, Ap.p, partials.p, d); break;
+        }
+        k_pcg_update<<<G, RB, 0, s>>>(n, x, r.p, p.p, Ap.p, partials.p, d);
+        count_launches(2);
+        CK_LAUNCH();
+        h = fetch();
+        if (h.status & 1) { rc = ERR_CURVATURE; msg = "<Ap, p> = " + std::to_string(h.app); break; }
+        if (h.status & 2) { rc = ERR_NOT_FINITE; msg = "non-finite value in PCG scalars"; break; }
+        norm = std::sqrt(h.rr);
+        it++;
+        if (!(norm / init > eps)) break;
+        apply(r.p, z.p);
+        napply++;
+        k_pcg_dot_rz<<<G, RB, 0, s>>>(n, r.p, z.p, rprev.p, partials.p, d, flexible ? 1 : 0);
+        k_pcg_beta<<<1, 1, 0, s>>>(d, flexible ? 1 : 0);
+        k_pcg_p<<<grid_for(n, 256), 256, 0, s>>>(n, p.p, z.p, d);
+        count_launches(3);
+        if (flexible) CK(cudaMemcpyAsync(rprev.p, r.p, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
+        CK_LAUNCH();
+    }
+    CK(cudaEventRecord(e1, s));
+    CK(cudaStreamSynchronize(s));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    st.niter = it;
+    st.final_norm = norm;
+    st.final_rel = norm / init;
+    st.t_total_ms = ms;
+    st.napply = napply;
+    if (rc == OK && it == 0) { rc = ERR_NO_ITER; msg = "No need to iterate"; }
+    if (rc != OK) set_last_error(msg);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
 // ChebSolver (modules/solvers/cheb.cc:9-100): the Chebyshev iteration as the
 // outer solver, for a preconditioner with known spectral bounds (uh_cheb's
 // level-0 lmin / lmax). Like PCG it runs as one graph: start, the first step,

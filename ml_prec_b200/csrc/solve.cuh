@@ -112,6 +112,13 @@ struct PcgStats {
 int pcg_solve(const DCSR& A, const double* b, Prec& P, double* x, double eps, uint32_t maxit, bool flexible,
               PcgStats& st, cudaStream_t s);
 
+// SymPrec support: S = A with a_ij = max(a_ij, a_ji) off the diagonal
+// (sym_prec.cc:19-40), and PCGSolver on natural-order device vectors with the
+// preconditioner given as a call z = B r.
+void symmetrize(const DCSR& A, DCSR& S, cudaStream_t s);
+int pcg_solve_cb(const DCSR& A, const double* b, const std::function<void(const double*, double*)>& apply,
+                 double* x, double eps, uint32_t maxit, bool flexible, PcgStats& st, cudaStream_t s);
+
 // ChebSolver (cheb.cc:9-100) with x0 of generate_x0, b and x device vectors in
 // natural order, spectral bounds lmin < lmax of the preconditioned operator.
 int cheb_solve(const DCSR& A, const double* b, Prec& P, double* x, double lmin, double lmax, double eps,

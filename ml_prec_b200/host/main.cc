@@ -98,7 +98,15 @@ int main(int argc, char* argv[]) {
         Vector x(A.size());
         SolverStats stats;
         for (uint i = 0; i < cfg.ntests; i++) {
-            PCGSolver(A, b, *B, x, stats, cfg.eps);
+            if (cfg.solver == CHEB_SOLVER) {
+                // main.cc:141-149: the uh_cheb preconditioner's level-0 bounds
+                const Prec& Bc = dynamic_cast<const Prec&>(*B);
+                double t0 = now();
+                ChebSolver(A, Bc.lmin(), Bc.lmax(), b, Bc, x, cfg.eps);
+                stats.t_sol = now() - t0;
+            } else {
+                PCGSolver(A, b, *B, x, stats, cfg.eps);
+            }
             stimes.push_back(stats.t_sol);
             log << "Solution time : " << stimes.back() << std::endl;
         }

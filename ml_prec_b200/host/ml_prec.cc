@@ -571,6 +571,25 @@ Prec::Prec(const SkylineMatrix& A, const Config& cfg) {
     create(A, c);
 }
 
+SymPrec::SymPrec(const SkylineMatrix& A, const Config& cfg) {
+    if (cfg.sigmas.empty() || cfg.niters.empty()) THROW_EXCEPTION("sigmas and niters must not be empty");
+    for (double s : cfg.sigmas)
+        if (s <= 1) THROW_EXCEPTION("All sigmas must be > 1");
+    std::vector<double> sig = cfg.sigmas;
+    std::vector<uint32_t> deg(cfg.niters.begin(), cfg.niters.end());
+    mlp_prec_cfg c;
+    std::memset(&c, 0, sizeof(c));
+    c.kind = MLP_PREC_SYM;
+    c.nsigma = sig.size();
+    c.sigma = sig.data();
+    c.nncheb = deg.size();
+    c.ncheb = deg.data();
+    c.use_tails = cfg.use_tails;
+    c.max_levels = 30;
+    c.fp32 = cfg.fp32;
+    create(A, c);
+}
+
 double Prec::lmin() const { return level_info(0).lmin; }
 double Prec::lmax() const { return level_info(0).lmax; }
 
@@ -578,7 +597,8 @@ PrecBase* make_prec(const SkylineMatrix& A, const Config& cfg) {
     switch (cfg.prec) {
         case MULTI_SPLIT_PREC: return new MultiSplitPrec(A, cfg);
         case UH_CHEB_PREC: return new Prec(A, cfg);
-        default: THROW_EXCEPTION("only the multi_split and uh_cheb preconditioners are implemented");
+        case SYM_SPLIT_PREC: return new SymPrec(A, cfg);
+        default: THROW_EXCEPTION("only the multi_split, uh_cheb and sym_split preconditioners are implemented");
     }
 }
 
@@ -610,6 +630,21 @@ void PCGSolver(const CSRMatrix& A, const Vector& b, const PrecBase& B, Vector& x
                   << st.final_norm << std::defaultfloat << std::endl;
 }
 
+void ChebSolver(const CSRMatrix& A, double lmin, double lmax, const Vector& b, const PrecBase& B, Vector& x,
+                double eps, NormType norm_type, bool silent) {
+    const DevicePrec* P = dynamic_cast<const DevicePrec*>(&B);
+    if (!P) THROW_EXCEPTION("ChebSolver: the preconditioner has no device implementation");
+    if (norm_type != NORM_L2) THROW_EXCEPTION("ChebSolver: only NORM_L2 is implemented");
+    if (b.size() != A.size()) THROW_EXCEPTION("Wrong size: " << b.size() << " != " << A.size());
+    if (x.size() != A.size()) THROW_EXCEPTION("Wrong size: " << x.size() << " != " << A.size());
+    mlp_stats st;
+    std::memset(&st, 0, sizeof(st));
+    mlp_check(mlp_cheb_solve(A.device(), b.data(), P->handle(), x.data(), lmin, lmax, eps, 0, &st), "ChebSolver");
+    if (!silent)
+        std::cout << "#" << st.niter << ": relative -> " << std::scientific << st.final_rel << "   absolute -> "
+                  << st.final_norm << std::defaultfloat << std::endl;
+}
+
 std::ostream& operator<<(std::ostream& os, const SolverStats& stats) {
     os << std::fixed << std::setprecision(3) << "\n";
     os << "Residual time       :  avg = " << stats.t_resid << "\t total = " << stats.t_resid_total << "\n";
@@ -634,8 +669,8 @@ static void usage() {
                  "  -m|--matrix FILE                 matrix input file (.dat binary, .crs ascii, .mm)\n"
                  "  -M|--max-levels N                maximum number of levels\n"
                  "  -N|--coarse-n N                  direct solve of coarse systems of order <= N\n"
-                 "  -o|--solver=pcg                  outer solver (only pcg)\n"
-                 "  -p|--prec={uh_cheb|multi_split}  preconditioner\n"
+                 "  -o|--solver={pcg|cheb}           outer solver\n"
+                 "  -p|--prec={uh_cheb|multi_split|sym_split}  preconditioner\n"
                  "  -s|--sigmas \"s0 s1 ..\"           level sigmas (uh_cheb, > 1) or q (multi_split, < 1)\n"
                  "  -t|--use_tails={yes|no}          tail elimination\n"
                  "  -v|--vector FILE                 right-hand side input file\n"
@@ -697,11 +732,13 @@ int set_params(int argc, char* argv[], Config& cfg) {
                 break;
             case 'o':
                 if (arg == "pcg") cfg.solver = PCG_SOLVER;
-                else THROW_EXCEPTION("Unknown solver type \"" << arg << "\" (only pcg is implemented)");
+                else if (arg == "cheb") cfg.solver = CHEB_SOLVER;
+                else THROW_EXCEPTION("Unknown solver type \"" << arg << "\" (pcg and cheb are implemented)");
                 break;
             case 'p':
                 if (arg == "uh_cheb") cfg.prec = UH_CHEB_PREC;
                 else if (arg == "multi_split") cfg.prec = MULTI_SPLIT_PREC;
+                else if (arg == "sym_split") cfg.prec = SYM_SPLIT_PREC;
                 else THROW_EXCEPTION("Unknown prec type \"" << arg << "\"");
                 break;
             case OPT_EPS: cfg.eps = std::atof(arg.c_str()); break;
@@ -712,9 +749,11 @@ int set_params(int argc, char* argv[], Config& cfg) {
             default: return 1;
         }
     }
-    if (cfg.prec == UH_CHEB_PREC)
+    if (cfg.prec == UH_CHEB_PREC || cfg.prec == SYM_SPLIT_PREC)
         for (double s : cfg.sigmas)
             if (s <= 1) THROW_EXCEPTION("All sigmas must be > 1");
+    if (cfg.solver == CHEB_SOLVER && cfg.prec != UH_CHEB_PREC)  // main_helper.cc:232-233
+        THROW_EXCEPTION("Trying to call Chebyshev solver for not UH Cheb preconditioner");
     if (cfg.prec == MULTI_SPLIT_PREC && cfg.prec_conf_file.empty())
         for (double s : cfg.sigmas)
             if (s >= 1) THROW_EXCEPTION("All sigmas must be < 1");

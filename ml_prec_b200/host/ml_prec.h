@@ -329,8 +329,15 @@ public:
     double lmax() const;
 };
 
+/* SymPrec(A, cfg) (sym_prec.h:13-27): the uh_cheb Prec of A's symmetric part
+ * (a_ij = max(a_ij, a_ji) off the diagonal), applied as a PCG solve to 1e-14. */
+class SymPrec : public DevicePrec {
+public:
+    SymPrec(const SkylineMatrix& A, const Config& cfg);
+};
+
 /* The preconditioner switch of main.cc:100-114 for the kinds this library
- * implements (MULTI_SPLIT_PREC, UH_CHEB_PREC); other kinds throw. */
+ * implements (MULTI_SPLIT_PREC, UH_CHEB_PREC, SYM_SPLIT_PREC); other kinds throw. */
 PrecBase* make_prec(const SkylineMatrix& A, const Config& cfg);
 
 /* ---- solver (solvers.h) ---------------------------------------------------- */
@@ -355,6 +362,12 @@ std::ostream& operator<<(std::ostream& os, const SolverStats& stats);
  * cap (10,000). */
 void PCGSolver(const CSRMatrix& A, const Vector& b, const PrecBase& B, Vector& x, SolverStats& stats,
                double eps = 1e-10, NormType norm_type = NORM_L2, bool silent = false);
+
+/* ChebSolver(A, lmin, lmax, b, B, x, eps, norm, silent) (solvers.h:33-34,
+ * cheb.cc:9-100) on the device: the Chebyshev iteration with preconditioner B
+ * (a device preconditioner; main.cc passes uh_cheb's level-0 lmin / lmax). */
+void ChebSolver(const CSRMatrix& A, double lmin, double lmax, const Vector& b, const PrecBase& B, Vector& x,
+                double eps = 1e-10, NormType norm_type = NORM_L2, bool silent = false);
 
 void generate_x0(Vector& x);
 

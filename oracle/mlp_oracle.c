@@ -538,7 +538,33 @@ static int ch_construct(or_prec* P, const or_prec_cfg* cfg, uint32_t level, char
 }
 
 /* ---- build / free ------------------------------------------------------- */
+/* SymPrec::SymPrec (sym_prec.cc:19-40): a_ij = max(a_ij, a_ji) off the
+ * diagonal (a missing a_ji counts as 0; the rows' order does not matter, the
+ * in-place loop gives the same result), then the uh_cheb Prec of it. */
+static or_prec* sym_build(const or_csr* A, const or_prec_cfg* cfg, char* err, int errlen) {
+    or_prec* P = (or_prec*)calloc(1, sizeof *P);
+    P->kind = OR_PREC_SYM;
+    csr_copy(&P->Asym, A);
+    or_csr* S = &P->Asym;
+    for (uint32_t i = 0; i < S->nrow; i++)
+        for (uint32_t j_ = S->ia[i] + 1; j_ < S->ia[i + 1]; j_++) {
+            uint32_t j = S->ja[j_];
+            uint32_t lo = S->ia[j] + 1, hi = S->ia[j + 1];
+            while (lo < hi) { uint32_t mid = (lo + hi) / 2; if (S->ja[mid] < i) lo = mid + 1; else hi = mid; }
+            double d = (lo < S->ia[j + 1] && S->ja[lo] == i) ? S->a[lo] : 0.0; /* Asym(j, i) */
+            if (d > S->a[j_]) S->a[j_] = d;
+        }
+    or_prec_cfg c1 = *cfg;
+    c1.kind = OR_PREC_CHEB;
+    P->inner = or_prec_build(S, &c1, err, errlen);
+    if (!P->inner) { or_csr_free(S); free(P); return NULL; }
+    P->nlevels = ((or_prec*)P->inner)->nlevels;
+    P->levels = NULL;
+    return P;
+}
+
 or_prec* or_prec_build(const or_csr* A, const or_prec_cfg* cfg, char* err, int errlen) {
+    if (cfg->kind == OR_PREC_SYM) return sym_build(A, cfg, err, errlen);
     or_prec* P = (or_prec*)calloc(1, sizeof *P);
     P->kind = cfg->kind;
     int rc = 0;
@@ -607,6 +633,12 @@ or_prec* or_prec_build(const or_csr* A, const or_prec_cfg* cfg, char* err, int e
 
 void or_prec_free(or_prec* P) {
     if (!P) return;
+    if (P->kind == OR_PREC_SYM) {
+        or_prec_free((or_prec*)P->inner);
+        or_csr_free(&P->Asym);
+        free(P);
+        return;
+    }
     for (uint32_t l = 0; l <= P->nlevels && P->levels; l++) {
         or_level* li = &P->levels[l];
         or_csr_free(&li->A); or_csr_free(&li->L); or_csr_free(&li->U);
@@ -616,7 +648,10 @@ void or_prec_free(or_prec* P) {
 }
 
 uint32_t or_prec_nlevels(const or_prec* P) { return P->nlevels; }
-const or_level* or_prec_level(const or_prec* P, uint32_t l) { return &P->levels[l]; }
+const or_level* or_prec_level(const or_prec* P, uint32_t l) {
+    if (P->kind == OR_PREC_SYM) return &((const or_prec*)P->inner)->levels[l];
+    return &P->levels[l];
+}
 
 /* ---- apply -------------------------------------------------------------- */
 static double* level_work(const or_prec* P, uint32_t level) {
@@ -761,7 +796,13 @@ static void ch_solve(const or_prec* P, uint32_t level, const double* f, double* 
 
 void or_prec_apply(const or_prec* P, const double* f, double* x) {
     if (P->kind == OR_PREC_MSPLIT) ms_solve((or_prec*)P, 0, f, x);  /* apply_err is the only write */
-    else ch_solve(P, 0, f, x);
+    else if (P->kind == OR_PREC_SYM) {
+        /* SymPrec::solve (sym_prec.cc:8-17): PCGSolver(Asym, f, B, x, 1e-14) from generate_x0 */
+        uint32_t it;
+        double rel;
+        int rc = or_pcg_ex(&P->Asym, f, (const or_prec*)P->inner, x, 1e-14, &it, &rel, 0, 0);
+        if (rc != 0) ((or_prec*)P)->apply_err = 1;
+    } else ch_solve(P, 0, f, x);
 }
 
 /* ---- ChebSolver (cheb.cc:9-100) -------------------------------------------- */

@@ -44,7 +44,7 @@ void or_generate_x0(double* x, uint32_t n);
 
 /* ---- multilevel preconditioners ---------------------------------------- */
 enum { OR_ORDER_NONE = 0, OR_ORDER_ORIGINAL = 1, OR_ORDER_BLOCK = 2, OR_ORDER_SIMPLE_1 = 3 };
-enum { OR_PREC_MSPLIT = 0, OR_PREC_CHEB = 1 };
+enum { OR_PREC_MSPLIT = 0, OR_PREC_CHEB = 1, OR_PREC_SYM = 2 };
 
 typedef struct {
     int kind;              /* OR_PREC_MSPLIT / OR_PREC_CHEB */
@@ -86,6 +86,10 @@ typedef struct {
     double* work;       /* scratch for apply */
     char err[256];
     int apply_err;      /* set when a dynamic level iteration hit its cap */
+    /* SymPrec (sym_prec.cc:8-40): the uh_cheb preconditioner of the symmetric
+     * part, applied as a PCG solve to eps = 1e-14 */
+    or_csr Asym;
+    void* inner;        /* or_prec* of the symmetric part */
 } or_prec;
 
 or_prec* or_prec_build(const or_csr* A, const or_prec_cfg* cfg, char* err, int errlen);

@@ -167,7 +167,7 @@ class Prec:
         sa = np.asarray(sigma, np.float64); ca = np.asarray(ncheb, np.uint32)
         ea = np.asarray(level_eps if level_eps is not None else [], np.float64)
         self._keep += [qa, na, sa, ca, ea, A]
-        cfg = PrecCfg(0 if kind == "msplit" else 1, len(qa), _p(qa, f64p), len(na), _p(na, u32p),
+        cfg = PrecCfg({"msplit": 0, "cheb": 1, "sym": 2}[kind], len(qa), _p(qa, f64p), len(na), _p(na, u32p),
                       coarse_n, max_levels, degree_max, ORDERS[order], int(use_tails),
                       len(sa), _p(sa, f64p), len(ca), _p(ca, u32p), len(ea), _p(ea, f64p) if len(ea) else None)
         err = C.create_string_buffer(256)

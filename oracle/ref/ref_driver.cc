@@ -47,6 +47,7 @@
 #include "modules/matrix/matrix.h"
 #include "modules/prec/multi_split/multi_split_prec.h"
 #include "modules/prec/cheb/cheb_prec.h"
+#include "modules/prec/sym/sym_prec.h"
 #include "modules/solvers/solvers.h"
 #include "project/config.h"
 #undef private
@@ -257,6 +258,9 @@ int main(int argc, char** argv) {
         } else if (a.prec == "cheb") {
             cfg.prec = UH_CHEB_PREC;
             B = new Prec(A, cfg);
+        } else if (a.prec == "sym") {
+            cfg.prec = SYM_SPLIT_PREC;
+            B = new SymPrec(A, cfg);
         } else {
             fprintf(stderr, "unknown prec %s\n", a.prec.c_str());
             return 2;
@@ -290,7 +294,8 @@ int main(int argc, char** argv) {
         }
         js << "\n  ]";
     } else {
-        Prec* P = (Prec*)B;
+        // uh_cheb, or SymPrec's uh_cheb of the symmetric part (sym_prec.h:15)
+        Prec* P = a.prec == "sym" ? ((SymPrec*)B)->B.get() : (Prec*)B;
         js << ",\n  \"nlevels\": " << P->nlevels << ",\n  \"levels\": [";
         for (uint l = 0; l < P->nlevels; l++) {
             const Prec::Level& L = P->levels[l];

@@ -45,6 +45,8 @@ CASES = {
     "ms_dynamic_12x22x6": ("iid", 1, 12, 22, 6, 1.0, "msplit", {"level_eps": "0 1e-1 1e-3"}),
     "ch_layered_16x22x8": ("layered", 2, 16, 22, 8, 1.0, "cheb", {"sigmas": [3.0], "niters": [4]}),
     "ch_iid_12x22x6": ("iid", 4, 12, 22, 6, 1.0, "cheb", {"sigmas": [3.0, 2.5], "niters": [2, 3]}),
+    # SymPrec (sym_prec.cc): uh_cheb of the symmetric part applied as a PCG solve to 1e-14
+    "sym_layered_16x22x8": ("layered", 2, 16, 22, 8, 1.0, "sym", {"sigmas": [3.0], "niters": [4]}),
     # the same preconditioner with ChebSolver as the outer iteration (x, niter are ChebSolver's)
     "chs_layered_16x22x8": ("layered", 2, 16, 22, 8, 1.0, "cheb", {"sigmas": [3.0], "niters": [4], "solver": "cheb"}),
 }

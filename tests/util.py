@@ -26,7 +26,7 @@ def prec_kwargs(g):
                     max_levels=o.get("max_levels", 15), degree_max=o.get("degree_max", 2),
                     order=o.get("elim_order", "simple_1"), use_tails=bool(o.get("use_tails", 1)),
                     level_eps=(tuple(float(t) for t in o["level_eps"].split()) if "level_eps" in o else None))
-    return dict(kind="cheb", sigma=tuple(o["sigmas"]), ncheb=tuple(o["niters"]), use_tails=True)
+    return dict(kind=g["prec"], sigma=tuple(o["sigmas"]), ncheb=tuple(o["niters"]), use_tails=True)
 
 
 def oracle_prec(A, g):
@@ -41,4 +41,6 @@ def gpu_prec(A, g, fp32=False):
     kind = kw.pop("kind")
     if kind == "msplit":
         return M.MultiSplitPrec(A, fp32=fp32, **kw)
+    if kind == "sym":
+        return M.SymPrec(A, fp32=fp32, **kw)
     return M.Prec(A, fp32=fp32, **kw)
