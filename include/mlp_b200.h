@@ -228,6 +228,21 @@ int mlp_ensemble_solve(mlp_ensemble* E, const double* const* b_dev, double* cons
                        mlp_stats* stats, double* t_ms, void* stream);
 int mlp_ensemble_destroy(mlp_ensemble* E);
 
+/* Gradient form of the ensemble (no reference counterpart): ONE graph whose
+ * branch i runs member i's forward solve A_i p_i = b_i, the misfit gradient
+ * dJ/dp at its observation cells (J = 0.5 sum_k (p[obs_k] - pobs_k)^2), the
+ * adjoint solve A_i lambda_i = dJ/dp and the dJ/d(ln K) kernel of
+ * mlp_matrix_grad_logk; both solves start from zero. A[i] must come from
+ * mlp_matrix_create_spe. obs_dev / pobs_dev (nobs[i] entries) and the outputs
+ * p_dev, lam_dev, grad_dev (device vectors of member i's cells) are bound at
+ * creation and must outlive the handle. Run it with mlp_ensemble_solve
+ * (x_dev may be NULL); stats then takes 2 * count entries: the forward solves,
+ * then the adjoint solves. */
+int mlp_ensemble_gradient_create(uint32_t count, const mlp_matrix* const* A, mlp_prec* const* P,
+                                 const uint32_t* const* obs_dev, const uint32_t* nobs, const double* const* pobs_dev,
+                                 double* const* p_dev, double* const* lam_dev, double* const* grad_dev,
+                                 int32_t flexible, mlp_ensemble** out);
+
 /* PCG that allocates no device memory. It has no counterpart in the
  * reference. It serves host applications that cannot let a library call
  * cudaMalloc while they solve: their device memory is owned by their own

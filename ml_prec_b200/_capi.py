@@ -25,6 +25,7 @@ EXPORTS = [
     "mlp_prec_level_info", "mlp_prec_level_export", "mlp_prec_bytes_per_apply", "mlp_prec_profile",
     "mlp_pcg", "mlp_pcg_device", "mlp_pcg_device_x0", "mlp_matrix_grad_logk", "mlp_pcg_device_noalloc",
     "mlp_launch_count", "mlp_generate_x0", "mlp_cheb_solve", "mlp_cheb_solve_device", "mlp_ensemble_create", "mlp_ensemble_solve", "mlp_ensemble_destroy",
+    "mlp_ensemble_gradient_create",
 ]
 
 
@@ -118,6 +119,9 @@ def lib():
         L.mlp_ensemble_solve.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.c_double, C.c_uint32,
                                          C.POINTER(Stats), C.POINTER(C.c_double), vp]
         L.mlp_ensemble_destroy.argtypes = [vp]
+        L.mlp_ensemble_gradient_create.argtypes = [C.c_uint32, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), u32p,
+                                                   C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
+                                                   C.c_int32, C.POINTER(vp)]
         _lib = L
     return _lib
 

@@ -564,27 +564,68 @@ int mlp_ensemble_create(uint32_t count, mlp_prec* const* P, int32_t flexible, in
     API_END
 }
 
+int mlp_ensemble_gradient_create(uint32_t count, const mlp_matrix* const* A, mlp_prec* const* P,
+                                 const uint32_t* const* obs_dev, const uint32_t* nobs, const double* const* pobs_dev,
+                                 double* const* p_dev, double* const* lam_dev, double* const* grad_dev,
+                                 int32_t flexible, mlp_ensemble** out) {
+    API_BEGIN
+    if (!A || !P || !obs_dev || !nobs || !pobs_dev || !p_dev || !lam_dev || !grad_dev || !out || !count)
+        MLP_THROW(ERR_ARG, "null pointer or empty ensemble");
+    std::vector<Prec*> members;
+    std::vector<GradMember> gm(count);
+    for (uint32_t i = 0; i < count; i++) {
+        if (!A[i] || !P[i]) MLP_THROW(ERR_ARG, "null member handle");
+        if (P[i]->sym) MLP_THROW(ERR_ARG, "an ensemble member cannot be a SymPrec handle");
+        if (!A[i]->field.p) MLP_THROW(ERR_ARG, "member matrix was not assembled from a permeability field");
+        for (uint32_t j = 0; j < i; j++)
+            if (P[j] == P[i]) MLP_THROW(ERR_ARG, "a handle appears twice in the ensemble");
+        if (nobs[i] && (!obs_dev[i] || !pobs_dev[i])) MLP_THROW(ERR_ARG, "null observation arrays");
+        if (!p_dev[i] || !lam_dev[i] || !grad_dev[i]) MLP_THROW(ERR_ARG, "null output vector");
+        members.push_back(P[i]->P.get());
+        GradMember& m = gm[i];
+        const size_t KN = 1122000;
+        m.nx = A[i]->nx; m.ny = A[i]->ny; m.nz = A[i]->nz;
+        m.kx = A[i]->field.p; m.ky = A[i]->field.p + KN; m.kz = A[i]->field.p + 2 * KN;
+        m.dirichlet = A[i]->dirichlet;
+        m.obs = obs_dev[i]; m.nobs = nobs[i]; m.pobs = pobs_dev[i];
+        m.p = p_dev[i]; m.lam = lam_dev[i]; m.grad = grad_dev[i];
+    }
+    auto* H = new mlp_ensemble();
+    try {
+        H->s = new_stream();
+        H->handles.assign(P, P + count);
+        H->E = make_ensemble_gradient(members, gm, flexible != 0, H->s);
+        CK(cudaStreamSynchronize(H->s));
+    } catch (...) {
+        delete H;
+        throw;
+    }
+    *out = H;
+    API_END
+}
+
 int mlp_ensemble_solve(mlp_ensemble* E, const double* const* b_dev, double* const* x_dev, double eps, uint32_t maxit,
                        mlp_stats* stats, double* t_ms, void* stream) {
     API_BEGIN
-    if (!E || !b_dev || !x_dev) MLP_THROW(ERR_ARG, "null pointer");
+    if (!E || !b_dev || (!x_dev && !E->E->gradient)) MLP_THROW(ERR_ARG, "null pointer");
     size_t K = E->handles.size();
     std::vector<const double*> b(b_dev, b_dev + K);
-    std::vector<double*> x(x_dev, x_dev + K);
+    std::vector<double*> x;
+    if (x_dev) x.assign(x_dev, x_dev + K);
     cudaStream_t s = stream ? (cudaStream_t)stream : E->s;
     std::vector<PcgStats> st;
     double ms = 0;
     int rc = ensemble_solve(*E->E, b, x, eps, maxit, st, ms, s);
     if (t_ms) *t_ms = ms;
     if (stats)
-        for (size_t i = 0; i < K; i++) {
+        for (size_t i = 0; i < st.size(); i++) {
             stats[i].niter = st[i].niter;
             stats[i].napply = st[i].napply;
             stats[i].init_norm = st[i].init_norm;
             stats[i].final_norm = st[i].final_norm;
             stats[i].final_rel = st[i].final_rel;
             stats[i].t_solve_ms = ms;
-            stats[i].t_setup_ms = E->handles[i]->setup_ms;
+            stats[i].t_setup_ms = E->handles[i % K]->setup_ms;
         }
     return rc;
     API_END

@@ -2046,7 +2046,8 @@ static uint64_t start_launches(const Prec& P, bool flexible) {
 // gather b and x0 into the frame, r = b - A x, the first apply, a conditional
 // WHILE node whose body is one iteration, and the scatter of x back. The
 // vectors live in P's PcgWork (b comes in through bnat, x leaves through xnat).
-static void append_pcg(cudaGraph_t g, Prec& P, uint32_t n, bool flexible, int x0m, cudaStream_t s) {
+static std::vector<cudaGraphNode_t> append_pcg(cudaGraph_t g, Prec& P, uint32_t n, bool flexible, int x0m,
+                                               cudaStream_t s, const std::vector<cudaGraphNode_t>& after = {}) {
     const Level& L0 = *P.H->lv[0];
     const DCSR& Af = L0.Af;
     PcgWork& W = P.pcg;
@@ -2058,7 +2059,8 @@ static void append_pcg(cudaGraph_t g, Prec& P, uint32_t n, bool flexible, int x0
     CK(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
     const double* x0 = x0m == X0_GENERATE ? x0_device(n, s) : nullptr;
     // start
-    CK(cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    CK(cudaStreamBeginCaptureToGraph(s, g, after.empty() ? nullptr : after.data(), nullptr, after.size(),
+                                     cudaStreamCaptureModeThreadLocal));
     k_zero_dev<<<1, 32, 0, s>>>(d);
     CK(cudaPeekAtLastError());
     gather(n, L0.phi.p, W.bnat.p, W.bf.p, s);
@@ -2101,8 +2103,11 @@ static void append_pcg(cudaGraph_t g, Prec& P, uint32_t n, bool flexible, int x0
     CK(cudaStreamBeginCaptureToGraph(s, g, &cnode, nullptr, 1, cudaStreamCaptureModeThreadLocal));
     scatter(n, L0.phi.p, W.xf.p, W.xnat.p, s);
     le = cudaGetLastError();
+    CK(cudaStreamGetCaptureInfo(s, &cs, nullptr, nullptr, &deps, &ndeps));
+    std::vector<cudaGraphNode_t> tail(deps, deps + ndeps);
     CK(cudaStreamEndCapture(s, &got));
     if (le != cudaSuccess) MLP_THROW(ERR_CUDA, cudaGetErrorString(le));
+    return tail;
 }
 
 static cudaGraphExec_t instantiate(cudaGraph_t g) {
@@ -2534,18 +2539,89 @@ std::unique_ptr<Ensemble> make_ensemble(const std::vector<Prec*>& members, bool 
     return E;
 }
 
+// dJ/dp of J = 0.5 sum_k (p[obs_k] - pobs_k)^2: zero, then the observed cells.
+__global__ void k_misfit_rhs(uint32_t nobs, const uint32_t* __restrict__ obs, const double* __restrict__ pobs,
+                             const double* __restrict__ p, double* __restrict__ g) {
+    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nobs) g[obs[k]] = p[obs[k]] - pobs[k];
+}
+
+__global__ void k_copy_pcgdev(const PcgDev* __restrict__ a, PcgDev* __restrict__ b) {
+    const uint32_t* s = reinterpret_cast<const uint32_t*>(a);
+    uint32_t* d = reinterpret_cast<uint32_t*>(b);
+    for (uint32_t i = threadIdx.x; i < sizeof(PcgDev) / 4; i += blockDim.x) d[i] = s[i];
+}
+
+// Gradient form of the ensemble: each member's branch of the one graph runs
+// the forward solve A p = b (zero start), forms the misfit gradient dJ/dp at
+// the observation cells, runs the adjoint solve A lambda = dJ/dp (zero start,
+// same hierarchy: A is symmetric) and the dT/dlogK gradient kernel; so one
+// launch gives every member's p, lambda and dJ/dlnK.
+std::unique_ptr<Ensemble> make_ensemble_gradient(const std::vector<Prec*>& members,
+                                                 const std::vector<GradMember>& gm, bool flexible,
+                                                 cudaStream_t s) {
+    if (gm.size() != members.size()) MLP_THROW(ERR_ARG, "one gradient description per member");
+    auto E = std::unique_ptr<Ensemble>(new Ensemble());
+    E->members = members;
+    E->flexible = flexible;
+    E->x0m = X0_ZERO;
+    E->gradient = true;
+    E->fwd.resize(members.size());
+    cudaGraph_t g;
+    CK(cudaGraphCreate(&g, 0));
+    try {
+        for (size_t i = 0; i < members.size(); i++) {
+            Prec& P = *members[i];
+            const GradMember& m = gm[i];
+            uint32_t n = P.H->lv[0]->N;
+            if (m.nx * m.ny * m.nz != n) MLP_THROW(ERR_ARG, "member mesh and preconditioner sizes differ");
+            pcg_work_alloc(P, n);
+            E->fwd[i].alloc(1);
+            std::vector<cudaGraphNode_t> t = append_pcg(g, P, n, flexible, X0_ZERO, s);
+            PcgWork& W = P.pcg;
+            CK(cudaStreamBeginCaptureToGraph(s, g, t.data(), nullptr, t.size(), cudaStreamCaptureModeThreadLocal));
+            k_copy_pcgdev<<<1, 32, 0, s>>>(W.d.p, E->fwd[i].p);
+            k_copy_d<<<grid_for(n, 256), 256, 0, s>>>(n, W.xnat.p, m.p);
+            k_fill_d<<<grid_for(n, 256), 256, 0, s>>>(n, W.bnat.p, 0.0);
+            if (m.nobs) k_misfit_rhs<<<grid_for(m.nobs, 256), 256, 0, s>>>(m.nobs, m.obs, m.pobs, m.p, W.bnat.p);
+            cudaError_t le = cudaGetLastError();
+            cudaStreamCaptureStatus cs;
+            const cudaGraphNode_t* deps = nullptr;
+            size_t ndeps = 0;
+            CK(cudaStreamGetCaptureInfo(s, &cs, nullptr, nullptr, &deps, &ndeps));
+            std::vector<cudaGraphNode_t> mid(deps, deps + ndeps);
+            cudaGraph_t got;
+            CK(cudaStreamEndCapture(s, &got));
+            if (le != cudaSuccess) MLP_THROW(ERR_CUDA, cudaGetErrorString(le));
+            t = append_pcg(g, P, n, flexible, X0_ZERO, s, mid);
+            CK(cudaStreamBeginCaptureToGraph(s, g, t.data(), nullptr, t.size(), cudaStreamCaptureModeThreadLocal));
+            k_copy_d<<<grid_for(n, 256), 256, 0, s>>>(n, W.xnat.p, m.lam);
+            spe_grad_logk(m.nx, m.ny, m.nz, m.kx, m.ky, m.kz, m.dirichlet, m.p, m.lam, m.grad, s);
+            le = cudaGetLastError();
+            CK(cudaStreamEndCapture(s, &got));
+            if (le != cudaSuccess) MLP_THROW(ERR_CUDA, cudaGetErrorString(le));
+        }
+    } catch (...) {
+        cudaGraphDestroy(g);
+        throw;
+    }
+    E->exec = instantiate(g);
+    return E;
+}
+
 int ensemble_solve(Ensemble& E, const std::vector<const double*>& b, const std::vector<double*>& x, double eps,
                    uint32_t maxit, std::vector<PcgStats>& st, double& ms_out, cudaStream_t s) {
     if (maxit == 0) maxit = PCG_DEFAULT_MAXIT;
     size_t K = E.members.size();
-    if (b.size() != K || x.size() != K) MLP_THROW(ERR_ARG, "one b and one x per ensemble member");
+    if (b.size() != K || (!E.gradient && x.size() != K)) MLP_THROW(ERR_ARG, "one b and one x per ensemble member");
     PcgParams prm{eps, maxit};
     for (size_t i = 0; i < K; i++) {
         Prec& P = *E.members[i];
         uint32_t n = P.pcg.n;
         CK(cudaMemcpyAsync(P.pcg.prm.p, &prm, sizeof prm, cudaMemcpyHostToDevice, s));
         CK(cudaMemcpyAsync(P.pcg.bnat.p, b[i], (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
-        if (E.x0m == X0_GIVEN) CK(cudaMemcpyAsync(P.pcg.xnat.p, x[i], (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
+        if (E.x0m == X0_GIVEN && !E.gradient)
+            CK(cudaMemcpyAsync(P.pcg.xnat.p, x[i], (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
     }
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
@@ -2553,11 +2629,12 @@ int ensemble_solve(Ensemble& E, const std::vector<const double*>& b, const std::
     CK(cudaEventRecord(e0, s));
     CK(cudaGraphLaunch(E.exec, s));
     CK(cudaEventRecord(e1, s));
-    std::vector<PcgDev> hs(K);
+    std::vector<PcgDev> hs(K), hf(E.gradient ? K : 0);
     for (size_t i = 0; i < K; i++) {
         Prec& P = *E.members[i];
-        CK(cudaMemcpyAsync(x[i], P.pcg.xnat.p, (size_t)P.pcg.n * 8, cudaMemcpyDeviceToDevice, s));
+        if (!E.gradient) CK(cudaMemcpyAsync(x[i], P.pcg.xnat.p, (size_t)P.pcg.n * 8, cudaMemcpyDeviceToDevice, s));
         CK(cudaMemcpyAsync(&hs[i], P.pcg.d.p, sizeof(PcgDev), cudaMemcpyDeviceToHost, s));
+        if (E.gradient) CK(cudaMemcpyAsync(&hf[i], E.fwd[i].p, sizeof(PcgDev), cudaMemcpyDeviceToHost, s));
     }
     CK(cudaStreamSynchronize(s));
     for (Prec* P : E.members) check_persist(*P, s);
@@ -2566,17 +2643,23 @@ int ensemble_solve(Ensemble& E, const std::vector<const double*>& b, const std::
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     ms_out = ms;
-    st.resize(K);
+    st.resize(E.gradient ? 2 * K : K);
     int rc_all = OK;
     std::string msg_all;
     for (size_t i = 0; i < K; i++) {
-        int rc;
-        std::string msg;
-        read_stats(hs[i], st[i], rc, msg);
-        st[i].t_total_ms = ms;
-        count_launches(start_launches(*E.members[i], E.flexible) +
-                       (uint64_t)hs[i].it * iteration_launches(*E.members[i], E.flexible));
-        if (rc != OK && rc_all == OK) { rc_all = rc; msg_all = "member " + std::to_string(i) + ": " + msg; }
+        // gradient form: entry i is member i's forward solve, entry K + i its adjoint solve
+        for (int pass = 0; pass < (E.gradient ? 2 : 1); pass++) {
+            const PcgDev& h = (E.gradient && pass == 0) ? hf[i] : hs[i];
+            PcgStats& so = st[(E.gradient && pass == 1) ? K + i : i];
+            int rc;
+            std::string msg;
+            read_stats(h, so, rc, msg);
+            so.t_total_ms = ms;
+            count_launches(start_launches(*E.members[i], E.flexible) +
+                           (uint64_t)h.it * iteration_launches(*E.members[i], E.flexible));
+            if (rc != OK && rc_all == OK) { rc_all = rc; msg_all = "member " + std::to_string(i) + ": " + msg; }
+        }
+        if (E.gradient) count_launches(6);
     }
     if (rc_all != OK) set_last_error(msg_all);
     return rc_all;

@@ -143,9 +143,27 @@ struct Ensemble {
     std::vector<Prec*> members;
     bool flexible = false;
     int x0m = 0;
+    bool gradient = false;             // forward, misfit, adjoint and gradient per member
+    std::vector<DBuf<PcgDev>> fwd;     // gradient form: the forward solves' scalars
     cudaGraphExec_t exec = nullptr;
     ~Ensemble();
 };
+
+// Gradient form of one member: its mesh and permeability field (device), the
+// observation cells and observed pressures (device), and where p, lambda and
+// dJ/dlnK go (device vectors of the mesh's cells, natural order).
+struct GradMember {
+    uint32_t nx = 0, ny = 0, nz = 0;
+    const double *kx = nullptr, *ky = nullptr, *kz = nullptr;
+    int dirichlet = 1;
+    const uint32_t* obs = nullptr;
+    uint32_t nobs = 0;
+    const double* pobs = nullptr;
+    double *p = nullptr, *lam = nullptr, *grad = nullptr;
+};
+std::unique_ptr<Ensemble> make_ensemble_gradient(const std::vector<Prec*>& members,
+                                                 const std::vector<GradMember>& gm, bool flexible,
+                                                 cudaStream_t s);
 std::unique_ptr<Ensemble> make_ensemble(const std::vector<Prec*>& members, bool flexible, int x0m, cudaStream_t s);
 int ensemble_solve(Ensemble& E, const std::vector<const double*>& b, const std::vector<double*>& x, double eps,
                    uint32_t maxit, std::vector<PcgStats>& st, double& ms, cudaStream_t s);

@@ -98,6 +98,39 @@ class Ensemble:
             self.g[i].copy_(torch.from_numpy(g))
         return self._solve(self.adj, self.g, self.lam, eps)
 
+    def gradient(self, p_obs, eps=1e-8):
+        """Forward solve, misfit gradient, adjoint solve and dJ/dlnK of every
+        member in ONE graph launch (mlp_ensemble_gradient_create); both solves
+        start from zero. Fills self.p, self.lam_g and self.grad; returns (ms,
+        forward iterations, adjoint iterations)."""
+        import torch
+        K = len(self.P)
+        if getattr(self, "grad_h", None) is None or self._pobs_shape != [len(o) for o in p_obs]:
+            if getattr(self, "grad_h", None):
+                lib().mlp_ensemble_destroy(self.grad_h)
+            self.obs_d = [torch.from_numpy(o.astype(np.uint32)).cuda() for o in self.obs]
+            self.pobs_d = [torch.zeros(len(o), dtype=torch.float64, device="cuda") for o in self.obs]
+            self.p = [torch.empty_like(b) for b in self.b]
+            self.lam_g = [torch.empty_like(b) for b in self.b]
+            self.grad = [torch.empty_like(b) for b in self.b]
+            vp = C.c_void_p
+            arr = lambda ts: (vp * K)(*[t.data_ptr() for t in ts])
+            h = C.c_void_p()
+            nobs = np.array([len(o) for o in self.obs], np.uint32)
+            check(lib().mlp_ensemble_gradient_create(
+                K, (vp * K)(*[A.h.value for A in self.A]), (vp * K)(*[P.h.value for P in self.P]),
+                arr(self.obs_d), nobs.ctypes.data_as(C.POINTER(C.c_uint32)), arr(self.pobs_d), arr(self.p),
+                arr(self.lam_g), arr(self.grad), int(self.fp32), C.byref(h)))
+            self.grad_h = h
+            self._pobs_shape = [len(o) for o in p_obs]
+        for i in range(K):
+            self.pobs_d[i].copy_(torch.from_numpy(np.asarray(p_obs[i], np.float64)))
+        bp = (C.c_void_p * K)(*[t.data_ptr() for t in self.b])
+        st = (Stats * (2 * K))()
+        t = C.c_double()
+        check(lib().mlp_ensemble_solve(self.grad_h, bp, None, eps, 0, st, C.byref(t), None))
+        return t.value, [st[i].niter for i in range(K)], [st[K + i].niter for i in range(K)]
+
     def looped_forward(self, eps=1e-8):
         """The same forward solves one handle at a time (single-instance path)."""
         import time
@@ -115,10 +148,10 @@ class Ensemble:
         return (time.perf_counter() - t0) * 1e3, its
 
     def close(self):
-        for h in (getattr(self, "fwd", None), getattr(self, "adj", None)):
+        for h in (getattr(self, "fwd", None), getattr(self, "adj", None), getattr(self, "grad_h", None)):
             if h:
                 lib().mlp_ensemble_destroy(h)
-        self.fwd = self.adj = None
+        self.fwd = self.adj = self.grad_h = None
 
     def __del__(self):
         try:
