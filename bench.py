@@ -113,6 +113,18 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(values):
+    """Every rank's timings, reduced with MAX over the ranks (each reported
+    time is the slowest rank's); the identity on one rank."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return [float(v) for v in values]
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t]
+
+
 def flush_l2(buf):
     buf.fill_(1.0)  # 256 MB write, larger than the 126 MB L2
 
@@ -535,10 +547,8 @@ def main():
         import torch
         import torch.distributed as dist
         e2e = res.get("e2e")
-        t = torch.tensor([t_step, ens["fwd_ms"] if ens else 0.0, ens["adj_ms"] if ens else 0.0,
-                          e2e["value"] if e2e else 0.0, ens["grad_one_launch_ms"] if ens else 0.0],
-                         dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)  # every timing is the slowest rank's
+        t = max_over_ranks([t_step, ens["fwd_ms"] if ens else 0.0, ens["adj_ms"] if ens else 0.0,
+                            e2e["value"] if e2e else 0.0, ens["grad_one_launch_ms"] if ens else 0.0])
         t_step = float(t[0])
         if ens:
             ens["fwd_ms"], ens["adj_ms"], ens["grad_one_launch_ms"] = float(t[1]), float(t[2]), float(t[4])
