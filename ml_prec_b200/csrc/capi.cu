@@ -1,7 +1,9 @@
 // extern "C" entry points (include/mlp_b200.h). Each one converts exceptions
 // into a status code plus a per-thread message.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
 
 #include "../../include/mlp_b200.h"
 #include "solve.cuh"
@@ -54,6 +56,43 @@ struct mlp_prec {
     }                                                           \
     return MLP_OK;
 
+// Whether every row is non-empty with its diagonal first, every column index
+// is below n and every value finite; row and entry ranges split over up to 8
+// host threads (the pass is bound by host memory bandwidth).
+static bool matrix_ok(uint32_t n, const uint32_t* ia, const uint32_t* ja, const double* a) {
+    uint32_t nnz = ia[n];
+    unsigned T = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    if ((uint64_t)nnz < (1u << 20)) T = 1;
+    std::vector<char> ok(T, 1);
+    auto work = [&](unsigned t) {
+        uint32_t r0 = (uint32_t)((uint64_t)n * t / T), r1 = (uint32_t)((uint64_t)n * (t + 1) / T);
+        bool good = true;
+        for (uint32_t i = r0; i < r1; i++) good &= (ia[i + 1] > ia[i]);
+        if (good)
+            for (uint32_t i = r0; i < r1; i++) good &= (ja[ia[i]] == i);
+        size_t k0 = (uint64_t)nnz * t / T, k1 = (uint64_t)nnz * (t + 1) / T;
+        uint32_t mx = 0;
+        uint64_t nonfinite = 0;
+        for (size_t k = k0; k < k1; k++) {
+            mx = ja[k] > mx ? ja[k] : mx;
+            uint64_t bits;
+            std::memcpy(&bits, a + k, 8);
+            nonfinite |= (uint64_t)((bits & 0x7ff0000000000000ull) == 0x7ff0000000000000ull);
+        }
+        ok[t] = good && (k1 == k0 || mx < n) && !nonfinite;
+    };
+    if (T == 1) {
+        work(0);
+    } else {
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < T; t++) th.emplace_back(work, t);
+        for (auto& x : th) x.join();
+    }
+    for (char c : ok)
+        if (!c) return false;
+    return true;
+}
+
 static cudaStream_t new_stream() {
     cudaStream_t s;
     CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
@@ -83,21 +122,28 @@ int mlp_matrix_create(uint32_t n, const uint32_t* ia, const uint32_t* ja, const 
     if (!out || !ia || (n && (!ja || !a))) MLP_THROW(ERR_ARG, "null pointer");
     if (ia[0] != 0) MLP_THROW(ERR_ARG, "ia[0] must be 0");
     uint32_t nnz = ia[n];
-    for (uint32_t i = 0; i < n; i++) {
-        if (ia[i + 1] <= ia[i]) MLP_THROW(ERR_ARG, "every row needs at least its diagonal (row " + std::to_string(i) + ")");
-        if (ja[ia[i]] != i) MLP_THROW(ERR_ARG, "diagonal must come first in row " + std::to_string(i));
-    }
-    for (uint32_t k = 0; k < nnz; k++) {
-        if (ja[k] >= n) MLP_THROW(ERR_ARG, "column index out of range");
-        if (!std::isfinite(a[k])) MLP_THROW(ERR_NOT_FINITE, "non-finite matrix value at entry " + std::to_string(k));
+    // The checks read the whole matrix (93 MB at 60x220x85), so they run as a
+    // branch-free pass split over host threads; only when it finds a fault does
+    // the serial pass below locate the first one for the message.
+    if (!matrix_ok(n, ia, ja, a)) {
+        for (uint32_t i = 0; i < n; i++) {
+            if (ia[i + 1] <= ia[i])
+                MLP_THROW(ERR_ARG, "every row needs at least its diagonal (row " + std::to_string(i) + ")");
+            if (ja[ia[i]] != i) MLP_THROW(ERR_ARG, "diagonal must come first in row " + std::to_string(i));
+        }
+        for (uint32_t k = 0; k < nnz; k++) {
+            if (ja[k] >= n) MLP_THROW(ERR_ARG, "column index out of range");
+            if (!std::isfinite(a[k]))
+                MLP_THROW(ERR_NOT_FINITE, "non-finite matrix value at entry " + std::to_string(k));
+        }
     }
     auto* M = new mlp_matrix();
     try {
         M->s = new_stream();
         M->A.alloc(n, n, nnz);
-        M->A.ia.upload(ia, (size_t)n + 1, M->s);
-        M->A.ja.upload(ja, nnz, M->s);
-        M->A.a.upload(a, nnz, M->s);
+        h2d_large(M->A.ia.p, ia, ((size_t)n + 1) * 4, M->s);
+        h2d_large(M->A.ja.p, ja, (size_t)nnz * 4, M->s);
+        h2d_large(M->A.a.p, a, (size_t)nnz * 8, M->s);
         csr_tile_stats(M->A, M->s);
         CK(cudaStreamSynchronize(M->s));
     } catch (...) {
@@ -412,7 +458,7 @@ int mlp_pcg(const mlp_matrix* A, const double* b_host, mlp_prec* P, double* x_ho
     uint32_t n = A->A.nrow;
     cudaStream_t s = P->s;
     DBuf<double> b(n), x(n);
-    CK(cudaMemcpyAsync(b.p, b_host, (size_t)n * 8, cudaMemcpyHostToDevice, s));
+    h2d_large(b.p, b_host, (size_t)n * 8, s);
     int rc = pcg_common(A, b.p, P, x.p, eps, maxit, flexible, stats, s);
     CK(cudaMemcpyAsync(x_host, x.p, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));

@@ -65,6 +65,10 @@ const char* last_error();
 // work, so it becomes reusable only at pool_recycle(dev), which callers invoke
 // right after a cudaDeviceSynchronize (the end of a build scope, the destroy
 // entry points); pool_sync_recycle() does both.
+// Host-to-device copy of a large pageable array through pinned staging buffers
+// (parallel host copies overlapped with the DMA); small copies go directly.
+void h2d_large(void* dst, const void* src, size_t bytes, cudaStream_t s);
+
 void* pool_alloc(size_t bytes);
 void pool_release(void* p);
 void pool_recycle(int dev);

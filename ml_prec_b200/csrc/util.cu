@@ -2,6 +2,8 @@
 #include "common.cuh"
 
 #include <algorithm>
+#include <cstring>
+#include <thread>
 #include <atomic>
 #include <chrono>
 #include <map>
@@ -135,6 +137,54 @@ size_t size_class(size_t b) {
     return (b + step - 1) & ~(step - 1);
 }
 }  // namespace
+
+// ---- large host-to-device copies ----------------------------------------------
+// A copy from pageable host memory is staged by the driver through its own
+// pinned buffers one piece at a time. Large inputs (the matrix arrays, 93 MB
+// at 60x220x85) go through two pinned staging buffers of this library
+// instead: host threads copy a chunk into one buffer while the DMA engine
+// moves the other, so the transfer runs near the link rate. The staging
+// buffers are pinned host memory (not device memory), made once per process.
+static constexpr size_t STAGE_BYTES = (size_t)16 << 20;
+static std::mutex g_stage_mu;
+static void* g_stage[2] = {nullptr, nullptr};
+static cudaEvent_t g_stage_ev[2] = {nullptr, nullptr};
+
+static void parallel_memcpy(void* dst, const void* src, size_t bytes) {
+    unsigned T = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    if (bytes < ((size_t)1 << 20)) T = 1;
+    if (T == 1) { std::memcpy(dst, src, bytes); return; }
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < T; t++) {
+        size_t a = bytes * t / T, b = bytes * (t + 1) / T;
+        th.emplace_back([=] { std::memcpy((char*)dst + a, (const char*)src + a, b - a); });
+    }
+    for (auto& x : th) x.join();
+}
+
+void h2d_large(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    if (bytes < ((size_t)8 << 20)) {
+        if (bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+        return;
+    }
+    std::lock_guard<std::mutex> lk(g_stage_mu);
+    if (!g_stage[0]) {
+        for (int k = 0; k < 2; k++) {
+            CK(cudaMallocHost(&g_stage[k], STAGE_BYTES));
+            CK(cudaEventCreateWithFlags(&g_stage_ev[k], cudaEventDisableTiming));
+            CK(cudaEventRecord(g_stage_ev[k], s));
+        }
+    }
+    size_t off = 0;
+    for (int k = 0; off < bytes; k ^= 1) {
+        size_t len = std::min(STAGE_BYTES, bytes - off);
+        CK(cudaEventSynchronize(g_stage_ev[k]));  // the buffer's previous copy has left it
+        parallel_memcpy(g_stage[k], (const char*)src + off, len);
+        CK(cudaMemcpyAsync((char*)dst + off, g_stage[k], len, cudaMemcpyHostToDevice, s));
+        CK(cudaEventRecord(g_stage_ev[k], s));
+        off += len;
+    }
+}
 
 void* pool_alloc(size_t bytes) {
     int dev = 0;
