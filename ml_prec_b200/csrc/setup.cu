@@ -385,24 +385,24 @@ __global__ void k_bucket_deg1(uint32_t N, const int* __restrict__ nlinks, uint8_
 // link. Only nodes that start with one link can ever be found with exactly one
 // link by the outer scan (a walk that leaves a node with one link continues
 // through it), so the scan runs over that candidate list in index order. The
-// walk is a sequential greedy process and runs on one thread.
-__global__ void k_cheb_tails(const uint32_t* __restrict__ ia, const uint32_t* __restrict__ ja,
-                             const uint32_t* __restrict__ slot, uint8_t* __restrict__ state,
-                             int* __restrict__ nlinks, const uint32_t* __restrict__ cand, uint32_t ncand,
-                             uint8_t* __restrict__ marked, uint32_t* __restrict__ map, uint32_t* __restrict__ out,
-                             int* __restrict__ err) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    uint32_t pind = 0;
-    for (uint32_t c = 0; c < ncand; c++) {
-        uint32_t i0 = cand[c];
+// walk is one ordered greedy pass (each step changes the link counts the next
+// reads), so it runs on the host over the marking kernels' link slots: an L2
+// round trip per step would make one GPU thread far slower at 1.12 M cells.
+// Returns the eliminated nodes in order; nlinks and marked are updated.
+static std::vector<uint32_t> cheb_tails(const std::vector<uint32_t>& ia, const std::vector<uint32_t>& ja,
+                                        const std::vector<uint32_t>& slot, std::vector<uint8_t> state,
+                                        std::vector<int>& nlinks, const std::vector<uint32_t>& cand,
+                                        std::vector<uint8_t>& marked) {
+    std::vector<uint32_t> order;
+    for (uint32_t i0 : cand) {
         if (nlinks[i0] != 1) continue;
         do {
-            map[pind++] = i0;
+            order.push_back(i0);
             marked[i0] = 1;
             uint32_t j_ = ia[i0] + 1, e = ia[i0 + 1];
             for (; j_ < e; j_++)
                 if (state[slot[j_]]) break;
-            if (j_ == e) { atomicOr(err, 4); out[0] = pind; return; }
+            if (j_ == e) MLP_THROW(ERR_INTERNAL, "Could not find remaining link");
             uint32_t i1 = ja[j_];
             state[slot[j_]] = 0;
             nlinks[i0] = -1;
@@ -410,12 +410,12 @@ __global__ void k_cheb_tails(const uint32_t* __restrict__ ia, const uint32_t* __
             i0 = i1;
         } while (nlinks[i0] == 1);
         if (nlinks[i0] == 0) {
-            map[pind++] = i0;
+            order.push_back(i0);
             marked[i0] = 1;
             nlinks[i0] = -1;
         }
     }
-    out[0] = pind;
+    return order;
 }
 
 __global__ void k_rmap(uint32_t N, const uint32_t* __restrict__ map, uint32_t* __restrict__ rmap) {
@@ -1122,19 +1122,21 @@ static void build_level_cheb(Hierarchy& H, const BuildCfg& cfg, uint32_t level, 
     S.marked.zero(s);
     uint32_t M = 0;
     if (cfg.use_tails) {
-        S.state.alloc(nnz ? nnz : 1);
-        CK(cudaMemcpyAsync(S.state.p, S.keep.p, nnz, cudaMemcpyDeviceToDevice, s));
         S.bucket.alloc(N);
         S.cand.alloc(N ? N : 1);
         k_bucket_deg1<<<grid_for(N, 256), 256, 0, s>>>(N, S.nlinks.p, S.bucket.p);
         CK_LAUNCH();
         std::vector<uint32_t> c1 = stable_partition(N, S.bucket.p, 1, 0, S.cand.p, 0, s);
-        S.cnt.alloc(1);
-        k_cheb_tails<<<1, 1, 0, s>>>(A.ia.p, A.ja.p, S.slot.p, S.state.p, S.nlinks.p, S.cand.p, c1[0], S.marked.p,
-                                     li.map.p, S.cnt.p, S.flag.p);
-        CK_LAUNCH();
-        M = read_u32(S.cnt.p, s);
-        if (read_flag(S.flag.p, s) & 4) MLP_THROW(ERR_INTERNAL, "Could not find remaining link");
+        std::vector<uint32_t> ia = A.ia.download(s, (size_t)N + 1), ja = A.ja.download(s, nnz);
+        std::vector<uint32_t> slot = S.slot.download(s, nnz), cand = S.cand.download(s, c1[0]);
+        std::vector<uint8_t> state = S.keep.download(s, nnz), marked(N, 0);  // the walk works on a copy
+        std::vector<int> nlinks = S.nlinks.download(s, N);
+        std::vector<uint32_t> tails = cheb_tails(ia, ja, slot, std::move(state), nlinks, cand, marked);
+        M = (uint32_t)tails.size();
+        if (M) CK(cudaMemcpyAsync(li.map.p, tails.data(), (size_t)M * 4, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(S.marked.p, marked.data(), N, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(S.nlinks.p, nlinks.data(), (size_t)N * 4, cudaMemcpyHostToDevice, s));
+        CK(cudaStreamSynchronize(s));  // the host vectors go out of scope
     }
     S.bucket.alloc(N);
     k_bucket_cheb_rest<<<grid_for(N, 256), 256, 0, s>>>(N, S.nlinks.p, S.marked.p, S.bucket.p);
