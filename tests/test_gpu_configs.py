@@ -54,7 +54,7 @@ def config1():
     A, b = M.CSRMatrix.spe(60, 220, 10, kx, ky, kz, c=1.0)
     Ao, bo = O.assemble(60, 220, 10, kx, ky, kz, 1.0, True)
     Po = O.Prec(Ao, "msplit", **MS2)
-    x12, it12, _, rc = O.pcg(Ao, bo, Po, 1e-12)
+    x12, it12, _, rc = O.pcg(Ao, bo, Po, 1e-12, maxit=500)
     assert rc == 0
     return A, b, Ao, bo, Po, x12
 
@@ -113,8 +113,10 @@ def test_fp32_form_full_size_against_oracle(M):
     kx, ky, kz = fields.field("layered", 2)
     A, b = M.CSRMatrix.spe(60, 220, 85, kx, ky, kz, c=1.0)
     Ao, bo = O.assemble(60, 220, 85, kx, ky, kz, 1.0, True)
-    xo, it, _, rc = O.pcg(Ao, bo, O.Prec(Ao, "msplit", **MS), 1e-12)
-    assert rc == 0
+    # 1e-11: at this size and contrast the FP64 iteration stagnates near 1e-12
+    # (rounding), so a tighter oracle tolerance would only run into the cap
+    xo, it, rel, rc = O.pcg(Ao, bo, O.Prec(Ao, "msplit", **MS), 1e-11, maxit=300)
+    assert rc == 0 and rel <= 1e-11
     P32 = M.MultiSplitPrec(A, fp32=True, **MS)
     nrm = np.linalg.norm(xo)
     for eps, bound in ((1e-8, 1e-4), (1e-10, 1e-6)):
