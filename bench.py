@@ -147,10 +147,12 @@ def run_ours(args, ws, rank, local):
     stream = torch.cuda.current_stream(dev)
     barrier = (lambda: torch.distributed.barrier()) if ws > 1 else (lambda: None)
 
-    def solve(P, fp32, eps=EPS):
+    def solve(P, fp32, eps=EPS, maxit=0):
         st = Stats()
-        check(lib().mlp_pcg_device(A.h, C.c_void_p(b_d.data_ptr()), P.h, C.c_void_p(x_d.data_ptr()), eps, 0,
-                                   int(fp32), C.byref(st), C.c_void_p(stream.cuda_stream)))
+        rc = lib().mlp_pcg_device(A.h, C.c_void_p(b_d.data_ptr()), P.h, C.c_void_p(x_d.data_ptr()), eps, maxit,
+                                  int(fp32), C.byref(st), C.c_void_p(stream.cuda_stream))
+        if rc != 0 and not (maxit and rc == 6):  # 6: the cap a caller asked for
+            check(rc)
         return st
 
     def timed(fp32, K, tag=None, autotune=False):
@@ -247,11 +249,11 @@ def run_ours(args, ws, rank, local):
         # the tight FP64 solution, with the device time of both forms there
         Pm = M.MultiSplitPrec(A, **MSPLIT)
         matched = None
-        for e_m in (1e-8, 1e-9, 1e-10, 1e-11, 1e-12):
-            xm, stm = host_solve(P32, e_m, True)
+        for e_m in (1e-8, 1e-9, 1e-10, 1e-11):
+            xm, stm = host_solve(P32, e_m, True, 1000)
             if np.linalg.norm(xm - x_true) / nrm <= 1e-8:
-                t32m = min(solve(P32, True, e_m).t_solve_ms for _ in range(3))
-                s64m = [solve(Pm, False, e_m) for _ in range(3)]
+                t32m = min(solve(P32, True, e_m, 1000).t_solve_ms for _ in range(3))
+                s64m = [solve(Pm, False, e_m, 1000) for _ in range(3)]
                 t64m = min(t.t_solve_ms for t in s64m)
                 matched = dict(eps=e_m, x_err=float(np.linalg.norm(xm - x_true) / nrm), iters=stm.niter,
                                solve_ms=t32m, fp64_iters=s64m[0].niter, fp64_solve_ms=t64m,
