@@ -1216,8 +1216,19 @@ struct Builder {
     // MultiSplitPrec::solve(level, f, x) (multi_split_solve.cc:59-157) with the
     // triangular solves in explicit form: each sweep is phase 1, the recursion
     // and phase 2; the correction sweeps update the residual in place.
+    // The recursion applies level l + 1 niter (or ncheb) times per call of
+    // level l, so a deep hierarchy with little coarsening multiplies the plan
+    // geometrically; past this many steps the build stops with an error.
+    static constexpr size_t PLAN_MAX_STEPS = 1000000;
+    void check_plan_size() const {
+        if (plan.ops.size() + (ps ? ps->size() : 0) > PLAN_MAX_STEPS)
+            MLP_THROW(ERR_LIMIT, "the preconditioner's application needs more than " + std::to_string(PLAN_MAX_STEPS) +
+                                     " steps (the hierarchy coarsens too little for its inner iterations)");
+    }
+
     void ms(uint32_t l, const T* f, T* x) {
         LevelScope scope(cur_level, l);
+        check_plan_size();
         if (persist_ok(l)) {
             persist_region([&] { ms(l, f, x); });
             return;
@@ -1380,6 +1391,7 @@ struct Builder {
     // Wavefront form of ms (the L and U solves one wavefront at a time).
     void ms_waves(uint32_t l, const T* f, T* x) {
         LevelScope scope(cur_level, l);
+        check_plan_size();
         Level& L = *H.lv[l];
         LevelWork<T>& w = W[l];
         uint32_t N = L.N, M = L.M;
@@ -1411,6 +1423,7 @@ struct Builder {
     // Prec::solve(level, f, x) (cheb_solve.cc:13-123)
     void ch(uint32_t l, const T* f, T* x) {
         LevelScope scope(cur_level, l);
+        check_plan_size();
         if (persist_ok(l)) {
             persist_region([&] { ch(l, f, x); });
             return;
@@ -1531,12 +1544,20 @@ static uint32_t small_budget() {
     return 200 * 1024;
 }
 
-// Persistent regions (k_persist) are on unless MLP_PERSIST=0; a region starts
-// at the first level of at most MLP_PERSIST_MAX_N rows (default 524,288, so
-// that a 1.12 M-cell level 0 keeps its bandwidth-bound separate kernels).
-static bool persist_enabled() {
+// Persistent regions (k_persist): MLP_PERSIST=1 turns them on, =0 off; unset,
+// they are used where they are needed, for dynamic inner iterations (on B200
+// the launch-per-step plan with programmatic dependent launch measured faster
+// for fixed iterations at 60x220x85: solve 18.0 ms against 29.8 ms). A region
+// starts at the first level of at most MLP_PERSIST_MAX_N rows (default
+// 524,288, so that a 1.12 M-cell level 0 keeps its bandwidth-bound separate
+// kernels).
+static bool persist_enabled(const Hierarchy& H) {
     const char* e = getenv("MLP_PERSIST");
-    return !(e && e[0] == '0');
+    if (e && e[0] == '1') return true;
+    if (e && e[0] == '0') return false;
+    for (uint32_t l = 0; l < H.nlevels; l++)
+        if (H.lv[l]->eps != 0) return true;
+    return false;
 }
 static uint32_t persist_max_n() {
     const char* e = getenv("MLP_PERSIST_MAX_N");
@@ -1546,7 +1567,7 @@ static uint32_t persist_max_n() {
 
 template <class T>
 static void builder_persist(Builder<T>& B, Prec& P) {
-    B.persist = persist_enabled();
+    B.persist = persist_enabled(B.H);
     B.persist_max_n = persist_max_n();
     B.pdesc = &P.pdesc;
     B.pbar = P.pbar.p;

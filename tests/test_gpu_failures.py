@@ -79,17 +79,25 @@ def test_multisplit_without_reaction_term_ends_in_the_direct_level(M):
     keeps all 1,584 unknowns until max_levels; like the reference built with
     its coarsest-level direct solver (multi_split_constr.cc:46-55 with
     HAVE_UMFPACK), the last level is then solved directly. Level sizes equal
-    the oracle's and the solve reaches the tolerance."""
+    the oracle's. With one inner iteration per level the application is a
+    chain of 15 levels; with five it would be 5^14 coarsest solves per
+    application, and the GPU build refuses that plan with MLP_ERR_LIMIT
+    instead of recording it."""
     from ml_prec_b200 import fields
     from oracle import oracle as O
     kx, ky, kz = fields.field("iid", 1)
+    one = dict(MSPLIT, niter=(1,))
     Ao, _ = O.assemble(12, 22, 6, kx, ky, kz, 0.0, False)
-    Po = O.Prec(Ao, "msplit", **MSPLIT)
+    Po = O.Prec(Ao, "msplit", **one)
     A, _ = M.CSRMatrix.spe(12, 22, 6, kx, ky, kz, c=0.0, dirichlet=False)
-    P = M.MultiSplitPrec(A, **MSPLIT)
+    P = M.MultiSplitPrec(A, **one)
     assert P.nlevels == Po.nlevels == 15
     assert [P.level(l)["N"] for l in range(15)] == [Po.level(l)["N"] for l in range(15)]
     assert P.level(14)["direct"]
+    assert np.isfinite(P.solve(np.random.default_rng(3).standard_normal(A.n))).all()
+    with pytest.raises(M.MlpError) as e:
+        M.MultiSplitPrec(A, **MSPLIT)
+    assert e.value.code == 9  # MLP_ERR_LIMIT
 
 
 def test_context_survives_the_failures(M):

@@ -25,13 +25,15 @@ def M():
 @pytest.fixture(params=["persistent", "persist_split", "dense", "separate", "small", "explicit", "waves"])
 def apply_path(request, monkeypatch):
     """Run each case through every apply path: the whole apply as one
-    persistent launch (default at these sizes), the finest level as separate
+    persistent launch (MLP_PERSIST=1 at these sizes), the finest level as separate
     launches around a persistent launch of the levels below it, the tabulated
     small-level operator with separate launches and the correction and
     phase-1 steps of the small levels merged, the same with every sweep step a
     separate kernel, the shared-memory small-level kernel (tabulation off),
     the launch path with explicit triangular solves (small kernel off), and
     the launch path with wavefront triangular solves."""
+    if request.param in ("persistent", "persist_split"):
+        monkeypatch.setenv("MLP_PERSIST", "1")
     if request.param == "persist_split":
         monkeypatch.setenv("MLP_PERSIST_MAX_N", "1200")
     if request.param in ("dense", "separate", "small", "explicit", "waves"):
@@ -187,7 +189,7 @@ def test_iteration_cap_ends_the_device_loop(M):
 @pytest.mark.parametrize("fp32", [False, True])
 def test_apply_forms_are_bit_identical(M, fp32, monkeypatch):
     """60x220x85 layered field: the levels below the finest one run as one
-    persistent launch (default); as separate launches with the correction and
+    persistent launch (MLP_PERSIST=1); as separate launches with the correction and
     phase-1 steps of the small levels merged; and as separate launches with
     every sweep step its own kernel. All three repeat the same arithmetic (same
     products, lane split and butterfly order), so the apply and the PCG
@@ -198,7 +200,7 @@ def test_apply_forms_are_bit_identical(M, fp32, monkeypatch):
     f = np.random.default_rng(5).standard_normal(A.n)
     kw = dict(q=(0.8,), niter=(5,), max_levels=15, degree_max=2, fp32=fp32)
     out = []
-    for env in ({}, {"MLP_PERSIST": "0"}, {"MLP_PERSIST": "0", "MLP_MERGE": "0"}):
+    for env in ({"MLP_PERSIST": "1"}, {"MLP_PERSIST": "0"}, {"MLP_PERSIST": "0", "MLP_MERGE": "0"}):
         for k in ("MLP_PERSIST", "MLP_MERGE"):
             monkeypatch.delenv(k, raising=False)
         for k, v in env.items():
