@@ -40,6 +40,13 @@ import time
 
 import numpy as np
 
+_T0 = time.perf_counter()
+
+
+def progress(msg):
+    """One line per finished phase on stderr (the JSON line stays on stdout)."""
+    print(f"[bench +{time.perf_counter() - _T0:7.1f}s] {msg}", file=sys.stderr, flush=True)
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -198,6 +205,7 @@ def run_ours(args, ws, rank, local):
     barrier()
     clk.stop()
     clocks = clk.summary()
+    progress("timed FP64 steps")
 
     out = dict(t64=t64, st64=st64, nb64=nb64, nlaunch=nlaunch, clocks=clocks, N=N, nnz=A.nnz())
     if not args.no_forms:
@@ -222,6 +230,7 @@ def run_ours(args, ws, rank, local):
         out["autotuned"] = dict(s_per_step=float(np.mean(ta)), iters=st_t.niter, solve_ms=st_t.t_solve_ms,
                                 setup_ms=st_t.t_setup_ms)
 
+        progress("autotuned FP64 steps")
     if not args.no_forms:
         # ---- FP32-stored hierarchy (flexible FP64 PCG) ----
         timed(True, 2)  # warm-up of the FP32 kernels and graphs
@@ -274,6 +283,7 @@ def run_ours(args, ws, rank, local):
                            x_diff_fp32_vs_fp64_1e8=float(np.linalg.norm(x32 - x64) / nrm),
                            within_1e8_of_fp64=matched)
 
+        progress("FP32 form")
         # ---- adjoint gradient on the same mesh ----
         rng = np.random.default_rng(2)
         obs = np.sort(rng.choice(N, 25, replace=False))
@@ -295,6 +305,7 @@ def run_ours(args, ws, rank, local):
                               setup_ms=prob.stats["forward"]["t_setup_ms"],
                               adjoint_iters=prob.stats["adjoint"]["niter"])
 
+        progress("adjoint")
         # ---- ensemble of 64 uneven realizations, sharded over the ranks ----
         dims = ensemble.realization_dims(64)
         mine = ensemble.shard(dims, rank, ws)
@@ -312,6 +323,7 @@ def run_ours(args, ws, rank, local):
                                looped_ms=float(np.median(loop)), members=len(mine),
                                cells=int(sum(np.prod(dims[i]) for i in mine)))
 
+        progress("ensemble")
     # ---- per-launch profile of one apply (the roofline's dominant kernel) ----
     # One apply of the plan, launch by launch, with CUDA events between the
     # launches (mlp_prec_profile): per launch group its time and algorithmic
@@ -328,6 +340,7 @@ def run_ours(args, ws, rank, local):
         g[2] += by
     out["apply_profile"] = sorted(([nm, c, ms_, by] for nm, (c, ms_, by) in groups.items()), key=lambda t: -t[2])
     out["apply_profile_ms"] = float(sum(t[1] for t in prof))
+    progress("apply profile")
     del Pp
 
     if not args.no_forms:
@@ -355,6 +368,7 @@ def run_ours(args, ws, rank, local):
         out["c01"] = dict(s_per_step=float(np.mean(t01)), iters=st01.niter, levels=nl01,
                           setup_ms=st01.t_setup_ms, solve_ms=st01.t_solve_ms, steps=len(t01))
         del A01
+        progress("c=0.1 steps")
 
     # ---- roofline: level-0 SpMV (staged kernel), events on its stream ----
     # 50 launches back to back between two events, alternating between two
@@ -396,6 +410,7 @@ def run_ours(args, ws, rank, local):
     e1.record(gs)
     e1.synchronize()
     out["spmv_ms"] = e0.elapsed_time(e1) / reps
+    progress("level-0 SpMV")
     del graph
     out["spmv_bytes"] = 12 * A.nnz() + 4 * (N + 1) + 8 * N + 8 * N
     del A2
@@ -420,6 +435,7 @@ def run_ours(args, ws, rank, local):
         out["e2e"] = {"value": float(np.mean(tt)), "unit": UNIT,
                       "h2d_bytes_per_step": int(ia.nbytes + ja.nbytes + a.nbytes + b.nbytes),
                       "d2h_bytes_per_step": int(8 * N)}
+        progress("e2e")
     return out
 
 
@@ -577,6 +593,7 @@ def main():
     cpu = None
     if not args.no_cpu_baseline:
         r = reference_cpu(1, 0)
+        progress("reference CPU step")
         if r:
             model, cores = cpu_info()
             cpu = {"value": r["value"], "unit": UNIT, "cores": 1, "kind": "reference",
@@ -585,10 +602,12 @@ def main():
                    "host_cpu": model, "host_cores": cores}
             if not args.no_forms:
                 r01 = reference_cpu(1, 0, c=0.1)
+                progress("reference CPU step, c=0.1")
                 if r01:
                     cpu["c01"] = {"value": r01["value"], "iters": r01["niter"], "setup_s": r01["setup"],
                                   "solve_s": r01["solve"]}
                 cpu["ensemble_concurrent"] = reference_ensemble(64)
+                progress("reference ensemble")
     line = {
         "metric": METRIC, "value": t_step, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t_step * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,

@@ -929,6 +929,8 @@ struct Builder {
     bool persist = false;                         // persistent regions allowed
     uint32_t persist_max_n = 0;                   // largest level that starts a region
     uint32_t persist_regions = 0, persist_steps = 0;
+    bool cluster = false;                         // cluster regions allowed
+    uint32_t cluster_max_n = 0;                   // largest level that starts one
 
     static PStep<T> pstep(uint32_t op, uint32_t lpr, uint32_t n0, uint32_t n1, const uint32_t* ia,
                           const uint32_t* ja, const T* a, const T* dval, const void* v0, const void* v1,
@@ -962,6 +964,19 @@ struct Builder {
         return true;
     }
 
+    // Whether the call of level l (l > 0, at most cluster_max_n rows) runs as
+    // one launch of the cluster form: outside persistent regions, and only
+    // where the level is not already a single launch (the small-level kernel
+    // or table, the direct solve).
+    bool cluster_ok(uint32_t l) const {
+        if (!cluster || ps || autotune || !explicit_solves || l == 0) return false;
+        const Level& L = *H.lv[l];
+        if (L.N > cluster_max_n || L.direct || dynamic()) return false;
+        if (small && small->valid() && small->first <= l) return false;
+        if (small64 && small64->valid() && small64->first <= l) return false;
+        return true;
+    }
+
     bool dynamic() const {
         for (uint32_t l = 0; l < H.nlevels; l++)
             if (H.lv[l]->eps != 0) return true;
@@ -969,7 +984,7 @@ struct Builder {
     }
 
     template <class Body>
-    void persist_region(Body body) {
+    void persist_region(Body body, bool in_cluster = false) {
         std::vector<PStep<T>> v;
         uint64_t b0 = bytes;
         ps = &v;
@@ -985,9 +1000,12 @@ struct Builder {
         const PStep<T>* dp = reinterpret_cast<const PStep<T>*>(d.p);
         uint32_t n = (uint32_t)v.size();
         PBar* bar = pbar;
-        op([=](cudaStream_t s) { launch_persist<T>(dp, n, bar, s); }, "persistent");
+        if (in_cluster) op([=](cudaStream_t s) { launch_persist_cluster<T>(dp, n, bar, s); }, "cluster");
+        else op([=](cudaStream_t s) { launch_persist<T>(dp, n, bar, s); }, "persistent");
         bytes += region;
-        persist_regions++;
+        // the host checks the error word after solves with grid regions
+        // (barrier limits, loop caps); cluster regions set none
+        if (!in_cluster) persist_regions++;
         persist_steps += n;
     }
 
@@ -1233,10 +1251,20 @@ struct Builder {
             persist_region([&] { ms(l, f, x); });
             return;
         }
+        if (cluster_ok(l)) {
+            persist_region([&] { ms(l, f, x); }, true);
+            return;
+        }
         if (small_call(l, f, x)) return;
         Level& L = *H.lv[l];
         if (L.direct) { direct(L, f, x); return; }
-        if (!explicit_solves) { ms_waves(l, f, x); return; }
+        if (!explicit_solves) {
+            if (L.eps != 0)
+                MLP_THROW(ERR_CONFIG, "inner_iter = dynamic needs the persistent apply, which needs the explicit "
+                                      "triangular solves (MLP_EXPLICIT=0 is set)");
+            ms_waves(l, f, x);
+            return;
+        }
         if (!ps && ms_merged(l, f, x)) return;
         if (L.eps != 0) { ms_dynamic(l, f, x); return; }
         LevelWork<T>& w = W[l];
@@ -1428,6 +1456,10 @@ struct Builder {
             persist_region([&] { ch(l, f, x); });
             return;
         }
+        if (cluster_ok(l)) {
+            persist_region([&] { ch(l, f, x); }, true);
+            return;
+        }
         if (small_call(l, f, x)) return;
         Level& L = *H.lv[l];
         LevelWork<T>& w = W[l];
@@ -1564,11 +1596,25 @@ static uint32_t persist_max_n() {
     if (e && *e) return (uint32_t)strtoul(e, nullptr, 10);
     return 1u << 19;
 }
+// Cluster regions (the cluster form of k_persist) take the calls of levels
+// below the finest with at most MLP_CLUSTER_MAX_N rows (default 65,536);
+// MLP_CLUSTER=0 turns them off.
+static bool cluster_enabled() {
+    const char* e = getenv("MLP_CLUSTER");
+    return !(e && e[0] == '0');
+}
+static uint32_t cluster_max_n() {
+    const char* e = getenv("MLP_CLUSTER_MAX_N");
+    if (e && *e) return (uint32_t)strtoul(e, nullptr, 10);
+    return 1u << 16;
+}
 
 template <class T>
 static void builder_persist(Builder<T>& B, Prec& P) {
     B.persist = persist_enabled(B.H);
     B.persist_max_n = persist_max_n();
+    B.cluster = cluster_enabled();
+    B.cluster_max_n = cluster_max_n();
     B.pdesc = &P.pdesc;
     B.pbar = P.pbar.p;
 }

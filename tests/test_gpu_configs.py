@@ -12,7 +12,8 @@ the golden fixtures, and run side by side in tests/test_oracle_vs_reference.py
 * uh_cheb (sigma 3, degree 4) on the 60x220x85 layered field: hierarchy
   bit-exact, PCG within one iteration and 1e-10.
 * The FP32 form on the 60x220x85 multi-split problem against the oracle.
-* Ensemble members against the oracle, forward and adjoint.
+* Ensemble members against the oracle, forward and adjoint (FP64 members to
+  1e-10; the FP32 form by true residual and to 1e-4).
 """
 import numpy as np
 import pytest
@@ -113,10 +114,11 @@ def test_fp32_form_full_size_against_oracle(M):
     kx, ky, kz = fields.field("layered", 2)
     A, b = M.CSRMatrix.spe(60, 220, 85, kx, ky, kz, c=1.0)
     Ao, bo = O.assemble(60, 220, 85, kx, ky, kz, 1.0, True)
-    # 1e-11: at this size and contrast the FP64 iteration stagnates near 1e-12
-    # (rounding), so a tighter oracle tolerance would only run into the cap
-    xo, it, rel, rc = O.pcg(Ao, bo, O.Prec(Ao, "msplit", **MS), 1e-11, maxit=300)
-    assert rc == 0 and rel <= 1e-11
+    # 1e-10: at this size and contrast the FP64 iteration stagnates between
+    # 1e-11 and 1e-12 (rounding), so a tighter oracle tolerance would only run
+    # into the cap
+    xo, it, rel, rc = O.pcg(Ao, bo, O.Prec(Ao, "msplit", **MS), 1e-10, maxit=300)
+    assert rc == 0 and rel <= 1e-10
     P32 = M.MultiSplitPrec(A, fp32=True, **MS)
     nrm = np.linalg.norm(xo)
     for eps, bound in ((1e-8, 1e-4), (1e-10, 1e-6)):
@@ -129,9 +131,12 @@ def test_fp32_form_full_size_against_oracle(M):
 
 def test_ensemble_members_against_oracle():
     """FP64 members (fixed launch shapes) equal the oracle's solves like single
-    solves do (iterations within 1, solution within 1e-10); the FP32 autotuned
-    ensemble reaches the tolerance and stays within 1e-5 of the oracle, forward
-    and adjoint."""
+    solves do (iterations within 1, solution within 1e-10). The FP32 autotuned
+    ensemble runs another iteration (FP32 preconditioner, flexible PCG), so it
+    is held to what the tolerance promises: a true FP64 residual within 10x
+    of the oracle's own, and a solution within 1e-4 of the oracle's (two
+    solutions with relative residual 1e-8 differ by up to cond(A) 1e-8),
+    forward and adjoint."""
     from ml_prec_b200 import ensemble, fields
     from oracle import oracle as O
     dims = [(30, 110, 10), (7, 11, 5), (12, 22, 6), (31, 17, 9), (16, 40, 12)]
@@ -142,10 +147,10 @@ def test_ensemble_members_against_oracle():
         Po = O.Prec(Ao, "msplit", **MS)
         xo, it, _, rc = O.pcg(Ao, bo, Po, 1e-8)
         assert rc == 0
-        ref.append((Ao, Po, xo, it))
+        ref.append((Ao, Po, xo, it, bo))
     E = ensemble.Ensemble(dims, fp32=False, autotune=False)
     _, its = E.forward(eps=1e-8)
-    for i, (Ao, Po, xo, it) in enumerate(ref):
+    for i, (Ao, Po, xo, it, bo) in enumerate(ref):
         x = E.x[i].cpu().numpy()
         assert abs(its[i] - it) <= 1, i
         assert np.linalg.norm(x - xo) <= 1e-10 * np.linalg.norm(xo), i
@@ -154,12 +159,17 @@ def test_ensemble_members_against_oracle():
     E.forward(eps=1e-8)
     p_obs = [np.zeros(len(o)) for o in E.obs]
     E.adjoint(p_obs, eps=1e-8)
-    for i, (Ao, Po, xo, it) in enumerate(ref):
+    def res(A, b, x):
+        return np.linalg.norm(b - O.spmv(A, x))
+
+    for i, (Ao, Po, xo, it, bo) in enumerate(ref):
         x = E.x[i].cpu().numpy()
-        assert np.linalg.norm(x - xo) <= 1e-5 * np.linalg.norm(xo), i
+        assert res(Ao, bo, x) <= 10 * res(Ao, bo, xo), i
+        assert np.linalg.norm(x - xo) <= 1e-4 * np.linalg.norm(xo), i
         g = E.g[i].cpu().numpy()
         lo, _, _, rc = O.pcg(Ao, g, Po, 1e-8, x0_zero=True)
         assert rc == 0
         lam = E.lam[i].cpu().numpy()
-        assert np.linalg.norm(lam - lo) <= 1e-5 * np.linalg.norm(lo), i
+        assert res(Ao, g, lam) <= 10 * res(Ao, g, lo), i
+        assert np.linalg.norm(lam - lo) <= 1e-4 * np.linalg.norm(lo), i
     E.close()
