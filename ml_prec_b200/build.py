@@ -26,7 +26,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
           "--expt-relaxed-constexpr", "-DNDEBUG"]
 NO_FMA = {"setup.cu"}
-SOURCES = ["util.cu", "setup.cu", "small.cu", "persist.cu", "cluster.cu", "solve.cu", "adjoint.cu", "capi.cu"]
+SOURCES = ["util.cu", "setup.cu", "small.cu", "persist.cu", "solve.cu", "adjoint.cu", "capi.cu"]
 
 
 def nvcc():

@@ -73,9 +73,8 @@ struct PBar {
     double red[2048];
 };
 
-// Threads per CTA of k_persist: grid form, cluster form.
+// Threads per CTA of k_persist.
 static constexpr int PK_THREADS = 512;
-static constexpr int PKC_THREADS = 1024;
 
 // Records the launch of k_persist<T> over steps[0, nsteps) on stream s (a
 // cooperative launch: every CTA is resident at once, which the barrier needs).
@@ -85,16 +84,5 @@ void launch_persist(const PStep<T>* steps, uint32_t nsteps, PBar* bar, cudaStrea
 // CTAs of one launch (a multiple of the SM count).
 template <class T>
 unsigned persist_grid();
-
-// The cluster form: one thread-block cluster runs the steps, with the
-// hardware cluster barrier between them (a programmatic dependent launch when
-// the plan's kernels are). No step may need more than the cluster's threads
-// for its bit-identical arithmetic: none does, rows are spread over warps.
-template <class T>
-void launch_persist_cluster(const PStep<T>* steps, uint32_t nsteps, PBar* bar, cudaStream_t s);
-
-// CTAs of the cluster (16, or fewer when that does not fit).
-template <class T>
-unsigned persist_cluster_size();
 
 }  // namespace mlp

@@ -12,7 +12,6 @@
 #include <map>
 #include <mutex>
 
-#include "cluster.cuh"
 #include "persist.cuh"
 #include "small.cuh"
 #include "solve.cuh"
@@ -930,10 +929,6 @@ struct Builder {
     bool persist = false;                         // persistent regions allowed
     uint32_t persist_max_n = 0;                   // largest level that starts a region
     uint32_t persist_regions = 0, persist_steps = 0;
-    bool cluster = false;                         // cluster regions allowed
-    bool cluster_smem = true;                     // the shared-memory form where it fits
-    uint32_t cluster_max_n = 0;                   // largest level that starts one
-    uint32_t cluster_smem_regions = 0;
 
     static PStep<T> pstep(uint32_t op, uint32_t lpr, uint32_t n0, uint32_t n1, const uint32_t* ia,
                           const uint32_t* ja, const T* a, const T* dval, const void* v0, const void* v1,
@@ -967,19 +962,6 @@ struct Builder {
         return true;
     }
 
-    // Whether the call of level l (l > 0, at most cluster_max_n rows) runs as
-    // one launch of the cluster form: outside persistent regions, and only
-    // where the level is not already a single launch (the small-level kernel
-    // or table, the direct solve).
-    bool cluster_ok(uint32_t l) const {
-        if (!cluster || ps || autotune || !explicit_solves || l == 0) return false;
-        const Level& L = *H.lv[l];
-        if (L.N > cluster_max_n || L.direct || dynamic()) return false;
-        if (small && small->valid() && small->first <= l) return false;
-        if (small64 && small64->valid() && small64->first <= l) return false;
-        return true;
-    }
-
     bool dynamic() const {
         for (uint32_t l = 0; l < H.nlevels; l++)
             if (H.lv[l]->eps != 0) return true;
@@ -987,7 +969,7 @@ struct Builder {
     }
 
     template <class Body>
-    void persist_region(Body body, bool in_cluster = false) {
+    void persist_region(Body body) {
         std::vector<PStep<T>> v;
         uint64_t b0 = bytes;
         ps = &v;
@@ -1003,50 +985,10 @@ struct Builder {
         const PStep<T>* dp = reinterpret_cast<const PStep<T>*>(d.p);
         uint32_t n = (uint32_t)v.size();
         PBar* bar = pbar;
-        if (in_cluster) op([=](cudaStream_t s) { launch_persist_cluster<T>(dp, n, bar, s); }, "cluster");
-        else op([=](cudaStream_t s) { launch_persist<T>(dp, n, bar, s); }, "persistent");
+        op([=](cudaStream_t s) { launch_persist<T>(dp, n, bar, s); }, "persistent");
         bytes += region;
-        // the host checks the error word after solves with grid regions
-        // (barrier limits, loop caps); cluster regions set none
-        if (!in_cluster) persist_regions++;
+        persist_regions++;
         persist_steps += n;
-    }
-
-    // The call of level l as one cluster launch: the shared-memory form when
-    // the level's data fit a 16-CTA cluster, else the cluster form of the
-    // persistent interpreter (vectors in global memory).
-    template <class Body>
-    void cluster_region(uint32_t l, const T* f, T* x, Body body) {
-        if (!cluster_smem) {
-            persist_region(body, true);
-            return;
-        }
-        std::vector<PStep<T>> v;
-        uint64_t b0 = bytes;
-        ps = &v;
-        body();
-        ps = nullptr;
-        std::vector<ClusterVec> vecs;
-        for (uint32_t k = l; k < H.nlevels; k++) {
-            vecs.push_back({W[k].w.p, (uint32_t)W[k].w.n});
-            vecs.push_back({W[k].r.p, (uint32_t)W[k].r.n});
-            vecs.push_back({W[k].u0.p, (uint32_t)W[k].u0.n});
-        }
-        DBuf<uint8_t> d;
-        uint32_t cs = 0, smem = 0;
-        if (v.empty() || !cluster_prog_build<T>(v, f, x, H.lv[l]->N, vecs, d, cs, smem, stream)) {
-            bytes = b0;
-            persist_region(body, true);
-            return;
-        }
-        uint64_t region = bytes - b0;
-        bytes = b0;
-        pdesc->push_back(std::move(d));
-        const CProg<T>* pp = reinterpret_cast<const CProg<T>*>(pdesc->back().p);
-        op([=](cudaStream_t s) { launch_cluster_level<T>(pp, cs, smem, s); }, "cluster_smem");
-        bytes += region;
-        persist_steps += (uint32_t)v.size();
-        cluster_smem_regions++;
     }
 
     // FP32 hierarchy: the tabulated operator of the small levels in FP64
@@ -1293,10 +1235,6 @@ struct Builder {
             persist_region([&] { ms(l, f, x); });
             return;
         }
-        if (cluster_ok(l)) {
-            cluster_region(l, f, x, [&] { ms(l, f, x); });
-            return;
-        }
         if (small_call(l, f, x)) return;
         Level& L = *H.lv[l];
         if (L.direct) { direct(L, f, x); return; }
@@ -1498,10 +1436,6 @@ struct Builder {
             persist_region([&] { ch(l, f, x); });
             return;
         }
-        if (cluster_ok(l)) {
-            cluster_region(l, f, x, [&] { ch(l, f, x); });
-            return;
-        }
         if (small_call(l, f, x)) return;
         Level& L = *H.lv[l];
         LevelWork<T>& w = W[l];
@@ -1638,32 +1572,10 @@ static uint32_t persist_max_n() {
     if (e && *e) return (uint32_t)strtoul(e, nullptr, 10);
     return 1u << 19;
 }
-// Cluster regions take the calls of levels below the finest with at most
-// MLP_CLUSTER_MAX_N rows (default 65,536): in shared memory (k_cluster_level)
-// where the level's data fit, else the cluster form of k_persist;
-// MLP_CLUSTER_SMEM=0 keeps every region in the k_persist form and
-// MLP_CLUSTER=0 turns them off.
-static bool cluster_enabled() {
-    const char* e = getenv("MLP_CLUSTER");
-    return !(e && e[0] == '0');
-}
-static bool cluster_smem_enabled() {
-    const char* e = getenv("MLP_CLUSTER_SMEM");
-    return !(e && e[0] == '0');
-}
-static uint32_t cluster_max_n() {
-    const char* e = getenv("MLP_CLUSTER_MAX_N");
-    if (e && *e) return (uint32_t)strtoul(e, nullptr, 10);
-    return 1u << 16;
-}
-
 template <class T>
 static void builder_persist(Builder<T>& B, Prec& P) {
     B.persist = persist_enabled(B.H);
     B.persist_max_n = persist_max_n();
-    B.cluster = cluster_enabled();
-    B.cluster_smem = cluster_smem_enabled();
-    B.cluster_max_n = cluster_max_n();
     B.pdesc = &P.pdesc;
     B.pbar = P.pbar.p;
 }

@@ -11,7 +11,8 @@ the golden fixtures, and run side by side in tests/test_oracle_vs_reference.py
   the solution error against the oracle's FP64 solution at 1e-12.
 * uh_cheb (sigma 3, degree 4) on the 60x220x85 layered field: hierarchy
   bit-exact, PCG within one iteration and 1e-10.
-* The FP32 form on the 60x220x85 multi-split problem against the oracle.
+* The FP32 form on the 60x220x85 multi-split problem against the oracle (at
+  1e-8 and 1e-9: there the FP64 iteration itself stagnates near 5.6e-10).
 * Ensemble members against the oracle, forward and adjoint (FP64 members to
   1e-10; the FP32 form by true residual and to 1e-4).
 """
@@ -114,14 +115,14 @@ def test_fp32_form_full_size_against_oracle(M):
     kx, ky, kz = fields.field("layered", 2)
     A, b = M.CSRMatrix.spe(60, 220, 85, kx, ky, kz, c=1.0)
     Ao, bo = O.assemble(60, 220, 85, kx, ky, kz, 1.0, True)
-    # 1e-10: at this size and contrast the FP64 iteration stagnates between
-    # 1e-11 and 1e-12 (rounding), so a tighter oracle tolerance would only run
-    # into the cap
-    xo, it, rel, rc = O.pcg(Ao, bo, O.Prec(Ao, "msplit", **MS), 1e-10, maxit=300)
-    assert rc == 0 and rel <= 1e-10
+    # 1e-9: at this size and contrast the FP64 iteration (the oracle's, like
+    # the reference's) stagnates near 5.6e-10 (rounding; 81 iterations reach
+    # 1e-9, 300 stop at 5.6e-10), so a tighter tolerance only runs into the cap
+    xo, it, rel, rc = O.pcg(Ao, bo, O.Prec(Ao, "msplit", **MS), 1e-9, maxit=300)
+    assert rc == 0 and rel <= 1e-9
     P32 = M.MultiSplitPrec(A, fp32=True, **MS)
     nrm = np.linalg.norm(xo)
-    for eps, bound in ((1e-8, 1e-4), (1e-10, 1e-6)):
+    for eps, bound in ((1e-8, 1e-4), (1e-9, 1e-5)):
         st = M.SolverStats()
         x = M.PCGSolver(A, b, P32, stats=st, eps=eps, flexible=True)
         err = np.linalg.norm(x - xo) / nrm

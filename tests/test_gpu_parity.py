@@ -22,16 +22,11 @@ def M():
     return M
 
 
-@pytest.fixture(params=["persistent", "persist_split", "cluster", "cluster_global", "dense", "separate", "small",
-                        "explicit", "waves"])
+@pytest.fixture(params=["persistent", "persist_split", "dense", "separate", "small", "explicit", "waves"])
 def apply_path(request, monkeypatch):
     """Run each case through every apply path: the whole apply as one
     persistent launch (MLP_PERSIST=1 at these sizes), the finest level as separate
-    launches around a persistent launch of the levels below it, the finest
-    level as separate launches around one cluster launch per call of the
-    levels below it (small-level kernel off, so that those levels have sweeps
-    to run), with the levels' data in the cluster's shared memory and with
-    them in global memory, the tabulated
+    launches around a persistent launch of the levels below it, the tabulated
     small-level operator with separate launches and the correction and
     phase-1 steps of the small levels merged, the same with every sweep step a
     separate kernel, the shared-memory small-level kernel (tabulation off),
@@ -43,12 +38,6 @@ def apply_path(request, monkeypatch):
         monkeypatch.setenv("MLP_PERSIST_MAX_N", "1200")
     if request.param in ("dense", "separate", "small", "explicit", "waves"):
         monkeypatch.setenv("MLP_PERSIST", "0")
-    if request.param in ("cluster", "cluster_global"):
-        monkeypatch.setenv("MLP_SMALL_BUDGET", "0")
-    else:
-        monkeypatch.setenv("MLP_CLUSTER", "0")
-    if request.param == "cluster_global":
-        monkeypatch.setenv("MLP_CLUSTER_SMEM", "0")
     if request.param == "separate":
         monkeypatch.setenv("MLP_MERGE", "0")
     if request.param == "small":
@@ -93,7 +82,7 @@ def launch_path_refuses_dynamic(M, g, A, apply_path):
     """Dynamic inner iterations (inner_iter = dynamic) decide the number of
     sweeps on the device inside the persistent launch; the launch-per-step
     paths refuse them with MLP_ERR_CONFIG. Returns True when that was checked."""
-    if "level_eps" not in g["options"] or apply_path in ("persistent", "persist_split", "cluster", "cluster_global"):
+    if "level_eps" not in g["options"] or apply_path in ("persistent", "persist_split"):
         return False
     with pytest.raises(M.MlpError) as e:
         gpu_prec(A, g)
@@ -200,22 +189,19 @@ def test_iteration_cap_ends_the_device_loop(M):
 @pytest.mark.parametrize("fp32", [False, True])
 def test_apply_forms_are_bit_identical(M, fp32, monkeypatch):
     """60x220x85 layered field: the levels below the finest one run as one
-    persistent launch (MLP_PERSIST=1); as separate launches with each call of
-    the 26,907-row level 2 one cluster launch, its data in the cluster's
-    shared memory (the default) or in global memory; as separate launches
-    with the correction and phase-1 steps of the small levels merged; and as
-    separate launches with every sweep step its own kernel. All five repeat
-    the same arithmetic (same products, lane split and butterfly order), so
-    the apply and the PCG iterates are bit-identical."""
+    persistent launch (MLP_PERSIST=1); as separate launches with the
+    correction and phase-1 steps of the small levels merged (the default);
+    and as separate launches with every sweep step its own kernel. All three
+    repeat the same arithmetic (same products, lane split and butterfly
+    order), so the apply and the PCG iterates are bit-identical."""
     from ml_prec_b200 import fields
     kx, ky, kz = fields.field("layered", 2)
     A, b = M.CSRMatrix.spe(60, 220, 85, kx, ky, kz, c=1.0)
     f = np.random.default_rng(5).standard_normal(A.n)
     kw = dict(q=(0.8,), niter=(5,), max_levels=15, degree_max=2, fp32=fp32)
     out = []
-    for env in ({"MLP_PERSIST": "1"}, {}, {"MLP_CLUSTER_SMEM": "0"}, {"MLP_CLUSTER": "0"},
-                {"MLP_CLUSTER": "0", "MLP_MERGE": "0"}):
-        for k in ("MLP_PERSIST", "MLP_MERGE", "MLP_CLUSTER", "MLP_CLUSTER_SMEM"):
+    for env in ({"MLP_PERSIST": "1"}, {}, {"MLP_MERGE": "0"}):
+        for k in ("MLP_PERSIST", "MLP_MERGE"):
             monkeypatch.delenv(k, raising=False)
         for k, v in env.items():
             monkeypatch.setenv(k, v)
