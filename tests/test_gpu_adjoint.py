@@ -63,3 +63,50 @@ def test_autograd_binding(problem):
     Jt.backward()
     assert abs(Jt.item() - J) <= 1e-12 * J
     assert np.allclose(th.grad.numpy(), g, rtol=1e-10, atol=1e-14 * np.abs(g).max())
+
+
+def test_full_size_gradient_against_oracle_and_central_differences():
+    """60x220x85 (1,122,000 cells): the adjoint gradient over all cells
+    against the oracle's FP64 gradient (forward and adjoint solves at 1e-12,
+    capped at 300 iterations: the FP64 iteration stagnates near there), and
+    central differences (step 1e-6) on 64 uniformly drawn cells and on the 16
+    cells of largest sensitivity. With 25 observation cells in a heterogeneous
+    field, 99 % of the cells have |dJ/dlnK| below 1e-22 (on this problem the
+    uniform draw finds none above 1e-28, against max |g| = 4.3e-9), where an
+    error relative to the cell's own value is meaningless; the uniform sample
+    is held to 1e-5 of max |g| per cell, the 16 largest to 1e-5 normwise."""
+    from ml_prec_b200 import adjoint
+    from oracle import oracle as O
+    dims = (60, 220, 85)
+    prob, theta = adjoint.make_problem(*dims, eps=1e-12, fp32=True)
+    J, g, lam, p = prob.gradient(theta)
+    kx, ky, kz = adjoint.field_from_theta(*dims, theta)
+    A, b = O.assemble(*dims, kx, ky, kz, 1.0, True)
+    P = O.Prec(A, "msplit")
+    po, _, _, rc = O.pcg(A, b, P, 1e-12, maxit=300, x0_zero=True)
+    assert rc in (0, -3)
+    r = po[prob.obs] - prob.p_obs
+    go = np.zeros(A.n)
+    go[prob.obs] = r
+    lo, _, _, rc = O.pcg(A, go, P, 1e-12, maxit=300, x0_zero=True)
+    assert rc in (0, -3)
+    gref = O.grad_logk(*dims, kx, ky, kz, po, lo)
+    assert abs(J - 0.5 * np.sum(r ** 2)) <= TOL * J
+    assert np.linalg.norm(g - gref) <= TOL * np.linalg.norm(gref)
+    rng = np.random.default_rng(11)
+    uniform = rng.choice(len(g), size=64, replace=False)
+    top = np.argsort(-np.abs(g))[:16]
+    h = 1e-6
+
+    def fd(cells):
+        out = np.empty(len(cells))
+        for t, c in enumerate(cells):
+            tp = theta.copy(); tp[c] += h
+            tm = theta.copy(); tm[c] -= h
+            out[t] = (prob.objective(tp)[0] - prob.objective(tm)[0]) / (2 * h)
+        return out
+
+    scale = np.abs(g).max()
+    assert np.abs(fd(uniform) - g[uniform]).max() <= TOL * scale
+    ft = fd(top)
+    assert np.linalg.norm(ft - g[top]) <= TOL * np.linalg.norm(g[top])
