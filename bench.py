@@ -257,9 +257,11 @@ def run_ours(args, ws, rank, local):
         # the loosest tolerance at which the FP32-form solution is within 1e-8 of
         # the tight FP64 solution, with the device time of both forms there
         Pm = M.MultiSplitPrec(A, **MSPLIT)
-        matched = None
-        for e_m in (1e-8, 1e-9, 1e-10, 1e-11):
+        matched, sweep = None, []
+        for e_m in (1e-8, 1e-9, 1e-10, 1e-11, 1e-12):
             xm, stm = host_solve(P32, e_m, True, 1000)
+            sweep.append(dict(eps=e_m, x_err=float(np.linalg.norm(xm - x_true) / nrm), iters=stm.niter,
+                              rel_res=stm.final_rel))
             if np.linalg.norm(xm - x_true) / nrm <= 1e-8:
                 t32m = min(solve(P32, True, e_m, 1000).t_solve_ms for _ in range(3))
                 s64m = [solve(Pm, False, e_m, 1000) for _ in range(3)]
@@ -281,7 +283,7 @@ def run_ours(args, ws, rank, local):
                            x_err_fp32_1e10=float(np.linalg.norm(x32b - x_true) / nrm),
                            iters_1e10=st10.niter, rel_res_1e10=st10.final_rel,
                            x_diff_fp32_vs_fp64_1e8=float(np.linalg.norm(x32 - x64) / nrm),
-                           within_1e8_of_fp64=matched)
+                           within_1e8_of_fp64=matched, x_err_sweep=sweep)
 
         progress("FP32 form")
         # ---- adjoint gradient on the same mesh ----
@@ -325,23 +327,46 @@ def run_ours(args, ws, rank, local):
                                cells=int(sum(np.prod(dims[i]) for i in mine)))
 
         progress("ensemble")
-    # ---- per-launch profile of one apply (the roofline's dominant kernel) ----
-    # One apply of the plan, launch by launch, with CUDA events between the
-    # launches (mlp_prec_profile): per launch group its time and algorithmic
-    # bytes. With a 126 MB L2 the levels below the finest one are largely
-    # L2-resident, so their GB/s can exceed the HBM peak.
+    # ---- per-launch time of one apply inside its graph (the roofline's kernel) ----
+    # mlp_prec_timeline: 10 back-to-back replays of the apply graph, each
+    # kernel stamping %globaltimer as it passes its dependent-launch wait; per
+    # launch group its in-graph time and algorithmic bytes. The levels below
+    # the finest one are L2-resident (126 MB L2), so their traffic is mostly
+    # not DRAM traffic. The launch-by-launch replay with events between the
+    # launches (mlp_prec_profile) is kept beside it: it adds an event and a
+    # launch gap to every launch, so it overstates the small launches.
     Pp = M.MultiSplitPrec(A, **MSPLIT)
     Pp.solve(np.random.default_rng(3).standard_normal(N))
+
+    def grouped(rows, scale):
+        groups = {}
+        for nm, t_, by in rows:
+            g = groups.setdefault(nm, [0, 0.0, 0])
+            g[0] += 1
+            g[1] += t_ * scale
+            g[2] += by
+        return sorted(([nm, c, t_, by] for nm, (c, t_, by) in groups.items()), key=lambda t: -t[2])
+
     prof = Pp.profile(5)
-    groups = {}
-    for nm, ms_, by in prof:
-        g = groups.setdefault(nm, [0, 0.0, 0])
-        g[0] += 1
-        g[1] += ms_
-        g[2] += by
-    out["apply_profile"] = sorted(([nm, c, ms_, by] for nm, (c, ms_, by) in groups.items()), key=lambda t: -t[2])
+    out["apply_profile"] = grouped(prof, 1.0)  # ms
     out["apply_profile_ms"] = float(sum(t[1] for t in prof))
-    progress("apply profile")
+    tl = Pp.timeline(10)
+    out["apply_timeline"] = grouped(tl, 1e-3)  # ms
+    out["apply_timeline_ms"] = float(sum(t[1] for t in tl)) / 1e3
+    # the whole apply (gather, graph, scatter) 20 times, events around them
+    fa = torch.randn(N, dtype=torch.float64, device=dev)
+    za = torch.empty_like(fa)
+    g0 = torch.cuda.Event(enable_timing=True)
+    g1 = torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    for _ in range(20):
+        check(lib().mlp_prec_apply(Pp.h, C.c_void_p(fa.data_ptr()), C.c_void_p(za.data_ptr()),
+                                   C.c_void_p(stream.cuda_stream)))
+    g1.record(stream)
+    g1.synchronize()
+    out["apply_graph_ms"] = g0.elapsed_time(g1) / 20
+    del fa, za
+    progress("apply timeline")
     del Pp
 
     if not args.no_forms:
@@ -600,12 +625,16 @@ def main():
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
     achieved = res["spmv_bytes"] / (res["spmv_ms"] / 1e3) / 1e9
-    prof = res["apply_profile"]
-    top = prof[0]  # [name, launches, ms, bytes] of the launch group with the most time in one apply
-    apply_groups = [{"launch": nm, "launches": c, "ms": round(ms_, 4), "MB": round(by / 1e6, 3),
-                     "GBps": round(by / (ms_ / 1e3) / 1e9, 1) if ms_ > 0 else None,
-                     "frac": round(by / (ms_ / 1e3) / 1e9 / hbm, 3) if ms_ > 0 else None}
-                    for nm, c, ms_, by in prof[:10]]
+    prof = res["apply_timeline"]
+    top = prof[0]  # [name, launches, ms, bytes] of the launch group with the most in-graph time per apply
+
+    def group_rows(rows):
+        return [{"launch": nm, "launches": c, "ms": round(ms_, 4), "MB": round(by / 1e6, 3),
+                 "GBps": round(by / (ms_ / 1e3) / 1e9, 1) if ms_ > 0 else None,
+                 "frac": round(by / (ms_ / 1e3) / 1e9 / hbm, 3) if ms_ > 0 else None}
+                for nm, c, ms_, by in rows[:12]]
+
+    apply_groups = group_rows(prof)
     st64 = res["st64"]
     cpu = None
     if not args.no_cpu_baseline:
@@ -646,16 +675,19 @@ def main():
         },
         "e2e": res.get("e2e"),
         "gpu_launches": res["nlaunch"],
-        "roofline": {"bound": "hbm", "kernel": f"{top[0]} (the apply's launch group with the most device time)",
+        "roofline": {"bound": "hbm", "kernel": f"{top[0]} (the apply's launch group with the most in-graph time)",
                      "achieved": top[3] / (top[2] / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
                      "frac": top[3] / (top[2] / 1e3) / 1e9 / hbm,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s",
                      "bytes_per_launch": top[3] / top[1], "ms_per_launch": top[2] / top[1],
-                     "timing": "one apply replayed launch by launch (mlp_prec_profile, 5 replays), CUDA events "
-                               "between the launches on the apply's stream",
+                     "timing": "in-graph time per launch (mlp_prec_timeline: %globaltimer stamped by each kernel "
+                               "as it passes its dependent-launch wait, 10 back-to-back replays of the apply graph)",
                      "traffic": None,
                      "traffic_source": "see profiles/ for the ncu DRAM traffic of this kernel",
                      "apply_groups": apply_groups,
+                     "apply_ms_in_graph": res["apply_timeline_ms"],
+                     "apply_graph_ms_events": res["apply_graph_ms"],
+                     "apply_groups_launch_by_launch": group_rows(res["apply_profile"]),
                      "apply_ms_launch_by_launch": res["apply_profile_ms"],
                      "spmv_level0": {"kernel": "level-0 CSR SpMV y = A x (k_spmv_staged, pipelined tiles)",
                                      "achieved": achieved, "frac": achieved / hbm,

@@ -169,6 +169,15 @@ int mlp_prec_bytes_per_apply(const mlp_prec* P, uint64_t* bytes);
  * entries are written. */
 int mlp_prec_profile(mlp_prec* P, uint32_t reps, uint32_t cap, uint32_t* nops, double* ms, uint64_t* bytes,
                      char* names, uint32_t name_len);
+/* Profiling aid without a reference counterpart: replays the apply graph reps
+ * (at least 2) times back to back and reports, per launch (the order and
+ * names of mlp_prec_profile), its mean time inside the graph in us, from
+ * %globaltimer stamps that each kernel writes as it passes its
+ * dependent-launch wait (the launch lasts until the next one passes its
+ * wait). Plans with launches of other kinds (the persistent or shared-memory
+ * small-level kernels) return MLP_ERR_INTERNAL; no other apply may run on the
+ * device meanwhile. */
+int mlp_prec_timeline(mlp_prec* P, uint32_t reps, uint32_t cap, uint32_t* nops, double* us);
 
 /* ---- solver ----------------------------------------------------------------
  * PCGSolver(A, b, B, x, stats, eps, NORM_L2) (solvers.h:31-32, pcg.cc:8-102):

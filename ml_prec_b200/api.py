@@ -268,6 +268,18 @@ class PrecBase:
         return [(raw[64 * k:64 * (k + 1)].split(b"\0", 1)[0].decode(), float(ms[k]), int(by[k]))
                 for k in range(cap)]
 
+    def timeline(self, reps=5):
+        """Per launch of the apply: (name, mean us inside the apply graph,
+        algorithmic bytes), from %globaltimer stamps over reps back-to-back
+        graph replays (mlp_prec_timeline); names and bytes as profile()."""
+        prof = self.profile(1)
+        n = C.c_uint32()
+        us = np.zeros(max(len(prof), 1))
+        check(lib().mlp_prec_timeline(self.h, reps, len(prof), C.byref(n), ptr(us, f64p)))
+        if n.value != len(prof):
+            raise RuntimeError("timeline and profile disagree on the number of launches")
+        return [(nm, float(us[k]), by) for k, (nm, _, by) in enumerate(prof)]
+
     @property
     def bytes_per_apply(self):
         b = C.c_uint64()

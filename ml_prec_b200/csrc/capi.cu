@@ -362,6 +362,16 @@ int mlp_prec_profile(mlp_prec* P, uint32_t reps, uint32_t cap, uint32_t* nops, d
     API_END
 }
 
+int mlp_prec_timeline(mlp_prec* P, uint32_t reps, uint32_t cap, uint32_t* nops, double* us) {
+    API_BEGIN
+    if (!P || !nops) MLP_THROW(ERR_ARG, "null pointer");
+    std::vector<double> t = timeline_apply(*P->P, reps, P->s);
+    *nops = (uint32_t)t.size();
+    for (uint32_t k = 0; k < t.size() && k < cap; k++)
+        if (us) us[k] = t[k];
+    API_END
+}
+
 int mlp_prec_nlevels(const mlp_prec* P, uint32_t* nl) {
     API_BEGIN
     if (!P || !nl) MLP_THROW(ERR_ARG, "null pointer");

@@ -193,7 +193,15 @@ struct DCSR {
 // its writes are visible; a no-op when launched without the attribute) and
 // then pdl_trigger() (lets the next kernel be scheduled while this one runs),
 // so the launch latency of each kernel overlaps its predecessor.
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// MLP_TIMELINE_HOOK: the in-graph timeline of the apply (mlp_prec_timeline)
+// stamps the time each kernel of solve.cu passes this wait; elsewhere empty.
+#ifndef MLP_TIMELINE_HOOK
+#define MLP_TIMELINE_HOOK()
+#endif
+__device__ __forceinline__ void pdl_wait() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    MLP_TIMELINE_HOOK();
+}
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" :::); }
 
 bool pdl_enabled();

@@ -12,6 +12,30 @@
 #include <map>
 #include <mutex>
 
+// In-graph timeline (mlp_prec_timeline): while c_tl_buf is set, thread 0 of
+// block 0 of every kernel of this file writes %globaltimer into it when it
+// passes the dependent-launch wait, so consecutive stamps bound each launch's
+// time inside the graph (with programmatic dependent launch the next kernel's
+// wait returns when this one has finished). Off (null) the cost is one
+// constant-cache load in one thread per kernel.
+namespace mlp {
+__constant__ unsigned long long* c_tl_buf;
+__constant__ unsigned c_tl_cap;
+__device__ unsigned g_tl_n;
+__device__ __forceinline__ void tl_stamp() {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        unsigned long long* b = c_tl_buf;
+        if (b) {
+            unsigned long long t;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            unsigned i = atomicAdd(&g_tl_n, 1u);
+            if (i < c_tl_cap) b[i] = t;
+        }
+    }
+}
+}  // namespace mlp
+#define MLP_TIMELINE_HOOK() ::mlp::tl_stamp()
+
 #include "persist.cuh"
 #include "small.cuh"
 #include "solve.cuh"
@@ -1733,6 +1757,54 @@ std::vector<OpProfile> profile_apply(Prec& P, uint32_t reps, cudaStream_t s) {
     }
     check_persist(P, s);
     return out;
+}
+
+std::vector<double> timeline_apply(Prec& P, uint32_t reps, cudaStream_t s) {
+    const Plan& pl = P.plan;
+    size_t n = pl.ops.size();
+    std::vector<double> us(n, 0.0);
+    if (!n) return us;
+    if (!P.graph) MLP_THROW(ERR_ARG, "the apply has no graph");
+    if (reps < 2) reps = 2;
+    size_t total = (size_t)reps * n;
+    DBuf<unsigned long long> buf(total + 64);
+    unsigned long long* bp = buf.p;
+    unsigned cap = (unsigned)(total + 64), zero = 0;
+    CK(cudaStreamSynchronize(s));
+    CK(cudaMemcpyToSymbol(c_tl_cap, &cap, sizeof cap));
+    CK(cudaMemcpyToSymbol(g_tl_n, &zero, sizeof zero));
+    CK(cudaMemcpyToSymbol(c_tl_buf, &bp, sizeof bp));
+    cudaError_t le = cudaSuccess;
+    for (uint32_t r = 0; r < reps && le == cudaSuccess; r++) le = cudaGraphLaunch(P.graph, s);
+    cudaError_t se = cudaStreamSynchronize(s);
+    unsigned long long* nul = nullptr;
+    unsigned got = 0;
+    CK(cudaMemcpyToSymbol(c_tl_buf, &nul, sizeof nul));
+    CK(cudaMemcpyFromSymbol(&got, g_tl_n, sizeof got));
+    CK(le);
+    CK(se);
+    count_launches((uint64_t)reps * pl.launches);
+    if (got != total)
+        MLP_THROW(ERR_INTERNAL, "timeline: " + std::to_string(got) + " stamps for " + std::to_string(total) +
+                                    " launches (a launch of the plan does not come from the solve kernels)");
+    std::vector<unsigned long long> t(total);
+    CK(cudaMemcpy(t.data(), bp, total * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    // op k of replay r lasts until the next stamp; the last op of the last
+    // replay has none and takes the mean of the earlier replays
+    for (size_t k = 0; k < n; k++) {
+        double sum = 0;
+        uint32_t cnt = 0;
+        for (uint32_t r = 0; r < reps; r++) {
+            size_t i = (size_t)r * n + k;
+            if (i + 1 < total) {
+                sum += (double)(t[i + 1] - t[i]) / 1e3;
+                cnt++;
+            }
+        }
+        us[k] = cnt ? sum / cnt : 0.0;
+    }
+    check_persist(P, s);
+    return us;
 }
 
 void prec_apply_frame(Prec& P, cudaStream_t s) {

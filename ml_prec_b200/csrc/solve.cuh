@@ -37,6 +37,9 @@ struct OpProfile {
 };
 struct Prec;
 std::vector<OpProfile> profile_apply(Prec& P, uint32_t reps, cudaStream_t s);
+// Replays the apply graph reps (>= 2) times back to back with the in-graph
+// timeline on; per launch of the plan its mean time inside the graph (us).
+std::vector<double> timeline_apply(Prec& P, uint32_t reps, cudaStream_t s);
 
 template <class T>
 struct SmallPlan;

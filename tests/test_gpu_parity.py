@@ -243,3 +243,25 @@ def test_autotuned_full_size_pcg(M):
     x2 = M.PCGSolver(A, b, M.MultiSplitPrec(A, **kw), stats=st2, eps=1e-8)
     assert abs(st1.niter - st2.niter) <= 1 and st1.final_rel <= 1e-8
     assert np.linalg.norm(x1 - x2) <= 1e-9 * np.linalg.norm(x2)
+
+
+def test_in_graph_timeline(M, monkeypatch):
+    """mlp_prec_timeline gives one positive in-graph time per launch of the
+    plan (names and bytes as the launch-by-launch profile); a plan with a
+    launch that stamps no time (the persistent kernel) is refused with
+    MLP_ERR_INTERNAL instead of returning misattributed times."""
+    g = load_golden("ms_layered_16x22x8_c01")
+    A = gpu_matrix(M, g)
+    monkeypatch.setenv("MLP_PERSIST", "0")
+    P = gpu_prec(A, g)
+    P.solve(g["f_in"])
+    tl = P.timeline(4)
+    prof = P.profile(1)
+    assert [t[0] for t in tl] == [p[0] for p in prof]
+    assert all(us > 0 for _, us, _ in tl)
+    monkeypatch.setenv("MLP_PERSIST", "1")
+    P1 = gpu_prec(A, g)
+    P1.solve(g["f_in"])
+    with pytest.raises(M.MlpError) as e:
+        P1.timeline(4)
+    assert e.value.code == 10
