@@ -1872,6 +1872,8 @@ __global__ void __launch_bounds__(RB) k_pcg_spmv_dot(uint32_t n, const uint32_t*
                                                      const uint32_t* __restrict__ ja, const double* __restrict__ a,
                                                      const double* __restrict__ p, double* __restrict__ Ap,
                                                      double* partials, PcgDev* d) {
+    pdl_wait();
+    pdl_trigger();
     double part = 0;
     const uint32_t groups = gridDim.x * (RB / LPR);
     int lane = threadIdx.x % LPR;
@@ -1939,17 +1941,27 @@ static void pipe_prepare_all(uint32_t tile_max) {
 // Launch of k_pcg_spmv_dot_staged; its grid never exceeds staged_grid(n), the
 // size the reduction scratch of every caller is made for.
 static void launch_pcg_spmv_dot_staged(uint32_t n, const DCSR& Af, const double* p, double* Ap, double* partials,
-                                       PcgDev* d, cudaStream_t s) {
+                                       PcgDev* d, cudaStream_t s, bool pdl = false) {
     uint32_t cap = pipe_cap<double>(Af.tile_max);
     size_t smem = pipe_smem_bytes<double, false>(Af.tile_max);
     unsigned g = std::min(pipe_grid(k_pcg_spmv_dot_staged<false>, n, smem), staged_grid(n));
-    k_pcg_spmv_dot_staged<false><<<g, ST_ROWS, smem, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p, Ap, partials, d, cap);
+    if (pdl)
+        launch_k(k_pcg_spmv_dot_staged<false>, g, ST_ROWS, smem, s, n, (const uint32_t*)Af.ia.p,
+                 (const uint32_t*)Af.ja.p, (const double*)Af.a.p, p, Ap, partials, d, cap);
+    else
+        k_pcg_spmv_dot_staged<false><<<g, ST_ROWS, smem, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p, Ap, partials, d, cap);
 }
 
-// x += alpha p; r -= alpha Ap; rr = (r, r)
+// x += alpha p; r -= alpha Ap; rr = (r, r). In the device loop (cond != 0)
+// the block that completes the reduction also ends the iteration: it counts
+// it and keeps the loop going while ||r||/||r0|| > eps (pcg.cc:42), no error
+// was flagged and the cap is not hit.
 __global__ void __launch_bounds__(RB) k_pcg_update(uint32_t n, double* __restrict__ x, double* __restrict__ r,
                                                    const double* __restrict__ p, const double* __restrict__ Ap,
-                                                   double* partials, PcgDev* d) {
+                                                   double* partials, PcgDev* d, cudaGraphConditionalHandle h,
+                                                   int cond) {
+    pdl_wait();
+    pdl_trigger();
     double alpha = d->alpha;
     double part = 0;
     for (uint32_t i = blockIdx.x * RB + threadIdx.x; i < n; i += gridDim.x * RB) {
@@ -1963,13 +1975,23 @@ __global__ void __launch_bounds__(RB) k_pcg_update(uint32_t n, double* __restric
     if (finish_reduce(part, partials, &d->ticket[1], &tot) && threadIdx.x == 0) {
         d->rr = tot;
         if (tot != tot || tot > 1e308) d->status |= 2;
+        if (cond) {
+            d->it++;
+            bool go = sqrt(tot) / d->init > d->eps && d->status == 0 && (d->maxit == 0 || d->it < d->maxit);
+            cudaGraphSetConditional(h, go ? 1u : 0u);
+        }
     }
 }
 
-// rz1 = (r, z); beta = rz1/rz0 (or Polak-Ribiere (r - r_prev, z)/rz0); rz0 = rz1.
+// rz1 = (r, z); beta = rz1/rz0 (or Polak-Ribiere (r - r_prev, z)/rz0); rz0 =
+// rz1. The block that completes the last reduction computes beta: with the
+// flexible form that is the last block of the second reduction, which every
+// block enters after the first, whose total is then already in d->rz1.
 __global__ void __launch_bounds__(RB) k_pcg_dot_rz(uint32_t n, const double* __restrict__ r,
                                                    const double* __restrict__ z, const double* __restrict__ rprev,
                                                    double* partials, PcgDev* d, int flexible) {
+    pdl_wait();
+    pdl_trigger();
     double part = 0, part2 = 0;
     for (uint32_t i = blockIdx.x * RB + threadIdx.x; i < n; i += gridDim.x * RB) {
         part += r[i] * z[i];
@@ -1978,26 +2000,35 @@ __global__ void __launch_bounds__(RB) k_pcg_dot_rz(uint32_t n, const double* __r
     part = block_sum(part);
     double tot;
     bool last = finish_reduce(part, partials, &d->ticket[2], &tot);
+    if (last && threadIdx.x == 0) {
+        d->rz1 = tot;
+        if (!flexible) {
+            double beta = tot / d->rz0;
+            d->beta = beta;
+            d->rz0 = tot;
+            if (beta != beta) d->status |= 2;
+        }
+    }
     if (flexible) {
         __syncthreads();
         part2 = block_sum(part2);
         double tot2;
         bool last2 = finish_reduce(part2, partials + gridDim.x, &d->ticket[3], &tot2);
-        if (last2 && threadIdx.x == 0) d->rz_prev = tot2;
-        (void)last;
+        if (last2 && threadIdx.x == 0) {
+            double rz1 = *(volatile double*)&d->rz1;
+            double beta = (rz1 - tot2) / d->rz0;
+            d->rz_prev = tot2;
+            d->beta = beta;
+            d->rz0 = rz1;
+            if (beta != beta) d->status |= 2;
+        }
     }
-    if (last && threadIdx.x == 0) d->rz1 = tot;
-}
-
-__global__ void k_pcg_beta(PcgDev* d, int flexible) {
-    double num = flexible ? d->rz1 - d->rz_prev : d->rz1;
-    d->beta = num / d->rz0;
-    d->rz0 = d->rz1;
-    if (d->beta != d->beta) d->status |= 2;
 }
 
 // p = beta p + z (dscal then daxpy, pcg.cc:71-72)
 __global__ void k_pcg_p(uint32_t n, double* __restrict__ p, const double* __restrict__ z, const PcgDev* d) {
+    pdl_wait();
+    pdl_trigger();
     double beta = d->beta;
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) p[i] = beta * p[i] + z[i];
@@ -2045,15 +2076,6 @@ const double* x0_device(uint32_t n, cudaStream_t s) {
 // ---------------------------------------------------------------------------
 // Device-resident PCG: one solve is one graph launch.
 // ---------------------------------------------------------------------------
-// End-of-iteration test: counts the iteration and keeps looping while
-// ||r||/||r0|| > eps (pcg.cc:42), no error was flagged and the cap is not hit.
-__global__ void k_pcg_check(PcgDev* d, cudaGraphConditionalHandle h) {
-    d->it++;
-    double norm = sqrt(d->rr);
-    bool go = norm / d->init > d->eps && d->status == 0 && (d->maxit == 0 || d->it < d->maxit);
-    cudaGraphSetConditional(h, go ? 1u : 0u);
-}
-
 __global__ void k_copy_d(uint32_t n, const double* __restrict__ a, double* __restrict__ b) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) b[i] = a[i];
@@ -2116,27 +2138,29 @@ static void record_iteration(Prec& P, const DCSR& Af, uint32_t n, bool flexible,
     bool staged = Af.tile_max && Af.tile_max <= ST_MAX_NNZ && n >= 4 * ST_ROWS;
     double avg = (double)Af.nnz / n;
     int lpr = avg <= 3 ? 2 : avg <= 6 ? 4 : avg <= 12 ? 8 : avg <= 24 ? 16 : 32;
+    // programmatic dependent launches like the apply's kernels: each waits
+    // for its predecessor before touching memory
     if (staged) {
-        launch_pcg_spmv_dot_staged(n, Af, W.p.p, W.Ap.p, W.partials.p, d, s);
+        launch_pcg_spmv_dot_staged(n, Af, W.p.p, W.Ap.p, W.partials.p, d, s, true);
     } else switch (lpr) {
-        case 2: k_pcg_spmv_dot<2><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, W.p.p, W.Ap.p, W.partials.p, d); break;
-        case 4: k_pcg_spmv_dot<4><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, W.p.p, W.Ap.p, W.partials.p, d); break;
-        case 8: k_pcg_spmv_dot<8><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, W.p.p, W.Ap.p, W.partials.p, d); break;
-        case 16: k_pcg_spmv_dot<16><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, W.p.p, W.Ap.p, W.partials.p, d); break;
-        default: k_pcg_spmv_dot<32><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, W.p.p, W.Ap.p, W.partials.p, d); break;
+        case 2: launch_k(k_pcg_spmv_dot<2>, G, RB, 0, s, n, Af.ia.p, Af.ja.p, Af.a.p, W.p.p, W.Ap.p, W.partials.p, d); break;
+        case 4: launch_k(k_pcg_spmv_dot<4>, G, RB, 0, s, n, Af.ia.p, Af.ja.p, Af.a.p, W.p.p, W.Ap.p, W.partials.p, d); break;
+        case 8: launch_k(k_pcg_spmv_dot<8>, G, RB, 0, s, n, Af.ia.p, Af.ja.p, Af.a.p, W.p.p, W.Ap.p, W.partials.p, d); break;
+        case 16: launch_k(k_pcg_spmv_dot<16>, G, RB, 0, s, n, Af.ia.p, Af.ja.p, Af.a.p, W.p.p, W.Ap.p, W.partials.p, d); break;
+        default: launch_k(k_pcg_spmv_dot<32>, G, RB, 0, s, n, Af.ia.p, Af.ja.p, Af.a.p, W.p.p, W.Ap.p, W.partials.p, d); break;
     }
-    k_pcg_update<<<G, RB, 0, s>>>(n, W.xf.p, r, W.p.p, W.Ap.p, W.partials.p, d);
-    k_pcg_check<<<1, 1, 0, s>>>(d, h);
+    launch_k(k_pcg_update, G, RB, 0, s, n, W.xf.p, r, (const double*)W.p.p, (const double*)W.Ap.p, W.partials.p, d,
+             h, 1);
     P.plan.run(s);
-    k_pcg_dot_rz<<<G, RB, 0, s>>>(n, r, z, W.rprev.p, W.partials.p, d, flexible ? 1 : 0);
-    k_pcg_beta<<<1, 1, 0, s>>>(d, flexible ? 1 : 0);
-    k_pcg_p<<<grid_for(n, 256), 256, 0, s>>>(n, W.p.p, z, d);
+    launch_k(k_pcg_dot_rz, G, RB, 0, s, n, (const double*)r, (const double*)z, (const double*)W.rprev.p,
+             W.partials.p, d, flexible ? 1 : 0);
+    launch_k(k_pcg_p, grid_for(n, 256), 256, 0, s, n, W.p.p, (const double*)z, (const PcgDev*)d);
     if (flexible) k_copy_d<<<grid_for(n, 256), 256, 0, s>>>(n, r, W.rprev.p);
 }
 
 // Launches per loop iteration and per start (launch accounting).
 static uint64_t iteration_launches(const Prec& P, bool flexible) {
-    return 3 + P.plan.launches + 3 + (flexible ? 1 : 0);
+    return 2 + P.plan.launches + 2 + (flexible ? 1 : 0);
 }
 static uint64_t start_launches(const Prec& P, bool flexible) {
     return 6 + P.plan.launches + 2 + (flexible ? 1 : 0) + 1;
@@ -2393,7 +2417,7 @@ int pcg_solve_cb(const DCSR& A, const double* b, const std::function<void(const 
             case 16: k_pcg_spmv_dot<16><<<G, RB, 0, s>>>(n, A.ia.p, A.ja.p, A.a.p, p.p, Ap.p, partials.p, d); break;
             default: k_pcg_spmv_dot<32><<<G, RB, 0, s>>>(n, A.ia.p, A.ja.p, A.a.p, p.p, Ap.p, partials.p, d); break;
         }
-        k_pcg_update<<<G, RB, 0, s>>>(n, x, r.p, p.p, Ap.p, partials.p, d);
+        k_pcg_update<<<G, RB, 0, s>>>(n, x, r.p, p.p, Ap.p, partials.p, d, 0, 0);
         count_launches(2);
         CK_LAUNCH();
         h = fetch();
@@ -2405,9 +2429,8 @@ int pcg_solve_cb(const DCSR& A, const double* b, const std::function<void(const 
         apply(r.p, z.p);
         napply++;
         k_pcg_dot_rz<<<G, RB, 0, s>>>(n, r.p, z.p, rprev.p, partials.p, d, flexible ? 1 : 0);
-        k_pcg_beta<<<1, 1, 0, s>>>(d, flexible ? 1 : 0);
         k_pcg_p<<<grid_for(n, 256), 256, 0, s>>>(n, p.p, z.p, d);
-        count_launches(3);
+        count_launches(2);
         if (flexible) CK(cudaMemcpyAsync(rprev.p, r.p, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
         CK_LAUNCH();
     }
@@ -2835,7 +2858,7 @@ int pcg_solve_hostloop(const DCSR& A, const double* b, Prec& P, double* x, doubl
             case 16: k_pcg_spmv_dot<16><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p.p, Ap.p, partials.p, d); break;
             default: k_pcg_spmv_dot<32><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p.p, Ap.p, partials.p, d); break;
         }
-        k_pcg_update<<<G, RB, 0, s>>>(n, xf.p, r, p.p, Ap.p, partials.p, d);
+        k_pcg_update<<<G, RB, 0, s>>>(n, xf.p, r, p.p, Ap.p, partials.p, d, 0, 0);
         count_launches(1);
         CK_LAUNCH();
         h = fetch();
@@ -2847,7 +2870,6 @@ int pcg_solve_hostloop(const DCSR& A, const double* b, Prec& P, double* x, doubl
         prec_apply_frame(P, s);
         napply++;
         k_pcg_dot_rz<<<G, RB, 0, s>>>(n, r, z, rprev.p, partials.p, d, flexible ? 1 : 0);
-        k_pcg_beta<<<1, 1, 0, s>>>(d, flexible ? 1 : 0);
         k_pcg_p<<<grid_for(n, 256), 256, 0, s>>>(n, p.p, z, d);
         count_launches(2);
         if (flexible) CK(cudaMemcpyAsync(rprev.p, r, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
@@ -3006,7 +3028,7 @@ int pcg_solve_noalloc(const DCSR& A, const double* b, Prec& P, double* x, double
             case 16: k_pcg_spmv_dot<16><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p, Ap, partials, d); break;
             default: k_pcg_spmv_dot<32><<<G, RB, 0, s>>>(n, Af.ia.p, Af.ja.p, Af.a.p, p, Ap, partials, d); break;
         }
-        k_pcg_update<<<G, RB, 0, s>>>(n, xf, r, p, Ap, partials, d);
+        k_pcg_update<<<G, RB, 0, s>>>(n, xf, r, p, Ap, partials, d, 0, 0);
         count_launches(1);
         CK_LAUNCH();
         h = fetch();
@@ -3018,7 +3040,6 @@ int pcg_solve_noalloc(const DCSR& A, const double* b, Prec& P, double* x, double
         prec_apply_frame(P, s);
         napply++;
         k_pcg_dot_rz<<<G, RB, 0, s>>>(n, r, z, rprev, partials, d, flexible ? 1 : 0);
-        k_pcg_beta<<<1, 1, 0, s>>>(d, flexible ? 1 : 0);
         k_pcg_p<<<grid_for(n, 256), 256, 0, s>>>(n, p, z, d);
         count_launches(2);
         if (flexible) CK(cudaMemcpyAsync(rprev, r, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
