@@ -650,6 +650,98 @@ __global__ void __launch_bounds__(512) k_phase2(uint32_t M, const uint32_t* __re
     if (active && lane == 0) out[row] = s;
 }
 
+// Phase 2 with the coarse solve folded in (launch plan; the level below is
+// one dense FP64 operator C, n x n). One launch computes
+//  * the coarse solution out_{M+k} = C_k . w_C, a warp per row with the
+//    arithmetic of k_dense_gemv (blocks [0, nb_c));
+//  * the nf rows of G with coarse columns (rows[0, nf)), a warp per row:
+//    out_q = sum_{j<M} G_qj w_j (in lanes, as k_phase2 with 32 lanes) + D_q . w_C,
+//    D = G_C C built at set-up in FP64 (blocks [nb_c, nb_c + nb_f));
+//  * the other rows (rows[nf, M), all columns < M) exactly as k_phase2.
+// So the apply needs no separate launch for the coarse solve; the folded rows
+// add G_C (C w_C) in the order (G_C C) w_C.
+template <class T, int LPR>
+__global__ void __launch_bounds__(256) k_phase2_fold(uint32_t M, uint32_t n, const uint32_t* __restrict__ ia,
+                                                     const uint32_t* __restrict__ ja, const T* __restrict__ a,
+                                                     const double* __restrict__ C, const double* __restrict__ D,
+                                                     const uint32_t* __restrict__ rows, uint32_t nf, uint32_t nb_c,
+                                                     uint32_t nb_f, const T* __restrict__ w, T* __restrict__ out) {
+    if (blockIdx.x < nb_c + nb_f) {
+        constexpr int CV = 16;
+        const bool coarse = blockIdx.x < nb_c;
+        const uint32_t r = (coarse ? blockIdx.x : blockIdx.x - nb_c) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+        const int lane = threadIdx.x & 31;
+        const uint32_t nr = coarse ? n : nf;
+        const double* c = (coarse ? C : D) + (size_t)(r < nr ? r : 0) * n;
+        double cv[CV];
+#pragma unroll
+        for (int k = 0; k < CV; k++) {
+            uint32_t j = lane + 32 * k;
+            cv[k] = (r < nr && j < n) ? c[j] : 0.0;
+        }
+        pdl_wait();
+        pdl_trigger();
+        if (r >= nr) return;
+        const T* wc = w + M;
+        double d = 0;
+#pragma unroll
+        for (int k = 0; k < CV; k++) {
+            uint32_t j = lane + 32 * k;
+            if (j < n) d = fmadd(cv[k], (double)wc[j], d);
+        }
+        for (uint32_t j = lane + 32 * CV; j < n; j += 32) d = fmadd(c[j], (double)wc[j], d);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+        if (coarse) {
+            if (lane == 0) out[M + r] = (T)d;
+            return;
+        }
+        const uint32_t q = rows[r];
+        T sp = 0;
+        for (uint32_t j = ia[q] + lane, e = ia[q + 1]; j < e; j += 32) {
+            uint32_t col = ja[j];
+            if (col < M) sp = fmadd(a[j], w[col], sp);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sp += __shfl_xor_sync(0xffffffffu, sp, o);
+        if (lane == 0) out[q] = (T)((double)sp + d);
+        return;
+    }
+    const uint32_t gid = (blockIdx.x - nb_c - nb_f) * blockDim.x + threadIdx.x;
+    const uint32_t k = gid / LPR;
+    const int lane = gid % LPR;
+    const bool active = k < M - nf;
+    const uint32_t row = active ? rows[nf + k] : 0;
+    RowPre<T, LPR> rp;
+    rp.load(active, row, lane, ia, ja, a);
+    pdl_wait();
+    pdl_trigger();
+    T s = rp.sum([&](uint32_t c) { return w[c]; }, ja, a);
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (active && lane == 0) out[row] = s;
+}
+
+// D = G_C C for the folded rows: block i takes row rows[i] of G, thread t the
+// columns t, t + blockDim.x, ... of D; the coarse entries of the row are
+// added in their stored order.
+template <class T>
+__global__ void k_fold_build(uint32_t nf, const uint32_t* __restrict__ rows, uint32_t M, uint32_t n,
+                             const uint32_t* __restrict__ ia, const uint32_t* __restrict__ ja,
+                             const T* __restrict__ a, const double* __restrict__ C, double* __restrict__ D) {
+    const uint32_t i = blockIdx.x;
+    if (i >= nf) return;
+    const uint32_t q = rows[i];
+    for (uint32_t t = threadIdx.x; t < n; t += blockDim.x) {
+        double s = 0;
+        for (uint32_t j = ia[q]; j < ia[q + 1]; j++) {
+            uint32_t col = ja[j];
+            if (col >= M) s = fmadd((double)a[j], C[(size_t)(col - M) * n + t], s);
+        }
+        D[(size_t)i * n + t] = s;
+    }
+}
+
 // Correction step of a level sweep: x += u0 and, when more sweeps follow,
 // r -= A u0 (the residual f - A x updated in place of recomputing it).
 template <class T, int LPR>
@@ -1200,6 +1292,110 @@ struct Builder {
         else op([=](cudaStream_t s) { launch(c, s); }, "phase2");
         bytes += (uint64_t)L.G.nnz * (4 + sizeof(T)) + 4ull * (M + 1) + sizeof(T) * (M + L.n + M);
     }
+    // ---- folded coarse solve (launch plan) ------------------------------
+    bool fold = true;  // MLP_FOLD=0 turns it off
+    // Largest D = G_C C kept per level (bytes): the folded phase 2 reads it
+    // once per call, so it must stay well below what a launch costs.
+    static constexpr size_t FOLD_MAX_BYTES = 8u << 20;
+
+    // Whether the call of level l + 1 is one dense FP64 product (the
+    // tabulated small levels or the direct coarsest solve); C and n are its
+    // operator and size.
+    bool dense_next(uint32_t l, const double*& C, uint32_t& n) const {
+        if (l + 1 >= H.nlevels) return false;
+        const Level& Ln = *H.lv[l + 1];
+        if (small64 && small64->valid() && small64->first <= l + 1) {
+            if (small64->first != l + 1 || !small64->dense.p) return false;
+            C = small64->dense.p;
+            n = small64->N0;
+            return true;
+        }
+        if (small && small->valid() && small->first <= l + 1) {
+            if (small->first != l + 1 || !small->dense.p || !std::is_same<T, double>::value) return false;
+            C = reinterpret_cast<const double*>(small->dense.p);
+            n = small->N0;
+            return true;
+        }
+        if (Ln.direct && Ln.cinv.p) {
+            C = Ln.cinv.p;
+            n = Ln.N;
+            return true;
+        }
+        return false;
+    }
+
+    // Builds (once per level) the row split and D = G_C C for the folded
+    // phase 2; false when the level does not qualify.
+    bool fold_ready(uint32_t l, const double* C, uint32_t n) {
+        LevelWork<T>& w = W[l];
+        if (w.fold_state) return w.fold_state > 0;
+        w.fold_state = -1;
+        const Level& L = *H.lv[l];
+        const uint32_t M = L.M;
+        if (!M || n != L.n || L.G.nnz == 0) return false;
+        std::vector<uint32_t> ia = L.G.ia.download(stream, (size_t)M + 1);
+        std::vector<uint32_t> ja = L.G.ja.download(stream, L.G.nnz);
+        std::vector<uint32_t> rows, plain;
+        for (uint32_t q = 0; q < M; q++) {
+            bool has = false;
+            for (uint32_t j = ia[q]; j < ia[q + 1]; j++) {
+                if (ja[j] >= M + n) return false;  // not a level of this shape
+                has |= ja[j] >= M;
+            }
+            (has ? rows : plain).push_back(q);
+        }
+        const uint32_t nf = (uint32_t)rows.size();
+        if ((size_t)nf * n * sizeof(double) > FOLD_MAX_BYTES) return false;
+        rows.insert(rows.end(), plain.begin(), plain.end());
+        w.fold_rows.alloc(M);
+        w.fold_rows.upload(rows.data(), M, stream);
+        w.fold_D.alloc((size_t)(nf ? nf : 1) * n);
+        if (nf) {
+            k_fold_build<T><<<nf, 256, 0, stream>>>(nf, w.fold_rows.p, M, n, L.G.ia.p, L.G.ja.p, vals<T>(L.G), C,
+                                                     w.fold_D.p);
+            CK_LAUNCH();
+        }
+        CK(cudaStreamSynchronize(stream));
+        w.fold_nf = nf;
+        w.fold_state = 1;
+        return true;
+    }
+
+    void phase2_fold(uint32_t l, const double* C, uint32_t n, const T* w, T* out) {
+        const Level& L = *H.lv[l];
+        const LevelWork<T>& lw = W[l];
+        const uint32_t M = L.M, nf = lw.fold_nf;
+        const uint32_t* ia = L.G.ia.p;
+        const uint32_t* ja = L.G.ja.p;
+        const T* a = vals<T>(L.G);
+        const double* D = lw.fold_D.p;
+        const uint32_t* rows = lw.fold_rows.p;
+        const uint32_t nb_c = (n + 7) / 8, nb_f = (nf + 7) / 8;
+        const int lpr = pick_lpr(M, L.G.nnz);
+        const uint32_t nb_p = grid_for((size_t)(M - nf) * (lpr < 1 ? 1 : lpr), 256);
+        op([=](cudaStream_t s) {
+            LPR_SWITCH_B(lpr < 1 ? 1 : lpr, k_phase2_fold, nb_c + nb_f + (M > nf ? nb_p : 0), 256, 0, s, M, n, ia,
+                         ja, a, C, D, rows, nf, nb_c, nb_f, w, out);
+        }, "phase2_fold");
+        bytes += (uint64_t)L.G.nnz * (4 + sizeof(T)) + 4ull * (M + 1) + 4ull * M + 8ull * n * (n + nf) +
+                 sizeof(T) * (M + n + M + n);
+    }
+
+    // The coarse call and phase 2 of a sweep of level l: one folded launch
+    // where it applies, else the recursion into level l + 1 and phase 2.
+    void coarse_phase2(uint32_t l, T* w, T* out) {
+        Level& L = *H.lv[l];
+        const bool next = l + 1 < H.nlevels && L.n;
+        const double* C = nullptr;
+        uint32_t n = 0;
+        if (next && fold && !ps && explicit_solves && !autotune && dense_next(l, C, n) && fold_ready(l, C, n)) {
+            phase2_fold(l, C, n, w, out);
+            return;
+        }
+        if (next) ms(l + 1, w + L.M, out + L.M);
+        phase2(L, w, out);
+    }
+
     void update(const Level& L, const T* u0, T* x, T* r, bool do_r) {
         uint32_t N = L.N;
         const uint32_t* ia = L.Af.ia.p;
@@ -1272,11 +1468,9 @@ struct Builder {
         if (!ps && ms_merged(l, f, x)) return;
         if (L.eps != 0) { ms_dynamic(l, f, x); return; }
         LevelWork<T>& w = W[l];
-        uint32_t N = L.N, M = L.M;
-        bool next = l + 1 < H.nlevels && L.n;
+        uint32_t N = L.N;
         phase1(L, f, w.w.p, x);
-        if (next) ms(l + 1, w.w.p + M, x + M);
-        phase2(L, w.w.p, x);
+        coarse_phase2(l, w.w.p, x);
         if (L.niter < 2) return;
         {
             const uint32_t* ia = L.Af.ia.p;
@@ -1290,8 +1484,7 @@ struct Builder {
         }
         for (uint32_t it = 2; it <= L.niter; it++) {
             phase1(L, w.r.p, w.w.p, w.u0.p);
-            if (next) ms(l + 1, w.w.p + M, w.u0.p + M);
-            phase2(L, w.w.p, w.u0.p);
+            coarse_phase2(l, w.w.p, w.u0.p);
             update(L, w.u0.p, x, w.r.p, it < L.niter);
         }
     }
@@ -1393,16 +1586,11 @@ struct Builder {
     bool ms_merged(uint32_t l, const T* f, T* x) {
         Level& L = *H.lv[l];
         if (!merge_enabled() || autotune || L.N > MERGE_MAX_N || L.niter < 2 || !merge_a_ok(L)) return false;
-        bool next = l + 1 < H.nlevels && L.n;
         LevelWork<T>& W_ = W[l];
         if (!W_.r2.p) W_.r2.alloc(L.N);
         if (!W_.u02.p) W_.u02.alloc(L.N);
-        uint32_t M = L.M;
         T* w = W_.w.p;
-        auto stepB = [&](T* out) {
-            if (next) ms(l + 1, w + M, out + M);
-            phase2(L, w, out);
-        };
+        auto stepB = [&](T* out) { coarse_phase2(l, w, out); };
         phase1(L, f, w, x);
         stepB(x);
         T *ra = W_.r.p, *rb = W_.r2.p, *ua = W_.u0.p, *ub = W_.u02.p;
@@ -1596,8 +1784,15 @@ static uint32_t persist_max_n() {
     if (e && *e) return (uint32_t)strtoul(e, nullptr, 10);
     return 1u << 19;
 }
+// The folded coarse solve (k_phase2_fold) is on unless MLP_FOLD=0.
+static bool fold_enabled() {
+    const char* e = getenv("MLP_FOLD");
+    return !(e && e[0] == '0');
+}
+
 template <class T>
 static void builder_persist(Builder<T>& B, Prec& P) {
+    B.fold = fold_enabled();
     B.persist = persist_enabled(B.H);
     B.persist_max_n = persist_max_n();
     B.pdesc = &P.pdesc;

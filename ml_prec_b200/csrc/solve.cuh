@@ -15,6 +15,13 @@ struct LevelWork {
     DBuf<T> r, w, u0;            // multi-split: residual, L-solve output, correction
     DBuf<T> r2, u02;             // second residual / correction buffers of the merged sweeps
     DBuf<T> cu0, cu1, cx2, ctmp; // uh_cheb: Chebyshev vectors on the coarse slice
+    // Folded coarse solve (launch plan): when the level below is one dense
+    // operator C, the rows of G with coarse columns keep their product with C
+    // (D = G_C C, FP64) so that phase 2 needs no separate coarse launch.
+    DBuf<uint32_t> fold_rows;    // the rows of G with coarse columns, then the others
+    DBuf<double> fold_D;         // fold_nf x n, row-major
+    uint32_t fold_nf = 0;
+    int fold_state = 0;          // 0 not tried, 1 built, -1 not applicable
 };
 
 // A recorded sequence of launches. Replaying it (directly or as a CUDA graph)

@@ -22,13 +22,14 @@ def M():
     return M
 
 
-@pytest.fixture(params=["persistent", "persist_split", "dense", "separate", "small", "explicit", "waves"])
+@pytest.fixture(params=["persistent", "persist_split", "dense", "nofold", "separate", "small", "explicit", "waves"])
 def apply_path(request, monkeypatch):
     """Run each case through every apply path: the whole apply as one
     persistent launch (MLP_PERSIST=1 at these sizes), the finest level as separate
     launches around a persistent launch of the levels below it, the tabulated
     small-level operator with separate launches and the correction and
-    phase-1 steps of the small levels merged, the same with every sweep step a
+    phase-1 steps of the small levels merged (the coarse product folded into
+    phase 2, and not), the same with every sweep step a
     separate kernel, the shared-memory small-level kernel (tabulation off),
     the launch path with explicit triangular solves (small kernel off), and
     the launch path with wavefront triangular solves."""
@@ -36,8 +37,10 @@ def apply_path(request, monkeypatch):
         monkeypatch.setenv("MLP_PERSIST", "1")
     if request.param == "persist_split":
         monkeypatch.setenv("MLP_PERSIST_MAX_N", "1200")
-    if request.param in ("dense", "separate", "small", "explicit", "waves"):
+    if request.param in ("dense", "nofold", "separate", "small", "explicit", "waves"):
         monkeypatch.setenv("MLP_PERSIST", "0")
+    if request.param == "nofold":
+        monkeypatch.setenv("MLP_FOLD", "0")
     if request.param == "separate":
         monkeypatch.setenv("MLP_MERGE", "0")
     if request.param == "small":
@@ -190,18 +193,21 @@ def test_iteration_cap_ends_the_device_loop(M):
 def test_apply_forms_are_bit_identical(M, fp32, monkeypatch):
     """60x220x85 layered field: the levels below the finest one run as one
     persistent launch (MLP_PERSIST=1); as separate launches with the
-    correction and phase-1 steps of the small levels merged (the default);
-    and as separate launches with every sweep step its own kernel. All three
-    repeat the same arithmetic (same products, lane split and butterfly
-    order), so the apply and the PCG iterates are bit-identical."""
+    correction and phase-1 steps of the small levels merged; and as separate
+    launches with every sweep step its own kernel (both with the coarse
+    product as its own launch, MLP_FOLD=0). All three repeat the same
+    arithmetic (same products, lane split and butterfly order), so the apply
+    and the PCG iterates are bit-identical. The default folds the coarse
+    product into phase 2 ((G_C C) w_C in place of G_C (C w_C)), which changes
+    the rounding: test_folded_coarse_product holds it to the unfolded form."""
     from ml_prec_b200 import fields
     kx, ky, kz = fields.field("layered", 2)
     A, b = M.CSRMatrix.spe(60, 220, 85, kx, ky, kz, c=1.0)
     f = np.random.default_rng(5).standard_normal(A.n)
     kw = dict(q=(0.8,), niter=(5,), max_levels=15, degree_max=2, fp32=fp32)
     out = []
-    for env in ({"MLP_PERSIST": "1"}, {}, {"MLP_MERGE": "0"}):
-        for k in ("MLP_PERSIST", "MLP_MERGE"):
+    for env in ({"MLP_PERSIST": "1"}, {"MLP_FOLD": "0"}, {"MLP_FOLD": "0", "MLP_MERGE": "0"}):
+        for k in ("MLP_PERSIST", "MLP_MERGE", "MLP_FOLD"):
             monkeypatch.delenv(k, raising=False)
         for k, v in env.items():
             monkeypatch.setenv(k, v)
@@ -265,3 +271,34 @@ def test_in_graph_timeline(M, monkeypatch):
     with pytest.raises(M.MlpError) as e:
         P1.timeline(4)
     assert e.value.code == 10
+
+
+@pytest.mark.parametrize("fp32", [False, True])
+def test_folded_coarse_product(M, fp32, monkeypatch):
+    """60x220x85 layered field: the default plan folds the tabulated 422-row
+    coarse operator into phase 2 of level 2 (one launch less per level-2
+    sweep). Against the unfolded plan: the apply within 1e-13 (FP64) / 1e-6
+    (FP32 form) relative, PCG within one iteration and 1e-10 / 1e-6."""
+    from ml_prec_b200 import fields
+    kx, ky, kz = fields.field("layered", 2)
+    A, b = M.CSRMatrix.spe(60, 220, 85, kx, ky, kz, c=1.0)
+    f = np.random.default_rng(5).standard_normal(A.n)
+    kw = dict(q=(0.8,), niter=(5,), max_levels=15, degree_max=2, fp32=fp32)
+    out = []
+    for env in ({}, {"MLP_FOLD": "0"}):
+        monkeypatch.delenv("MLP_FOLD", raising=False)
+        for k, v in env.items():
+            monkeypatch.setenv(k, v)
+        P = M.MultiSplitPrec(A, **kw)
+        z = P.solve(f)
+        names = [t[0] for t in P.profile(1)]
+        st = M.SolverStats()
+        x = M.PCGSolver(A, b, P, stats=st, eps=1e-8, flexible=fp32)
+        out.append((z, st.niter, x, names))
+    (zf, itf, xf, nf), (zu, itu, xu, nu) = out
+    assert any(n.startswith("phase2_fold") for n in nf) and not any(n.startswith("phase2_fold") for n in nu)
+    assert len(nf) < len(nu)
+    tol = 1e-6 if fp32 else 1e-13
+    assert np.linalg.norm(zf - zu) <= tol * np.linalg.norm(zu)
+    assert abs(itf - itu) <= 1
+    assert np.linalg.norm(xf - xu) <= (1e-6 if fp32 else 1e-10) * np.linalg.norm(xu)
