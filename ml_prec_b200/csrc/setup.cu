@@ -1069,9 +1069,9 @@ static void build_level_msplit(Hierarchy& H, const BuildCfg& cfg, uint32_t level
     H.lv.emplace_back(new Level());
     Level& ln = *H.lv[level + 1];
     Level& lc = *H.lv[level];  // re-fetch: emplace_back may move unique_ptrs (not the objects)
-    trace("ms mark+order");
+    trace(("ms mark+order L" + std::to_string(level)).c_str());
     sparse_lu_level(lc, ln, S.keep.p, S.aux.p, S.rmap.p, 1.0, s);
-    trace("ms sparse lu");
+    trace(("ms sparse lu L" + std::to_string(level) + " (" + std::to_string(lc.nwave_l) + " rounds)").c_str());
     lc.n = N - lc.M - lc.Md;
     lc.dval.alloc(lc.Md ? lc.Md : 1);
     if (lc.Md) {
@@ -1218,6 +1218,8 @@ static void build_explicit(Level& li, cudaStream_t s, uint32_t& p1_cap, uint32_t
         CK_LAUNCH();
         CK(cudaStreamSynchronize(s));
         p1_cap = cap;
+        trace(("  explicit: P1 (" + std::to_string(li.lw_off.size() - 1) + " waves, slot " + std::to_string(cap) +
+               ")").c_str());
         break;
     }
     // G
@@ -1244,6 +1246,8 @@ static void build_explicit(Level& li, cudaStream_t s, uint32_t& p1_cap, uint32_t
         CK_LAUNCH();
         CK(cudaStreamSynchronize(s));
         g_cap = cap;
+        trace(("  explicit: G (" + std::to_string(li.uw_off.size() - 1) + " waves, slot " + std::to_string(cap) +
+               ")").c_str());
         break;
     }
 }
@@ -1287,6 +1291,7 @@ static void build_frames(Hierarchy& H, cudaStream_t s) {
         }
         k_perm_to_frame<<<grid_for(N, 256), 256, 0, s>>>(N, M, n, einv.p, iphi_next, p2f.p);
         CK_LAUNCH();
+        trace("  frame: E order + maps");
         // Lf: rows pi(q), q < R; columns (E, permuted) -> frame
         {
             Tmp<uint32_t> len(R + 1);
@@ -1338,6 +1343,7 @@ static void build_frames(Hierarchy& H, cudaStream_t s) {
                 if (left >= prev_left) MLP_THROW(ERR_INTERNAL, "U schedule makes no progress");
                 prev_left = left;
             }
+            trace(("  frame: Lf, Uf, U schedule (" + std::to_string(round) + " rounds)").c_str());
             std::vector<int> ul = lev.download(s, M);
             std::vector<uint32_t> uoff, urows;
             counting_sort(ul, M, uoff, urows);
@@ -1375,7 +1381,7 @@ static void build_frames(Hierarchy& H, cudaStream_t s) {
                 li.As.nrow = li.As.ncol = N; li.As.nnz = z;
             }
         }
-        trace("frame operators");
+        trace(("frame operators L" + std::to_string(l)).c_str());
         csr_tile_stats(li.Af, s);
         if (H.kind == PREC_CHEB && l > 0) csr_tile_stats(li.As, s);
         if (!li.direct) {
@@ -1383,7 +1389,7 @@ static void build_frames(Hierarchy& H, cudaStream_t s) {
             csr_tile_stats(li.P1, s);
             csr_tile_stats(li.G, s);
         }
-        trace("explicit solves");
+        trace(("explicit solves L" + std::to_string(l)).c_str());
     }
 }
 
