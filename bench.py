@@ -353,16 +353,20 @@ def run_ours(args, ws, rank, local):
     tl = Pp.timeline(10)
     out["apply_timeline"] = grouped(tl, 1e-3)  # ms
     out["apply_timeline_ms"] = float(sum(t[1] for t in tl)) / 1e3
-    # the whole apply (gather, graph, scatter) 20 times, events around them
+    # the whole apply (gather, graph, scatter) 20 times, events around them on
+    # a stream of its own (a null stream handle would select the handle's
+    # stream, which the events on torch's default stream do not wait for)
     fa = torch.randn(N, dtype=torch.float64, device=dev)
     za = torch.empty_like(fa)
+    sa = torch.cuda.Stream(dev)
+    sa.wait_stream(stream)
     g0 = torch.cuda.Event(enable_timing=True)
     g1 = torch.cuda.Event(enable_timing=True)
-    g0.record(stream)
+    g0.record(sa)
     for _ in range(20):
         check(lib().mlp_prec_apply(Pp.h, C.c_void_p(fa.data_ptr()), C.c_void_p(za.data_ptr()),
-                                   C.c_void_p(stream.cuda_stream)))
-    g1.record(stream)
+                                   C.c_void_p(sa.cuda_stream)))
+    g1.record(sa)
     g1.synchronize()
     out["apply_graph_ms"] = g0.elapsed_time(g1) / 20
     del fa, za

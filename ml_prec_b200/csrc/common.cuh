@@ -239,5 +239,15 @@ int num_sms();
 uint32_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n, cudaStream_t s);
 // Same, total left on the device at out[n] (no host synchronisation).
 void exclusive_scan_u32_async(const uint32_t* in, uint32_t* out, uint32_t n, cudaStream_t s);
+// Several scans with one host synchronisation; returns their totals.
+struct ScanJob {
+    const uint32_t* in;
+    uint32_t* out;
+    uint32_t n;
+};
+std::vector<uint32_t> exclusive_scans_u32(const std::vector<ScanJob>& jobs, cudaStream_t s);
+// Copies `words` 32-bit device words (any addresses) to the host with one
+// synchronisation.
+std::vector<uint32_t> read_words(const std::vector<const uint32_t*>& words, cudaStream_t s);
 
 }  // namespace mlp

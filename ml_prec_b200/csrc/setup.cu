@@ -836,6 +836,18 @@ struct Scratch {
     Tmp<uint32_t> rmap, tpos, slot, cand, cnt;
 };
 
+// First slot capacity for `rows` rows: as large as a 2 GB slot area allows
+// (at most 256 entries; never below what the previously built, coarser level
+// needed: rows get longer towards the fine levels), so that the usual rows
+// never overflow and the build is not repeated. The slots are scratch of the
+// build, and the rows computed do not depend on the capacity.
+static uint32_t slot_cap0(uint32_t rows, uint32_t prev) {
+    uint64_t fit = ((uint64_t)1 << 31) / ((uint64_t)(rows ? rows : 1) * 12);
+    uint32_t cap = 16;
+    while (cap < 256 && (uint64_t)cap * 2 <= fit) cap *= 2;
+    return std::max(cap, prev);
+}
+
 static void sparse_lu_level(Level& li, Level& ln, const uint8_t* keep, const double* aux, const uint32_t* rmap,
                             double beta, cudaStream_t s) {
     const DCSR& A = li.A;
@@ -844,7 +856,7 @@ static void sparse_lu_level(Level& li, Level& ln, const uint8_t* keep, const dou
     li.done.zero(s);
     Tmp<uint32_t> slen(R ? R : 1), sldiv(R ? R : 1), wait(R ? R : 1);
     Tmp<int> flags(1);
-    uint32_t cap = 32;
+    uint32_t cap = slot_cap0(R, 32);
     for (int attempt = 0;; attempt++) {
         Tmp<uint32_t> scol((size_t)R * cap + 1);
         Tmp<double> sval((size_t)R * cap + 1);
@@ -873,35 +885,38 @@ static void sparse_lu_level(Level& li, Level& ln, const uint8_t* keep, const dou
                     std::swap(pin, pout);
                     std::swap(cin, cout);
                 }
-                uint32_t left = read_u32(cin, s);
-                if ((read_flag(flags.p, s) & 1) || left == 0) break;
+                std::vector<uint32_t> h = read_words({cin, reinterpret_cast<const uint32_t*>(flags.p)}, s);
+                uint32_t left = h[0];
+                if ((h[1] & 1) || left == 0) break;
                 // every round finishes at least the rows whose dependencies are
                 // done; no progress over sixteen rounds means a cycle
                 if (left >= prev_left) MLP_THROW(ERR_INTERNAL, "elimination makes no progress");
                 prev_left = left;
             }
         }
-        if (!(read_flag(flags.p, s) & 1) && R > M) {
+        // k_lu_coarse runs also after an overflow (its rows then fail fast
+        // on the flag); one read of the flags decides
+        if (R > M) {
             k_lu_coarse<<<grid_for(R - M, 128), 128, 0, s>>>(g);
             CK_LAUNCH();
         }
         int fl = read_flag(flags.p, s);
-        if (fl & 8) MLP_THROW(ERR_INTERNAL, "coarse row met an unfinished U row");
-        if (fl & 1) {
+        if (fl & 1) {  // an overflow (the coarse rows may then also have met unfinished rows)
             if (cap >= 4096) MLP_THROW(ERR_LIMIT, "elimination row exceeds 4096 entries");
             cap *= 2;
             continue;
         }
+        if (fl & 8) MLP_THROW(ERR_INTERNAL, "coarse row met an unfinished U row");
         // compaction
         Tmp<uint32_t> lc(R + 1), uc(M + 1), nc(R - M + 1);
         k_lu_counts<<<grid_for(R, 256), 256, 0, s>>>(R, M, slen.p, sldiv.p, lc.p, uc.p, nc.p);
         CK_LAUNCH();
         li.L.ia.alloc((size_t)R + 1);
-        uint32_t lnnz = exclusive_scan_u32(lc.p, li.L.ia.p, R, s);
         li.U.ia.alloc((size_t)M + 1);
-        uint32_t unnz = exclusive_scan_u32(uc.p, li.U.ia.p, M, s);
         ln.A.ia.alloc((size_t)(R - M) + 1);
-        uint32_t nnnz = exclusive_scan_u32(nc.p, ln.A.ia.p, R - M, s);
+        std::vector<uint32_t> tot = exclusive_scans_u32({{lc.p, li.L.ia.p, R}, {uc.p, li.U.ia.p, M},
+                                                         {nc.p, ln.A.ia.p, R - M}}, s);
+        uint32_t lnnz = tot[0], unnz = tot[1], nnnz = tot[2];
         li.L.nrow = li.L.ncol = R; li.L.nnz = lnnz;
         li.L.ja.alloc(lnnz ? lnnz : 1); li.L.a.alloc(lnnz ? lnnz : 1);
         li.U.nrow = M; li.U.ncol = R; li.U.nnz = unnz;
@@ -915,7 +930,6 @@ static void sparse_lu_level(Level& li, Level& ln, const uint8_t* keep, const dou
             CK_LAUNCH();
         }
         li.nwave_l = (uint32_t)rounds;  // upper bound, refined by the frame build
-        CK(cudaStreamSynchronize(s));
         break;
     }
 }
@@ -1187,15 +1201,12 @@ static void counting_sort(const std::vector<int>& lev, uint32_t nrows, std::vect
 
 
 // Explicit forms of the level's triangular solves (P1 and G, setup.cuh).
-// Slot capacities start from the ones the previously built (coarser) level
-// needed (p1_cap, g_cap; updated on return): rows get longer towards the fine
-// levels, so this saves the attempts that would overflow. The rows computed do
-// not depend on the capacity.
 static void build_explicit(Level& li, cudaStream_t s, uint32_t& p1_cap, uint32_t& g_cap) {
     uint32_t M = li.M, R = li.N - li.Md;
     Tmp<int> flags(1);
+    const uint32_t* flag_word = reinterpret_cast<const uint32_t*>(flags.p);
     // P1
-    for (uint32_t cap = std::max<uint32_t>(16, p1_cap);; cap *= 2) {
+    for (uint32_t cap = slot_cap0(R, p1_cap);; cap *= 2) {
         if (cap > 65536) MLP_THROW(ERR_LIMIT, "explicit L solve row exceeds 65536 entries");
         Tmp<uint32_t> scol((size_t)R * cap + 1), slen(R + 1);
         Tmp<double> sval((size_t)R * cap + 1);
@@ -1209,14 +1220,17 @@ static void build_explicit(Level& li, cudaStream_t s, uint32_t& p1_cap, uint32_t
             k_p1_rows<<<grid_for(R - M, 128), 128, 0, s>>>(M, R, li.Lf.ia.p, li.Lf.ja.p, li.Lf.a.p, cap, scol.p,
                                                          sval.p, slen.p, flags.p);
         CK_LAUNCH();
-        if (read_flag(flags.p, s)) continue;
+        // the row pointers are scanned before the overflow flag is known, so
+        // that one read brings back both
         li.P1.ia.alloc((size_t)R + 1);
-        uint32_t z = exclusive_scan_u32(slen.p, li.P1.ia.p, R, s);
+        exclusive_scan_u32_async(slen.p, li.P1.ia.p, R, s);
+        std::vector<uint32_t> h = read_words({flag_word, li.P1.ia.p + R}, s);
+        if (h[0]) continue;
+        uint32_t z = h[1];
         li.P1.nrow = R; li.P1.ncol = R; li.P1.nnz = z;
         li.P1.ja.alloc(z ? z : 1); li.P1.a.alloc(z ? z : 1);
         if (R) k_slots_emit<<<grid_for(R, 128), 128, 0, s>>>(R, cap, scol.p, sval.p, li.P1.ia.p, li.P1.ja.p, li.P1.a.p);
         CK_LAUNCH();
-        CK(cudaStreamSynchronize(s));
         p1_cap = cap;
         trace(("  explicit: P1 (" + std::to_string(li.lw_off.size() - 1) + " waves, slot " + std::to_string(cap) +
                ")").c_str());
@@ -1225,7 +1239,7 @@ static void build_explicit(Level& li, cudaStream_t s, uint32_t& p1_cap, uint32_t
     // G
     li.G.nrow = M; li.G.ncol = R; li.G.nnz = 0;
     if (!M) { li.G.ia.alloc(1); li.G.ia.zero(s); li.G.ja.alloc(1); li.G.a.alloc(1); return; }
-    for (uint32_t cap = std::max<uint32_t>(16, g_cap);; cap *= 2) {
+    for (uint32_t cap = slot_cap0(M, g_cap);; cap *= 2) {
         if (cap > 65536) MLP_THROW(ERR_LIMIT, "explicit U solve row exceeds 65536 entries");
         Tmp<uint32_t> scol((size_t)M * cap + 1), slen(M + 1);
         Tmp<double> sval((size_t)M * cap + 1);
@@ -1237,14 +1251,15 @@ static void build_explicit(Level& li, cudaStream_t s, uint32_t& p1_cap, uint32_t
                                                                         slen.p, flags.p);
         }
         CK_LAUNCH();
-        if (read_flag(flags.p, s)) continue;
         li.G.ia.alloc((size_t)M + 1);
-        uint32_t z = exclusive_scan_u32(slen.p, li.G.ia.p, M, s);
+        exclusive_scan_u32_async(slen.p, li.G.ia.p, M, s);
+        std::vector<uint32_t> h = read_words({flag_word, li.G.ia.p + M}, s);
+        if (h[0]) continue;
+        uint32_t z = h[1];
         li.G.nnz = z;
         li.G.ja.alloc(z ? z : 1); li.G.a.alloc(z ? z : 1);
         k_slots_emit<<<grid_for(M, 128), 128, 0, s>>>(M, cap, scol.p, sval.p, li.G.ia.p, li.G.ja.p, li.G.a.p);
         CK_LAUNCH();
-        CK(cudaStreamSynchronize(s));
         g_cap = cap;
         trace(("  explicit: G (" + std::to_string(li.uw_off.size() - 1) + " waves, slot " + std::to_string(cap) +
                ")").c_str());
@@ -1298,7 +1313,9 @@ static void build_frames(Hierarchy& H, cudaStream_t s) {
             k_row_len_perm<<<grid_for(R, 256), 256, 0, s>>>(R, pi.p, li.L.ia.p, len.p);
             CK_LAUNCH();
             li.Lf.ia.alloc((size_t)R + 1);
-            uint32_t z = exclusive_scan_u32(len.p, li.Lf.ia.p, R, s);
+            // the rows are L's, permuted: the total is known (checked below)
+            exclusive_scan_u32_async(len.p, li.Lf.ia.p, R, s);
+            uint32_t z = li.L.nnz;
             li.Lf.nrow = R; li.Lf.ncol = M; li.Lf.nnz = z;
             li.Lf.ja.alloc(z ? z : 1); li.Lf.a.alloc(z ? z : 1);
             k_gather_rows<<<grid_for(R, 256), 256, 0, s>>>(R, pi.p, li.L.ia.p, li.L.ja.p, li.L.a.p, p2f.p,
@@ -1311,7 +1328,8 @@ static void build_frames(Hierarchy& H, cudaStream_t s) {
             k_row_len_perm<<<grid_for(M, 256), 256, 0, s>>>(M, li.eperm.p, li.U.ia.p, len.p);
             CK_LAUNCH();
             li.Uf.ia.alloc((size_t)M + 1);
-            uint32_t z = exclusive_scan_u32(len.p, li.Uf.ia.p, M, s);
+            exclusive_scan_u32_async(len.p, li.Uf.ia.p, M, s);
+            uint32_t z = li.U.nnz;
             li.Uf.nrow = M; li.Uf.ncol = R; li.Uf.nnz = z;
             li.Uf.ja.alloc(z ? z : 1); li.Uf.a.alloc(z ? z : 1);
             k_gather_rows<<<grid_for(M, 256), 256, 0, s>>>(M, li.eperm.p, li.U.ia.p, li.U.ja.p, li.U.a.p, p2f.p,
@@ -1361,7 +1379,8 @@ static void build_frames(Hierarchy& H, cudaStream_t s) {
             k_row_len_perm<<<grid_for(N, 256), 256, 0, s>>>(N, li.phi.p, A.ia.p, len.p);
             CK_LAUNCH();
             li.Af.ia.alloc((size_t)N + 1);
-            uint32_t z = exclusive_scan_u32(len.p, li.Af.ia.p, N, s);
+            exclusive_scan_u32_async(len.p, li.Af.ia.p, N, s);
+            uint32_t z = A.nnz;
             li.Af.nrow = li.Af.ncol = N; li.Af.nnz = z;
             li.Af.ja.alloc(z ? z : 1); li.Af.a.alloc(z ? z : 1);
             k_gather_rows<<<grid_for(N, 256), 256, 0, s>>>(N, li.phi.p, A.ia.p, A.ja.p, A.a.p, li.iphi.p,
@@ -1382,13 +1401,26 @@ static void build_frames(Hierarchy& H, cudaStream_t s) {
             }
         }
         trace(("frame operators L" + std::to_string(l)).c_str());
-        csr_tile_stats(li.Af, s);
-        if (H.kind == PREC_CHEB && l > 0) csr_tile_stats(li.As, s);
+        if (!li.direct) build_explicit(li, s, p1_cap, g_cap);
+        // tile statistics of the level's operators and the check of the
+        // permuted row pointers' totals, in one read
+        std::vector<DCSR*> ms{&li.Af};
+        std::vector<const uint32_t*> ends{li.Af.ia.p + N};
+        std::vector<uint32_t> want{li.A.nnz};
+        if (H.kind == PREC_CHEB && l > 0) ms.push_back(&li.As);
         if (!li.direct) {
-            build_explicit(li, s, p1_cap, g_cap);
-            csr_tile_stats(li.P1, s);
-            csr_tile_stats(li.G, s);
+            ms.push_back(&li.P1);
+            ms.push_back(&li.G);
+            ends.push_back(li.Lf.ia.p + R);
+            want.push_back(li.L.nnz);
+            if (M) {
+                ends.push_back(li.Uf.ia.p + M);
+                want.push_back(li.U.nnz);
+            }
         }
+        std::vector<uint32_t> got;
+        csr_tile_stats_batch(ms, ends, got, s);
+        if (got != want) MLP_THROW(ERR_INTERNAL, "permuted operator has the wrong number of entries");
         trace(("explicit solves L" + std::to_string(l)).c_str());
     }
 }

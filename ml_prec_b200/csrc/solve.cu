@@ -259,6 +259,30 @@ void csr_tile_stats(DCSR& m, cudaStream_t s) {
     if (m.tile_max && m.tile_max <= ST_MAX_NNZ) pipe_prepare_all(m.tile_max);
 }
 
+void csr_tile_stats_batch(const std::vector<DCSR*>& ms, const std::vector<const uint32_t*>& extra,
+                          std::vector<uint32_t>& extra_out, cudaStream_t s) {
+    Tmp<uint32_t> d(ms.size() + 1);
+    d.zero(s);
+    std::vector<const uint32_t*> words;
+    for (size_t i = 0; i < ms.size(); i++) {
+        const DCSR& m = *ms[i];
+        if (m.nrow) {
+            uint32_t nt = (m.nrow + ST_ROWS - 1) / ST_ROWS;
+            k_tile_max<<<grid_for(nt, 256), 256, 0, s>>>(m.nrow, m.ia.p, d.p + i);
+            CK_LAUNCH();
+        }
+        words.push_back(d.p + i);
+    }
+    for (const uint32_t* w : extra) words.push_back(w);
+    std::vector<uint32_t> h = read_words(words, s);
+    for (size_t i = 0; i < ms.size(); i++) {
+        DCSR& m = *ms[i];
+        m.tile_max = m.nrow ? h[i] : 0;
+        if (m.tile_max && m.tile_max <= ST_MAX_NNZ) pipe_prepare_all(m.tile_max);
+    }
+    extra_out.assign(h.begin() + ms.size(), h.end());
+}
+
 static unsigned staged_grid(uint32_t n) {
     uint32_t nt = (n + ST_ROWS - 1) / ST_ROWS;
     return (unsigned)std::max<uint32_t>(1, std::min<uint32_t>(nt, (uint32_t)num_sms() * 5));
@@ -1388,7 +1412,7 @@ struct Builder {
         const bool next = l + 1 < H.nlevels && L.n;
         const double* C = nullptr;
         uint32_t n = 0;
-        if (next && fold && !ps && explicit_solves && !autotune && dense_next(l, C, n) && fold_ready(l, C, n)) {
+        if (next && fold && !ps && explicit_solves && dense_next(l, C, n) && fold_ready(l, C, n)) {
             phase2_fold(l, C, n, w, out);
             return;
         }

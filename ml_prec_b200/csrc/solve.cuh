@@ -102,6 +102,10 @@ void check_persist(Prec& P, cudaStream_t s);
 
 // Records the largest nnz of a 256-row tile (decides the staged SpMV).
 void csr_tile_stats(DCSR& m, cudaStream_t s);
+// The same for several matrices with one host synchronisation; the device
+// words `extra` are read back in the same copy (into extra_out).
+void csr_tile_stats_batch(const std::vector<DCSR*>& ms, const std::vector<const uint32_t*>& extra,
+                          std::vector<uint32_t>& extra_out, cudaStream_t s);
 
 // y = A x for a CSR matrix (any level, frame or natural order).
 void spmv(const DCSR& A, const double* x, double* y, cudaStream_t s);

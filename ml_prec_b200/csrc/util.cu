@@ -362,7 +362,29 @@ void exclusive_scan_u32_async(const uint32_t* in, uint32_t* out, uint32_t n, cud
     CK_LAUNCH();
     k_tile_scan<<<nt, SCAN_T, 0, s>>>(in, out, n, sums.p);
     CK_LAUNCH();
-    CK(cudaStreamSynchronize(s));  // sums is released on return
+    // no synchronisation for `sums`: scratch released here is reused only
+    // after the device has been synchronised (arena scopes end with a device
+    // synchronisation; released pool blocks wait in a pending list until one)
+}
+
+std::vector<uint32_t> read_words(const std::vector<const uint32_t*>& words, cudaStream_t s) {
+    std::vector<uint32_t> h(words.size(), 0);
+    if (words.empty()) return h;
+    Tmp<uint32_t> d(words.size());
+    for (size_t i = 0; i < words.size(); i++)
+        CK(cudaMemcpyAsync(d.p + i, words[i], 4, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(h.data(), d.p, 4 * words.size(), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return h;
+}
+
+std::vector<uint32_t> exclusive_scans_u32(const std::vector<ScanJob>& jobs, cudaStream_t s) {
+    std::vector<const uint32_t*> ends;
+    for (const ScanJob& j : jobs) {
+        exclusive_scan_u32_async(j.in, j.out, j.n, s);
+        ends.push_back(j.out + j.n);
+    }
+    return read_words(ends, s);
 }
 
 uint32_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n, cudaStream_t s) {
