@@ -1200,6 +1200,94 @@ static void counting_sort(const std::vector<int>& lev, uint32_t nrows, std::vect
 }
 
 
+// ---- the same sort on the device --------------------------------------------
+// Rows in blocks of KS_BLOCK: per-block bin counts (bin-major, so one scan of
+// them gives every block's start in every bin), then each block scatters its
+// rows; within a block a row's place is the rows of its bin in earlier warps
+// plus its rank among the lanes of its warp with the same key, so the order
+// within a bin is the index order (a stable sort, as counting_sort).
+constexpr uint32_t KS_BLOCK = 1024;
+constexpr uint32_t KS_MAXK = 64;
+
+__global__ void __launch_bounds__(KS_BLOCK) k_key_hist(const int* __restrict__ key, uint32_t n, uint32_t K,
+                                                       uint32_t nblk, uint32_t* __restrict__ bcnt,
+                                                       int* __restrict__ bad) {
+    __shared__ uint32_t h[KS_MAXK];
+    for (uint32_t t = threadIdx.x; t < K; t += blockDim.x) h[t] = 0;
+    __syncthreads();
+    uint32_t i = blockIdx.x * KS_BLOCK + threadIdx.x;
+    if (i < n) {
+        int k = key[i];
+        if (k >= 1 && (uint32_t)k <= K) atomicAdd(&h[k - 1], 1u);
+        else atomicOr(bad, 1);
+    }
+    __syncthreads();
+    for (uint32_t t = threadIdx.x; t < K; t += blockDim.x) bcnt[(size_t)t * nblk + blockIdx.x] = h[t];
+}
+
+__global__ void __launch_bounds__(KS_BLOCK) k_key_scatter(const int* __restrict__ key, uint32_t n, uint32_t K,
+                                                          uint32_t nblk, const uint32_t* __restrict__ bpos,
+                                                          uint32_t* __restrict__ rows) {
+    __shared__ uint32_t wc[KS_BLOCK / 32][KS_MAXK];
+    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+    for (uint32_t t = threadIdx.x; t < (KS_BLOCK / 32) * KS_MAXK; t += blockDim.x) (&wc[0][0])[t] = 0;
+    __syncthreads();
+    const uint32_t i = blockIdx.x * KS_BLOCK + threadIdx.x;
+    const bool act = i < n;
+    int k = act ? key[i] - 1 : -1;
+    if (act && (k < 0 || (uint32_t)k >= K)) k = -1;  // reported by k_key_hist; placed nowhere
+    const unsigned peers = __match_any_sync(0xffffffffu, k);
+    const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+    if (k >= 0 && lane == (uint32_t)(__ffs(peers) - 1)) wc[w][k] = __popc(peers);
+    __syncthreads();
+    for (uint32_t t = threadIdx.x; t < K; t += blockDim.x) {
+        uint32_t acc = 0;
+        for (uint32_t v = 0; v < KS_BLOCK / 32; v++) {
+            uint32_t c = wc[v][t];
+            wc[v][t] = acc;
+            acc += c;
+        }
+    }
+    __syncthreads();
+    if (k >= 0) rows[bpos[(size_t)k * nblk + blockIdx.x] + wc[w][k] + rank] = i;
+}
+
+// off[d] = start of bin d (bpos of block 0), off[K] = n; off[K + 1] = the bad flag
+__global__ void k_key_offsets(uint32_t n, uint32_t K, uint32_t nblk, const uint32_t* __restrict__ bpos,
+                              const int* __restrict__ bad, uint32_t* __restrict__ off) {
+    uint32_t d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d < K) off[d] = bpos[(size_t)d * nblk];
+    if (d == K) off[K] = n;
+    if (d == K + 1) off[K + 1] = (uint32_t)*bad;
+}
+
+// counting_sort of the device keys key[0, n) (each in [1, K]) into rows_out on
+// the device and off on the host; false (nothing written) when K is above
+// KS_MAXK or a key is out of range, and the caller sorts on the host.
+static bool device_key_sort(const int* key, uint32_t n, uint32_t K, uint32_t* rows_out, std::vector<uint32_t>& off,
+                            cudaStream_t s) {
+    if (!n || !K || K > KS_MAXK) return false;
+    const uint32_t nblk = (n + KS_BLOCK - 1) / KS_BLOCK;
+    Tmp<uint32_t> bcnt((size_t)K * nblk + 1), bpos((size_t)K * nblk + 1), offs(K + 2);
+    Tmp<int> bad(1);
+    bad.zero(s);
+    k_key_hist<<<nblk, KS_BLOCK, 0, s>>>(key, n, K, nblk, bcnt.p, bad.p);
+    CK_LAUNCH();
+    exclusive_scan_u32_async(bcnt.p, bpos.p, K * nblk, s);
+    k_key_offsets<<<1, 128, 0, s>>>(n, K, nblk, bpos.p, bad.p, offs.p);
+    CK_LAUNCH();
+    std::vector<uint32_t> h(K + 2);
+    CK(cudaMemcpyAsync(h.data(), offs.p, (K + 2) * 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (h[K + 1]) return false;
+    k_key_scatter<<<nblk, KS_BLOCK, 0, s>>>(key, n, K, nblk, bpos.p, rows_out);
+    CK_LAUNCH();
+    // counting_sort's offsets: bins up to the last non-empty one, then n
+    off.assign(h.begin(), h.begin() + K + 1);
+    while (off.size() > 1 && off[off.size() - 2] == n) off.pop_back();
+    return true;
+}
+
 // Explicit forms of the level's triangular solves (P1 and G, setup.cuh).
 static void build_explicit(Level& li, cudaStream_t s, uint32_t& p1_cap, uint32_t& g_cap) {
     uint32_t M = li.M, R = li.N - li.Md;
@@ -1284,15 +1372,18 @@ static void build_frames(Hierarchy& H, cudaStream_t s) {
         uint32_t M = li.M, n = li.n, R = N - li.Md;
         if (!li.direct) {
         // E block order: by L wavefront (elimination round), then permuted index
-        std::vector<int> done = li.done.download(s, M);
-        std::vector<uint32_t> off, rows;
-        counting_sort(done, M, off, rows);
+        std::vector<uint32_t> off;
+        li.eperm.alloc(M ? M : 1);
+        if (!device_key_sort(li.done.p, M, li.nwave_l, li.eperm.p, off, s)) {
+            std::vector<int> done = li.done.download(s, M);
+            std::vector<uint32_t> rows;
+            counting_sort(done, M, off, rows);
+            if (M) li.eperm.upload(rows.data(), M, s);
+        }
         li.lw_off = off;
         li.nwave_l = (uint32_t)off.size() - 1;
         li.lw_off_d.alloc(off.size());
         li.lw_off_d.upload(off.data(), off.size(), s);
-        li.eperm.alloc(M ? M : 1);
-        if (M) li.eperm.upload(rows.data(), M, s);
         Tmp<uint32_t> pi(N), einv(M ? M : 1), p2f(N);
         const uint32_t* phi_next = (l + 1 < (int)H.nlevels) ? H.lv[l + 1]->phi.p : nullptr;
         const uint32_t* iphi_next = (l + 1 < (int)H.nlevels) ? H.lv[l + 1]->iphi.p : nullptr;
@@ -1362,14 +1453,17 @@ static void build_frames(Hierarchy& H, cudaStream_t s) {
                 prev_left = left;
             }
             trace(("  frame: Lf, Uf, U schedule (" + std::to_string(round) + " rounds)").c_str());
-            std::vector<int> ul = lev.download(s, M);
-            std::vector<uint32_t> uoff, urows;
-            counting_sort(ul, M, uoff, urows);
+            std::vector<uint32_t> uoff;
+            li.uw_rows.alloc(M);
+            if (!device_key_sort(lev.p, M, (uint32_t)round, li.uw_rows.p, uoff, s)) {
+                std::vector<int> ul = lev.download(s, M);
+                std::vector<uint32_t> urows;
+                counting_sort(ul, M, uoff, urows);
+                li.uw_rows.upload(urows.data(), M, s);
+            }
             li.uw_off = uoff;
             li.uw_off_d.alloc(uoff.size());
             li.uw_off_d.upload(uoff.data(), uoff.size(), s);
-            li.uw_rows.alloc(M);
-            li.uw_rows.upload(urows.data(), M, s);
         }
         }  // !direct
         // Af: rows phi(q), columns -> iphi
