@@ -59,6 +59,11 @@ MSPLIT = dict(q=(0.8,), niter=(5,), max_levels=15, degree_max=2, order="simple_1
 # (106.84 MB read + 4.79 MB written): the matrix and x stream once; part of y
 # is still in L2 when the kernel ends.
 SPMV_DRAM_TRAFFIC = 111.63e6
+# DRAM bytes (read + write) of one launch of the folded level-2 phase 2
+# (k_phase2_fold) on this matrix, from the ncu capture summarised in
+# profiles/phase2_fold_level2_60x220x85.md (cold caches: in the graph its
+# operators stay in L2). Not measured in the run.
+FOLD_DRAM_TRAFFIC = {"phase2_fold L2": 4.42e6}
 
 
 def dist_env():
@@ -686,8 +691,10 @@ def main():
                      "bytes_per_launch": top[3] / top[1], "ms_per_launch": top[2] / top[1],
                      "timing": "in-graph time per launch (mlp_prec_timeline: %globaltimer stamped by each kernel "
                                "as it passes its dependent-launch wait, 10 back-to-back replays of the apply graph)",
-                     "traffic": None,
-                     "traffic_source": "see profiles/ for the ncu DRAM traffic of this kernel",
+                     "traffic": FOLD_DRAM_TRAFFIC.get(top[0]),
+                     "traffic_source": ("taken from profiles/phase2_fold_level2_60x220x85.md (ncu, one launch, cold "
+                                        "caches), not measured in this run" if top[0] in FOLD_DRAM_TRAFFIC
+                                        else "no ncu capture of this launch group on this matrix"),
                      "apply_groups": apply_groups,
                      "apply_ms_in_graph": res["apply_timeline_ms"],
                      "apply_graph_ms_events": res["apply_graph_ms"],
