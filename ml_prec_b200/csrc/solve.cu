@@ -691,7 +691,7 @@ __global__ void __launch_bounds__(256) k_phase2_fold(uint32_t M, uint32_t n, con
                                                      const uint32_t* __restrict__ rows, uint32_t nf, uint32_t nb_c,
                                                      uint32_t nb_f, const T* __restrict__ w, T* __restrict__ out) {
     if (blockIdx.x < nb_c + nb_f) {
-        constexpr int CV = 8;  // prefetched FP64 values per lane (40 registers a thread)
+        constexpr int CV = 16;
         const bool coarse = blockIdx.x < nb_c;
         const uint32_t r = (coarse ? blockIdx.x : blockIdx.x - nb_c) * (blockDim.x >> 5) + (threadIdx.x >> 5);
         const int lane = threadIdx.x & 31;
@@ -833,13 +833,8 @@ __device__ __forceinline__ T lane_split_sum(uint32_t jb, uint32_t je, const uint
     return p[0];
 }
 
-// Lanes of step A per P1 row: the small levels' P1 rows hold about two
-// entries, so four lanes keep the launch small (fewer CTAs hold the SMs'
-// registers while the next launch wants to become resident).
-static constexpr uint32_t MERGE_GP = 4;
-
 // Step A. Blocks [0, nbu): the rows of Af with LPU lanes per row (the
-// correction kernel's layout); blocks [nbu, ...): MERGE_GP lanes per P1 row.
+// correction kernel's layout); blocks [nbu, ...): one thread per P1 row.
 // MODE 0: r' = f - Af x (second sweep); MODE 1: x += u0; r' = r - Af u0.
 template <class T, int LPU, int LPP, int MODE>
 __global__ void __launch_bounds__(256) k_merge_a(uint32_t N, uint32_t R, uint32_t nbu, const uint32_t* __restrict__ af_ia,
@@ -875,15 +870,13 @@ __global__ void __launch_bounds__(256) k_merge_a(uint32_t N, uint32_t R, uint32_
             if (row >= R) u_out[row] = d * rn;
         }
     } else {
-        // MERGE_GP lanes per P1 row: lane e of a row's group recomputes the
-        // entry r'_k of the row's entries e, e + GP, ... (the group's lanes at
-        // once), then every lane of the group adds the products in entry order
-        // with k_phase1's lane split. The row's first GP entries and their Af
-        // row bounds are loaded before the wait.
-        constexpr uint32_t GP = MERGE_GP;
-        const uint32_t lane = threadIdx.x & 31u, sub = lane & (GP - 1), gbase = lane & ~(GP - 1);
-        const uint32_t q = (((blockIdx.x - nbu) * blockDim.x + threadIdx.x) >> 5) * (32 / GP) + lane / GP;
-        const bool act = q < R;
+        // One warp per P1 row: lane e recomputes the entry r'_k of the row's
+        // entries e, e + 32, ... (all lanes at once), then the products are
+        // added in entry order with k_phase1's lane split. The row's first 32
+        // entries and their Af row bounds are loaded before the wait.
+        uint32_t q = ((blockIdx.x - nbu) * blockDim.x + threadIdx.x) >> 5;
+        int lane = threadIdx.x & 31;
+        bool act = q < R;
         uint32_t jb = 0, je = 0;
         if (act) {
             jb = p1_ia[q];
@@ -891,26 +884,22 @@ __global__ void __launch_bounds__(256) k_merge_a(uint32_t N, uint32_t R, uint32_
         }
         uint32_t k0 = 0, kb0 = 0, ke0 = 0;
         T a0 = 0;
-        if (jb + sub < je) {
-            k0 = p1_ja[jb + sub];
-            a0 = p1_a[jb + sub];
+        if (jb + lane < je) {
+            k0 = p1_ja[jb + lane];
+            a0 = p1_a[jb + lane];
             kb0 = af_ia[k0];
             ke0 = af_ia[k0 + 1];
         }
         pdl_wait();
         pdl_trigger();
-        if (!__any_sync(0xffffffffu, act)) return;  // the whole warp
+        if (!act) return;  // the whole warp
         T p[LPP];
 #pragma unroll
         for (int l = 0; l < LPP; l++) p[l] = 0;
-        // every lane of the warp takes the shuffles until the longest row of
-        // its eight groups is done
-        for (uint32_t base = jb;; base += GP) {
-            const bool more = act && base < je;
-            if (!__any_sync(0xffffffffu, more)) break;
-            const uint32_t j = base + sub;
+        for (uint32_t base = jb; base < je; base += 32) {
+            uint32_t j = base + lane;
             T av = 0, rv = 0;
-            if (more && j < je) {
+            if (j < je) {
                 uint32_t k = k0, kb = kb0, ke = ke0;
                 av = a0;
                 if (base != jb) {
@@ -922,16 +911,13 @@ __global__ void __launch_bounds__(256) k_merge_a(uint32_t N, uint32_t R, uint32_
                 T t = lane_split_sum<T, LPU>(kb, ke, af_ja, af_a, [&](uint32_t c) { return v[c]; });
                 rv = (MODE == 0 ? f[k] : r_in[k]) - t;
             }
-            const uint32_t cnt = more ? min(GP, je - base) : 0u;
+            uint32_t cnt = min(32u, je - base);
+            for (uint32_t e = 0; e < cnt; e++) {
+                T ae = __shfl_sync(0xffffffffu, av, e), re = __shfl_sync(0xffffffffu, rv, e);
+                int l = (int)((base - jb + e) & (LPP - 1));
 #pragma unroll
-            for (uint32_t e = 0; e < GP; e++) {
-                T ae = __shfl_sync(0xffffffffu, av, gbase + e), re = __shfl_sync(0xffffffffu, rv, gbase + e);
-                if (e < cnt) {
-                    int l = (int)((base - jb + e) & (LPP - 1));
-#pragma unroll
-                    for (int m = 0; m < LPP; m++)
-                        if (m == l) p[m] = fmadd(ae, re, p[m]);
-                }
+                for (int m = 0; m < LPP; m++)
+                    if (m == l) p[m] = fmadd(ae, re, p[m]);
             }
         }
 #pragma unroll
@@ -942,7 +928,7 @@ __global__ void __launch_bounds__(256) k_merge_a(uint32_t N, uint32_t R, uint32_
 #pragma unroll
             for (int l = 0; l < LPP; l++) p[l] = t2[l];
         }
-        if (act && sub == 0) w[q] = p[0];
+        if (lane == 0) w[q] = p[0];
     }
 }
 
@@ -1591,7 +1577,7 @@ struct Builder {
         bool staged = L.Af.tile_max && L.Af.tile_max <= ST_MAX_NNZ && N >= 4 * ST_ROWS;
         int lpu = mode == 0 ? (staged ? 1 : pick_lpr(N, L.Af.nnz)) : pick_lpr(N, L.Af.nnz);
         int lpp = pick_lpr(R, L.P1.nnz);
-        uint32_t nbu = grid_for((size_t)N * lpu, 256), nbp = R ? grid_for((size_t)R * MERGE_GP, 256) : 0;
+        uint32_t nbu = grid_for((size_t)N * lpu, 256), nbp = R ? grid_for((size_t)R * 32, 256) : 0;
         const uint32_t *aia = L.Af.ia.p, *aja = L.Af.ja.p, *pia = L.P1.ia.p, *pja = L.P1.ja.p;
         const T *aa = vals<T>(L.Af), *pa = vals<T>(L.P1), *dv = dvals<T>(L);
         auto go = [=](auto kern, cudaStream_t s) {
