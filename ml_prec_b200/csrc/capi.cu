@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <exception>
 #include <thread>
 
 #include "../../include/mlp_b200.h"
@@ -67,7 +68,7 @@ static bool matrix_ok(uint32_t n, const uint32_t* ia, const uint32_t* ja, const 
     auto work = [&](unsigned t) {
         uint32_t r0 = (uint32_t)((uint64_t)n * t / T), r1 = (uint32_t)((uint64_t)n * (t + 1) / T);
         bool good = true;
-        for (uint32_t i = r0; i < r1; i++) good &= (ia[i + 1] > ia[i]);
+        for (uint32_t i = r0; i < r1; i++) good &= (ia[i + 1] > ia[i]) & (ia[i + 1] <= nnz);
         if (good)
             for (uint32_t i = r0; i < r1; i++) good &= (ja[ia[i]] == i);
         size_t k0 = (uint64_t)nnz * t / T, k1 = (uint64_t)nnz * (t + 1) / T;
@@ -123,21 +124,13 @@ int mlp_matrix_create(uint32_t n, const uint32_t* ia, const uint32_t* ja, const 
     if (ia[0] != 0) MLP_THROW(ERR_ARG, "ia[0] must be 0");
     uint32_t nnz = ia[n];
     // The checks read the whole matrix (93 MB at 60x220x85), so they run as a
-    // branch-free pass split over host threads; only when it finds a fault does
-    // the serial pass below locate the first one for the message.
-    if (!matrix_ok(n, ia, ja, a)) {
-        for (uint32_t i = 0; i < n; i++) {
-            if (ia[i + 1] <= ia[i])
-                MLP_THROW(ERR_ARG, "every row needs at least its diagonal (row " + std::to_string(i) + ")");
-            if (ja[ia[i]] != i) MLP_THROW(ERR_ARG, "diagonal must come first in row " + std::to_string(i));
-        }
-        for (uint32_t k = 0; k < nnz; k++) {
-            if (ja[k] >= n) MLP_THROW(ERR_ARG, "column index out of range");
-            if (!std::isfinite(a[k]))
-                MLP_THROW(ERR_NOT_FINITE, "non-finite matrix value at entry " + std::to_string(k));
-        }
-    }
+    // branch-free pass split over host threads, while the upload runs; only
+    // when it finds a fault does the serial pass below locate the first one for
+    // the message (a fault is reported before any error of the upload).
+    bool valid = true;
+    std::thread check([&] { valid = matrix_ok(n, ia, ja, a); });
     auto* M = new mlp_matrix();
+    std::exception_ptr up;
     try {
         M->s = new_stream();
         M->A.alloc(n, n, nnz);
@@ -147,9 +140,25 @@ int mlp_matrix_create(uint32_t n, const uint32_t* ia, const uint32_t* ja, const 
         csr_tile_stats(M->A, M->s);
         CK(cudaStreamSynchronize(M->s));
     } catch (...) {
-        delete M;
-        throw;
+        up = std::current_exception();
     }
+    check.join();
+    if (!valid || up) delete M;
+    if (!valid) {
+        for (uint32_t i = 0; i < n; i++) {
+            if (ia[i + 1] <= ia[i])
+                MLP_THROW(ERR_ARG, "every row needs at least its diagonal (row " + std::to_string(i) + ")");
+            if (ia[i + 1] > nnz) MLP_THROW(ERR_ARG, "row pointer beyond ia[n] (row " + std::to_string(i) + ")");
+            if (ja[ia[i]] != i) MLP_THROW(ERR_ARG, "diagonal must come first in row " + std::to_string(i));
+        }
+        for (uint32_t k = 0; k < nnz; k++) {
+            if (ja[k] >= n) MLP_THROW(ERR_ARG, "column index out of range");
+            if (!std::isfinite(a[k]))
+                MLP_THROW(ERR_NOT_FINITE, "non-finite matrix value at entry " + std::to_string(k));
+        }
+        MLP_THROW(ERR_INTERNAL, "matrix checks disagree");
+    }
+    if (up) std::rethrow_exception(up);
     *out = M;
     API_END
 }
