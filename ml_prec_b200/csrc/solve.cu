@@ -1775,8 +1775,89 @@ static void make_f32(const DBuf<double>& src, DBuf<float>& dst, size_t n, cudaSt
 }
 static void make_f32(DCSR& m, cudaStream_t s) { make_f32(m.a, m.a32, m.nnz, s); }
 
+// ---- instantiated graphs of released handles ------------------------------
+// Instantiating a graph of a few hundred nodes costs about a millisecond. A
+// handle built for the same problem shape records the same launches with
+// other pointers, so when a handle is released its instantiated graphs are
+// kept (by a key naming the device, the size and every launch of the plan),
+// and the next handle of that shape updates one in place
+// (cudaGraphExecUpdate) instead of instantiating its own; an update the
+// runtime refuses falls back to instantiation.
+namespace {
+struct ExecCache {
+    std::mutex mu;
+    std::multimap<std::string, cudaGraphExec_t> spare;
+    uint64_t updates = 0, instantiations = 0;
+};
+ExecCache& exec_cache() {
+    static ExecCache* c = new ExecCache();  // never destroyed: handles may be released during exit
+    return *c;
+}
+constexpr size_t EXEC_SPARE_MAX = 16;
+}  // namespace
+
+std::string plan_key(const Prec& P, const std::string& what) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::string k = what + "|" + std::to_string(dev) + "|" + std::to_string(P.plan.launches);
+    for (const std::string& nm : P.plan.names) k += "|" + nm;
+    return k;
+}
+
+void exec_release(const std::string& key, cudaGraphExec_t ex) {
+    if (!ex) return;
+    ExecCache& c = exec_cache();
+    {
+        std::lock_guard<std::mutex> lk(c.mu);
+        if (!key.empty() && c.spare.size() < EXEC_SPARE_MAX && c.spare.count(key) < 2) {
+            c.spare.emplace(key, ex);
+            return;
+        }
+    }
+    cudaGraphExecDestroy(ex);
+}
+
+// An executable graph for g (which is destroyed): a released one of the same
+// key updated to g, else a new instantiation.
+cudaGraphExec_t exec_for(const std::string& key, cudaGraph_t g) {
+    ExecCache& c = exec_cache();
+    cudaGraphExec_t ex = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(c.mu);
+        auto it = c.spare.find(key);
+        if (it != c.spare.end()) {
+            ex = it->second;
+            c.spare.erase(it);
+        }
+    }
+    if (ex) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(ex, g, &info) == cudaSuccess) {
+            cudaGraphDestroy(g);
+            std::lock_guard<std::mutex> lk(c.mu);
+            c.updates++;
+            return ex;
+        }
+        cudaGetLastError();
+        cudaGraphExecDestroy(ex);
+    }
+    cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) MLP_THROW(ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+    std::lock_guard<std::mutex> lk(c.mu);
+    c.instantiations++;
+    return ex;
+}
+
+void exec_cache_counts(uint64_t& updates, uint64_t& instantiations) {
+    ExecCache& c = exec_cache();
+    std::lock_guard<std::mutex> lk(c.mu);
+    updates = c.updates;
+    instantiations = c.instantiations;
+}
+
 Prec::~Prec() {
-    if (graph) cudaGraphExecDestroy(graph);
+    exec_release(graph_key, graph);
 }
 Prec::Prec() = default;
 
@@ -1937,9 +2018,8 @@ std::unique_ptr<Prec> make_prec(const DCSR& A, const BuildCfg& cfg, bool fp32, c
     cudaError_t le = cudaGetLastError();
     CK(cudaStreamEndCapture(s, &g));
     if (le != cudaSuccess) { cudaGraphDestroy(g); MLP_THROW(ERR_CUDA, cudaGetErrorString(le)); }
-    cudaError_t ie = cudaGraphInstantiate(&P->graph, g, 0);
-    cudaGraphDestroy(g);
-    if (ie != cudaSuccess) MLP_THROW(ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+    P->graph_key = plan_key(*P, "apply");
+    P->graph = exec_for(P->graph_key, g);
     trace("graph");
     trace_flush();
     return P;
@@ -2328,15 +2408,16 @@ __global__ void k_pcg_start(PcgDev* d, const PcgParams* prm, cudaGraphConditiona
 }
 
 PcgWork::~PcgWork() {
-    for (auto& g : full)
-        if (g) cudaGraphExecDestroy(g);
+    for (int k = 0; k < 6; k++) exec_release(full_key[k], full[k]);
 }
 
 static void pcg_work_alloc(Prec& P, uint32_t n) {
     PcgWork& W = P.pcg;
     if (W.n == n) return;
-    for (auto& g : W.full)
-        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    for (int k = 0; k < 6; k++) {
+        exec_release(W.full_key[k], W.full[k]);
+        W.full[k] = nullptr;
+    }
     W.n = n;
     W.xf.alloc(n); W.bf.alloc(n); W.p.alloc(n); W.Ap.alloc(n); W.rprev.alloc(n);
     W.bnat.alloc(n); W.xnat.alloc(n);
@@ -2462,7 +2543,8 @@ static cudaGraphExec_t instantiate(cudaGraph_t g) {
 }
 
 static cudaGraphExec_t full_graph(Prec& P, uint32_t n, bool flexible, int x0m, cudaStream_t s) {
-    cudaGraphExec_t& ex = P.pcg.full[(flexible ? 1 : 0) * 3 + x0m];
+    const int k = (flexible ? 1 : 0) * 3 + x0m;
+    cudaGraphExec_t& ex = P.pcg.full[k];
     if (ex) return ex;
     cudaGraph_t g;
     CK(cudaGraphCreate(&g, 0));
@@ -2472,7 +2554,8 @@ static cudaGraphExec_t full_graph(Prec& P, uint32_t n, bool flexible, int x0m, c
         cudaGraphDestroy(g);
         throw;
     }
-    ex = instantiate(g);
+    P.pcg.full_key[k] = plan_key(P, "pcg|" + std::to_string(n) + "|" + std::to_string(k));
+    ex = exec_for(P.pcg.full_key[k], g);
     return ex;
 }
 

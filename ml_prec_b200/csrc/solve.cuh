@@ -44,6 +44,12 @@ struct OpProfile {
 };
 struct Prec;
 std::vector<OpProfile> profile_apply(Prec& P, uint32_t reps, cudaStream_t s);
+// Executable graphs of released handles, kept by shape and updated in place
+// for the next handle of that shape (instantiation costs about a millisecond).
+std::string plan_key(const Prec& P, const std::string& what);
+void exec_release(const std::string& key, cudaGraphExec_t ex);
+cudaGraphExec_t exec_for(const std::string& key, cudaGraph_t g);
+void exec_cache_counts(uint64_t& updates, uint64_t& instantiations);
 // Replays the apply graph reps (>= 2) times back to back with the in-graph
 // timeline on; per launch of the plan its mean time inside the graph (us).
 std::vector<double> timeline_apply(Prec& P, uint32_t reps, cudaStream_t s);
@@ -66,6 +72,7 @@ struct PcgWork {
     DBuf<PcgDev> d;
     DBuf<PcgParams> prm;
     cudaGraphExec_t full[6] = {};  // [flexible * 3 + x0 mode]
+    std::string full_key[6];       // their shape keys (released for reuse, see exec_for)
     ~PcgWork();
 };
 
@@ -83,6 +90,7 @@ struct Prec {
     double* fout = nullptr;
     DBuf<double> fin_buf, fout_buf;
     cudaGraphExec_t graph = nullptr;
+    std::string graph_key;  // its shape key (released for reuse)
     cudaStream_t stream = nullptr;
     uint64_t bytes_per_apply = 0;  // algorithmic bytes of one apply
     // persistent regions of the plan: step descriptors and the grid barrier
