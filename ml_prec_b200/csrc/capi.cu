@@ -479,8 +479,7 @@ int mlp_pcg(const mlp_matrix* A, const double* b_host, mlp_prec* P, double* x_ho
     DBuf<double> b(n), x(n);
     h2d_large(b.p, b_host, (size_t)n * 8, s);
     int rc = pcg_common(A, b.p, P, x.p, eps, maxit, flexible, stats, s);
-    CK(cudaMemcpyAsync(x_host, x.p, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
+    d2h_large(x_host, x.p, (size_t)n * 8, s);
     return rc;
     API_END
 }

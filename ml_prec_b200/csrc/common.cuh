@@ -68,6 +68,10 @@ const char* last_error();
 // Host-to-device copy of a large pageable array through pinned staging buffers
 // (parallel host copies overlapped with the DMA); small copies go directly.
 void h2d_large(void* dst, const void* src, size_t bytes, cudaStream_t s);
+// The reverse: device to pageable host memory through the same staging
+// buffers (the DMA fills one while host threads drain the other); returns
+// when the data are in dst.
+void d2h_large(void* dst, const void* src, size_t bytes, cudaStream_t s);
 
 void* pool_alloc(size_t bytes);
 void pool_release(void* p);

@@ -162,19 +162,24 @@ static void parallel_memcpy(void* dst, const void* src, size_t bytes) {
     for (auto& x : th) x.join();
 }
 
+// The staging buffers' events mark the last copy that used each buffer
+// (either direction); callers hold g_stage_mu.
+static void stage_init(cudaStream_t s) {
+    if (g_stage[0]) return;
+    for (int k = 0; k < 2; k++) {
+        CK(cudaMallocHost(&g_stage[k], STAGE_BYTES));
+        CK(cudaEventCreateWithFlags(&g_stage_ev[k], cudaEventDisableTiming));
+        CK(cudaEventRecord(g_stage_ev[k], s));
+    }
+}
+
 void h2d_large(void* dst, const void* src, size_t bytes, cudaStream_t s) {
     if (bytes < ((size_t)8 << 20)) {
         if (bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
         return;
     }
     std::lock_guard<std::mutex> lk(g_stage_mu);
-    if (!g_stage[0]) {
-        for (int k = 0; k < 2; k++) {
-            CK(cudaMallocHost(&g_stage[k], STAGE_BYTES));
-            CK(cudaEventCreateWithFlags(&g_stage_ev[k], cudaEventDisableTiming));
-            CK(cudaEventRecord(g_stage_ev[k], s));
-        }
-    }
+    stage_init(s);
     size_t off = 0;
     for (int k = 0; off < bytes; k ^= 1) {
         size_t len = std::min(STAGE_BYTES, bytes - off);
@@ -183,6 +188,33 @@ void h2d_large(void* dst, const void* src, size_t bytes, cudaStream_t s) {
         CK(cudaMemcpyAsync((char*)dst + off, g_stage[k], len, cudaMemcpyHostToDevice, s));
         CK(cudaEventRecord(g_stage_ev[k], s));
         off += len;
+    }
+}
+
+void d2h_large(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    if (bytes < ((size_t)8 << 20)) {
+        if (bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        return;
+    }
+    std::lock_guard<std::mutex> lk(g_stage_mu);
+    stage_init(s);
+    const size_t nch = (bytes + STAGE_BYTES - 1) / STAGE_BYTES;
+    auto issue = [&](size_t c) {
+        const int k = (int)(c & 1);
+        const size_t off = c * STAGE_BYTES, len = std::min(STAGE_BYTES, bytes - off);
+        CK(cudaEventSynchronize(g_stage_ev[k]));  // the buffer's previous copy is done
+        CK(cudaMemcpyAsync(g_stage[k], (const char*)src + off, len, cudaMemcpyDeviceToHost, s));
+        CK(cudaEventRecord(g_stage_ev[k], s));
+    };
+    issue(0);
+    if (nch > 1) issue(1);
+    for (size_t c = 0; c < nch; c++) {
+        const int k = (int)(c & 1);
+        const size_t off = c * STAGE_BYTES, len = std::min(STAGE_BYTES, bytes - off);
+        CK(cudaEventSynchronize(g_stage_ev[k]));  // the chunk has arrived
+        parallel_memcpy((char*)dst + off, g_stage[k], len);
+        if (c + 2 < nch) issue(c + 2);
     }
 }
 
