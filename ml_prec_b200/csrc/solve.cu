@@ -3036,6 +3036,7 @@ std::unique_ptr<Ensemble> make_ensemble(const std::vector<Prec*>& members, bool 
     E->members = members;
     E->flexible = flexible;
     E->x0m = x0m;
+    PdlOff no_pdl;  // the members' branches run concurrently
     cudaGraph_t g;
     CK(cudaGraphCreate(&g, 0));
     try {
@@ -3080,6 +3081,7 @@ std::unique_ptr<Ensemble> make_ensemble_gradient(const std::vector<Prec*>& membe
     E->x0m = X0_ZERO;
     E->gradient = true;
     E->fwd.resize(members.size());
+    PdlOff no_pdl;  // the members' branches run concurrently
     cudaGraph_t g;
     CK(cudaGraphCreate(&g, 0));
     try {

@@ -24,13 +24,17 @@ uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
 void set_last_error(const std::string& s) { g_last_error = s; }
 const char* last_error() { return g_last_error.c_str(); }
 
+static thread_local int t_pdl_off = 0;
+PdlOff::PdlOff() { t_pdl_off++; }
+PdlOff::~PdlOff() { t_pdl_off--; }
+
 bool pdl_enabled() {
     static int on = -1;
     if (on < 0) {
         const char* e = getenv("MLP_PDL");
         on = (e && e[0] == '0') ? 0 : 1;
     }
-    return on == 1;
+    return on == 1 && t_pdl_off == 0;
 }
 
 static bool trace_on() {
