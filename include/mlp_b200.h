@@ -266,10 +266,9 @@ int mlp_ensemble_gradient_create(uint32_t count, const mlp_matrix* const* A, mlp
  * been created beforehand (those calls allocate). Every call looks up the
  * array's address on the current device; the first call on a device (unless
  * an earlier call into the library on that device did it) loads the library's
- * device code there, which is what places the array, so make that first call
- * before any stream capture. All calls share the one array, which keeps the
- * last call's contents: calls that overlap on the GPU (other threads, other
- * streams) race and must be serialised by the caller. The call waits on the
+ * device code there, which is what places the array. All calls share the one
+ * array, which keeps the last call's contents: calls that overlap on the GPU
+ * (other threads, other streams) race and must be serialised by the caller. The call waits on the
  * host for the device after every iteration. t_solve_ms is host wall time. */
 int mlp_pcg_device_noalloc(const mlp_matrix* A, const double* b_dev, mlp_prec* P, double* x_dev, double eps,
                            uint32_t maxit, int32_t flexible, mlp_stats* stats, void* stream);
