@@ -626,33 +626,24 @@ struct RowPre {
 // eliminated and coarse rows) and out = dval * src on the diagonal rows
 // [R, N). The first nb1 blocks take the P1 rows with LPR lanes per row, the
 // rest one diagonal row per thread.
-// RPT: row slots per thread. A grid larger than what is resident at once runs
-// in waves, and only the first wave's CTAs load their rows before the
-// dependent-launch wait; with RPT slots a thread loads all of its rows first
-// (slot k is global thread gid + k * threads), so that the launch fits one wave.
-template <class T, int LPR, int RPT = 1>
+template <class T, int LPR>
 __global__ void __launch_bounds__(512) k_phase1(uint32_t R, uint32_t N, uint32_t nb1, const uint32_t* __restrict__ ia,
                                                 const uint32_t* __restrict__ ja, const T* __restrict__ a,
                                                 const T* __restrict__ dval, const T* __restrict__ src,
                                                 T* __restrict__ w, T* __restrict__ out) {
     if (blockIdx.x < nb1) {
-        const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x, nth = nb1 * blockDim.x;
-        RowPre<T, LPR> rp[RPT];
-#pragma unroll
-        for (int k = 0; k < RPT; k++) {
-            uint32_t g = gid + k * nth, row = g / LPR;
-            rp[k].load(row < R, row, g % LPR, ia, ja, a);
-        }
+        uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+        uint32_t row = gid / LPR;
+        int lane = gid % LPR;
+        bool active = row < R;
+        RowPre<T, LPR> rp;
+        rp.load(active, row, lane, ia, ja, a);
         pdl_wait();
         pdl_trigger();
+        T s = rp.sum([&](uint32_t c) { return src[c]; }, ja, a);
 #pragma unroll
-        for (int k = 0; k < RPT; k++) {
-            uint32_t g = gid + k * nth, row = g / LPR;
-            T s = rp[k].sum([&](uint32_t c) { return src[c]; }, ja, a);
-#pragma unroll
-            for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (row < R && g % LPR == 0) w[row] = s;
-        }
+        for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (active && lane == 0) w[row] = s;
     } else {
         uint32_t q = R + (blockIdx.x - nb1) * blockDim.x + threadIdx.x;
         T d = q < N ? dval[q - R] : T(0);
@@ -665,27 +656,22 @@ __global__ void __launch_bounds__(512) k_phase1(uint32_t R, uint32_t N, uint32_t
 // Phase 2: out_q = sum_j G_qj y_j on the eliminated rows q < M, where
 // y_j = w_j for eliminated columns (j < M) and out_j (the coarse solution the
 // recursion wrote) for coarse columns.
-template <class T, int LPR, int RPT = 1>
+template <class T, int LPR>
 __global__ void __launch_bounds__(512) k_phase2(uint32_t M, const uint32_t* __restrict__ ia,
                                                 const uint32_t* __restrict__ ja, const T* __restrict__ a,
                                                 const T* __restrict__ w, T* out) {
-    const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
-    RowPre<T, LPR> rp[RPT];
-#pragma unroll
-    for (int k = 0; k < RPT; k++) {
-        uint32_t g = gid + k * nth, row = g / LPR;
-        rp[k].load(row < M, row, g % LPR, ia, ja, a);
-    }
+    uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t row = gid / LPR;
+    int lane = gid % LPR;
+    bool active = row < M;
+    RowPre<T, LPR> rp;
+    rp.load(active, row, lane, ia, ja, a);
     pdl_wait();
     pdl_trigger();
+    T s = rp.sum([&](uint32_t c) { return c < M ? w[c] : out[c]; }, ja, a);
 #pragma unroll
-    for (int k = 0; k < RPT; k++) {
-        uint32_t g = gid + k * nth, row = g / LPR;
-        T s = rp[k].sum([&](uint32_t c) { return c < M ? w[c] : out[c]; }, ja, a);
-#pragma unroll
-        for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (row < M && g % LPR == 0) out[row] = s;
-    }
+    for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (active && lane == 0) out[row] = s;
 }
 
 // Phase 2 with the coarse solve folded in (launch plan; the level below is
@@ -782,30 +768,25 @@ __global__ void k_fold_build(uint32_t nf, const uint32_t* __restrict__ rows, uin
 
 // Correction step of a level sweep: x += u0 and, when more sweeps follow,
 // r -= A u0 (the residual f - A x updated in place of recomputing it).
-template <class T, int LPR, int RPT = 1>
+template <class T, int LPR>
 __global__ void __launch_bounds__(512) k_update(uint32_t n, const uint32_t* __restrict__ ia,
                                                 const uint32_t* __restrict__ ja, const T* __restrict__ a,
                                                 const T* __restrict__ u0, T* __restrict__ x, T* __restrict__ r,
                                                 int do_r) {
-    const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
-    RowPre<T, LPR> rp[RPT];
-#pragma unroll
-    for (int k = 0; k < RPT; k++) {
-        uint32_t g = gid + k * nth, row = g / LPR;
-        rp[k].load(row < n && do_r, row, g % LPR, ia, ja, a);
-    }
+    uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t row = gid / LPR;
+    int lane = gid % LPR;
+    bool active = row < n;
+    RowPre<T, LPR> rp;
+    rp.load(active && do_r, row, lane, ia, ja, a);
     pdl_wait();
     pdl_trigger();
+    T s = rp.sum([&](uint32_t c) { return u0[c]; }, ja, a);
 #pragma unroll
-    for (int k = 0; k < RPT; k++) {
-        uint32_t g = gid + k * nth, row = g / LPR;
-        T s = rp[k].sum([&](uint32_t c) { return u0[c]; }, ja, a);
-#pragma unroll
-        for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (row < n && g % LPR == 0) {
-            x[row] += u0[row];
-            if (do_r) r[row] -= s;
-        }
+    for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (active && lane == 0) {
+        x[row] += u0[row];
+        if (do_r) r[row] -= s;
     }
 }
 
@@ -1043,62 +1024,6 @@ static LaunchShape tune_shape(int kind, int tsize, uint32_t rows, uint32_t nnz, 
         case 8: launch_k(KERNEL<T, 8>, __VA_ARGS__); break;               \
         case 16: launch_k(KERNEL<T, 16>, __VA_ARGS__); break;             \
         default: launch_k(KERNEL<T, 32>, __VA_ARGS__); break;             \
-    }
-
-// Row slots per thread (RPT of k_phase1 / k_phase2 / k_update): 2 when the
-// one-slot grid for `threads` lanes needs more than one wave of resident CTAs
-// and the two-slot grid needs fewer waves (the prefetched entries take
-// registers, so two slots halve the CTAs but also the resident ones); else 1.
-// `fixed` (the autotuner's shapes) keeps 1.
-static int rows_rpt(const void* k1, const void* k2, size_t threads, unsigned block, bool fixed) {
-    if (fixed || !threads) return 1;
-    static std::mutex mu;
-    static std::map<std::pair<const void*, unsigned>, int> occ;
-    const void* ks[2] = {k1, k2};
-    const int rs[2] = {1, 2};
-    double waves[2] = {0, 0};
-    for (int i = 0; i < 2; i++) {
-        int per = 0;
-        {
-            std::lock_guard<std::mutex> lk(mu);
-            auto key = std::make_pair(ks[i], block);
-            auto it = occ.find(key);
-            if (it == occ.end()) {
-                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, ks[i], (int)block, 0));
-                occ[key] = per;
-            } else {
-                per = it->second;
-            }
-        }
-        size_t blocks = (threads + (size_t)block * rs[i] - 1) / ((size_t)block * rs[i]);
-        waves[i] = per > 0 ? std::ceil((double)blocks / ((double)per * num_sms())) : 1e30;
-    }
-    return waves[0] > 1 && waves[1] < waves[0] ? 2 : 1;
-}
-
-#define RPT_PTRS(lpr, KERNEL, p1, p2)                                                              \
-    switch (lpr) {                                                                                     \
-        case 1: p1 = (const void*)KERNEL<T, 1, 1>; p2 = (const void*)KERNEL<T, 1, 2>; break;    \
-        case 2: p1 = (const void*)KERNEL<T, 2, 1>; p2 = (const void*)KERNEL<T, 2, 2>; break;    \
-        case 4: p1 = (const void*)KERNEL<T, 4, 1>; p2 = (const void*)KERNEL<T, 4, 2>; break;    \
-        case 8: p1 = (const void*)KERNEL<T, 8, 1>; p2 = (const void*)KERNEL<T, 8, 2>; break;    \
-        case 16: p1 = (const void*)KERNEL<T, 16, 1>; p2 = (const void*)KERNEL<T, 16, 2>; break; \
-        default: p1 = (const void*)KERNEL<T, 32, 1>; p2 = (const void*)KERNEL<T, 32, 2>; break; \
-    }
-
-#define RPT_LAUNCH_L(L, rpt, KERNEL, ...)                      \
-    switch (rpt) {                                             \
-        case 1: launch_k(KERNEL<T, L, 1>, __VA_ARGS__); break; \
-        default: launch_k(KERNEL<T, L, 2>, __VA_ARGS__); break; \
-    }
-#define LPR_RPT_SWITCH(lpr, rpt, KERNEL, ...)                      \
-    switch (lpr) {                                                 \
-        case 1: RPT_LAUNCH_L(1, rpt, KERNEL, __VA_ARGS__); break;  \
-        case 2: RPT_LAUNCH_L(2, rpt, KERNEL, __VA_ARGS__); break;  \
-        case 4: RPT_LAUNCH_L(4, rpt, KERNEL, __VA_ARGS__); break;  \
-        case 8: RPT_LAUNCH_L(8, rpt, KERNEL, __VA_ARGS__); break;  \
-        case 16: RPT_LAUNCH_L(16, rpt, KERNEL, __VA_ARGS__); break; \
-        default: RPT_LAUNCH_L(32, rpt, KERNEL, __VA_ARGS__); break; \
     }
 
 // ---------------------------------------------------------------------------
@@ -1350,19 +1275,15 @@ struct Builder {
         bool st = staged_ok(L, L.P1, R);
         uint32_t cap = st ? pipe_cap<T>(L.P1.tile_max) : 0;
         size_t smem = st ? pipe_smem_bytes<T, false>(L.P1.tile_max) : 0;
-        const bool tuned = autotune;  // the tuner's shapes keep one row slot per thread
         auto launch = [=](LaunchShape c, cudaStream_t s) {
             if (c.lpr == 0) {
                 launch_k(k_phase1_staged<T>, pipe_grid(k_phase1_staged<T>, R, smem), ST_ROWS, smem, s, R, N, ia, ja,
                          a, dv, src, w, out, cap);
                 return;
             }
-            const void *k1, *k2;
-            RPT_PTRS(c.lpr, k_phase1, k1, k2);
-            int rpt = rows_rpt(k1, k2, (size_t)R * c.lpr, c.block, tuned);
-            uint32_t nb1 = R ? grid_for((size_t)R * c.lpr, c.block * rpt) : 0;
+            uint32_t nb1 = R ? grid_for((size_t)R * c.lpr, c.block) : 0;
             uint32_t nb2 = N > R ? grid_for(N - R, c.block) : 0;
-            LPR_RPT_SWITCH(c.lpr, rpt, k_phase1, nb1 + nb2, c.block, 0, s, R, N, nb1, ia, ja, a, dv, src, w, out);
+            LPR_SWITCH_B(c.lpr, k_phase1, nb1 + nb2, c.block, 0, s, R, N, nb1, ia, ja, a, dv, src, w, out);
         };
         LaunchShape c{pick_lpr(R, L.P1.nnz), 256};
         if (autotune) c = tune_shape(1, sizeof(T), R, L.P1.nnz, tune_stream(), launch, st);
@@ -1379,18 +1300,13 @@ struct Builder {
         bool st = staged_ok(L, L.G, M);
         uint32_t cap = st ? pipe_cap<T>(L.G.tile_max) : 0;
         size_t smem = st ? pipe_smem_bytes<T, false>(L.G.tile_max) : 0;
-        const bool tuned = autotune;  // the tuner's shapes keep one row slot per thread
         auto launch = [=](LaunchShape c, cudaStream_t s) {
             if (c.lpr == 0) {
                 launch_k(k_phase2_staged<T>, pipe_grid(k_phase2_staged<T>, M, smem), ST_ROWS, smem, s, M, ia, ja, a, w,
                          out, cap);
                 return;
             }
-            const void *k1, *k2;
-            RPT_PTRS(c.lpr, k_phase2, k1, k2);
-            int rpt = rows_rpt(k1, k2, (size_t)M * c.lpr, c.block, tuned);
-            LPR_RPT_SWITCH(c.lpr, rpt, k_phase2, grid_for((size_t)M * c.lpr, c.block * rpt), c.block, 0, s, M, ia, ja,
-                           a, w, out);
+            LPR_SWITCH_B(c.lpr, k_phase2, grid_for((size_t)M * c.lpr, c.block), c.block, 0, s, M, ia, ja, a, w, out);
         };
         LaunchShape c{pick_lpr(M, L.G.nnz), 256};
         if (autotune) c = tune_shape(2, sizeof(T), M, L.G.nnz, tune_stream(), launch, st);
@@ -1513,18 +1429,14 @@ struct Builder {
         bool st = do_r && staged_ok(L, L.Af, N);
         uint32_t cap = st ? pipe_cap<T>(L.Af.tile_max) : 0;
         size_t smem = st ? pipe_smem_bytes<T, false>(L.Af.tile_max) : 0;
-        const bool tuned = autotune;  // the tuner's shapes keep one row slot per thread
         auto launch = [=](LaunchShape c, cudaStream_t s) {
             if (c.lpr == 0) {
                 launch_k(k_update_staged<T>, pipe_grid(k_update_staged<T>, N, smem), ST_ROWS, smem, s, N, ia, ja, a, u0,
                          x, r, cap);
                 return;
             }
-            const void *k1, *k2;
-            RPT_PTRS(c.lpr, k_update, k1, k2);
-            int rpt = rows_rpt(k1, k2, (size_t)N * c.lpr, c.block, tuned);
-            LPR_RPT_SWITCH(c.lpr, rpt, k_update, grid_for((size_t)N * c.lpr, c.block * rpt), c.block, 0, s, N, ia, ja,
-                           a, u0, x, r, dr);
+            LPR_SWITCH_B(c.lpr, k_update, grid_for((size_t)N * c.lpr, c.block), c.block, 0, s, N, ia, ja, a, u0, x, r,
+                         dr);
         };
         LaunchShape c{do_r ? pick_lpr(N, L.Af.nnz) : 1, 256};
         // the tuning runs x += u0 on scratch: every buffer of the plan is
