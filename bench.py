@@ -513,7 +513,7 @@ def reference_cpu(steps, warmup, timeout=1800, c=C_REACT):
                 niter=r["niter"], steps=len(per))
 
 
-def reference_ensemble(count, timeout=120):
+def reference_ensemble(count, timeout=30):
     """min(count, cores) concurrent single-threaded reference processes, one
     ensemble realization each (the ensemble form's meshes and fields, matrices
     written in the reference's BINARY CSR format and loaded by its own reader):

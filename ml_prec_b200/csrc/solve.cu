@@ -2129,6 +2129,11 @@ struct PcgDev {
 };
 static int take_x0_mode();
 
+// All four pointers 16-byte aligned (pairs of doubles move in one access).
+__device__ __forceinline__ bool aligned16(const void* a, const void* b, const void* c, const void* e) {
+    return (((uintptr_t)a | (uintptr_t)b | (uintptr_t)c | (uintptr_t)e) & 15u) == 0;
+}
+
 __device__ __forceinline__ double block_sum(double v) {
     __shared__ double sh[32];
     int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -2263,11 +2268,44 @@ __global__ void __launch_bounds__(RB) k_pcg_update(uint32_t n, double* __restric
     pdl_trigger();
     double alpha = d->alpha;
     double part = 0;
-    for (uint32_t i = blockIdx.x * RB + threadIdx.x; i < n; i += gridDim.x * RB) {
-        x[i] += alpha * p[i];
-        double ri = r[i] - alpha * Ap[i];
-        r[i] = ri;
-        part += ri * ri;
+    const uint32_t t0 = blockIdx.x * RB + threadIdx.x, stride = gridDim.x * RB;
+    if (aligned16(x, r, p, Ap)) {
+        // pairs of elements in 16-byte accesses, two pairs in flight per thread
+        double2* x2 = reinterpret_cast<double2*>(x);
+        double2* r2 = reinterpret_cast<double2*>(r);
+        const double2* p2 = reinterpret_cast<const double2*>(p);
+        const double2* a2 = reinterpret_cast<const double2*>(Ap);
+        const uint32_t n2 = n >> 1;
+        for (uint32_t i = t0; i < n2; i += 2 * stride) {
+            const uint32_t j = i + stride;
+            const bool two = j < n2;
+            double2 xv = x2[i], pv = p2[i], rv = r2[i], av = a2[i];
+            double2 xw = two ? x2[j] : xv, pw = two ? p2[j] : pv, rw = two ? r2[j] : rv, aw = two ? a2[j] : av;
+            xv.x += alpha * pv.x; xv.y += alpha * pv.y;
+            rv.x = rv.x - alpha * av.x; rv.y = rv.y - alpha * av.y;
+            x2[i] = xv; r2[i] = rv;
+            part += rv.x * rv.x; part += rv.y * rv.y;
+            if (two) {
+                xw.x += alpha * pw.x; xw.y += alpha * pw.y;
+                rw.x = rw.x - alpha * aw.x; rw.y = rw.y - alpha * aw.y;
+                x2[j] = xw; r2[j] = rw;
+                part += rw.x * rw.x; part += rw.y * rw.y;
+            }
+        }
+        if ((n & 1) && t0 == 0) {
+            const uint32_t i = n - 1;
+            x[i] += alpha * p[i];
+            double ri = r[i] - alpha * Ap[i];
+            r[i] = ri;
+            part += ri * ri;
+        }
+    } else {
+        for (uint32_t i = t0; i < n; i += stride) {
+            x[i] += alpha * p[i];
+            double ri = r[i] - alpha * Ap[i];
+            r[i] = ri;
+            part += ri * ri;
+        }
     }
     part = block_sum(part);
     double tot;
@@ -2292,9 +2330,29 @@ __global__ void __launch_bounds__(RB) k_pcg_dot_rz(uint32_t n, const double* __r
     pdl_wait();
     pdl_trigger();
     double part = 0, part2 = 0;
-    for (uint32_t i = blockIdx.x * RB + threadIdx.x; i < n; i += gridDim.x * RB) {
-        part += r[i] * z[i];
-        if (flexible) part2 += rprev[i] * z[i];
+    const uint32_t t0 = blockIdx.x * RB + threadIdx.x, stride = gridDim.x * RB;
+    if (aligned16(r, z, rprev, r)) {
+        const double2* r2 = reinterpret_cast<const double2*>(r);
+        const double2* z2 = reinterpret_cast<const double2*>(z);
+        const double2* q2 = reinterpret_cast<const double2*>(rprev);
+        const uint32_t n2 = n >> 1;
+        for (uint32_t i = t0; i < n2; i += stride) {
+            double2 rv = r2[i], zv = z2[i];
+            part += rv.x * zv.x; part += rv.y * zv.y;
+            if (flexible) {
+                double2 qv = q2[i];
+                part2 += qv.x * zv.x; part2 += qv.y * zv.y;
+            }
+        }
+        if ((n & 1) && t0 == 0) {
+            part += r[n - 1] * z[n - 1];
+            if (flexible) part2 += rprev[n - 1] * z[n - 1];
+        }
+    } else {
+        for (uint32_t i = t0; i < n; i += stride) {
+            part += r[i] * z[i];
+            if (flexible) part2 += rprev[i] * z[i];
+        }
     }
     part = block_sum(part);
     double tot;
@@ -2324,13 +2382,30 @@ __global__ void __launch_bounds__(RB) k_pcg_dot_rz(uint32_t n, const double* __r
     }
 }
 
-// p = beta p + z (dscal then daxpy, pcg.cc:71-72)
+// p = beta p + z (dscal then daxpy, pcg.cc:71-72), a pair of elements a
+// thread. p and z were written before the preceding launch (the (r, z)
+// reduction), so they are loaded before the wait; only beta comes from it.
 __global__ void k_pcg_p(uint32_t n, double* __restrict__ p, const double* __restrict__ z, const PcgDev* d) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t e = 2 * i;
+    double p0 = 0, p1 = 0, z0 = 0, z1 = 0;
+    const bool vec = aligned16(p, z, p, z);
+    if (vec && e + 1 < n) {
+        double2 pv = reinterpret_cast<const double2*>(p)[i], zv = reinterpret_cast<const double2*>(z)[i];
+        p0 = pv.x; p1 = pv.y; z0 = zv.x; z1 = zv.y;
+    } else {
+        if (e < n) { p0 = p[e]; z0 = z[e]; }
+        if (e + 1 < n) { p1 = p[e + 1]; z1 = z[e + 1]; }
+    }
     pdl_wait();
     pdl_trigger();
-    double beta = d->beta;
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) p[i] = beta * p[i] + z[i];
+    const double beta = d->beta;
+    if (vec && e + 1 < n) {
+        reinterpret_cast<double2*>(p)[i] = make_double2(beta * p0 + z0, beta * p1 + z1);
+    } else {
+        if (e < n) p[e] = beta * p0 + z0;
+        if (e + 1 < n) p[e + 1] = beta * p1 + z1;
+    }
 }
 
 __global__ void k_dot_simple(uint32_t n, const double* __restrict__ a, const double* __restrict__ b,
@@ -2454,7 +2529,7 @@ static void record_iteration(Prec& P, const DCSR& Af, uint32_t n, bool flexible,
     P.plan.run(s);
     launch_k(k_pcg_dot_rz, G, RB, 0, s, n, (const double*)r, (const double*)z, (const double*)W.rprev.p,
              W.partials.p, d, flexible ? 1 : 0);
-    launch_k(k_pcg_p, grid_for(n, 256), 256, 0, s, n, W.p.p, (const double*)z, (const PcgDev*)d);
+    launch_k(k_pcg_p, grid_for((n + 1) / 2, 256), 256, 0, s, n, W.p.p, (const double*)z, (const PcgDev*)d);
     if (flexible) k_copy_d<<<grid_for(n, 256), 256, 0, s>>>(n, r, W.rprev.p);
 }
 
@@ -2731,7 +2806,7 @@ int pcg_solve_cb(const DCSR& A, const double* b, const std::function<void(const 
         apply(r.p, z.p);
         napply++;
         k_pcg_dot_rz<<<G, RB, 0, s>>>(n, r.p, z.p, rprev.p, partials.p, d, flexible ? 1 : 0);
-        k_pcg_p<<<grid_for(n, 256), 256, 0, s>>>(n, p.p, z.p, d);
+        k_pcg_p<<<grid_for((n + 1) / 2, 256), 256, 0, s>>>(n, p.p, z.p, d);
         count_launches(2);
         if (flexible) CK(cudaMemcpyAsync(rprev.p, r.p, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
         CK_LAUNCH();
@@ -3174,7 +3249,7 @@ int pcg_solve_hostloop(const DCSR& A, const double* b, Prec& P, double* x, doubl
         prec_apply_frame(P, s);
         napply++;
         k_pcg_dot_rz<<<G, RB, 0, s>>>(n, r, z, rprev.p, partials.p, d, flexible ? 1 : 0);
-        k_pcg_p<<<grid_for(n, 256), 256, 0, s>>>(n, p.p, z, d);
+        k_pcg_p<<<grid_for((n + 1) / 2, 256), 256, 0, s>>>(n, p.p, z, d);
         count_launches(2);
         if (flexible) CK(cudaMemcpyAsync(rprev.p, r, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
         CK_LAUNCH();
@@ -3344,7 +3419,7 @@ int pcg_solve_noalloc(const DCSR& A, const double* b, Prec& P, double* x, double
         prec_apply_frame(P, s);
         napply++;
         k_pcg_dot_rz<<<G, RB, 0, s>>>(n, r, z, rprev, partials, d, flexible ? 1 : 0);
-        k_pcg_p<<<grid_for(n, 256), 256, 0, s>>>(n, p, z, d);
+        k_pcg_p<<<grid_for((n + 1) / 2, 256), 256, 0, s>>>(n, p, z, d);
         count_launches(2);
         if (flexible) CK(cudaMemcpyAsync(rprev, r, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
         CK_LAUNCH();
