@@ -375,6 +375,13 @@ def run_ours(args, ws, rank, local):
     g1.synchronize()
     out["apply_graph_ms"] = g0.elapsed_time(g1) / 20
     del fa, za
+    # the PCG's own launches inside the solve graph (mlp_pcg_timeline, one
+    # iteration near the end), with their algorithmic bytes
+    nnz = A.nnz()
+    pcg_bytes = {"pcg spmv_dot": 12 * nnz + 4 * (N + 1) + 16 * N, "pcg update": 48 * N, "pcg dot_rz": 16 * N,
+                 "pcg p": 24 * N}
+    out["pcg_timeline"] = [[nm, us_, pcg_bytes[nm]] for nm, us_ in Pp.pcg_timeline(A, b_d, x_d, EPS)
+                           if nm in pcg_bytes]
     progress("apply timeline")
     del Pp
 
@@ -644,6 +651,10 @@ def main():
                 for nm, c, ms_, by in rows[:12]]
 
     apply_groups = group_rows(prof)
+    pcg_kernels = [{"launch": nm, "us": round(us_, 2), "MB": round(by / 1e6, 2),
+                    "GBps": round(by / (us_ / 1e6) / 1e9, 1) if us_ > 0 else None,
+                    "frac": round(by / (us_ / 1e6) / 1e9 / hbm, 3) if us_ > 0 else None}
+                   for nm, us_, by in res["pcg_timeline"]]
     st64 = res["st64"]
     cpu = None
     if not args.no_cpu_baseline:
@@ -696,6 +707,7 @@ def main():
                                         "caches), not measured in this run" if top[0] in FOLD_DRAM_TRAFFIC
                                         else "no ncu capture of this launch group on this matrix"),
                      "apply_groups": apply_groups,
+                     "pcg_kernels": pcg_kernels,
                      "apply_ms_in_graph": res["apply_timeline_ms"],
                      "apply_graph_ms_events": res["apply_graph_ms"],
                      "apply_groups_launch_by_launch": group_rows(res["apply_profile"]),

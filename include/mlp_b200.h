@@ -178,6 +178,14 @@ int mlp_prec_profile(mlp_prec* P, uint32_t reps, uint32_t cap, uint32_t* nops, d
  * small-level kernels) return MLP_ERR_INTERNAL; no other apply may run on the
  * device meanwhile. */
 int mlp_prec_timeline(mlp_prec* P, uint32_t reps, uint32_t cap, uint32_t* nops, double* us);
+/* The same for a whole solve: one mlp_pcg_device-like solve (x0 from
+ * generate_x0, stream of the handle) with the stamps on, and per launch of one
+ * iteration near its end, in order (the SpMV with (Ap, p), the update, the
+ * application's launches, the (r, z) reduction, the p update), its name and
+ * time in us inside the graph. *n receives the number of launches; at most cap
+ * entries are written. */
+int mlp_pcg_timeline(const mlp_matrix* A, const double* b_dev, mlp_prec* P, double* x_dev, double eps,
+                     int32_t flexible, uint32_t cap, uint32_t* n, double* us, char* names, uint32_t name_len);
 
 /* ---- solver ----------------------------------------------------------------
  * PCGSolver(A, b, B, x, stats, eps, NORM_L2) (solvers.h:31-32, pcg.cc:8-102):

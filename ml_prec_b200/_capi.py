@@ -23,7 +23,7 @@ EXPORTS = [
     "mlp_matrix_download", "mlp_spmv", "mlp_spmv_host",
     "mlp_prec_create", "mlp_prec_destroy", "mlp_prec_apply", "mlp_prec_apply_host", "mlp_prec_nlevels",
     "mlp_prec_level_info", "mlp_prec_level_export", "mlp_prec_bytes_per_apply", "mlp_prec_profile",
-    "mlp_prec_timeline",
+    "mlp_prec_timeline", "mlp_pcg_timeline",
     "mlp_pcg", "mlp_pcg_device", "mlp_pcg_device_x0", "mlp_matrix_grad_logk", "mlp_pcg_device_noalloc",
     "mlp_launch_count", "mlp_generate_x0", "mlp_cheb_solve", "mlp_cheb_solve_device", "mlp_ensemble_create", "mlp_ensemble_solve", "mlp_ensemble_destroy",
     "mlp_ensemble_gradient_create",
@@ -104,6 +104,8 @@ def lib():
         L.mlp_prec_profile.argtypes = [vp, C.c_uint32, C.c_uint32, u32p, f64p, C.POINTER(C.c_uint64), C.c_char_p,
                                        C.c_uint32]
         L.mlp_prec_timeline.argtypes = [vp, C.c_uint32, C.c_uint32, u32p, f64p]
+        L.mlp_pcg_timeline.argtypes = [vp, vp, vp, vp, C.c_double, C.c_int32, C.c_uint32, u32p, f64p, C.c_char_p,
+                                       C.c_uint32]
         L.mlp_pcg.argtypes = [vp, f64p, vp, f64p, C.c_double, C.c_uint32, C.c_int32, C.POINTER(Stats)]
         L.mlp_pcg_device.argtypes = [vp, vp, vp, vp, C.c_double, C.c_uint32, C.c_int32, C.POINTER(Stats), vp]
         L.mlp_generate_x0.argtypes = [f64p, C.c_uint32]

@@ -280,6 +280,19 @@ class PrecBase:
             raise RuntimeError("timeline and profile disagree on the number of launches")
         return [(nm, float(us[k]), by) for k, (nm, _, by) in enumerate(prof)]
 
+    def pcg_timeline(self, A, b_dev, x_dev, eps=1e-8, flexible=False):
+        """One device solve (torch CUDA tensors b_dev, x_dev) with the in-graph
+        timeline on: per launch of one iteration near the end, (name, us)
+        (mlp_pcg_timeline)."""
+        cap = 4096
+        n = C.c_uint32()
+        us = np.zeros(cap)
+        names = C.create_string_buffer(64 * cap)
+        check(lib().mlp_pcg_timeline(A.h, C.c_void_p(b_dev.data_ptr()), self.h, C.c_void_p(x_dev.data_ptr()), eps,
+                                     int(flexible), cap, C.byref(n), ptr(us, f64p), names, 64))
+        raw = names.raw
+        return [(raw[64 * k:64 * (k + 1)].split(b"\0", 1)[0].decode(), float(us[k])) for k in range(min(n.value, cap))]
+
     @property
     def bytes_per_apply(self):
         b = C.c_uint64()

@@ -381,6 +381,23 @@ int mlp_prec_timeline(mlp_prec* P, uint32_t reps, uint32_t cap, uint32_t* nops, 
     API_END
 }
 
+int mlp_pcg_timeline(const mlp_matrix* A, const double* b_dev, mlp_prec* P, double* x_dev, double eps,
+                     int32_t flexible, uint32_t cap, uint32_t* n, double* us, char* names, uint32_t name_len) {
+    API_BEGIN
+    if (!A || !b_dev || !P || !x_dev || !n) MLP_THROW(ERR_ARG, "null pointer");
+    if (P->sym) MLP_THROW(ERR_ARG, "the timeline covers the device-resident PCG of a multilevel handle");
+    std::vector<std::pair<std::string, double>> t = timeline_pcg(A->A, b_dev, *P->P, x_dev, eps, flexible != 0, P->s);
+    *n = (uint32_t)t.size();
+    for (uint32_t k = 0; k < t.size() && k < cap; k++) {
+        if (us) us[k] = t[k].second;
+        if (names && name_len) {
+            strncpy(names + (size_t)k * name_len, t[k].first.c_str(), name_len - 1);
+            names[(size_t)k * name_len + name_len - 1] = 0;
+        }
+    }
+    API_END
+}
+
 int mlp_prec_nlevels(const mlp_prec* P, uint32_t* nl) {
     API_BEGIN
     if (!P || !nl) MLP_THROW(ERR_ARG, "null pointer");

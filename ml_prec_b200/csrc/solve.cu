@@ -2058,6 +2058,29 @@ std::vector<OpProfile> profile_apply(Prec& P, uint32_t reps, cudaStream_t s) {
     return out;
 }
 
+// Turns the stamping on with room for `cap` stamps (the stream is idle).
+static void tl_begin(DBuf<unsigned long long>& buf, size_t cap, cudaStream_t s) {
+    buf.alloc(cap);
+    unsigned long long* bp = buf.p;
+    unsigned c = (unsigned)cap, zero = 0;
+    CK(cudaStreamSynchronize(s));
+    CK(cudaMemcpyToSymbol(c_tl_cap, &c, sizeof c));
+    CK(cudaMemcpyToSymbol(g_tl_n, &zero, sizeof zero));
+    CK(cudaMemcpyToSymbol(c_tl_buf, &bp, sizeof bp));
+}
+// Waits for the stream, turns the stamping off and returns the stamps (at most
+// the capacity) and, in `got`, how many kernels stamped.
+static std::vector<unsigned long long> tl_end(const DBuf<unsigned long long>& buf, unsigned& got, cudaStream_t s) {
+    cudaError_t se = cudaStreamSynchronize(s);
+    unsigned long long* nul = nullptr;
+    CK(cudaMemcpyToSymbol(c_tl_buf, &nul, sizeof nul));
+    CK(cudaMemcpyFromSymbol(&got, g_tl_n, sizeof got));
+    CK(se);
+    std::vector<unsigned long long> t(std::min<size_t>(got, buf.n));
+    if (!t.empty()) CK(cudaMemcpy(t.data(), buf.p, t.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    return t;
+}
+
 std::vector<double> timeline_apply(Prec& P, uint32_t reps, cudaStream_t s) {
     const Plan& pl = P.plan;
     size_t n = pl.ops.size();
@@ -2066,28 +2089,17 @@ std::vector<double> timeline_apply(Prec& P, uint32_t reps, cudaStream_t s) {
     if (!P.graph) MLP_THROW(ERR_ARG, "the apply has no graph");
     if (reps < 2) reps = 2;
     size_t total = (size_t)reps * n;
-    DBuf<unsigned long long> buf(total + 64);
-    unsigned long long* bp = buf.p;
-    unsigned cap = (unsigned)(total + 64), zero = 0;
-    CK(cudaStreamSynchronize(s));
-    CK(cudaMemcpyToSymbol(c_tl_cap, &cap, sizeof cap));
-    CK(cudaMemcpyToSymbol(g_tl_n, &zero, sizeof zero));
-    CK(cudaMemcpyToSymbol(c_tl_buf, &bp, sizeof bp));
+    DBuf<unsigned long long> buf;
+    tl_begin(buf, total + 64, s);
     cudaError_t le = cudaSuccess;
     for (uint32_t r = 0; r < reps && le == cudaSuccess; r++) le = cudaGraphLaunch(P.graph, s);
-    cudaError_t se = cudaStreamSynchronize(s);
-    unsigned long long* nul = nullptr;
     unsigned got = 0;
-    CK(cudaMemcpyToSymbol(c_tl_buf, &nul, sizeof nul));
-    CK(cudaMemcpyFromSymbol(&got, g_tl_n, sizeof got));
+    std::vector<unsigned long long> t = tl_end(buf, got, s);
     CK(le);
-    CK(se);
     count_launches((uint64_t)reps * pl.launches);
     if (got != total)
         MLP_THROW(ERR_INTERNAL, "timeline: " + std::to_string(got) + " stamps for " + std::to_string(total) +
                                     " launches (a launch of the plan does not come from the solve kernels)");
-    std::vector<unsigned long long> t(total);
-    CK(cudaMemcpy(t.data(), bp, total * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
     // op k of replay r lasts until the next stamp; the last op of the last
     // replay has none and takes the mean of the earlier replays
     for (size_t k = 0; k < n; k++) {
@@ -2694,6 +2706,41 @@ int pcg_solve(const DCSR& A, const double* b, Prec& P, double* x, double eps, ui
     st.t_total_ms = ms;
     if (rc != OK) set_last_error(msg);
     return rc;
+}
+
+std::vector<std::pair<std::string, double>> timeline_pcg(const DCSR& A, const double* b, Prec& P, double* x,
+                                                         double eps, bool flexible, cudaStream_t s) {
+    const size_t nops = P.plan.ops.size(), per = nops + 4;
+    // the solve's kernels that pass a dependent-launch wait: the start's
+    // residual SpMV and first application, then per iteration the SpMV with
+    // (Ap, p), the update, the application, the (r, z) reduction and p
+    DBuf<unsigned long long> buf;
+    tl_begin(buf, 1 + nops + (size_t)PCG_DEFAULT_MAXIT * per + 64, s);
+    PcgStats st;
+    int rc = OK;
+    try {
+        rc = pcg_solve(A, b, P, x, eps, 0, flexible, st, s);
+    } catch (...) {
+        unsigned g = 0;
+        tl_end(buf, g, s);
+        throw;
+    }
+    unsigned got = 0;
+    std::vector<unsigned long long> t = tl_end(buf, got, s);
+    if (rc != OK && rc != ERR_NO_ITER) MLP_THROW(rc, "timeline: the solve failed");
+    const size_t want = 1 + nops + (size_t)st.niter * per;
+    if (got != want || st.niter < 2)
+        MLP_THROW(ERR_INTERNAL, "timeline: " + std::to_string(got) + " stamps where the solve's launches give " +
+                                    std::to_string(want));
+    // an iteration from the end, with the next one's first stamp after it
+    const size_t k = st.niter >= 3 ? st.niter - 3 : 0, base = 1 + nops + k * per;
+    std::vector<std::pair<std::string, double>> out;
+    std::vector<std::string> names{"pcg spmv_dot", "pcg update"};
+    names.insert(names.end(), P.plan.names.begin(), P.plan.names.end());
+    names.push_back("pcg dot_rz");
+    names.push_back("pcg p");
+    for (size_t i = 0; i < per; i++) out.emplace_back(names[i], (double)(t[base + i + 1] - t[base + i]) / 1e3);
+    return out;
 }
 
 // ---------------------------------------------------------------------------

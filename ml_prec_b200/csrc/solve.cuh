@@ -53,6 +53,12 @@ void exec_cache_counts(uint64_t& updates, uint64_t& instantiations);
 // Replays the apply graph reps (>= 2) times back to back with the in-graph
 // timeline on; per launch of the plan its mean time inside the graph (us).
 std::vector<double> timeline_apply(Prec& P, uint32_t reps, cudaStream_t s);
+// One PCG solve (x0 from generate_x0) with the in-graph timeline on; per
+// launch of one iteration near the end (its SpMV with (Ap, p), the update, the
+// application's launches, the (r, z) reduction, the p update) its name and
+// time in us.
+std::vector<std::pair<std::string, double>> timeline_pcg(const DCSR& A, const double* b, Prec& P, double* x,
+                                                         double eps, bool flexible, cudaStream_t s);
 
 template <class T>
 struct SmallPlan;

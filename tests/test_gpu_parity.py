@@ -253,7 +253,8 @@ def test_autotuned_full_size_pcg(M):
 
 def test_in_graph_timeline(M, monkeypatch):
     """mlp_prec_timeline gives one positive in-graph time per launch of the
-    plan (names and bytes as the launch-by-launch profile); a plan with a
+    plan (names and bytes as the launch-by-launch profile), mlp_pcg_timeline
+    one per launch of a PCG iteration; a plan with a
     launch that stamps no time (the persistent kernel) is refused with
     MLP_ERR_INTERNAL instead of returning misattributed times."""
     g = load_golden("ms_layered_16x22x8_c01")
@@ -265,6 +266,12 @@ def test_in_graph_timeline(M, monkeypatch):
     prof = P.profile(1)
     assert [t[0] for t in tl] == [p[0] for p in prof]
     assert all(us > 0 for _, us, _ in tl)
+    import torch
+    b = torch.from_numpy(np.ascontiguousarray(g["b"], dtype=np.float64)).cuda()
+    x = torch.empty_like(b)
+    pt = P.pcg_timeline(A, b, x, 1e-8)
+    assert [t[0] for t in pt] == ["pcg spmv_dot", "pcg update"] + [p[0] for p in prof] + ["pcg dot_rz", "pcg p"]
+    assert all(us > 0 for _, us in pt)
     monkeypatch.setenv("MLP_PERSIST", "1")
     P1 = gpu_prec(A, g)
     P1.solve(g["f_in"])
