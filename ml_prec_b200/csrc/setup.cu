@@ -513,8 +513,15 @@ __device__ int lu_row(const LUArgs& g, uint32_t i, int round) {
     return 1;
 }
 
+// Rounds run back to back as programmatic dependent launches; of three
+// counters the round reads one (the rows left by the previous round), adds to
+// the next and clears the third, which the following round will add to.
 __global__ void k_lu_round(LUArgs g, const uint32_t* __restrict__ pin, const uint32_t* __restrict__ npin,
-                           uint32_t* __restrict__ pout, uint32_t* __restrict__ npout, int round) {
+                           uint32_t* __restrict__ pout, uint32_t* __restrict__ npout, uint32_t* __restrict__ nclear,
+                           int round) {
+    pdl_wait();
+    pdl_trigger();
+    if (blockIdx.x == 0 && threadIdx.x == 0) *nclear = 0;
     uint32_t n = *npin;
     for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
         uint32_t i = pin[idx];
@@ -684,10 +691,14 @@ __global__ void k_sym_values(uint32_t N, const uint32_t* __restrict__ ia, const 
 // Level schedule of a triangular DAG given as CSR dependencies (diagonal entry
 // skipped when it equals the row): level[i] = 1 + max level of its
 // dependencies, computed in rounds like the elimination.
+// Counters as k_lu_round.
 __global__ void k_dag_round(uint32_t R, const uint32_t* __restrict__ ia, const uint32_t* __restrict__ ja,
                             uint32_t depmax, int* __restrict__ lev, const uint32_t* __restrict__ pin,
                             const uint32_t* __restrict__ npin, uint32_t* __restrict__ pout,
-                            uint32_t* __restrict__ npout, int round) {
+                            uint32_t* __restrict__ npout, uint32_t* __restrict__ nclear, int round) {
+    pdl_wait();
+    pdl_trigger();
+    if (blockIdx.x == 0 && threadIdx.x == 0) *nclear = 0;
     uint32_t n = *npin;
     for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
         uint32_t i = pin[idx];
@@ -868,24 +879,25 @@ static void sparse_lu_level(Level& li, Level& ln, const uint8_t* keep, const dou
         // E rows in rounds
         int rounds = 0;
         if (M) {
-            Tmp<uint32_t> pa(M), pb(M), cnt(2);
+            Tmp<uint32_t> pa(M), pb(M), cnt(3);
+            cnt.zero(s);
             k_iota<<<grid_for(M, 256), 256, 0, s>>>(M, pa.p);
             CK_LAUNCH();
             CK(cudaMemcpyAsync(cnt.p, &M, 4, cudaMemcpyHostToDevice, s));
             uint32_t* pin = pa.p; uint32_t* pout = pb.p;
-            uint32_t* cin = cnt.p; uint32_t* cout = cnt.p + 1;
             unsigned grid = (unsigned)std::min<size_t>(grid_for(M, 256), (size_t)num_sms() * 8);
             uint32_t prev_left = M;
             for (;;) {
                 for (int b = 0; b < 16; b++) {
                     rounds++;
-                    CK(cudaMemsetAsync(cout, 0, 4, s));
-                    k_lu_round<<<grid, 256, 0, s>>>(g, pin, cin, pout, cout, rounds);
+                    launch_k(k_lu_round, grid, 256, 0, s, g, (const uint32_t*)pin,
+                             (const uint32_t*)(cnt.p + (rounds - 1) % 3), pout, cnt.p + rounds % 3,
+                             cnt.p + (rounds + 1) % 3, rounds);
                     CK_LAUNCH();
                     std::swap(pin, pout);
-                    std::swap(cin, cout);
                 }
-                std::vector<uint32_t> h = read_words({cin, reinterpret_cast<const uint32_t*>(flags.p)}, s);
+                std::vector<uint32_t> h =
+                    read_words({cnt.p + rounds % 3, reinterpret_cast<const uint32_t*>(flags.p)}, s);
                 uint32_t left = h[0];
                 if ((h[1] & 1) || left == 0) break;
                 // every round finishes at least the rows whose dependencies are
@@ -1429,25 +1441,25 @@ static void build_frames(Hierarchy& H, cudaStream_t s) {
             // U-solve wavefronts: row q depends on the E columns of its row
             Tmp<int> lev(M);
             lev.zero(s);
-            Tmp<uint32_t> pa(M), pb(M), cnt(2);
+            Tmp<uint32_t> pa(M), pb(M), cnt(3);
+            cnt.zero(s);
             k_iota<<<grid_for(M, 256), 256, 0, s>>>(M, pa.p);
             CK_LAUNCH();
             CK(cudaMemcpyAsync(cnt.p, &M, 4, cudaMemcpyHostToDevice, s));
-            uint32_t *pin = pa.p, *pout = pb.p, *cin = cnt.p, *cout = cnt.p + 1;
+            uint32_t *pin = pa.p, *pout = pb.p;
             int round = 0;
             uint32_t prev_left = M;
             unsigned grid = (unsigned)std::min<size_t>(grid_for(M, 256), (size_t)num_sms() * 8);
             for (;;) {
                 for (int b = 0; b < 16; b++) {
                     round++;
-                    CK(cudaMemsetAsync(cout, 0, 4, s));
-                    k_dag_round<<<grid, 256, 0, s>>>(M, li.Uf.ia.p, li.Uf.ja.p, M, lev.p, pin, cin, pout, cout,
-                                                     round);
+                    launch_k(k_dag_round, grid, 256, 0, s, M, (const uint32_t*)li.Uf.ia.p, (const uint32_t*)li.Uf.ja.p,
+                             M, lev.p, (const uint32_t*)pin, (const uint32_t*)(cnt.p + (round - 1) % 3), pout,
+                             cnt.p + round % 3, cnt.p + (round + 1) % 3, round);
                     CK_LAUNCH();
                     std::swap(pin, pout);
-                    std::swap(cin, cout);
                 }
-                uint32_t left = read_u32(cin, s);
+                uint32_t left = read_u32(cnt.p + round % 3, s);
                 if (left == 0) break;
                 if (left >= prev_left) MLP_THROW(ERR_INTERNAL, "U schedule makes no progress");
                 prev_left = left;
