@@ -283,9 +283,14 @@ void csr_tile_stats_batch(const std::vector<DCSR*>& ms, const std::vector<const 
     extra_out.assign(h.begin() + ms.size(), h.end());
 }
 
+// Largest grid of the staged PCG SpMV (and so the size of its callers'
+// reduction scratch): one tile per CTA, at most eight CTAs per SM, the
+// occupancy the tile pipeline reaches (pipe_grid); at five per SM the
+// in-graph SpMV with (Ap, p) ran at 0.53 of the HBM bandwidth against 0.77
+// for the SpMV alone at eight.
 static unsigned staged_grid(uint32_t n) {
     uint32_t nt = (n + ST_ROWS - 1) / ST_ROWS;
-    return (unsigned)std::max<uint32_t>(1, std::min<uint32_t>(nt, (uint32_t)num_sms() * 5));
+    return (unsigned)std::max<uint32_t>(1, std::min<uint32_t>(nt, (uint32_t)num_sms() * 8));
 }
 
 // Grid of a pipelined staged kernel: the CTAs that fit on the device at once
@@ -2394,29 +2399,39 @@ __global__ void __launch_bounds__(RB) k_pcg_dot_rz(uint32_t n, const double* __r
     }
 }
 
-// p = beta p + z (dscal then daxpy, pcg.cc:71-72), a pair of elements a
-// thread. p and z were written before the preceding launch (the (r, z)
+// p = beta p + z (dscal then daxpy, pcg.cc:71-72), PCG_P_PAIRS pairs of
+// elements a thread (pair t and t + T, T the grid's threads, so that the grid
+// fits one wave). p and z were written before the preceding launch (the (r, z)
 // reduction), so they are loaded before the wait; only beta comes from it.
+constexpr uint32_t PCG_P_PAIRS = 2;
 __global__ void k_pcg_p(uint32_t n, double* __restrict__ p, const double* __restrict__ z, const PcgDev* d) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t e = 2 * i;
-    double p0 = 0, p1 = 0, z0 = 0, z1 = 0;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x, T = gridDim.x * blockDim.x;
     const bool vec = aligned16(p, z, p, z);
-    if (vec && e + 1 < n) {
-        double2 pv = reinterpret_cast<const double2*>(p)[i], zv = reinterpret_cast<const double2*>(z)[i];
-        p0 = pv.x; p1 = pv.y; z0 = zv.x; z1 = zv.y;
-    } else {
-        if (e < n) { p0 = p[e]; z0 = z[e]; }
-        if (e + 1 < n) { p1 = p[e + 1]; z1 = z[e + 1]; }
+    double pv[PCG_P_PAIRS][2], zv[PCG_P_PAIRS][2];
+#pragma unroll
+    for (uint32_t k = 0; k < PCG_P_PAIRS; k++) {
+        const uint32_t i = t + k * T, e = 2 * i;
+        pv[k][0] = pv[k][1] = zv[k][0] = zv[k][1] = 0;
+        if (vec && e + 1 < n) {
+            double2 a = reinterpret_cast<const double2*>(p)[i], b = reinterpret_cast<const double2*>(z)[i];
+            pv[k][0] = a.x; pv[k][1] = a.y; zv[k][0] = b.x; zv[k][1] = b.y;
+        } else {
+            if (e < n) { pv[k][0] = p[e]; zv[k][0] = z[e]; }
+            if (e + 1 < n) { pv[k][1] = p[e + 1]; zv[k][1] = z[e + 1]; }
+        }
     }
     pdl_wait();
     pdl_trigger();
     const double beta = d->beta;
-    if (vec && e + 1 < n) {
-        reinterpret_cast<double2*>(p)[i] = make_double2(beta * p0 + z0, beta * p1 + z1);
-    } else {
-        if (e < n) p[e] = beta * p0 + z0;
-        if (e + 1 < n) p[e + 1] = beta * p1 + z1;
+#pragma unroll
+    for (uint32_t k = 0; k < PCG_P_PAIRS; k++) {
+        const uint32_t i = t + k * T, e = 2 * i;
+        if (vec && e + 1 < n) {
+            reinterpret_cast<double2*>(p)[i] = make_double2(beta * pv[k][0] + zv[k][0], beta * pv[k][1] + zv[k][1]);
+        } else {
+            if (e < n) p[e] = beta * pv[k][0] + zv[k][0];
+            if (e + 1 < n) p[e + 1] = beta * pv[k][1] + zv[k][1];
+        }
     }
 }
 
@@ -2536,12 +2551,16 @@ static void record_iteration(Prec& P, const DCSR& Af, uint32_t n, bool flexible,
         case 16: launch_k(k_pcg_spmv_dot<16>, G, RB, 0, s, n, Af.ia.p, Af.ja.p, Af.a.p, W.p.p, W.Ap.p, W.partials.p, d); break;
         default: launch_k(k_pcg_spmv_dot<32>, G, RB, 0, s, n, Af.ia.p, Af.ja.p, Af.a.p, W.p.p, W.Ap.p, W.partials.p, d); break;
     }
-    launch_k(k_pcg_update, G, RB, 0, s, n, W.xf.p, r, (const double*)W.p.p, (const double*)W.Ap.p, W.partials.p, d,
+    // the vector kernels with up to eight CTAs per SM (the partials hold
+    // 2 * max(G, staged_grid(n)) slots)
+    const unsigned Gv = std::max(G, std::min(staged_grid(n), (unsigned)grid_for((n + 1) / 2, RB)));
+    launch_k(k_pcg_update, Gv, RB, 0, s, n, W.xf.p, r, (const double*)W.p.p, (const double*)W.Ap.p, W.partials.p, d,
              h, 1);
     P.plan.run(s);
-    launch_k(k_pcg_dot_rz, G, RB, 0, s, n, (const double*)r, (const double*)z, (const double*)W.rprev.p,
+    launch_k(k_pcg_dot_rz, Gv, RB, 0, s, n, (const double*)r, (const double*)z, (const double*)W.rprev.p,
              W.partials.p, d, flexible ? 1 : 0);
-    launch_k(k_pcg_p, grid_for((n + 1) / 2, 256), 256, 0, s, n, W.p.p, (const double*)z, (const PcgDev*)d);
+    launch_k(k_pcg_p, grid_for(((n + 1) / 2 + PCG_P_PAIRS - 1) / PCG_P_PAIRS, 256), 256, 0, s, n, W.p.p,
+             (const double*)z, (const PcgDev*)d);
     if (flexible) k_copy_d<<<grid_for(n, 256), 256, 0, s>>>(n, r, W.rprev.p);
 }
 
@@ -2853,7 +2872,7 @@ int pcg_solve_cb(const DCSR& A, const double* b, const std::function<void(const 
         apply(r.p, z.p);
         napply++;
         k_pcg_dot_rz<<<G, RB, 0, s>>>(n, r.p, z.p, rprev.p, partials.p, d, flexible ? 1 : 0);
-        k_pcg_p<<<grid_for((n + 1) / 2, 256), 256, 0, s>>>(n, p.p, z.p, d);
+        k_pcg_p<<<grid_for(((n + 1) / 2 + PCG_P_PAIRS - 1) / PCG_P_PAIRS, 256), 256, 0, s>>>(n, p.p, z.p, d);
         count_launches(2);
         if (flexible) CK(cudaMemcpyAsync(rprev.p, r.p, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
         CK_LAUNCH();
@@ -3296,7 +3315,7 @@ int pcg_solve_hostloop(const DCSR& A, const double* b, Prec& P, double* x, doubl
         prec_apply_frame(P, s);
         napply++;
         k_pcg_dot_rz<<<G, RB, 0, s>>>(n, r, z, rprev.p, partials.p, d, flexible ? 1 : 0);
-        k_pcg_p<<<grid_for((n + 1) / 2, 256), 256, 0, s>>>(n, p.p, z, d);
+        k_pcg_p<<<grid_for(((n + 1) / 2 + PCG_P_PAIRS - 1) / PCG_P_PAIRS, 256), 256, 0, s>>>(n, p.p, z, d);
         count_launches(2);
         if (flexible) CK(cudaMemcpyAsync(rprev.p, r, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
         CK_LAUNCH();
@@ -3466,7 +3485,7 @@ int pcg_solve_noalloc(const DCSR& A, const double* b, Prec& P, double* x, double
         prec_apply_frame(P, s);
         napply++;
         k_pcg_dot_rz<<<G, RB, 0, s>>>(n, r, z, rprev, partials, d, flexible ? 1 : 0);
-        k_pcg_p<<<grid_for((n + 1) / 2, 256), 256, 0, s>>>(n, p, z, d);
+        k_pcg_p<<<grid_for(((n + 1) / 2 + PCG_P_PAIRS - 1) / PCG_P_PAIRS, 256), 256, 0, s>>>(n, p, z, d);
         count_launches(2);
         if (flexible) CK(cudaMemcpyAsync(rprev, r, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
         CK_LAUNCH();
