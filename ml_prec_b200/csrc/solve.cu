@@ -2551,10 +2551,11 @@ static void record_iteration(Prec& P, const DCSR& Af, uint32_t n, bool flexible,
         case 16: launch_k(k_pcg_spmv_dot<16>, G, RB, 0, s, n, Af.ia.p, Af.ja.p, Af.a.p, W.p.p, W.Ap.p, W.partials.p, d); break;
         default: launch_k(k_pcg_spmv_dot<32>, G, RB, 0, s, n, Af.ia.p, Af.ja.p, Af.a.p, W.p.p, W.Ap.p, W.partials.p, d); break;
     }
-    // the vector kernels with up to eight CTAs per SM (the partials hold
-    // 2 * max(G, staged_grid(n)) slots)
+    // the (r, z) reduction with up to eight CTAs per SM (the partials hold
+    // 2 * max(G, staged_grid(n)) slots: 6.4 against 7.3 us at 60x220x85; the
+    // update measured slower so, 13.6 against 12.0 us)
     const unsigned Gv = std::max(G, std::min(staged_grid(n), (unsigned)grid_for((n + 1) / 2, RB)));
-    launch_k(k_pcg_update, Gv, RB, 0, s, n, W.xf.p, r, (const double*)W.p.p, (const double*)W.Ap.p, W.partials.p, d,
+    launch_k(k_pcg_update, G, RB, 0, s, n, W.xf.p, r, (const double*)W.p.p, (const double*)W.Ap.p, W.partials.p, d,
              h, 1);
     P.plan.run(s);
     launch_k(k_pcg_dot_rz, Gv, RB, 0, s, n, (const double*)r, (const double*)z, (const double*)W.rprev.p,
