@@ -403,11 +403,8 @@ unsigned persist_grid() {
         int per_sm = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persist<T, PK_THREADS>, PK_THREADS, 0));
         if (per_sm < 1) MLP_THROW(ERR_INTERNAL, "persistent apply kernel does not fit on an SM");
-        // CTAs per SM: 2 by default; MLP_PERSIST_CPS=1 halves the grid (fewer
-        // barrier arrivals, fewer warps per step)
-        int cps = 2;
-        if (const char* e = getenv("MLP_PERSIST_CPS")) cps = std::max(1, atoi(e));
-        g = (unsigned)num_sms() * (unsigned)std::min(per_sm, cps);
+        // two CTAs per SM where they fit
+        g = (unsigned)num_sms() * (unsigned)std::min(per_sm, 2);
         if (g > sizeof(PBar::red) / sizeof(double))
             MLP_THROW(ERR_INTERNAL, "persistent apply grid exceeds its reduction buffer");
     }

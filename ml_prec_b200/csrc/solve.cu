@@ -554,23 +554,9 @@ __global__ void k_scatter(uint32_t n, const uint32_t* __restrict__ idx, const do
     if (i < n) dst[idx[i]] = src[i];
 }
 
-// Replays the recorded launches. With MLP_CAPTURE_DEBUG=1 every launch is
-// checked right away, so a failure names the launch that caused it.
+// Replays the recorded launches.
 void Plan::run(cudaStream_t s) const {
-    static int dbg = -1;
-    if (dbg < 0) {
-        const char* e = getenv("MLP_CAPTURE_DEBUG");
-        dbg = (e && e[0] == '1') ? 1 : 0;
-    }
-    for (size_t i = 0; i < ops.size(); i++) {
-        ops[i](s);
-        if (dbg) {
-            cudaError_t e = cudaPeekAtLastError();
-            if (e != cudaSuccess)
-                MLP_THROW(ERR_CUDA, "plan op " + std::to_string(i) + " of " + std::to_string(ops.size()) + ": " +
-                                        cudaGetErrorString(e));
-        }
-    }
+    for (const auto& op : ops) op(s);
 }
 
 void gather(uint32_t n, const uint32_t* idx, const double* src, double* dst, cudaStream_t s) {

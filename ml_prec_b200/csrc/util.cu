@@ -28,14 +28,7 @@ static thread_local int t_pdl_off = 0;
 PdlOff::PdlOff() { t_pdl_off++; }
 PdlOff::~PdlOff() { t_pdl_off--; }
 
-bool pdl_enabled() {
-    static int on = -1;
-    if (on < 0) {
-        const char* e = getenv("MLP_PDL");
-        on = (e && e[0] == '0') ? 0 : 1;
-    }
-    return on == 1 && t_pdl_off == 0;
-}
+bool pdl_enabled() { return t_pdl_off == 0; }
 
 static bool trace_on() {
     static int on = -1;
