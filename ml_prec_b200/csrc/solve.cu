@@ -674,7 +674,11 @@ __global__ void __launch_bounds__(512) k_phase2(uint32_t M, const uint32_t* __re
 //    D = G_C C built at set-up in FP64 (blocks [nb_c, nb_c + nb_f));
 //  * the other rows (rows[nf, M), all columns < M) exactly as k_phase2.
 // So the apply needs no separate launch for the coarse solve; the folded rows
-// add G_C (C w_C) in the order (G_C C) w_C.
+// add G_C (C w_C) in the order (G_C C) w_C. In FP32 a folded row's bounds and
+// each lane's first G entry are loaded before the dependent-launch wait and its
+// first gather is issued with those of w_C (FP32 solve at 60x220x85 on B200
+// 11.60 -> 10.69 ms); in FP64 that measured slower (16.23 -> 16.45 ms), so
+// there the row is read after the wait.
 template <class T, int LPR>
 __global__ void __launch_bounds__(256) k_phase2_fold(uint32_t M, uint32_t n, const uint32_t* __restrict__ ia,
                                                      const uint32_t* __restrict__ ja, const T* __restrict__ a,
@@ -694,10 +698,25 @@ __global__ void __launch_bounds__(256) k_phase2_fold(uint32_t M, uint32_t n, con
             uint32_t j = lane + 32 * k;
             cv[k] = (r < nr && j < n) ? c[j] : 0.0;
         }
+        // FP32: a folded row's G row, its bounds and each lane's first entry
+        constexpr bool PRE = sizeof(T) == 4;
+        uint32_t q = 0, gj = 0, ge = 0, gc = 0;
+        T ga = 0;
+        if (PRE && !coarse && r < nr) {
+            q = rows[r];
+            gj = ia[q] + lane;
+            ge = ia[q + 1];
+            if (gj < ge) {
+                gc = ja[gj];
+                ga = a[gj];
+            }
+        }
         pdl_wait();
         pdl_trigger();
         if (r >= nr) return;
         const T* wc = w + M;
+        const bool g0 = PRE && !coarse && gj < ge && gc < M;
+        const T wg = g0 ? w[gc] : T(0);
         double d = 0;
 #pragma unroll
         for (int k = 0; k < CV; k++) {
@@ -711,11 +730,19 @@ __global__ void __launch_bounds__(256) k_phase2_fold(uint32_t M, uint32_t n, con
             if (lane == 0) out[M + r] = (T)d;
             return;
         }
-        const uint32_t q = rows[r];
         T sp = 0;
-        for (uint32_t j = ia[q] + lane, e = ia[q + 1]; j < e; j += 32) {
-            uint32_t col = ja[j];
-            if (col < M) sp = fmadd(a[j], w[col], sp);
+        if constexpr (PRE) {
+            if (g0) sp = fmadd(ga, wg, sp);
+            for (uint32_t j = gj + 32; j < ge; j += 32) {
+                uint32_t col = ja[j];
+                if (col < M) sp = fmadd(a[j], w[col], sp);
+            }
+        } else {
+            q = rows[r];
+            for (uint32_t j = ia[q] + lane, e = ia[q + 1]; j < e; j += 32) {
+                uint32_t col = ja[j];
+                if (col < M) sp = fmadd(a[j], w[col], sp);
+            }
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) sp += __shfl_xor_sync(0xffffffffu, sp, o);
@@ -824,11 +851,53 @@ __device__ __forceinline__ T lane_split_sum(uint32_t jb, uint32_t je, const uint
     return p[0];
 }
 
+// lane_split_sum with the row's first K entries (column indices pc, values pa)
+// already in registers: their K gathers are issued together, then the sum
+// goes on in entry order exactly as lane_split_sum adds it.
+template <class T, int LP, int K, class V>
+__device__ __forceinline__ T lane_split_sum_pre(uint32_t jb, uint32_t je, const uint32_t (&pc)[K], const T (&pa)[K],
+                                                const uint32_t* __restrict__ ja, const T* __restrict__ a, V val) {
+    T xv[K];
+#pragma unroll
+    for (int t = 0; t < K; t++) xv[t] = jb + t < je ? val(pc[t]) : T(0);
+    T p[LP];
+#pragma unroll
+    for (int l = 0; l < LP; l++) p[l] = 0;
+#pragma unroll
+    for (int t = 0; t < K; t++)
+        if (jb + t < je) p[t & (LP - 1)] = fmadd(pa[t], xv[t], p[t & (LP - 1)]);
+    for (uint32_t j = jb + K; j < je; j++) {
+        T av = a[j], x = val(ja[j]);
+        int l = (int)((j - jb) & (LP - 1));
+#pragma unroll
+        for (int m = 0; m < LP; m++)
+            if (m == l) p[m] = fmadd(av, x, p[m]);
+    }
+#pragma unroll
+    for (int o = LP / 2; o > 0; o >>= 1) {
+        T q[LP];
+#pragma unroll
+        for (int l = 0; l < LP; l++) q[l] = p[l] + p[l ^ o];
+#pragma unroll
+        for (int l = 0; l < LP; l++) p[l] = q[l];
+    }
+    return p[0];
+}
+
 // Step A. Blocks [0, nbu): the rows of Af with LPU lanes per row (the
-// correction kernel's layout); blocks [nbu, ...): one thread per P1 row.
+// correction kernel's layout); blocks [nbu, ...): a warp per P1 row.
 // MODE 0: r' = f - Af x (second sweep); MODE 1: x += u0; r' = r - Af u0.
+// In FP32 the first Af entries of a P1 row's entries are loaded before the
+// dependent-launch wait, with the kernel held to five 256-thread CTAs an SM
+// so that a level-2 grid of the 60x220x85 field (706 CTAs) stays one wave:
+// FP32 solve 10.69 -> 10.36 ms on B200. In FP64 the same prefetch measured
+// slower (16.45 -> 17.04 ms: the extra registers spill or split the grid into
+// two waves), so FP64 loads them after the wait.
+template <class T>
+constexpr int merge_a_min_ctas() { return sizeof(T) == 4 ? 5 : 0; }  // 0: no bound
 template <class T, int LPU, int LPP, int MODE>
-__global__ void __launch_bounds__(256) k_merge_a(uint32_t N, uint32_t R, uint32_t nbu, const uint32_t* __restrict__ af_ia,
+__global__ void __launch_bounds__(256, merge_a_min_ctas<T>()) k_merge_a(uint32_t N, uint32_t R, uint32_t nbu,
+                                                 const uint32_t* __restrict__ af_ia,
                                                  const uint32_t* __restrict__ af_ja, const T* __restrict__ af_a,
                                                  const uint32_t* __restrict__ p1_ia, const uint32_t* __restrict__ p1_ja,
                                                  const T* __restrict__ p1_a, const T* __restrict__ dval,
@@ -864,10 +933,13 @@ __global__ void __launch_bounds__(256) k_merge_a(uint32_t N, uint32_t R, uint32_
         // One warp per P1 row: lane e recomputes the entry r'_k of the row's
         // entries e, e + 32, ... (all lanes at once), then the products are
         // added in entry order with k_phase1's lane split. The row's first 32
-        // entries and their Af row bounds are loaded before the wait.
-        uint32_t q = ((blockIdx.x - nbu) * blockDim.x + threadIdx.x) >> 5;
-        int lane = threadIdx.x & 31;
-        bool act = q < R;
+        // entries and their Af row bounds (and in FP32 the first AFK entries
+        // of those Af rows) are loaded before the wait.
+        constexpr bool PRE = sizeof(T) == 4;
+        constexpr int AFK = PRE ? 4 : 1;
+        const uint32_t q = ((blockIdx.x - nbu) * blockDim.x + threadIdx.x) >> 5;
+        const int lane = threadIdx.x & 31;
+        const bool act = q < R;
         uint32_t jb = 0, je = 0;
         if (act) {
             jb = p1_ia[q];
@@ -875,15 +947,31 @@ __global__ void __launch_bounds__(256) k_merge_a(uint32_t N, uint32_t R, uint32_
         }
         uint32_t k0 = 0, kb0 = 0, ke0 = 0;
         T a0 = 0;
+        uint32_t fc[AFK];
+        T fa[AFK];
+#pragma unroll
+        for (int t = 0; t < AFK; t++) {
+            fc[t] = 0;
+            fa[t] = 0;
+        }
         if (jb + lane < je) {
             k0 = p1_ja[jb + lane];
             a0 = p1_a[jb + lane];
             kb0 = af_ia[k0];
             ke0 = af_ia[k0 + 1];
+            if constexpr (PRE) {
+#pragma unroll
+                for (int t = 0; t < AFK; t++)
+                    if (kb0 + t < ke0) {
+                        fc[t] = af_ja[kb0 + t];
+                        fa[t] = af_a[kb0 + t];
+                    }
+            }
         }
         pdl_wait();
         pdl_trigger();
         if (!act) return;  // the whole warp
+        auto vv = [&](uint32_t c) { return v[c]; };
         T p[LPP];
 #pragma unroll
         for (int l = 0; l < LPP; l++) p[l] = 0;
@@ -891,16 +979,22 @@ __global__ void __launch_bounds__(256) k_merge_a(uint32_t N, uint32_t R, uint32_
             uint32_t j = base + lane;
             T av = 0, rv = 0;
             if (j < je) {
-                uint32_t k = k0, kb = kb0, ke = ke0;
-                av = a0;
-                if (base != jb) {
-                    k = p1_ja[j];
-                    av = p1_a[j];
-                    kb = af_ia[k];
-                    ke = af_ia[k + 1];
+                if (PRE && base == jb) {
+                    av = a0;
+                    T fk = MODE == 0 ? f[k0] : r_in[k0];
+                    rv = fk - lane_split_sum_pre<T, LPU, AFK>(kb0, ke0, fc, fa, af_ja, af_a, vv);
+                } else {
+                    uint32_t k = k0, kb = kb0, ke = ke0;
+                    av = a0;
+                    if (base != jb) {
+                        k = p1_ja[j];
+                        av = p1_a[j];
+                        kb = af_ia[k];
+                        ke = af_ia[k + 1];
+                    }
+                    T t = lane_split_sum<T, LPU>(kb, ke, af_ja, af_a, vv);
+                    rv = (MODE == 0 ? f[k] : r_in[k]) - t;
                 }
-                T t = lane_split_sum<T, LPU>(kb, ke, af_ja, af_a, [&](uint32_t c) { return v[c]; });
-                rv = (MODE == 0 ? f[k] : r_in[k]) - t;
             }
             uint32_t cnt = min(32u, je - base);
             for (uint32_t e = 0; e < cnt; e++) {
@@ -1565,7 +1659,7 @@ struct Builder {
         const char* e = getenv("MLP_MERGE");
         return !(e && e[0] == '0');
     }
-    // rows of Af with the correction kernel's lane count, P1 rows one per thread
+    // rows of Af with the correction kernel's lane count, P1 rows a warp each
     void step_a(const Level& L, int mode, const T* f, T* x, const T* r_in, T* r_out, const T* u_in, T* u_out,
                 T* w) {
         uint32_t N = L.N, R = L.N - L.Md;
