@@ -17,13 +17,15 @@ FP64 path, max over ranks (every rank solves its own replica; no data-path
 collective; "weak" scaling). `e2e`: the same step through the C ABI with host
 buffers (matrix and right-hand side uploaded, solution downloaded), host-timed.
 `forms`: the FP64 step with launch shapes from the build-time autotuner, the
-FP32-stored hierarchy inside flexible FP64 PCG (time with fixed and tuned
+c = 0.1 problem, the uh_cheb preconditioner (sigma 3, degree 4) on the same
+matrix, the FP32-stored hierarchy inside flexible FP64 PCG (time with fixed and tuned
 shapes, accuracy against a tight FP64 solve), the adjoint gradient (time
 against one forward solve), and the 64-realization ensemble solved in one
 graph launch per rank (sharded over ranks). `roofline`: the level-0 CSR SpMV
 (pipelined tile kernel), 50 graph-recorded launches over two alternating
 matrix copies, with the DRAM traffic of an ncu capture. `cpu_baseline`: the
-reference itself (oracle/_ref, single-threaded) on the same problem.
+reference itself (oracle/_ref, single-threaded) on the same problem (and on
+the c = 0.1 and uh_cheb forms).
 `--no-forms` and `--no-cpu-baseline` leave out those extra measurements (the
 profiling runs use them); the timed steps are the same.
 """
@@ -55,6 +57,8 @@ UNIT = "s"
 NX, NY, NZ, C_REACT, SEED = 60, 220, 85, 1.0, 2
 EPS = 1e-8
 MSPLIT = dict(q=(0.8,), niter=(5,), max_levels=15, degree_max=2, order="simple_1")
+# uh_cheb as `ml_prec -p uh_cheb -s 3 -b 4` runs it: sigma 3, Chebyshev degree 4
+UH_CHEB = dict(sigma=(3.0,), ncheb=(4,), use_tails=True)
 # DRAM bytes of one level-0 SpMV launch on this matrix from an ncu capture
 # (106.84 MB read + 4.79 MB written): the matrix and x stream once; part of y
 # is still in L2 when the kernel ends.
@@ -412,6 +416,30 @@ def run_ours(args, ws, rank, local):
         del A01
         progress("c=0.1 steps")
 
+        # ---- uh_cheb (sigma 3, Chebyshev degree 4 on every level, tails) ----
+        # the same matrix and PCG; one warm-up step, then three timed ones
+        tch, stch, nlch = [], None, 0
+        for k in range(4):
+            flush_l2(flush)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            Pc = M.Prec(A, **UH_CHEB)
+            stch = Stats()
+            check(lib().mlp_pcg_device(A.h, C.c_void_p(b_d.data_ptr()), Pc.h, C.c_void_p(x_d.data_ptr()),
+                                       EPS, 0, 0, C.byref(stch), C.c_void_p(stream.cuda_stream)))
+            e1.record(stream)
+            e1.synchronize()
+            nlch = Pc.nlevels
+            if k >= 1:
+                tch.append(e0.elapsed_time(e1) / 1e3)
+            del Pc
+        out["uh_cheb"] = dict(s_per_step=float(np.mean(tch)), iters=stch.niter, levels=nlch,
+                              setup_ms=stch.t_setup_ms, solve_ms=stch.t_solve_ms, steps=len(tch),
+                              params="sigma 3, degree 4 per level, tails (-p uh_cheb -s 3 -b 4)")
+        progress("uh_cheb steps")
+
     # ---- roofline: level-0 SpMV (staged kernel), events on its stream ----
     # 50 launches back to back between two events, alternating between two
     # copies of the matrix and vectors (2 x 116 MB > the 126 MB L2), so every
@@ -498,8 +526,9 @@ def cpu_info():
     return model, cores
 
 
-def reference_cpu(steps, warmup, timeout=1800, c=C_REACT):
-    """The reference's own CPU build (oracle/_ref/ref_driver) on the same problem."""
+def reference_cpu(steps, warmup, timeout=1800, c=C_REACT, prec="msplit"):
+    """The reference's own CPU build (oracle/_ref/ref_driver) on the same problem
+    (prec "cheb": uh_cheb with the UH_CHEB parameters)."""
     from oracle import oracle as O
     from ml_prec_b200 import fields
     if not O.ref_available():
@@ -511,8 +540,13 @@ def reference_cpu(steps, warmup, timeout=1800, c=C_REACT):
         cfg = os.path.join(td, "msplit.cfg")
         with open(cfg, "w") as f:
             f.write(O.msplit_cfg_text())
-        r = O.run_ref(os.path.join(td, "out"), perm=perm, nx=NX, ny=NY, nz=NZ, c=c, prec="msplit",
-                      cfg=cfg, eps=EPS, reps=warmup + steps, timeout=timeout)
+        if prec == "cheb":
+            r = O.run_ref(os.path.join(td, "out"), perm=perm, nx=NX, ny=NY, nz=NZ, c=c, prec="cheb",
+                          sigmas=UH_CHEB["sigma"], niters=UH_CHEB["ncheb"], eps=EPS, reps=warmup + steps,
+                          timeout=timeout)
+        else:
+            r = O.run_ref(os.path.join(td, "out"), perm=perm, nx=NX, ny=NY, nz=NZ, c=c, prec="msplit",
+                          cfg=cfg, eps=EPS, reps=warmup + steps, timeout=timeout)
     su = r["t_setup_all"][warmup:]
     so = r["t_solve_all"][warmup:]
     per = [x + y for x, y in zip(su, so)]
@@ -672,6 +706,11 @@ def main():
                 if r01:
                     cpu["c01"] = {"value": r01["value"], "iters": r01["niter"], "setup_s": r01["setup"],
                                   "solve_s": r01["solve"]}
+                rch = reference_cpu(1, 0, prec="cheb")
+                progress("reference CPU step, uh_cheb")
+                if rch:
+                    cpu["uh_cheb"] = {"value": rch["value"], "iters": rch["niter"], "setup_s": rch["setup"],
+                                      "solve_s": rch["solve"]}
                 cpu["ensemble_concurrent"] = reference_ensemble(64)
                 progress("reference ensemble")
     line = {
@@ -687,6 +726,7 @@ def main():
         "forms": None if ens is None else {
             "autotuned_fp64": res.get("autotuned"),
             "c01": res.get("c01"),
+            "uh_cheb": res.get("uh_cheb"),
             "fp32_prec": res["fp32"],
             "adjoint": res["adjoint"],
             "ensemble": dict(ens, realizations=64, solves_per_s=64 / (ens["fwd_ms"] / 1e3),
