@@ -1659,16 +1659,18 @@ struct Builder {
         const char* e = getenv("MLP_MERGE");
         return !(e && e[0] == '0');
     }
-    // rows of Af with the correction kernel's lane count, P1 rows a warp each
+    // rows of the residual's matrix (Af, or As for uh_cheb's Chebyshev
+    // residual) with the correction kernel's lane count, P1 rows a warp each
     void step_a(const Level& L, int mode, const T* f, T* x, const T* r_in, T* r_out, const T* u_in, T* u_out,
-                T* w) {
+                T* w, const DCSR* Am = nullptr) {
+        const DCSR& A_ = Am ? *Am : L.Af;
         uint32_t N = L.N, R = L.N - L.Md;
-        bool staged = L.Af.tile_max && L.Af.tile_max <= ST_MAX_NNZ && N >= 4 * ST_ROWS;
-        int lpu = mode == 0 ? (staged ? 1 : pick_lpr(N, L.Af.nnz)) : pick_lpr(N, L.Af.nnz);
+        bool staged = A_.tile_max && A_.tile_max <= ST_MAX_NNZ && N >= 4 * ST_ROWS;
+        int lpu = mode == 0 ? (staged ? 1 : pick_lpr(N, A_.nnz)) : pick_lpr(N, A_.nnz);
         int lpp = pick_lpr(R, L.P1.nnz);
         uint32_t nbu = grid_for((size_t)N * lpu, 256), nbp = R ? grid_for((size_t)R * 32, 256) : 0;
-        const uint32_t *aia = L.Af.ia.p, *aja = L.Af.ja.p, *pia = L.P1.ia.p, *pja = L.P1.ja.p;
-        const T *aa = vals<T>(L.Af), *pa = vals<T>(L.P1), *dv = dvals<T>(L);
+        const uint32_t *aia = A_.ia.p, *aja = A_.ja.p, *pia = L.P1.ia.p, *pja = L.P1.ja.p;
+        const T *aa = vals<T>(A_), *pa = vals<T>(L.P1), *dv = dvals<T>(L);
         auto go = [=](auto kern, cudaStream_t s) {
             launch_k(kern, nbu + nbp, 256, 0, s, N, R, nbu, aia, aja, aa, pia, pja, pa, dv, f, x, r_in, r_out, u_in,
                      u_out, w);
@@ -1692,6 +1694,24 @@ struct Builder {
         int l0 = staged ? 1 : pick_lpr(N, L.Af.nnz), l1 = pick_lpr(N, L.Af.nnz), lp = pick_lpr(R, L.P1.nnz);
         return l0 <= 8 && l1 <= 8 && lp <= 8;
     }
+    // uh_cheb: the residual F - As u of a Chebyshev step and phase 1 of the
+    // level-l call that follows it as one step-A launch (MODE 0, As in place of
+    // Af), where that call takes the plan's regular path (not persistent, not
+    // a small or tabulated level) and the residual uses the tile kernel, whose
+    // serial row sums step A repeats with one lane per row: the merged and the
+    // separate launches give bit-identical results.
+    bool ch_merge_ok(uint32_t l) const {
+        if (!merge_enabled() || autotune || ps || !explicit_solves || l >= H.nlevels || persist_ok(l)) return false;
+        if (small64 && small64->valid() && small64->dense.p && l == small64->first) return false;
+        if (small && small->valid() && l == small->first) return false;
+        const Level& L = *H.lv[l];
+        if (L.direct || L.N > MERGE_MAX_N) return false;
+        const DCSR& As = L.As;
+        bool staged = As.tile_max && As.tile_max <= ST_MAX_NNZ && L.N >= 4 * ST_ROWS;
+        return staged && pick_lpr(L.N - L.Md, L.P1.nnz) <= 8;
+    }
+    // set by a merged step A: the next ch() call's phase 1 is already done
+    bool ch_phase1_done = false;
     // MultiSplitPrec::solve(l, f, x) with merged steps: sweep 1 = phase 1,
     // step B (or the recursion and phase 2); sweep 2 = step A (residual),
     // step B; sweeps 3.. = step A (correction of the previous sweep), step B;
@@ -1766,7 +1786,8 @@ struct Builder {
         LevelWork<T>& w = W[l];
         uint32_t M = L.M;
         if (explicit_solves) {
-            phase1(L, f, w.w.p, x);
+            if (ch_phase1_done) ch_phase1_done = false;
+            else phase1(L, f, w.w.p, x);
         } else {
             lsolve(L, f, w.w.p);
             coarse_diag(L, f, w.w.p, x);
@@ -1794,14 +1815,29 @@ struct Builder {
                 if (ps) ps->push_back(pstep(PS_RESID, spmv_lpr(n, snnz, stm), n, 0, sia, sja, sa, nullptr, u, y, F));
                 else op([=](cudaStream_t s) { launch_spmv<T>(n, snnz, sia, sja, sa, u, y, F, s, stm); }, "residual");
             };
+            // y = F - As u, then out = solve(l + 1, y)
+            auto resid_solve = [&](T* u, T* y, T* out) {
+                if (ch_merge_ok(l + 1)) {
+                    LevelScope sc(cur_level, l + 1);  // named by the level whose data it reads
+                    step_a(Ln, 0, F, u, nullptr, y, nullptr, out, W[l + 1].w.p, &Ln.As);
+                    bytes += (uint64_t)Ln.P1.nnz * (4 + sizeof(T)) + sizeof(T) * (uint64_t)Ln.N;
+                    ch_phase1_done = true;
+                } else {
+                    resid(u, y);
+                }
+                ch(l + 1, y, out);
+            };
+            // The last step of the recurrence writes the coarse part of x
+            // itself (no copy of the final iterate).
+            T* xo = x + M;
             if (nch > 1) { ch(l + 1, F, u1); scale(u1, alpha); }
-            else { ch(l + 1, F, x2); scale(x2, alpha); }
+            else { ch(l + 1, F, xo); scale(xo, alpha); }
+            if (nch == 2) x2 = xo;
             if (nch > 1) {
                 alpha = 4 / (lmax - lmin) * cheb_poly(eta, 1) / cheb_poly(eta, 2);
                 beta = cheb_poly(eta, 0) / cheb_poly(eta, 2);
-                resid(u1, tmp);
-                // tmp = F - A u1 above; the reference forms A u1 - F: negate via the scalars
-                ch(l + 1, tmp, x2);
+                // tmp = F - A u1; the reference forms A u1 - F: negate via the scalars
+                resid_solve(u1, tmp, x2);
                 // x2 := -alpha * solve(A u1 - F) + (1+beta) u1 = alpha * solve(F - A u1) + (1+beta) u1
                 double c = is_equal1(1 + beta) ? 1.0 : 1 + beta;
                 T ma = (T)alpha, cc = (T)c;
@@ -1811,10 +1847,10 @@ struct Builder {
             }
             for (uint32_t i = 3; i <= nch; i++) {
                 T* t = u0; u0 = u1; u1 = x2; x2 = t;  // cheb_solve.cc:87-89
+                if (i == nch) x2 = xo;
                 alpha = 4 / (lmax - lmin) * cheb_poly(eta, i - 1) / cheb_poly(eta, i);
                 beta = cheb_poly(eta, i - 2) / cheb_poly(eta, i);
-                resid(u1, tmp);
-                ch(l + 1, tmp, x2);
+                resid_solve(u1, tmp, x2);
                 // x2 = u1 - alpha*solve(A u1 - F) + beta*(u1-u0) = u1 + alpha*solve(F - A u1) + ...
                 T ma = (T)(-alpha), bb = (T)beta;
                 T* u0c = u0; T* u1c = u1; T* x2c = x2;
@@ -1822,10 +1858,6 @@ struct Builder {
                 else op([=](cudaStream_t s) { launch_k(k_chebk<T>, grid_for(n, 256), 256, 0, s, n, x2c, (const T*)u1c, (const T*)u0c, ma, bb); }, "chebk");
                 bytes += spmv_bytes(Ln.As) + 4ull * sizeof(T) * n;
             }
-            T* xo = x + M;
-            T* fin = x2;
-            if (ps) ps->push_back(pstep(PS_COPY, 1, n, 0, nullptr, nullptr, nullptr, nullptr, fin, xo));
-            else op([=](cudaStream_t s) { launch_k(k_copy<T>, grid_for(n, 256), 256, 0, s, n, (const T*)fin, xo); }, "copy");
         }
         if (explicit_solves) phase2(L, w.w.p, x);
         else usolve(L, w.w.p, x);

@@ -10,7 +10,8 @@ the golden fixtures, and run side by side in tests/test_oracle_vs_reference.py
   coarsest solve in FP64, flexible FP64 PCG) at 1e-8 and 1e-10: iterations and
   the solution error against the oracle's FP64 solution at 1e-12.
 * uh_cheb (sigma 3, degree 4) on the 60x220x85 layered field: hierarchy
-  bit-exact, PCG within one iteration and 1e-10.
+  bit-exact, PCG within one iteration and 1e-10; its merged residual + phase-1
+  launches bit-identical to the separate ones.
 * The FP32 form on the 60x220x85 multi-split problem against the oracle (at
   1e-8 and 1e-9: there the FP64 iteration itself stagnates near 5.6e-10).
 * Ensemble members against the oracle, forward and adjoint (FP64 members to
@@ -107,6 +108,34 @@ def test_uh_cheb_full_size(M):
     xo, it, _, rc = O.pcg(Ao, bo, Po, 1e-8)
     assert rc == 0 and abs(st.niter - it) <= 1
     assert np.linalg.norm(x - xo) <= 1e-10 * np.linalg.norm(xo)
+
+
+@pytest.mark.parametrize("fp32", [False, True])
+def test_uh_cheb_merged_residual_is_bit_identical(M, fp32, monkeypatch):
+    """uh_cheb (sigma 3, degree 4) on the 60x220x85 layered field, whose level
+    4 (11,452 rows) is called 256 times per application: the Chebyshev
+    residual F - As u and phase 1 of the level call after it as one launch
+    (k_merge_a with As) give the same application and PCG iterates, bit for
+    bit, as the two launches (MLP_MERGE=0)."""
+    from ml_prec_b200 import fields
+    kx, ky, kz = fields.field("layered", 2)
+    A, b = M.CSRMatrix.spe(60, 220, 85, kx, ky, kz, c=1.0)
+    f = np.random.default_rng(7).standard_normal(A.n)
+    out = []
+    for env in ("1", "0"):
+        monkeypatch.setenv("MLP_MERGE", env)
+        P = M.Prec(A, fp32=fp32, sigma=(3.0,), ncheb=(4,), use_tails=True)
+        z = P.solve(f)
+        names = [nm for nm, _, _ in P.profile(1)]
+        st = M.SolverStats()
+        x = M.PCGSolver(A, b, P, stats=st, eps=1e-8)
+        out.append((names, z, st.niter, x))
+        del P
+    (n1, z1, it1, x1), (n0, z0, it0, x0) = out
+    assert "merge_a L4" in n1 and not any(nm.startswith("merge_a") for nm in n0)
+    assert len(n1) < len(n0)
+    assert np.array_equal(z1, z0)
+    assert it1 == it0 and np.array_equal(x1, x0)
 
 
 def test_fp32_form_full_size_against_oracle(M):
