@@ -26,7 +26,8 @@ sys.path.insert(0, ROOT)
 from ml_prec_b200 import fields  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 
-REF = os.environ.get("MLP_REF_SRC", "/root/reference")
+# the reference tree: MLP_REF_SRC, else the `reference` tree beside this repository
+REF = os.environ.get("MLP_REF_SRC", os.path.join(os.path.dirname(ROOT), "reference"))
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 # name: (field model, field seed, nx, ny, nz, c, prec, options)
