@@ -502,9 +502,15 @@ __global__ void k_chebk(uint32_t n, T* __restrict__ x2, const T* __restrict__ u1
 // Dense coarsest level: x = C^{-1} f, one warp per row. The operator's type
 // CT may be wider than the vectors' T: the FP32 hierarchy keeps its coarsest
 // solve (the dense inverse, or the tabulated small-level operator standing in
-// for it) in FP64 and accumulates in FP64.
-template <class T, class CT = T>
-__global__ void k_dense_gemv(uint32_t n, const CT* __restrict__ C, const T* __restrict__ f, T* __restrict__ x) {
+// for it) in FP64 and accumulates in FP64. EPI > 0 applies the Chebyshev
+// update that follows a tabulated level call to the row's result, with the
+// arithmetic of the separate kernel: 1 k_scale (x = v ea), 2 k_cheb2
+// (x = v ea + eb u1), 3 k_chebk (x = u1 - ea v + eb (u1 - u0), ea = alpha).
+enum { EPI_NONE = 0, EPI_SCALE = 1, EPI_CHEB2 = 2, EPI_CHEBK = 3 };
+template <class T, class CT, int EPI>
+__device__ __forceinline__ void dense_gemv_body(uint32_t n, const CT* __restrict__ C, const T* __restrict__ f,
+                                                T* __restrict__ x, const T* __restrict__ u1,
+                                                const T* __restrict__ u0, T ea, T eb) {
     // the operator is constant: its row is loaded before the wait (see RowPre)
     constexpr int CV = 16;
     uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -528,7 +534,27 @@ __global__ void k_dense_gemv(uint32_t n, const CT* __restrict__ C, const T* __re
     for (uint32_t j = lane + 32 * CV; j < n; j += 32) s = fmadd(c[j], (CT)f[j], s);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) x[row] = (T)s;
+    if (lane == 0) {
+        T v = (T)s;
+        if (EPI == EPI_SCALE) {
+            v *= ea;
+        } else if (EPI == EPI_CHEB2) {
+            v = fmadd(v, ea, eb * u1[row]);
+        } else if (EPI == EPI_CHEBK) {
+            T a1 = u1[row];
+            v = fmadd(eb, a1 - u0[row], fmadd(-ea, v, a1));
+        }
+        x[row] = v;
+    }
+}
+template <class T, class CT = T>
+__global__ void k_dense_gemv(uint32_t n, const CT* __restrict__ C, const T* __restrict__ f, T* __restrict__ x) {
+    dense_gemv_body<T, CT, EPI_NONE>(n, C, f, x, nullptr, nullptr, T(0), T(0));
+}
+template <class T, class CT, int EPI>
+__global__ void k_dense_gemv_epi(uint32_t n, const CT* __restrict__ C, const T* __restrict__ f, T* __restrict__ x,
+                                 const T* __restrict__ u1, const T* __restrict__ u0, T ea, T eb) {
+    dense_gemv_body<T, CT, EPI>(n, C, f, x, u1, u0, ea, eb);
 }
 
 __global__ void k_to_f32(uint32_t n, const double* __restrict__ a, float* __restrict__ b) {
@@ -1261,6 +1287,47 @@ struct Builder {
         return true;
     }
 
+    // uh_cheb: the call of level l when it is the tabulated small-level
+    // operator, with the Chebyshev update that follows it applied in the
+    // GEMV's epilogue (one launch in place of two; same arithmetic, so the
+    // result is bit-identical). False, and nothing recorded, where level l is
+    // not a tabulated operator, inside a persistent region, or with MLP_MERGE=0.
+    bool dense_epi(uint32_t l, const T* f, T* x, int mode, const T* u1, const T* u0, T ea, T eb) {
+        if (ps || !merge_enabled() || persist_ok(l)) return false;
+        const double* C64 = nullptr;
+        const T* CT_ = nullptr;
+        uint32_t n = 0;
+        if (small64 && small64->valid() && small64->dense.p && l == small64->first) {
+            C64 = small64->dense.p;
+            n = small64->N0;
+        } else if (small && small->valid() && l == small->first && small->dense.p) {
+            CT_ = small->dense.p;
+            n = small->N0;
+        } else {
+            return false;
+        }
+        LevelScope scope(cur_level, l);
+        check_plan_size();
+        unsigned g = grid_for((size_t)n * 32, 256);
+        auto rec = [&](auto kern, const auto* Cm) {
+            op([=](cudaStream_t s) { launch_k(kern, g, 256, 0, s, n, Cm, f, x, u1, u0, ea, eb); }, "dense_step");
+        };
+#define DENSE_EPI_CASE(E)                                                      \
+    case E:                                                                    \
+        if (C64) rec(k_dense_gemv_epi<T, double, E>, C64);                     \
+        else rec(k_dense_gemv_epi<T, T, E>, CT_);                              \
+        break;
+        switch (mode) {
+            DENSE_EPI_CASE(EPI_SCALE)
+            DENSE_EPI_CASE(EPI_CHEB2)
+            DENSE_EPI_CASE(EPI_CHEBK)
+            default: MLP_THROW(ERR_INTERNAL, "dense step: unknown update");
+        }
+#undef DENSE_EPI_CASE
+        bytes += (uint64_t)n * n * (C64 ? 8 : sizeof(T)) + (2ull + (uint64_t)mode) * n * sizeof(T);
+        return true;
+    }
+
     // Level whose call is being recorded (names the ops for profiling).
     uint32_t cur_level = 0;
     struct LevelScope {
@@ -1815,8 +1882,10 @@ struct Builder {
                 if (ps) ps->push_back(pstep(PS_RESID, spmv_lpr(n, snnz, stm), n, 0, sia, sja, sa, nullptr, u, y, F));
                 else op([=](cudaStream_t s) { launch_spmv<T>(n, snnz, sia, sja, sa, u, y, F, s, stm); }, "residual");
             };
-            // y = F - As u, then out = solve(l + 1, y)
-            auto resid_solve = [&](T* u, T* y, T* out) {
+            // y = F - As u, then out = solve(l + 1, y), followed by the step's
+            // update (mode, u1, u0, ea, eb as k_dense_gemv_epi takes them).
+            // True when the update went into the level call's epilogue.
+            auto resid_solve = [&](T* u, T* y, T* out, int mode, const T* e1, const T* e0, T ea, T eb) {
                 if (ch_merge_ok(l + 1)) {
                     LevelScope sc(cur_level, l + 1);  // named by the level whose data it reads
                     step_a(Ln, 0, F, u, nullptr, y, nullptr, out, W[l + 1].w.p, &Ln.As);
@@ -1824,25 +1893,34 @@ struct Builder {
                     ch_phase1_done = true;
                 } else {
                     resid(u, y);
+                    if (dense_epi(l + 1, y, out, mode, e1, e0, ea, eb)) return true;
                 }
                 ch(l + 1, y, out);
+                return false;
+            };
+            // out = alpha solve(l + 1, F)
+            auto first = [&](T* out) {
+                if (!is_equal1(alpha) && dense_epi(l + 1, F, out, EPI_SCALE, nullptr, nullptr, (T)alpha, T(0)))
+                    return;
+                ch(l + 1, F, out);
+                scale(out, alpha);
             };
             // The last step of the recurrence writes the coarse part of x
             // itself (no copy of the final iterate).
             T* xo = x + M;
-            if (nch > 1) { ch(l + 1, F, u1); scale(u1, alpha); }
-            else { ch(l + 1, F, xo); scale(xo, alpha); }
+            first(nch > 1 ? u1 : xo);
             if (nch == 2) x2 = xo;
             if (nch > 1) {
                 alpha = 4 / (lmax - lmin) * cheb_poly(eta, 1) / cheb_poly(eta, 2);
                 beta = cheb_poly(eta, 0) / cheb_poly(eta, 2);
-                // tmp = F - A u1; the reference forms A u1 - F: negate via the scalars
-                resid_solve(u1, tmp, x2);
                 // x2 := -alpha * solve(A u1 - F) + (1+beta) u1 = alpha * solve(F - A u1) + (1+beta) u1
                 double c = is_equal1(1 + beta) ? 1.0 : 1 + beta;
                 T ma = (T)alpha, cc = (T)c;
-                if (ps) ps->push_back(pstep(PS_CHEB2, 1, n, 0, nullptr, nullptr, nullptr, nullptr, x2, u1, nullptr, (double)ma, (double)cc));
-                else op([=](cudaStream_t s) { launch_k(k_cheb2<T>, grid_for(n, 256), 256, 0, s, n, x2, (const T*)u1, ma, cc); }, "cheb2");
+                // tmp = F - A u1; the reference forms A u1 - F: negate via the scalars
+                if (!resid_solve(u1, tmp, x2, EPI_CHEB2, u1, nullptr, ma, cc)) {
+                    if (ps) ps->push_back(pstep(PS_CHEB2, 1, n, 0, nullptr, nullptr, nullptr, nullptr, x2, u1, nullptr, (double)ma, (double)cc));
+                    else op([=](cudaStream_t s) { launch_k(k_cheb2<T>, grid_for(n, 256), 256, 0, s, n, x2, (const T*)u1, ma, cc); }, "cheb2");
+                }
                 bytes += spmv_bytes(Ln.As) + 3ull * sizeof(T) * n;
             }
             for (uint32_t i = 3; i <= nch; i++) {
@@ -1850,12 +1928,13 @@ struct Builder {
                 if (i == nch) x2 = xo;
                 alpha = 4 / (lmax - lmin) * cheb_poly(eta, i - 1) / cheb_poly(eta, i);
                 beta = cheb_poly(eta, i - 2) / cheb_poly(eta, i);
-                resid_solve(u1, tmp, x2);
                 // x2 = u1 - alpha*solve(A u1 - F) + beta*(u1-u0) = u1 + alpha*solve(F - A u1) + ...
                 T ma = (T)(-alpha), bb = (T)beta;
                 T* u0c = u0; T* u1c = u1; T* x2c = x2;
-                if (ps) ps->push_back(pstep(PS_CHEBK, 1, n, 0, nullptr, nullptr, nullptr, nullptr, x2c, u1c, u0c, (double)ma, (double)bb));
-                else op([=](cudaStream_t s) { launch_k(k_chebk<T>, grid_for(n, 256), 256, 0, s, n, x2c, (const T*)u1c, (const T*)u0c, ma, bb); }, "chebk");
+                if (!resid_solve(u1, tmp, x2, EPI_CHEBK, u1c, u0c, ma, bb)) {
+                    if (ps) ps->push_back(pstep(PS_CHEBK, 1, n, 0, nullptr, nullptr, nullptr, nullptr, x2c, u1c, u0c, (double)ma, (double)bb));
+                    else op([=](cudaStream_t s) { launch_k(k_chebk<T>, grid_for(n, 256), 256, 0, s, n, x2c, (const T*)u1c, (const T*)u0c, ma, bb); }, "chebk");
+                }
                 bytes += spmv_bytes(Ln.As) + 4ull * sizeof(T) * n;
             }
         }

@@ -115,8 +115,10 @@ def test_uh_cheb_merged_residual_is_bit_identical(M, fp32, monkeypatch):
     """uh_cheb (sigma 3, degree 4) on the 60x220x85 layered field, whose level
     4 (11,452 rows) is called 256 times per application: the Chebyshev
     residual F - As u and phase 1 of the level call after it as one launch
-    (k_merge_a with As) give the same application and PCG iterates, bit for
-    bit, as the two launches (MLP_MERGE=0)."""
+    (k_merge_a with As), and each call of the tabulated small levels with the
+    Chebyshev update after it as one launch (k_dense_gemv_epi), give the same
+    application and PCG iterates, bit for bit, as the separate launches
+    (MLP_MERGE=0)."""
     from ml_prec_b200 import fields
     kx, ky, kz = fields.field("layered", 2)
     A, b = M.CSRMatrix.spe(60, 220, 85, kx, ky, kz, c=1.0)
@@ -133,6 +135,7 @@ def test_uh_cheb_merged_residual_is_bit_identical(M, fp32, monkeypatch):
         del P
     (n1, z1, it1, x1), (n0, z0, it0, x0) = out
     assert "merge_a L4" in n1 and not any(nm.startswith("merge_a") for nm in n0)
+    assert any(nm.startswith("dense_step") for nm in n1) and not any(nm.startswith("dense_step") for nm in n0)
     assert len(n1) < len(n0)
     assert np.array_equal(z1, z0)
     assert it1 == it0 and np.array_equal(x1, x0)
